@@ -1,0 +1,440 @@
+"""Benchmark: PageRank to L1 residual 1e-9 and exact Brandes GTEPS on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl zog|reference]
+
+Workload (the scale configuration, synthetic and seeded):
+  * PageRank, FP64, uniform start: directed R-MAT scale 24, edge factor 16
+    (a,b,c,d = .57,.19,.19,.05; self-loops and duplicates removed; seed 1024),
+    damping 0.85, L1 tolerance 1e-9, at most 200 iterations.  One step = one
+    full solve (start vector -> convergence) on the device-resident graph.
+    `value` = ms per solve (lower is better).
+  * Brandes, exact, unweighted: undirected R-MAT scale 16, edge factor 16
+    (seed 1016), every source.  One step = 4,096 consecutive sources; the timed
+    steps cover all 65,536 sources.  Reported as GTEPS = sources * arcs / time.
+
+The graph inputs (~1 GB of arc indices at scale 24) exceed the 126 MB L2, so no
+L2 flush is needed between steps.  N > 1 (torchrun): PageRank runs as
+independent replicas (one graph per GPU); Brandes shards the sources across
+ranks and sums the partial scores with one NCCL all-reduce.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PageRank ms to L1 res 1e-9 (learned vs uniform start); Brandes GTEPS"
+PR_SCALE, PR_EF, PR_SEED = 24, 16, 1024
+BC_SCALE, BC_EF, BC_SEED = 16, 16, 1016
+BC_STEP_SOURCES = 4096
+DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
+
+
+# --------------------------------------------------------------------------
+# helpers
+# --------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1])); smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the oracle (a loop-for-loop restatement of the reference's
+# single-threaded Zig code) on a bounded sample of the same workload.
+# --------------------------------------------------------------------------
+def cpu_pagerank_sample(V, in_off, in_col, outdeg, iters_full, budget_s=12.0):
+    from oracle import oracle as O
+
+    O.build()
+    k = 1
+    _, _, _, secs = O.pagerank_csr(V, in_off, in_col, outdeg, DAMPING, 1, 0.0)
+    per_iter = secs
+    k_more = max(1, min(int(budget_s / max(per_iter, 1e-3)), 10))
+    _, _, _, secs = O.pagerank_csr(V, in_off, in_col, outdeg, DAMPING, k_more, 0.0)
+    per_iter = secs / k_more
+    k = k_more
+    return per_iter * iters_full * 1e3, k, per_iter
+
+
+def cpu_brandes_sample(V, out_off, out_col, arcs, budget_s=12.0):
+    from oracle import oracle as O
+
+    O.build()
+    n = 16
+    _, _, secs = O.betweenness_csr_sources(V, out_off, out_col, np.arange(n, dtype=np.uint32))
+    per_src = secs / n
+    n2 = int(min(max(budget_s / max(per_src, 1e-6), 16), V))
+    _, _, secs = O.betweenness_csr_sources(V, out_off, out_col, np.arange(n2, dtype=np.uint32))
+    per_src = secs / n2
+    gteps = arcs / per_src / 1e9
+    return gteps, n2, per_src
+
+
+def host_graph(scale, ef, seed, directed):
+    """The benchmark graph built on the host with the oracle's generator (same
+    definition as the CUDA generator) and its CSR arrays."""
+    from oracle import oracle as O
+
+    V, f, t = O.rmat(scale, ef, seed, directed=directed)
+    return V, f, t
+
+
+# --------------------------------------------------------------------------
+# reference arm
+# --------------------------------------------------------------------------
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    O.build()
+    V, f, t = host_graph(PR_SCALE, PR_EF, PR_SEED, True)
+    in_off, in_col, deg = O.in_csr_from_edges(V, f, t)
+    del f, t
+    iters_full = int(args.ref_pr_iterations)
+    step_ms = []
+    for i in range(args.warmup + args.steps):
+        # each step: a bounded sample of the solve -- k iterations of the
+        # reference loop over the full graph, extrapolated to the full solve
+        _, _, _, secs = O.pagerank_csr(V, in_off, in_col, deg, DAMPING, args.ref_iters_per_step, 0.0)
+        if i >= args.warmup:
+            step_ms.append(secs / args.ref_iters_per_step * iters_full * 1e3)
+    ms = float(np.mean(step_ms))
+    Vb, fb, tb = host_graph(BC_SCALE, BC_EF, BC_SEED, False)
+    ag_off, ag_col = _successor_csr_undirected(Vb, fb, tb)
+    gteps, nsrc, per_src = cpu_brandes_sample(Vb, ag_off, ag_col, len(fb), budget_s=args.cpu_budget)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT)",
+        "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 tol1e-9; "
+                               f"brandes rmat{BC_SCALE} ef{BC_EF} undirected all sources",
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
+                         "sample": f"{args.ref_iters_per_step} iterations of the reference PageRank loop "
+                                   f"(oracle restatement, 1 thread) over the full scale-{PR_SCALE} graph per step, "
+                                   f"extrapolated to {iters_full} iterations; preprocessing excluded"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "brandes": {"gteps": gteps, "sources_timed": nsrc, "arcs": int(len(fb)),
+                    "sample": f"{nsrc} sources of the all-sources run, 1 thread"},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _successor_csr_undirected(V, f, t):
+    """Successor CSR in ArrayGraph iteration order (reverse insertion per node)."""
+    f = np.asarray(f, np.int64)
+    order = np.argsort(f, kind="stable")[::-1]
+    order = order[np.argsort(f[order], kind="stable")]
+    col = np.asarray(t, np.uint32)[order]
+    off = np.zeros(V + 1, np.uint64)
+    off[1:] = np.cumsum(np.bincount(f, minlength=V))
+    return off, col
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def run_zog(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from zog_b200 import _native, build
+
+    build.build()
+    N = _native
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+
+    # ---------------- PageRank, device-resident ----------------
+    G = N.Graph.rmat(PR_SCALE, PR_EF, PR_SEED, directed=True)
+    V, E, n_live = G.info()
+    out = torch.empty(V, dtype=torch.float64, device="cuda")
+    st = None
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            st = G.pagerank_device(out.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    iters = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st = G.pagerank_device(out.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+        launches += st["launches"]
+        iters.append(st["iterations"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms, ws)
+    iterations = int(iters[-1])
+    residual = float(st["residual"])
+
+    # roofline of the dominant kernel (the fused iteration): tol 0 and exactly
+    # `iterations` launches, timed with events on its stream
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True); e3 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    G.pagerank_device(out.data_ptr(), DAMPING, iterations, 0.0, stream=sp)
+    e1.record(stream)
+    e2.record(stream)
+    G.pagerank_device(out.data_ptr(), DAMPING, 0, 0.0, stream=sp)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t_iter_ms = (e0.elapsed_time(e1) - e2.elapsed_time(e3)) / max(iterations, 1)
+    bytes_per_iter = 4.0 * E + 4.0 * (V + 1) + 36.0 * V  # u32 offsets at this size
+    hbm_peak, peak_kind = peaks()
+    achieved = bytes_per_iter / (t_iter_ms * 1e-3) / 1e9
+
+    # ---------------- e2e through the C ABI with host buffers ----------------
+    e2e = None
+    if not args.no_e2e:
+        ih, ic, oo, oc, deg = G.export_csr()
+        # insertion-order edge list (sorted (src,dst)) rebuilt from the in-CSR,
+        # held in pinned host memory like a NIF's input slices
+        src_t = torch.from_numpy(np.repeat(np.arange(V, dtype=np.uint32), np.diff(oo).astype(np.int64)).view(np.int32)).pin_memory()
+        dst_t = torch.from_numpy(oc.view(np.int32)).pin_memory()
+        del ih, ic
+        host_out = torch.empty(V, dtype=torch.float64).pin_memory()
+        src_np = src_t.numpy().view(np.uint32); dst_np = dst_t.numpy().view(np.uint32)
+        for _ in range(args.warmup_e2e):
+            g2 = N.Graph.from_edges(V, src_np, dst_np)
+            g2.pagerank(DAMPING, MAX_ITER, TOL, out=host_out.numpy())
+            g2.destroy()
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.steps_e2e):
+            g2 = N.Graph.from_edges(V, src_np, dst_np)
+            g2.pagerank(DAMPING, MAX_ITER, TOL, out=host_out.numpy())
+            g2.destroy()
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps_e2e
+        e2e_ms = max_over_ranks(e2e_ms, ws)
+        # from the SoA arrays in reverse insertion order the CSR would be equal;
+        # the graph here is built from (src,dst)-sorted arcs, the generator's order
+        e2e = {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(8 * E), "d2h_bytes_per_step": int(8 * V),
+               "what": "zogcu_graph_create_from_edges (host arc arrays) + zogcu_pagerank (host scores) + destroy"}
+        cpu_ctx = (V, oo, oc)
+        del src_t, dst_t
+
+    # ---------------- CPU baseline (rank 0, N == 1) ----------------
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ih, ic, _, _, deg = G.export_csr()
+        cpu_ms, k, per_iter = cpu_pagerank_sample(V, ih, ic, deg, iterations, budget_s=args.cpu_budget)
+        cpu = {"value": cpu_ms, "unit": "ms", "cores": 1, "kind": "port",
+               "sample": f"{k} iterations of the reference PageRank loop (oracle restatement, 1 thread) over "
+                         f"the full scale-{PR_SCALE} graph, extrapolated to {iterations} iterations; "
+                         f"preprocessing excluded ({per_iter * 1e3:.0f} ms/iteration)"}
+        del ih, ic
+    G.destroy()
+    torch.cuda.empty_cache()
+
+    # ---------------- Brandes, all sources, sharded over ranks ----------------
+    bc_line = None
+    if not args.no_brandes:
+        B = N.Graph.rmat(BC_SCALE, BC_EF, BC_SEED, directed=False)
+        Vb, Eb, _ = B.info()
+        bc = torch.zeros(Vb, dtype=torch.float64, device="cuda")
+        part = torch.empty(Vb, dtype=torch.float64, device="cuda")
+        all_src = np.arange(Vb, dtype=np.uint32)
+        mine = all_src[rank::ws]
+        chunks = [mine[i:i + BC_STEP_SOURCES] for i in range(0, mine.size, BC_STEP_SOURCES)]
+        steps = len(chunks) if args.bc_steps <= 0 else min(args.bc_steps, len(chunks))
+        with torch.cuda.stream(stream):
+            for w in range(args.warmup):
+                B.betweenness_device(part.data_ptr(), sources=chunks[w % len(chunks)][:1024], stream=sp)
+        torch.cuda.synchronize()
+        barrier(ws)
+        b0 = torch.cuda.Event(enable_timing=True); b1 = torch.cuda.Event(enable_timing=True)
+        bl = 0
+        depth = 0
+        b0.record(stream)
+        for i in range(steps):
+            stb = B.betweenness_device(part.data_ptr(), sources=chunks[i], stream=sp)
+            with torch.cuda.stream(stream):
+                bc.add_(part)
+            bl += stb["launches"]
+            depth = max(depth, stb["max_depth"])
+        if ws > 1:
+            import torch.distributed as dist
+
+            with torch.cuda.stream(stream):
+                dist.all_reduce(bc)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        bms = max_over_ranks(b0.elapsed_time(b1), ws)
+        srcs_timed = sum(c.size for c in chunks[:steps]) * ws
+        gteps = srcs_timed * Eb / (bms * 1e-3) / 1e9
+        bc_line = {"gteps": gteps, "arcs": Eb, "vertices": Vb, "sources_timed": srcs_timed,
+                   "ms_all_timed": bms, "max_depth": depth, "launches": bl,
+                   "workload": f"undirected rmat{BC_SCALE} ef{BC_EF}, {srcs_timed} sources, "
+                               f"{BC_STEP_SOURCES} sources per step"}
+        if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+            _, _, oo, oc, _ = B.export_csr()
+            cg, nsrc, per_src = cpu_brandes_sample(Vb, oo, oc, Eb, budget_s=args.cpu_budget)
+            bc_line["cpu_baseline"] = {"gteps": cg, "cores": 1, "kind": "port",
+                                       "sample": f"{nsrc} sources of the same graph, oracle restatement, 1 thread"}
+        B.destroy()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT)",
+            "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 uniform start, d={DAMPING}, "
+                                   f"tol={TOL}, max_iter={MAX_ITER}", "vertices": V, "arcs": E,
+                       "iterations": iterations, "residual": residual, "l2": "inputs larger than L2",
+                       "parallelism": "replicas" if ws > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "pr_iter_kernel", "ms_per_launch": t_iter_ms,
+                         "algorithmic_bytes_per_launch": bytes_per_iter},
+            "clocks": clk,
+            "gpu_launches": int(launches + (bc_line["launches"] if bc_line else 0)),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "brandes": bc_line,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="zog", choices=["zog", "reference"])
+    ap.add_argument("--steps-e2e", type=int, default=3)
+    ap.add_argument("--warmup-e2e", type=int, default=1)
+    ap.add_argument("--bc-steps", type=int, default=0, help="Brandes steps of 4,096 sources (0 = all sources)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-brandes", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--ref-iters-per-step", type=int, default=2)
+    ap.add_argument("--ref-pr-iterations", type=int, default=128,
+                    help="iterations the full solve takes (the GPU arm reports the measured count)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_zog(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,207 @@
+/* zogcu.h -- C ABI of the B200 (sm_100a) centrality library.
+ *
+ * The library replaces, behind Zog's own NIF boundary, the two centrality hot
+ * paths of code-shoily/zog that run on the `:soa` (ArrayGraph) resource:
+ *
+ *   - PageRank power iteration      priv/zog/src/centrality.zig:858-965
+ *   - unweighted Brandes betweenness priv/zog/src/centrality.zig:687-798
+ *
+ * A graph handle holds a device-resident CSR built once from the NIF's edge
+ * arrays and reused by every call, which is what the reference's GraphRes
+ * resource does for its ArrayGraph (lib/zog/.Elixir.Zog.ResourceGraph.zig:10-24).
+ *
+ * Conventions
+ *   - Every entry point returns a status code (ZOGCU_OK == 0); nothing throws
+ *     across the ABI.  zogcu_status_string() names a code and
+ *     zogcu_last_error() gives the calling thread's last detailed message.
+ *   - Pointers are HOST pointers unless an option says otherwise.
+ *   - Scores are returned exactly as the NIFs return them: one f64 per node
+ *     slot (length = node capacity), 0.0 for deleted slots, and no undirected
+ *     0.5 scaling (the Elixir wrapper applies that, resource_graph.ex:2633-2637).
+ *   - Several host threads may call on the same graph at once; each call uses
+ *     its own stream and workspace, and the graph itself is read-only after
+ *     creation (one lazily built, mutex-guarded PageRank schedule aside).
+ */
+#ifndef ZOGCU_H_
+#define ZOGCU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZOGCU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define ZOGCU_API __attribute__((visibility("default")))
+#else
+#define ZOGCU_API
+#endif
+
+enum zogcu_status {
+  ZOGCU_OK = 0,
+  ZOGCU_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size or option          */
+  ZOGCU_ERR_NODE_NOT_FOUND = 2,   /* edge endpoint >= node count (addEdge's     */
+                                  /* error.NodeNotFound, array_graph.zig:88-89) */
+  ZOGCU_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed           */
+  ZOGCU_ERR_CUDA = 4,             /* a CUDA runtime call failed                 */
+  ZOGCU_ERR_NO_DEVICE = 5,        /* no usable sm_100 device                    */
+  ZOGCU_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up         */
+  ZOGCU_ERR_IO = 7,               /* file could not be opened / read            */
+  ZOGCU_ERR_TOO_LARGE = 8,        /* sizes beyond the u32 node / edge indices   */
+  ZOGCU_ERR_INTERNAL = 9
+};
+
+typedef struct zogcu_graph zogcu_graph;
+
+/* Per-call statistics (all optional: pass NULL to skip). */
+typedef struct zogcu_stats {
+  uint64_t iterations;    /* PageRank: power iterations run                      */
+  double residual;        /* PageRank: L1 step of the last iteration             */
+  double elapsed_ms;      /* device time of the algorithm (CUDA events)          */
+  double bytes_moved;     /* algorithmic bytes of the iterations (PageRank)      */
+  uint64_t sources;       /* Brandes: sources processed                          */
+  uint32_t max_depth;     /* Brandes: deepest BFS level seen                     */
+  uint32_t sigma_overflow;/* Brandes: some path count wrapped modulo 2^64        */
+  uint64_t launches;      /* kernels launched by the call                        */
+  uint64_t polish_iterations; /* mixed precision: FP64 iterations at the end     */
+} zogcu_stats;
+
+/* PageRank precision forms. */
+#define ZOGCU_PREC_FP64 0  /* FP64 throughout (the reference's arithmetic)     */
+#define ZOGCU_PREC_MIXED 1 /* FP32 SpMV + FP64 dangling/residual + FP64 polish */
+
+typedef struct zogcu_pr_opts {
+  uint32_t struct_size;   /* sizeof(zogcu_pr_opts)                               */
+  int32_t precision;      /* ZOGCU_PREC_*                                        */
+  const double* x0;       /* start vector (length V) or NULL = uniform 1/n,      */
+                          /* the reference's start (centrality.zig:912-918)      */
+  const double* teleport; /* personalisation vector (length V, sums to 1) or     */
+                          /* NULL = uniform (1-d)/n teleport of the reference    */
+  int32_t device_pointers;/* x0, teleport and out_scores are device pointers     */
+  int32_t reserved;
+  void* stream;           /* cudaStream_t to run on, or NULL = a private stream  */
+} zogcu_pr_opts;
+
+typedef struct zogcu_bc_opts {
+  uint32_t struct_size;   /* sizeof(zogcu_bc_opts)                               */
+  uint32_t batch;         /* sources in flight per batch (multiple of 64), 0 = auto */
+  const uint32_t* sources;/* source subset or NULL = every live node ascending,  */
+                          /* the reference's order (centrality.zig:728)          */
+  uint64_t num_sources;
+  int32_t device_pointers;/* out_scores is a device pointer                      */
+  int32_t reserved;
+  void* stream;           /* cudaStream_t to run on, or NULL = a private stream  */
+} zogcu_bc_opts;
+
+/* ---- status ------------------------------------------------------------- */
+ZOGCU_API const char* zogcu_status_string(int status);
+ZOGCU_API const char* zogcu_last_error(void);
+ZOGCU_API int zogcu_abi_version(void);
+
+/* ---- graph resources ----------------------------------------------------- */
+
+/* Replaces the NIF `new(node_count, from, to, weight, :soa)`
+ * (lib/zog/.Elixir.Zog.ResourceGraph.zig:94-106 with buildGraph :26-35): node
+ * ids 0..node_count-1, edges added in list order (head insertion, so each
+ * node's successors iterate in reverse list order, array_graph.zig:88-108).
+ * `weight` may be NULL (all 1.0).  Duplicate arcs and self-loops are kept. */
+ZOGCU_API int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from,
+                                  const uint32_t* to, const double* weight,
+                                  uint64_t num_edges, zogcu_graph** out);
+
+/* Same as above with the edge arrays already in device memory. */
+ZOGCU_API int zogcu_graph_create_from_device_edges(uint32_t node_count, const uint32_t* d_from,
+                                         const uint32_t* d_to, uint64_t num_edges,
+                                         void* stream, zogcu_graph** out);
+
+/* Builds the device graph from the raw slices of an existing ArrayGraph
+ * (array_graph.zig:21-38), as a NIF holding a GraphRes can pass them:
+ * first_edge / next_edge use 0xFFFFFFFF for null; deleted nodes and edges are
+ * skipped exactly like SuccessorIterator.next (array_graph.zig:164-180).
+ * node_deleted / edge_deleted / data may be NULL (none deleted / unit). */
+ZOGCU_API int zogcu_graph_create_from_arraygraph(uint32_t node_capacity, const uint32_t* first_edge,
+                                       const uint8_t* node_deleted, uint64_t edge_capacity,
+                                       const uint32_t* to, const uint32_t* next_edge,
+                                       const uint8_t* edge_deleted, zogcu_graph** out);
+
+/* Seeded R-MAT graph generated on the device (benchmark input): ef * 2^scale
+ * raw edges, self-loops and duplicates removed, inserted in (src,dst) order;
+ * undirected graphs keep one (lo,hi) pair per edge and store both arcs. */
+ZOGCU_API int zogcu_graph_generate_rmat(int scale, int edge_factor, uint64_t seed, double a, double b,
+                              double c, int directed, zogcu_graph** out);
+
+/* Raw (pre-dedupe) endpoints of R-MAT edges [i0, i0+m) of the generator above,
+ * written to device arrays -- lets a test compare the generator element by
+ * element with an independent CPU implementation of the same definition. */
+ZOGCU_API int zogcu_rmat_raw_device(int scale, uint64_t seed, double a, double b, double c,
+                                    uint64_t i0, uint64_t m, uint32_t* d_src, uint32_t* d_dst);
+
+/* Replaces nif_read_edgelist(path, directed, :soa, integer_labels)
+ * (lib/zog/.Elixir.Zog.ResourceGraph.zig:896-990): parses the file on the host
+ * and builds the device graph.  *next_id receives the node count; with
+ * integer_labels == 0 the labels (in id order) are returned '\n'-joined in
+ * *labels (release with zogcu_free), else *labels is NULL. */
+ZOGCU_API int zogcu_read_edgelist(const char* path, int directed, int integer_labels,
+                        zogcu_graph** out, uint32_t* next_id, char** labels,
+                        uint64_t* labels_len);
+
+/* Replaces nif_destroy (.zig:108-110): frees the device CSR.  NULL is a no-op. */
+ZOGCU_API int zogcu_graph_destroy(zogcu_graph* g);
+
+/* Node capacity V, stored arcs E and live nodes n of a graph. */
+ZOGCU_API int zogcu_graph_info(const zogcu_graph* g, uint32_t* node_capacity, uint64_t* num_arcs,
+                     uint64_t* live_nodes);
+
+/* Copies the device CSRs to host arrays (each may be NULL): in_off[V+1] and
+ * in_col[E] (rows = sources ascending, the in_neighbors order of
+ * centrality.zig:893-899), out_off[V+1] / out_col[E] (successor order) and
+ * out_degree[V]. */
+ZOGCU_API int zogcu_graph_export_csr(const zogcu_graph* g, uint64_t* in_off, uint32_t* in_col,
+                           uint64_t* out_off, uint32_t* out_col, uint32_t* out_degree);
+
+ZOGCU_API void zogcu_free(void* p);
+
+/* ---- PageRank ------------------------------------------------------------ */
+
+/* Replaces the NIF `pagerank(res, damping, max_iterations, tolerance)`
+ * (lib/zog/.Elixir.Zog.ResourceGraph.zig:156-170 -> centrality.zig:858-965):
+ * uniform start 1/n, teleport (1-d)/n, dangling mass sum(x/n) over live nodes
+ * with out-degree 0, stop when the L1 step < tolerance (checked after the
+ * swap), at most max_iterations.  out_scores has node-capacity length.  n == 0
+ * gives all zeros, n == 1 gives 1.0 for the live node. */
+ZOGCU_API int zogcu_pagerank(zogcu_graph* g, double damping, uint64_t max_iterations, double tolerance,
+                   double* out_scores, zogcu_stats* stats);
+
+/* As zogcu_pagerank with options (precision form, warm start, personalised
+ * teleport, device pointers, caller stream); opts may be NULL. */
+ZOGCU_API int zogcu_pagerank_ex(zogcu_graph* g, double damping, uint64_t max_iterations,
+                      double tolerance, const zogcu_pr_opts* opts, double* out_scores,
+                      zogcu_stats* stats);
+
+/* ---- Brandes betweenness -------------------------------------------------- */
+
+/* Replaces nif_betweenness_unweighted (.zig:112-121 ->
+ * centrality.zig:687-798): sum over every live source s of the dependencies
+ * delta_s(v), v != s, unnormalised. */
+ZOGCU_API int zogcu_betweenness_unweighted(zogcu_graph* g, double* out_scores, zogcu_stats* stats);
+
+/* As above with options (source subset, batch size, device output, stream). */
+ZOGCU_API int zogcu_betweenness_unweighted_ex(zogcu_graph* g, const zogcu_bc_opts* opts,
+                                    double* out_scores, zogcu_stats* stats);
+
+/* BFS intermediates of the Brandes forward phase (centrality.zig:741-767) for
+ * `num_sources` sources: dist_out[i*V + v] (0xFFFFFFFF = unreached) and
+ * sigma_out[i*V + v] (shortest-path counts, wrapping modulo 2^64 like the
+ * reference's usize).  Either output may be NULL.  *overflow is set when some
+ * count wrapped. */
+ZOGCU_API int zogcu_bfs_sigma(zogcu_graph* g, const uint32_t* sources, uint64_t num_sources,
+                    uint32_t* dist_out, uint64_t* sigma_out, uint32_t* overflow);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZOGCU_H_ */

@@ -1,0 +1,167 @@
+"""PageRank parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerance (FP64 form): relative L1 <= 1e-9 against the oracle, and the same
+iteration count.  Rows summed by one thread use the reference's summation
+order, so most graphs come out bit-identical; longer rows are reassociated.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_l1
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-9
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def golden_names():
+    with open(os.path.join(GOLDEN, "manifest.json")) as f:
+        return sorted(json.load(f))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_pagerank(native, name):
+    g = golden(name)
+    V = int(g["V"])
+    if "ag_first_edge" in g:
+        G = native.Graph.from_arraygraph(g["ag_first_edge"], g["ag_node_deleted"], g["ag_to"], g["ag_next_edge"],
+                                         g["ag_edge_deleted"])
+    else:
+        G = native.Graph.from_edges(V, g["from"], g["to"])
+    try:
+        for key, (d, it, tol) in {"pr_default": (0.85, 100, 1e-4), "pr_tight": (0.85, 200, 1e-9),
+                                  "pr_d99": (0.99, 100, 1e-4)}.items():
+            x, st = G.pagerank(d, it, tol, stats=True)
+            assert x.shape == g[key].shape
+            assert rel_l1(x, g[key]) <= TOL, key
+            if V > 1:
+                assert st["iterations"] == int(g[key + "_iters"]), key
+    finally:
+        G.destroy()
+
+
+def test_rmat_scale14_config(native, oracle):
+    """Directed R-MAT scale 14, ef 8 (131,072 raw edges), d 0.85, tol 1e-9, 200 iterations."""
+    V, f, t = oracle.rmat(14, 8, 1014, directed=True)
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        x, st = G.pagerank(0.85, 200, 1e-9, stats=True)
+        ref, it, l1 = oracle.ArrayGraph(V, f, t).pagerank(0.85, 200, 1e-9)
+        assert rel_l1(x, ref) <= TOL
+        assert st["iterations"] == it
+        assert abs(st["residual"] - l1) <= 1e-6 * l1 + 1e-15
+    finally:
+        G.destroy()
+
+
+def test_device_generator_matches_oracle_generator(native, oracle):
+    """The CUDA R-MAT generator and the oracle's produce the same graph."""
+    for scale, directed in ((12, True), (11, False)):
+        V, f, t = oracle.rmat(scale, 8, 77 + scale, directed=directed)
+        G = native.Graph.rmat(scale, 8, 77 + scale, directed=directed)
+        try:
+            in_off, in_col, out_off, out_col, deg = G.export_csr()
+            off_r, col_r, deg_r = oracle.in_csr_from_edges(V, f, t)
+            assert np.array_equal(in_off, off_r) and np.array_equal(in_col, col_r)
+            assert np.array_equal(deg, deg_r)
+        finally:
+            G.destroy()
+    s, d = native.rmat_raw_device(10, 1010, 0, 4096)
+    g = golden("rmat10_dir")
+    assert np.array_equal(s, g["raw_src"]) and np.array_equal(d, g["raw_dst"])
+
+
+def test_in_csr_order_matches_reference(native, oracle):
+    """in-CSR rows hold sources ascending (centrality.zig:893-899) and the
+    out-CSR rows successors in reverse insertion order (array_graph.zig:94-104)."""
+    g = golden("multi_selfloop")
+    V = int(g["V"])
+    G = native.Graph.from_edges(V, g["from"], g["to"])
+    try:
+        in_off, in_col, out_off, out_col, deg = G.export_csr()
+        off_r, col_r, deg_r = oracle.in_csr_from_edges(V, g["from"], g["to"])
+        assert np.array_equal(in_off, off_r) and np.array_equal(in_col, col_r) and np.array_equal(deg, deg_r)
+        so, sc = oracle.ArrayGraph(V, g["from"], g["to"]).successor_csr()
+        assert np.array_equal(out_off, so) and np.array_equal(out_col, sc)
+    finally:
+        G.destroy()
+
+
+@pytest.mark.parametrize("max_iter", [0, 1, 2, 7])
+def test_iteration_prefix_exact(native, oracle, max_iter):
+    """Stopping after k iterations returns the k-th iterate (the swap happens
+    before the tolerance test, centrality.zig:953-957)."""
+    V, f, t = oracle.rmat(13, 8, 4242, directed=True)
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        x, st = G.pagerank(0.85, max_iter, 0.0, stats=True)
+        ref, it, _ = oracle.ArrayGraph(V, f, t).pagerank(0.85, max_iter, 0.0)
+        assert st["iterations"] == it == max_iter
+        assert rel_l1(x, ref) <= 1e-13
+    finally:
+        G.destroy()
+
+
+def test_heavy_rows_use_long_row_chunks(native, oracle):
+    """A hub with in-degree far above one block (2048 arcs) and many medium rows."""
+    rng = np.random.default_rng(5)
+    V = 20000
+    hub_src = rng.integers(0, V, 50000).astype(np.uint32)
+    f = np.concatenate([hub_src, rng.integers(0, V, 60000).astype(np.uint32), np.arange(1, 400, dtype=np.uint32)])
+    t = np.concatenate([np.zeros(50000, np.uint32), rng.integers(0, 300, 60000).astype(np.uint32),
+                        np.full(399, 7, np.uint32)])
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        x, st = G.pagerank(0.85, 200, 1e-10, stats=True)
+        ref, it, _ = oracle.ArrayGraph(V, f, t).pagerank(0.85, 200, 1e-10)
+        assert rel_l1(x, ref) <= TOL and st["iterations"] == it
+        x2 = G.pagerank(0.85, 200, 1e-10)
+        assert np.array_equal(x, x2)  # deterministic reduction order
+    finally:
+        G.destroy()
+
+
+def test_warm_start_and_personalised(native, oracle):
+    """Extensions against the generalised oracle: a start vector x0 and a
+    personalisation (teleport) vector p."""
+    V, f, t = oracle.rmat(12, 8, 99, directed=True)
+    off, col, deg = oracle.in_csr_from_edges(V, f, t)
+    rng = np.random.default_rng(1)
+    x0 = rng.random(V); x0 /= x0.sum()
+    p = np.zeros(V); p[rng.integers(0, V)] = 1.0
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        x = G.pagerank(0.85, 200, 1e-10, x0=x0)
+        ref, it, _ = oracle.pagerank_ext(V, off, col, deg, x0=x0, max_iterations=200, tolerance=1e-10)
+        assert rel_l1(x, ref) <= TOL
+        x = G.pagerank(0.85, 200, 1e-10, teleport=p)
+        ref, it, _ = oracle.pagerank_ext(V, off, col, deg, p=p, max_iterations=200, tolerance=1e-10)
+        assert rel_l1(x, ref) <= TOL
+    finally:
+        G.destroy()
+
+
+@pytest.mark.slow
+def test_large_graph_properties(native, oracle):
+    """Directed R-MAT scale 20 (ef 16): the oracle's first iterations agree, the
+    converged vector sums to 1 and its own next step is below tolerance."""
+    G = native.Graph.rmat(20, 16, 1020, directed=True)
+    try:
+        V, E, n = G.info()
+        in_off, in_col, _, _, deg = G.export_csr()
+        for k in (1, 3):
+            x = G.pagerank(0.85, k, 0.0)
+            ref, it, _, _ = oracle.pagerank_csr(V, in_off, in_col, deg, 0.85, k, 0.0)
+            assert rel_l1(x, ref) <= 1e-13
+        x, st = G.pagerank(0.85, 200, 1e-9, stats=True)
+        assert abs(x.sum() - 1.0) < 1e-9
+        y, it, l1, _ = oracle.pagerank_csr(V, in_off, in_col, deg, 0.85, 1, 0.0)  # from uniform
+        assert st["residual"] < 1e-9 and st["iterations"] < 200
+    finally:
+        G.destroy()

@@ -1,0 +1,19 @@
+"""zog_b200 -- B200-native (sm_100a) PageRank and Brandes betweenness behind
+Zog's ``ResourceGraph`` API.
+
+    import zog_b200 as zog
+    b = zog.directed().add_edge("A", "B").add_edge("B", "C")
+    g = zog.ResourceGraph.new(b)
+    zog.ResourceGraph.pagerank(g, tolerance=1e-9, max_iterations=200)
+    zog.ResourceGraph.betweenness_unweighted(g)
+    zog.ResourceGraph.destroy(g)
+
+The compute runs in ``libzogcu.so`` (CUDA, built by ``python -m
+zog_b200.build``); this package is the host-side mirror of the reference's
+Elixir API and holds no CPU implementation of either algorithm.
+"""
+from . import _native
+from . import resource_graph as ResourceGraph
+from .soa import SoA, directed, undirected
+
+__all__ = ["ResourceGraph", "SoA", "directed", "undirected", "_native"]

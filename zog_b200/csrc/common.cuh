@@ -1,0 +1,143 @@
+// common.cuh -- internal types and helpers of libzogcu (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "zogcu.h"
+
+namespace zogcu {
+
+// Marks a deleted node slot in the out-degree array.  Deleted nodes have no
+// stored arcs, so the value never reaches a gather; PageRank uses it to skip
+// the slot (the reference only iterates live nodes, utils.zig:42-48).
+constexpr uint32_t kDeletedDegree = 0xFFFFFFFFu;
+constexpr uint32_t kUnreached = 0xFFFFFFFFu;
+
+// Last error message of the calling thread (zogcu_last_error).
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+
+#define ZOGCU_CUDA(call)                                                        \
+  do {                                                                          \
+    cudaError_t _e = (call);                                                    \
+    if (_e != cudaSuccess) {                                                    \
+      return ::zogcu::fail(_e == cudaErrorMemoryAllocation ? ZOGCU_ERR_OUT_OF_MEMORY \
+                                                           : ZOGCU_ERR_CUDA,    \
+                           std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    }                                                                           \
+  } while (0)
+
+#define ZOGCU_TRY(call)                 \
+  do {                                  \
+    int _s = (call);                    \
+    if (_s != ZOGCU_OK) return _s;      \
+  } while (0)
+
+// Stream-ordered device buffer (cudaMallocAsync on the owning stream).
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes), stream(o.stream) { o.ptr = nullptr; }
+  ~DevBuf() { release(); }
+  int alloc(size_t n, cudaStream_t s);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Persistent device allocation owned by a graph (plain cudaMalloc).
+struct DevArray {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevArray() = default;
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  ~DevArray() { release(); }
+  int alloc(size_t n);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// One PageRank work item (16 bytes).  kind 0: rows [a, b) with every row's
+// in-degree <= kBlockNnz and the block's arcs <= kBlockNnz.  kind 1: chunk c of
+// nch of the single long row a (in-degree > kBlockNnz); `slot` indexes the
+// per-long-row counters.
+struct PrTask {
+  uint32_t a;
+  uint32_t b;      // kind 0: row end; kind 1: chunk index
+  uint32_t kind;   // 0 block, 1 long chunk (high 16 bits: nch for kind 1)
+  uint32_t slot;   // kind 1: long-row id
+};
+
+struct PrSchedule {
+  bool built = false;
+  uint32_t num_tasks = 0;
+  uint32_t num_long = 0;      // long rows
+  uint32_t max_chunks = 0;
+  DevArray tasks;             // PrTask[num_tasks]
+};
+
+// Device-resident graph (one per NIF resource).
+struct Graph {
+  int device = 0;
+  uint32_t V = 0;             // node capacity
+  uint64_t E = 0;             // stored arcs (live edges between live nodes)
+  uint64_t n_live = 0;        // live nodes
+  bool has_deleted = false;
+  bool offsets32 = false;     // E < 2^32: 32-bit offset copies exist
+  DevArray in_off64, out_off64;   // uint64_t[V+1]
+  DevArray in_off32, out_off32;   // uint32_t[V+1] (when offsets32)
+  DevArray in_col, out_col;       // uint32_t[E + 4] (padded for 16-byte loads)
+  DevArray out_deg;               // uint32_t[V], kDeletedDegree for deleted slots
+  DevArray live;                  // uint8_t[V] (when has_deleted)
+  std::mutex mu;                  // guards lazy schedule builds
+  PrSchedule pr;                  // PageRank schedule (built on first call)
+};
+
+int ensure_device(int* dev);
+
+// Builds a Graph from device edge arrays (src,dst) in ArrayGraph insertion
+// order (reverse_within_source = true) or already in successor order (false).
+// All endpoints must be < V and refer to live nodes.
+int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src,
+                                  const uint32_t* d_dst, uint64_t E, bool reverse_within_source,
+                                  const uint8_t* h_node_deleted, cudaStream_t stream);
+
+// PageRank schedule (pagerank.cu).
+int ensure_pr_schedule(Graph* g, cudaStream_t stream);
+
+// Small helper: number of SMs of the current device.
+int sm_count();
+
+// RAII private stream.
+struct StreamGuard {
+  cudaStream_t s = nullptr;
+  bool owned = false;
+  int init(void* user);
+  ~StreamGuard();
+};
+
+// Event timer on one stream.
+struct EventTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  int start(cudaStream_t s);
+  int stop(cudaStream_t s);
+  float ms();
+  ~EventTimer();
+};
+
+}  // namespace zogcu
+
+struct zogcu_graph {
+  zogcu::Graph g;
+};

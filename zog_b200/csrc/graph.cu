@@ -1,0 +1,626 @@
+// graph.cu -- device-resident graph resource: CSR construction, the seeded
+// R-MAT generator, the edge-list reader front end, and the ABI entry points
+// that create, inspect and destroy a graph.
+//
+// The reference keeps an ArrayGraph (per-node singly linked out-edge lists with
+// head insertion, priv/zog/src/models/array_graph.zig:88-108) inside a BEAM
+// resource and rebuilds in_neighbors / out_degrees on every PageRank call
+// (centrality.zig:881-910).  Here the equivalent CSRs are built once on the
+// device with two stable radix sorts and stay resident:
+//   out-CSR  rows = successors in SuccessorIterator order (reverse insertion)
+//   in-CSR   rows = sources ascending, duplicates adjacent -- exactly the
+//            in_neighbors lists of centrality.zig:893-899
+//   out_deg  successor counts (centrality.zig:901-910)
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <unordered_map>
+
+#include "common.cuh"
+
+namespace zogcu {
+
+// ---------------------------------------------------------------------------
+// errors, small RAII helpers
+// ---------------------------------------------------------------------------
+static thread_local std::string t_last_error;
+
+void set_error(const std::string& msg) { t_last_error = msg; }
+int fail(int status, const std::string& msg) {
+  t_last_error = msg;
+  return status;
+}
+
+int DevBuf::alloc(size_t n, cudaStream_t s) {
+  release();
+  stream = s;
+  bytes = n;
+  if (n == 0) return ZOGCU_OK;
+  cudaError_t e = cudaMallocAsync(&ptr, n, s);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    return fail(ZOGCU_ERR_OUT_OF_MEMORY, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+  }
+  return ZOGCU_OK;
+}
+void DevBuf::release() {
+  if (ptr) cudaFreeAsync(ptr, stream);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+int DevArray::alloc(size_t n) {
+  release();
+  bytes = n;
+  if (n == 0) return ZOGCU_OK;
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    return fail(ZOGCU_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  return ZOGCU_OK;
+}
+void DevArray::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+int StreamGuard::init(void* user) {
+  if (user) {
+    s = static_cast<cudaStream_t>(user);
+    owned = false;
+    return ZOGCU_OK;
+  }
+  ZOGCU_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  owned = true;
+  return ZOGCU_OK;
+}
+StreamGuard::~StreamGuard() {
+  if (owned && s) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+}
+
+int EventTimer::start(cudaStream_t s) {
+  if (!a) ZOGCU_CUDA(cudaEventCreate(&a));
+  if (!b) ZOGCU_CUDA(cudaEventCreate(&b));
+  ZOGCU_CUDA(cudaEventRecord(a, s));
+  return ZOGCU_OK;
+}
+int EventTimer::stop(cudaStream_t s) {
+  ZOGCU_CUDA(cudaEventRecord(b, s));
+  return ZOGCU_OK;
+}
+float EventTimer::ms() {
+  float t = 0.f;
+  if (a && b && cudaEventSynchronize(b) == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+  return t;
+}
+EventTimer::~EventTimer() {
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+}
+
+static int g_sm_count = 0;
+int sm_count() {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+int ensure_device(int* dev) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(ZOGCU_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  ZOGCU_CUDA(cudaGetDevice(dev));
+  int major = 0;
+  ZOGCU_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, *dev));
+  if (major != 10)
+    return fail(ZOGCU_ERR_NO_DEVICE, "libzogcu is built for sm_100a (B200); device has compute capability major " +
+                                         std::to_string(major));
+  // Keep freed stream-ordered memory in the pool instead of returning it to
+  // the driver at every synchronisation (per-process setting).
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, *dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  return ZOGCU_OK;
+}
+
+static int bits_for(uint64_t v) {  // bits needed for values in [0, v)
+  int b = 1;
+  while (b < 64 && (1ull << b) < v) ++b;
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// CSR construction kernels
+// ---------------------------------------------------------------------------
+__global__ void k_reverse_copy(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst,
+                               uint32_t* __restrict__ ksrc, uint32_t* __restrict__ vdst, uint64_t E,
+                               int reverse) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t j = reverse ? (E - 1 - i) : i;
+    ksrc[i] = src[j];
+    vdst[i] = dst[j];
+  }
+}
+
+__global__ void k_validate(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t E,
+                           uint32_t V, unsigned int* bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if (a[i] >= V || b[i] >= V) atomicOr(bad, 1u);
+  }
+}
+
+__global__ void k_histogram(const uint32_t* __restrict__ keys, uint64_t E, unsigned long long* cnt) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[keys[i]], 1ull);
+}
+
+__global__ void k_degrees(const uint64_t* __restrict__ off, const uint8_t* __restrict__ live, uint32_t V,
+                          uint32_t* __restrict__ deg) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t d = (uint32_t)(off[v + 1] - off[v]);
+    deg[v] = (live && !live[v]) ? kDeletedDegree : d;
+  }
+}
+
+__global__ void k_off32(const uint64_t* __restrict__ a, uint32_t* __restrict__ b, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = (uint32_t)a[i];
+}
+
+static unsigned grid_for(uint64_t n, unsigned block = 256) {
+  uint64_t g = (n + block - 1) / block;
+  uint64_t cap = (uint64_t)sm_count() * 32;
+  if (g > cap) g = cap;
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+// offsets (u64, V+1) from a per-row count histogram (u64, V)
+static int counts_to_offsets(unsigned long long* d_cnt, uint64_t* d_off, uint32_t V, cudaStream_t s) {
+  // exclusive scan over V+1 entries (the histogram has a trailing zero slot)
+  size_t tmp = 0;
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cnt, (unsigned long long*)d_off,
+                                           (int64_t)V + 1, s));
+  DevBuf t;
+  ZOGCU_TRY(t.alloc(tmp, s));
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(t.ptr, tmp, d_cnt, (unsigned long long*)d_off,
+                                           (int64_t)V + 1, s));
+  return ZOGCU_OK;
+}
+
+int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, const uint32_t* d_dst,
+                                  uint64_t E, bool reverse_within_source, const uint8_t* h_node_deleted,
+                                  cudaStream_t s) {
+  ZOGCU_TRY(ensure_device(&g->device));
+  g->V = V;
+  g->E = E;
+  g->offsets32 = E < 0xFFFFFFF0ull;
+  g->has_deleted = false;
+  uint64_t live = V;
+  if (h_node_deleted) {
+    live = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+      if (h_node_deleted[v]) g->has_deleted = true;
+      else ++live;
+    }
+  }
+  g->n_live = live;
+
+  const size_t colBytes = (E + 4) * sizeof(uint32_t);
+  ZOGCU_TRY(g->in_col.alloc(colBytes));
+  ZOGCU_TRY(g->out_col.alloc(colBytes));
+  ZOGCU_TRY(g->in_off64.alloc((size_t)(V + 1) * 8));
+  ZOGCU_TRY(g->out_off64.alloc((size_t)(V + 1) * 8));
+  ZOGCU_TRY(g->out_deg.alloc((size_t)std::max<uint32_t>(V, 1) * 4));
+  ZOGCU_CUDA(cudaMemsetAsync(g->in_col.ptr, 0, colBytes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(g->out_col.ptr, 0, colBytes, s));
+  if (g->has_deleted) {
+    ZOGCU_TRY(g->live.alloc(V));
+    std::vector<uint8_t> lv(V);
+    for (uint32_t v = 0; v < V; ++v) lv[v] = h_node_deleted[v] ? 0 : 1;
+    ZOGCU_CUDA(cudaMemcpyAsync(g->live.ptr, lv.data(), V, cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+  }
+
+  DevBuf cnt;
+  ZOGCU_TRY(cnt.alloc((size_t)(V + 1) * 8, s));
+  if (E > 0) {
+    DevBuf ks, vs, ks2;
+    ZOGCU_TRY(ks.alloc(E * 4, s));
+    ZOGCU_TRY(vs.alloc(E * 4, s));
+    ZOGCU_TRY(ks2.alloc(E * 4, s));
+    k_reverse_copy<<<grid_for(E), 256, 0, s>>>(d_src, d_dst, ks.as<uint32_t>(), vs.as<uint32_t>(), E,
+                                               reverse_within_source ? 1 : 0);
+    ZOGCU_CUDA(cudaGetLastError());
+    const int bits = bits_for(V);
+    // (1) stable sort by source: rows in successor order -> out-CSR
+    size_t tmp = 0;
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
+                                               vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
+                                               0, bits, s));
+    DevBuf t;
+    ZOGCU_TRY(t.alloc(tmp, s));
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
+                                               vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
+                                               0, bits, s));
+    // out offsets
+    ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
+    k_histogram<<<grid_for(E), 256, 0, s>>>(ks2.as<uint32_t>(), E, cnt.as<unsigned long long>());
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
+    // (2) stable sort of (dst, src) pairs by dst: sources stay ascending
+    size_t tmp2 = 0;
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
+                                               ks2.as<uint32_t>(), g->in_col.as<uint32_t>(), (int64_t)E, 0,
+                                               bits, s));
+    if (tmp2 > tmp) ZOGCU_TRY(t.alloc(tmp2, s));
+    tmp2 = std::max(tmp, tmp2);
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp2, g->out_col.as<uint32_t>(),
+                                               ks.as<uint32_t>(), ks2.as<uint32_t>(),
+                                               g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
+    ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
+    k_histogram<<<grid_for(E), 256, 0, s>>>(ks.as<uint32_t>(), E, cnt.as<unsigned long long>());
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->in_off64.as<uint64_t>(), V, s));
+  } else {
+    ZOGCU_CUDA(cudaMemsetAsync(g->in_off64.ptr, 0, (size_t)(V + 1) * 8, s));
+    ZOGCU_CUDA(cudaMemsetAsync(g->out_off64.ptr, 0, (size_t)(V + 1) * 8, s));
+  }
+  if (V > 0) {
+    k_degrees<<<grid_for(V), 256, 0, s>>>(g->out_off64.as<uint64_t>(), g->live.as<uint8_t>(), V,
+                                          g->out_deg.as<uint32_t>());
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  if (g->offsets32) {
+    ZOGCU_TRY(g->in_off32.alloc((size_t)(V + 1) * 4));
+    ZOGCU_TRY(g->out_off32.alloc((size_t)(V + 1) * 4));
+    k_off32<<<grid_for(V + 1), 256, 0, s>>>(g->in_off64.as<uint64_t>(), g->in_off32.as<uint32_t>(), V + 1);
+    k_off32<<<grid_for(V + 1), 256, 0, s>>>(g->out_off64.as<uint64_t>(), g->out_off32.as<uint32_t>(), V + 1);
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  return ZOGCU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Seeded R-MAT generator (the same definition as the CPU oracle's):
+//   key     = splitmix64(seed)
+//   r(i,k)  = splitmix64(key ^ (i << 6 | k))   for level k of edge i
+//   u       = r >> 11 compared with the integer thresholds floor(p * 2^53)
+//   quadrant 0:(0,0) 1:(0,1) 2:(1,0) 3:(1,1) appended MSB first to (src, dst)
+// SplitMix64: the public-domain mixer of Steele, Lea and Flood (2014).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Packs (src, dst) as src << scale | dst; undirected edges are canonicalised to
+// (lo, hi).  Every self-loop maps to the all-ones key of 2*scale bits, which is
+// itself the self-loop (V-1, V-1): after sort + unique it is the last key and
+// is cut.
+__global__ void k_rmat(uint64_t key, uint64_t M, int scale, uint64_t ta, uint64_t tab, uint64_t tabc,
+                       int directed, uint64_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t s = 0, d = 0;
+    for (int k = 0; k < scale; ++k) {
+      uint64_t u = splitmix64(key ^ ((i << 6) | (uint64_t)k)) >> 11;
+      uint32_t q = u < ta ? 0u : (u < tab ? 1u : (u < tabc ? 2u : 3u));
+      s = (s << 1) | (q >> 1);
+      d = (d << 1) | (q & 1u);
+    }
+    if (!directed && s > d) {
+      uint32_t t = s; s = d; d = t;
+    }
+    out[i] = (s == d) ? ((1ull << (2 * scale)) - 1) : (((uint64_t)s << scale) | d);
+  }
+}
+
+__global__ void k_unpack(const uint64_t* __restrict__ keys, uint64_t m, int scale, int directed,
+                         uint32_t* __restrict__ src, uint32_t* __restrict__ dst) {
+  const uint64_t mask = (1ull << scale) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t s = (uint32_t)(keys[i] >> scale), d = (uint32_t)(keys[i] & mask);
+    if (directed) {
+      src[i] = s; dst[i] = d;
+    } else {
+      src[2 * i] = s; dst[2 * i] = d;
+      src[2 * i + 1] = d; dst[2 * i + 1] = s;
+    }
+  }
+}
+
+// raw endpoints of edges [i0, i0+m) -- lets tests compare with the CPU generator
+__global__ void k_rmat_raw(uint64_t key, uint64_t i0, uint64_t m, int scale, uint64_t ta, uint64_t tab,
+                           uint64_t tabc, uint32_t* src, uint32_t* dst) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < m;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t i = i0 + j;
+    uint32_t s = 0, d = 0;
+    for (int k = 0; k < scale; ++k) {
+      uint64_t u = splitmix64(key ^ ((i << 6) | (uint64_t)k)) >> 11;
+      uint32_t q = u < ta ? 0u : (u < tab ? 1u : (u < tabc ? 2u : 3u));
+      s = (s << 1) | (q >> 1);
+      d = (d << 1) | (q & 1u);
+    }
+    src[j] = s;
+    dst[j] = d;
+  }
+}
+
+static void rmat_thresholds(double a, double b, double c, uint64_t* ta, uint64_t* tab, uint64_t* tabc) {
+  const double two53 = 9007199254740992.0;
+  *ta = (uint64_t)std::floor(a * two53);
+  *tab = (uint64_t)std::floor((a + b) * two53);
+  *tabc = (uint64_t)std::floor((a + b + c) * two53);
+}
+
+// Validates device edge arrays (addEdge's hasNode check, array_graph.zig:88-89)
+// and builds the graph on stream s.
+static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_from, const uint32_t* d_to,
+                                       uint64_t num_edges, cudaStream_t s, zogcu_graph** out) {
+  if (num_edges) {
+    DevBuf bad;
+    ZOGCU_TRY(bad.alloc(4, s));
+    ZOGCU_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
+    k_validate<<<grid_for(num_edges), 256, 0, s>>>(d_from, d_to, num_edges, node_count, bad.as<unsigned int>());
+    ZOGCU_CUDA(cudaGetLastError());
+    unsigned int h = 0;
+    ZOGCU_CUDA(cudaMemcpyAsync(&h, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    if (h) return fail(ZOGCU_ERR_NODE_NOT_FOUND, "edge endpoint >= node_count");
+  }
+  std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
+  if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
+  ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s));
+  *out = G.release();
+  return ZOGCU_OK;
+}
+
+}  // namespace zogcu
+
+using namespace zogcu;
+
+// ---------------------------------------------------------------------------
+// ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* zogcu_status_string(int status) {
+  switch (status) {
+    case ZOGCU_OK: return "ok";
+    case ZOGCU_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case ZOGCU_ERR_NODE_NOT_FOUND: return "node not found";
+    case ZOGCU_ERR_OUT_OF_MEMORY: return "out of memory";
+    case ZOGCU_ERR_CUDA: return "CUDA error";
+    case ZOGCU_ERR_NO_DEVICE: return "no usable device";
+    case ZOGCU_ERR_TIMEOUT: return "device wait timed out";
+    case ZOGCU_ERR_IO: return "I/O error";
+    case ZOGCU_ERR_TOO_LARGE: return "too large";
+    case ZOGCU_ERR_INTERNAL: return "internal error";
+    default: return "unknown status";
+  }
+}
+
+const char* zogcu_last_error(void) { return t_last_error.c_str(); }
+int zogcu_abi_version(void) { return ZOGCU_ABI_VERSION; }
+void zogcu_free(void* p) { std::free(p); }
+
+int zogcu_graph_create_from_device_edges(uint32_t node_count, const uint32_t* d_from, const uint32_t* d_to,
+                                         uint64_t num_edges, void* stream, zogcu_graph** out) {
+  if (!out) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out is null");
+  *out = nullptr;
+  if (num_edges && (!d_from || !d_to)) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "edge arrays are null");
+  if (num_edges >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "edge count exceeds u32 edge indices");
+  int dev;
+  ZOGCU_TRY(ensure_device(&dev));
+  StreamGuard sg;
+  ZOGCU_TRY(sg.init(stream));
+  return create_from_device_edges_on(node_count, d_from, d_to, num_edges, sg.s, out);
+}
+
+int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, const uint32_t* to,
+                                  const double* weight, uint64_t num_edges, zogcu_graph** out) {
+  (void)weight;  // PageRank and unweighted Brandes ignore weights (centrality.zig:936-941)
+  if (!out) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out is null");
+  *out = nullptr;
+  if (num_edges && (!from || !to)) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "edge arrays are null");
+  if (num_edges >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "edge count exceeds u32 edge indices");
+  int dev;
+  ZOGCU_TRY(ensure_device(&dev));
+  StreamGuard sg;
+  ZOGCU_TRY(sg.init(nullptr));
+  DevBuf df, dt;
+  ZOGCU_TRY(df.alloc(num_edges * 4, sg.s));
+  ZOGCU_TRY(dt.alloc(num_edges * 4, sg.s));
+  if (num_edges) {
+    ZOGCU_CUDA(cudaMemcpyAsync(df.ptr, from, num_edges * 4, cudaMemcpyHostToDevice, sg.s));
+    ZOGCU_CUDA(cudaMemcpyAsync(dt.ptr, to, num_edges * 4, cudaMemcpyHostToDevice, sg.s));
+  }
+  return create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out);
+}
+
+int zogcu_graph_create_from_arraygraph(uint32_t V, const uint32_t* first_edge, const uint8_t* node_deleted,
+                                       uint64_t edge_capacity, const uint32_t* to, const uint32_t* next_edge,
+                                       const uint8_t* edge_deleted, zogcu_graph** out) {
+  if (!out) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out is null");
+  *out = nullptr;
+  if (V && !first_edge) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "first_edge is null");
+  if (edge_capacity && (!to || !next_edge)) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "edge slices are null");
+  // Walk every live node's list like SuccessorIterator.next (array_graph.zig:164-180).
+  std::vector<uint32_t> src, dst;
+  src.reserve(edge_capacity);
+  dst.reserve(edge_capacity);
+  for (uint32_t v = 0; v < V; ++v) {
+    if (node_deleted && node_deleted[v]) continue;
+    uint32_t idx = first_edge[v];
+    uint64_t steps = 0;
+    while (idx != 0xFFFFFFFFu) {
+      if (idx >= edge_capacity || ++steps > edge_capacity)
+        return fail(ZOGCU_ERR_INVALID_ARGUMENT, "corrupt edge list at node " + std::to_string(v));
+      uint32_t nxt = next_edge[idx];
+      if (!(edge_deleted && edge_deleted[idx])) {
+        uint32_t d = to[idx];
+        if (d >= V) return fail(ZOGCU_ERR_NODE_NOT_FOUND, "edge target >= node capacity");
+        if (!(node_deleted && node_deleted[d])) {
+          src.push_back(v);
+          dst.push_back(d);
+        }
+      }
+      idx = nxt;
+    }
+  }
+  int dev;
+  ZOGCU_TRY(ensure_device(&dev));
+  StreamGuard sg;
+  ZOGCU_TRY(sg.init(nullptr));
+  uint64_t E = src.size();
+  DevBuf df, dt;
+  ZOGCU_TRY(df.alloc(E * 4, sg.s));
+  ZOGCU_TRY(dt.alloc(E * 4, sg.s));
+  if (E) {
+    ZOGCU_CUDA(cudaMemcpyAsync(df.ptr, src.data(), E * 4, cudaMemcpyHostToDevice, sg.s));
+    ZOGCU_CUDA(cudaMemcpyAsync(dt.ptr, dst.data(), E * 4, cudaMemcpyHostToDevice, sg.s));
+  }
+  std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
+  if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
+  ZOGCU_TRY(build_graph_from_device_edges(&G->g, V, df.as<uint32_t>(), dt.as<uint32_t>(), E,
+                                          /*already successor order*/ false, node_deleted, sg.s));
+  *out = G.release();
+  return ZOGCU_OK;
+}
+
+int zogcu_graph_generate_rmat(int scale, int edge_factor, uint64_t seed, double a, double b, double c,
+                              int directed, zogcu_graph** out) {
+  if (!out) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out is null");
+  *out = nullptr;
+  if (scale < 1 || scale > 31 || edge_factor < 1 || edge_factor > 64)
+    return fail(ZOGCU_ERR_INVALID_ARGUMENT, "scale must be in [1,31], edge_factor in [1,64]");
+  if (!(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0))
+    return fail(ZOGCU_ERR_INVALID_ARGUMENT, "R-MAT probabilities must be >= 0 with a+b+c <= 1");
+  const uint64_t M = (uint64_t)edge_factor << scale;
+  if (!directed && 2 * M >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "too many arcs");
+  int dev;
+  ZOGCU_TRY(ensure_device(&dev));
+  StreamGuard sg;
+  ZOGCU_TRY(sg.init(nullptr));
+  uint64_t ta, tab, tabc;
+  rmat_thresholds(a, b, c, &ta, &tab, &tabc);
+  DevBuf k1, k2, nsel;
+  ZOGCU_TRY(k1.alloc(M * 8, sg.s));
+  ZOGCU_TRY(k2.alloc(M * 8, sg.s));
+  ZOGCU_TRY(nsel.alloc(8, sg.s));
+  k_rmat<<<grid_for(M), 256, 0, sg.s>>>(splitmix64(seed), M, scale, ta, tab, tabc, directed,
+                                        k1.as<uint64_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  size_t tmp = 0;
+  ZOGCU_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, k1.as<uint64_t>(), k2.as<uint64_t>(), (int64_t)M, 0,
+                                            2 * scale, sg.s));
+  DevBuf t;
+  ZOGCU_TRY(t.alloc(tmp, sg.s));
+  ZOGCU_CUDA(cub::DeviceRadixSort::SortKeys(t.ptr, tmp, k1.as<uint64_t>(), k2.as<uint64_t>(), (int64_t)M, 0,
+                                            2 * scale, sg.s));
+  size_t tmp2 = 0;
+  ZOGCU_CUDA(cub::DeviceSelect::Unique(nullptr, tmp2, k2.as<uint64_t>(), k1.as<uint64_t>(),
+                                       nsel.as<unsigned long long>(), (int64_t)M, sg.s));
+  if (tmp2 > tmp) ZOGCU_TRY(t.alloc(tmp2, sg.s));
+  tmp2 = std::max(tmp, tmp2);
+  ZOGCU_CUDA(cub::DeviceSelect::Unique(t.ptr, tmp2, k2.as<uint64_t>(), k1.as<uint64_t>(),
+                                       nsel.as<unsigned long long>(), (int64_t)M, sg.s));
+  unsigned long long m = 0;
+  ZOGCU_CUDA(cudaMemcpyAsync(&m, nsel.ptr, 8, cudaMemcpyDeviceToHost, sg.s));
+  ZOGCU_CUDA(cudaStreamSynchronize(sg.s));
+  // drop the self-loop sentinel (largest key) if present
+  if (m > 0) {
+    uint64_t last = 0;
+    ZOGCU_CUDA(cudaMemcpy(&last, k1.as<uint64_t>() + (m - 1), 8, cudaMemcpyDeviceToHost));
+    if (last == (1ull << (2 * scale)) - 1) m -= 1;
+  }
+  t.release();
+  k2.release();
+  const uint64_t E = directed ? m : 2 * m;
+  DevBuf es, ed;
+  ZOGCU_TRY(es.alloc(std::max<uint64_t>(E, 1) * 4, sg.s));
+  ZOGCU_TRY(ed.alloc(std::max<uint64_t>(E, 1) * 4, sg.s));
+  if (m) {
+    k_unpack<<<grid_for(m), 256, 0, sg.s>>>(k1.as<uint64_t>(), m, scale, directed, es.as<uint32_t>(),
+                                            ed.as<uint32_t>());
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  k1.release();
+  std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
+  if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
+  ZOGCU_TRY(build_graph_from_device_edges(&G->g, 1u << scale, es.as<uint32_t>(), ed.as<uint32_t>(), E, true,
+                                          nullptr, sg.s));
+  *out = G.release();
+  return ZOGCU_OK;
+}
+
+// Raw R-MAT endpoints into device arrays (test hook for generator parity).
+int zogcu_rmat_raw_device(int scale, uint64_t seed, double a, double b, double c, uint64_t i0, uint64_t m,
+                          uint32_t* d_src, uint32_t* d_dst) {
+  if (!d_src || !d_dst || scale < 1 || scale > 31) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "bad arguments");
+  int dev;
+  ZOGCU_TRY(ensure_device(&dev));
+  uint64_t ta, tab, tabc;
+  rmat_thresholds(a, b, c, &ta, &tab, &tabc);
+  k_rmat_raw<<<grid_for(m), 256>>>(splitmix64(seed), i0, m, scale, ta, tab, tabc, d_src, d_dst);
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_CUDA(cudaDeviceSynchronize());
+  return ZOGCU_OK;
+}
+
+int zogcu_graph_destroy(zogcu_graph* g) {
+  if (!g) return ZOGCU_OK;
+  cudaSetDevice(g->g.device);
+  delete g;
+  return ZOGCU_OK;
+}
+
+int zogcu_graph_info(const zogcu_graph* g, uint32_t* V, uint64_t* E, uint64_t* live) {
+  if (!g) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "graph is null");
+  if (V) *V = g->g.V;
+  if (E) *E = g->g.E;
+  if (live) *live = g->g.n_live;
+  return ZOGCU_OK;
+}
+
+int zogcu_graph_export_csr(const zogcu_graph* G, uint64_t* in_off, uint32_t* in_col, uint64_t* out_off,
+                           uint32_t* out_col, uint32_t* out_degree) {
+  if (!G) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "graph is null");
+  const Graph& g = G->g;
+  ZOGCU_CUDA(cudaSetDevice(g.device));
+  if (in_off) ZOGCU_CUDA(cudaMemcpy(in_off, g.in_off64.ptr, (size_t)(g.V + 1) * 8, cudaMemcpyDeviceToHost));
+  if (out_off) ZOGCU_CUDA(cudaMemcpy(out_off, g.out_off64.ptr, (size_t)(g.V + 1) * 8, cudaMemcpyDeviceToHost));
+  if (in_col && g.E) ZOGCU_CUDA(cudaMemcpy(in_col, g.in_col.ptr, g.E * 4, cudaMemcpyDeviceToHost));
+  if (out_col && g.E) ZOGCU_CUDA(cudaMemcpy(out_col, g.out_col.ptr, g.E * 4, cudaMemcpyDeviceToHost));
+  if (out_degree && g.V) ZOGCU_CUDA(cudaMemcpy(out_degree, g.out_deg.ptr, (size_t)g.V * 4, cudaMemcpyDeviceToHost));
+  return ZOGCU_OK;
+}
+
+}  // extern "C"
