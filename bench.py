@@ -428,9 +428,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
+    ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
+    ap.add_argument("--bc-scale", type=int, default=BC_SCALE, help="R-MAT scale of the Brandes graph")
     ap.add_argument("--ref-pr-iterations", type=int, default=128,
                     help="iterations the full solve takes (the GPU arm reports the measured count)")
     args = ap.parse_args()
+    global PR_SCALE, PR_SEED, BC_SCALE, BC_SEED
+    if args.pr_scale != PR_SCALE:
+        PR_SCALE, PR_SEED = args.pr_scale, 1000 + args.pr_scale
+    if args.bc_scale != BC_SCALE:
+        BC_SCALE, BC_SEED = args.bc_scale, 1000 + args.bc_scale
     if args.impl == "reference":
         return run_reference(args)
     return run_zog(args)
