@@ -415,6 +415,7 @@ def run_zog(args):
 
 
 def main():
+    global PR_SCALE, PR_SEED, BC_SCALE, BC_SEED
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -433,7 +434,6 @@ def main():
     ap.add_argument("--ref-pr-iterations", type=int, default=128,
                     help="iterations the full solve takes (the GPU arm reports the measured count)")
     args = ap.parse_args()
-    global PR_SCALE, PR_SEED, BC_SCALE, BC_SEED
     if args.pr_scale != PR_SCALE:
         PR_SCALE, PR_SEED = args.pr_scale, 1000 + args.pr_scale
     if args.bc_scale != BC_SCALE:
