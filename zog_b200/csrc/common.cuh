@@ -68,23 +68,31 @@ struct DevArray {
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
-// One PageRank work item (16 bytes).  kind 0: rows [a, b) with every row's
-// in-degree <= kBlockNnz and the block's arcs <= kBlockNnz.  kind 1: chunk c of
-// nch of the single long row a (in-degree > kBlockNnz); `slot` indexes the
-// per-long-row counters.
+// One PageRank work item (8 bytes): kind = b >> 30.
+//   kind 0: rows [a, b & 0x3FFFFFFF) of the degree-ranked in-CSR
+//   kind 1: the single row a
+//   kind 2: chunk (b & 0xFFFF) of the long row a
 struct PrTask {
   uint32_t a;
-  uint32_t b;      // kind 0: row end; kind 1: chunk index
-  uint32_t kind;   // 0 block, 1 long chunk (high 16 bits: nch for kind 1)
-  uint32_t slot;   // kind 1: long-row id
+  uint32_t b;
 };
 
+// PageRank view of a graph, built on the first PageRank call: nodes renumbered
+// by out-degree (descending; deleted slots last), so the most gathered
+// contributions form a contiguous prefix that fits in shared memory, with the
+// in-CSR re-laid in that order (each row keeps the reference's ascending
+// source order) and the schedule of warp work items.
 struct PrSchedule {
   bool built = false;
   uint32_t num_tasks = 0;
-  uint32_t num_long = 0;      // long rows
-  uint32_t max_chunks = 0;
+  uint32_t num_long = 0;      // rows split into chunks
+  DevArray rank;              // uint32_t[V]: rank of node v
+  DevArray perm;              // uint32_t[V]: node of rank p
+  DevArray off;               // uint32_t[V+1] (or uint64_t when E >= 2^32)
+  DevArray col;               // uint32_t[E+4]: ranks of the sources
+  DevArray deg;               // uint32_t[V]: out-degree of rank p
   DevArray tasks;             // PrTask[num_tasks]
+  DevArray long_first;        // uint32_t[num_long]: first chunk task of each long row
 };
 
 // Device-resident graph (one per NIF resource).

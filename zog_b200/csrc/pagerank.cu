@@ -7,23 +7,38 @@
 //     l1       = sum |x'[v] - x[v]|                                (:947-950)
 // swaps, and stops once l1 < tol (:953-957).
 //
-// B200 design (one fused, persistent pass per iteration):
-//   * pull SpMV over the in-CSR with a precomputed contribution vector
-//     c[u] = x[u]/deg(u) (the reference's per-term quotient, bit for bit);
-//   * degree-binned schedule built once per graph: rows are packed into blocks
-//     of <= kBlockNnz arcs and <= kRowCap rows; inside a block, rows of
-//     in-degree <= kShortLen are summed by one thread each (sequentially, in
-//     the reference's ascending-source order), longer rows by a warp, and rows
-//     longer than kBlockNnz are split into CTA-sized chunks whose partials the
-//     last-arriving CTA combines;
-//   * arc indices stream in as 16-byte vectors (ld.global.cs, evict-first) and
-//     the gathered c values are staged in shared memory;
-//   * the epilogue writes x', c' = x'/deg, and accumulates |x'-x| and the
-//     dangling mass of x' (the next iteration's sink) -- warp shuffle, CTA
-//     reduction, then a deterministic last-CTA reduction over fixed slots;
-//   * the convergence test runs on the device: the last CTA publishes l1 and a
-//     converged flag, and later launches of the same chain exit at once, so the
-//     host enqueues max_iterations launches without a round trip.
+// B200 design (one fused pass per iteration, warp-granular work):
+//   * a PageRank view of the graph built on the first call: nodes renumbered
+//     by out-degree (descending), so the contributions gathered most often --
+//     c[u] = x[u]/deg(u), the reference's per-term quotient bit for bit -- form
+//     a contiguous prefix; each row keeps the reference's ascending-source
+//     order.  Random 8-byte gathers are limited by the L1 tag stage (about one
+//     128-byte line per SM clock); the prefix of c (the "hub" part, 192 KB) is
+//     copied into shared memory at the start of every iteration and gathered
+//     from there instead;
+//   * degree-binned schedule, one warp per work item:
+//       A  a block of consecutive rows, each of in-degree <= kWarpNnz, with
+//          <= kWarpNnz arcs and <= kWarpRows rows in total: 16-byte index loads,
+//          gathers staged in the warp's shared-memory slice, rows of in-degree
+//          <= kShortLen summed by one lane each in the reference's order,
+//          longer ones by the warp;
+//       B  one row with kWarpNnz < in-degree <= kLongChunk, reduced by a warp;
+//       C  one kLongChunk-arc chunk of a longer row; the last warp to finish a
+//          row (arrival counter) adds the chunk partials in chunk order and
+//          runs the row's epilogue;
+//     warps never wait on each other inside the pass and prefetch their next
+//     work item;
+//   * arc indices stream with an L2 evict-first policy, bypassing L1; gathered
+//     contributions use an L2 evict-last policy;
+//   * the epilogue writes x', c' = x'/deg and accumulates |x'-x| and the
+//     dangling mass of x' (the next iteration's sink): lane -> warp -> CTA
+//     partials, then a deterministic last-CTA reduction over fixed slots;
+//   * convergence is decided on the device: the last CTA publishes l1 and a
+//     converged flag, later launches of the chain exit at once, and the host
+//     enqueues max_iterations launches with no round trip.
+#include <cub/cub.cuh>
+
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -32,10 +47,15 @@
 
 namespace zogcu {
 
-constexpr int kPrThreads = 256;
-constexpr int kBlockNnz = 2048;   // arcs per block / per long-row chunk
-constexpr int kRowCap = 512;      // rows per block
-constexpr int kShortLen = 32;     // rows up to this in-degree: one thread each
+constexpr int kPrThreads = 1024;         // one CTA per SM
+constexpr int kPrWarps = kPrThreads / 32;
+constexpr int kWarpNnz = 128;            // arcs per row block (4 per lane)
+constexpr int kWarpRows = 64;            // rows per row block (2 per lane)
+constexpr int kShortLen = 32;            // in-degree summed by a single lane
+constexpr int kLongChunk = 4096;         // arcs per chunk of a long row
+constexpr int kHubBytes = 192 * 1024;    // shared-memory copy of the hottest contributions
+
+enum : uint32_t { kTaskBlock = 0, kTaskRow = 1, kTaskChunk = 2 };
 
 struct PrState {
   unsigned long long iter;  // iterations completed
@@ -52,28 +72,67 @@ struct PrArgs {
   const uint32_t* col;
   const uint32_t* deg;
   const PrTask* tasks;
+  const uint32_t* long_first;
   uint32_t ntasks;
   uint32_t nlong;
+  uint32_t hub;          // contributions [0, hub) are read from shared memory
   double* x0;
   double* x1;
   CT* c0;
   CT* c1;
   double* cta_part;      // [2 * gridDim.x]
   double* chunk_part;    // [ntasks]
-  unsigned int* long_cnt;// [nlong]
-  double* long_part;     // [2 * nlong]
+  unsigned int* long_cnt;// [ntasks], indexed by a long row's first chunk task
+  double* long_part;     // [2 * ntasks], same indexing
   PrState* st;
-  const double* teleport;  // personalised teleport p[v] or null (uniform)
+  const double* teleport;  // personalised teleport p (ranked order) or null
   double damping;
   double n_f;
   double tol;
   unsigned long long max_iter;
 };
 
-__device__ __forceinline__ uint4 ld_stream_u4(const uint4* p) { return __ldcs(p); }
+// ---- cache-policy loads ------------------------------------------------------
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint4 ld_arcs(const uint4* a, uint64_t pol) {
+  uint4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_contrib(const double* a, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_contrib(const float* a, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return (double)v;
+}
 
 template <typename CT>
-__device__ __forceinline__ double to_d(CT v) { return (double)v; }
+__device__ __forceinline__ double gather(uint32_t p, const CT* __restrict__ hub, uint32_t nhub,
+                                         const CT* __restrict__ c, uint64_t pol) {
+  return p < nhub ? (double)hub[p] : ld_contrib(c + p, pol);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 // Epilogue of one row: the reference's update (centrality.zig:943) evaluated
 // with explicit round-to-nearest operations (no FMA contraction), then the
@@ -97,16 +156,40 @@ __device__ __forceinline__ void pr_row_epilogue(const PrArgs<OffT, CT>& A, uint3
   }
 }
 
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
+// Sum of c[col[e]] over e in [e0, e1) by one warp (lane partials, then a fixed
+// shuffle tree), two 16-byte index vectors per lane per step.
+template <typename OffT, typename CT>
+__device__ __forceinline__ double warp_range_sum(const uint32_t* __restrict__ col, const CT* __restrict__ c,
+                                                 const CT* __restrict__ hub, uint32_t nhub, OffT e0, OffT e1,
+                                                 int lane, uint64_t pol_arc, uint64_t pol_c) {
+  const OffT base = e0 & ~(OffT)3;
+  const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
+  const uint4* cv = reinterpret_cast<const uint4*>(col + base);
+  double s = 0.0;
+  for (uint32_t j = lane; j < nvec; j += 64) {
+    const uint4 q0 = ld_arcs(cv + j, pol_arc);
+    uint4 q1 = make_uint4(0, 0, 0, 0);
+    const bool two = j + 32 < nvec;
+    if (two) q1 = ld_arcs(cv + j + 32, pol_arc);
+    const OffT ea = base + 4 * (OffT)j, eb = ea + 128;
+    double v[8];
+    v[0] = (ea >= e0 && ea < e1) ? gather(q0.x, hub, nhub, c, pol_c) : 0.0;
+    v[1] = (ea + 1 >= e0 && ea + 1 < e1) ? gather(q0.y, hub, nhub, c, pol_c) : 0.0;
+    v[2] = (ea + 2 >= e0 && ea + 2 < e1) ? gather(q0.z, hub, nhub, c, pol_c) : 0.0;
+    v[3] = (ea + 3 >= e0 && ea + 3 < e1) ? gather(q0.w, hub, nhub, c, pol_c) : 0.0;
+    v[4] = (two && eb < e1) ? gather(q1.x, hub, nhub, c, pol_c) : 0.0;
+    v[5] = (two && eb + 1 < e1) ? gather(q1.y, hub, nhub, c, pol_c) : 0.0;
+    v[6] = (two && eb + 2 < e1) ? gather(q1.z, hub, nhub, c, pol_c) : 0.0;
+    v[7] = (two && eb + 3 < e1) ? gather(q1.w, hub, nhub, c, pol_c) : 0.0;
+    s += ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+  }
+  return warp_sum(s);
 }
 
 // Deterministic CTA sum of two doubles; result valid in thread 0.
 __device__ __forceinline__ void cta_sum2(double& a, double& b, double* s_red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
   a = warp_sum(a);
   b = warp_sum(b);
   __syncthreads();
@@ -117,7 +200,7 @@ __device__ __forceinline__ void cta_sum2(double& a, double& b, double* s_red) {
   __syncthreads();
   if (threadIdx.x == 0) {
     double ra = 0.0, rb = 0.0;
-    for (int w = 0; w < kPrThreads / 32; ++w) {
+    for (int w = 0; w < nw; ++w) {
       ra += s_red[2 * w];
       rb += s_red[2 * w + 1];
     }
@@ -129,16 +212,17 @@ __device__ __forceinline__ void cta_sum2(double& a, double& b, double* s_red) {
 // Last-CTA reduction of the per-CTA and per-long-row partial slots, in a fixed
 // order, then publication of the iteration's result.
 __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta, const double* long_part,
-                             uint32_t nlong, unsigned long long next_iter, double tol, bool set_l1,
-                             double* s_red) {
+                             const uint32_t* long_first, uint32_t nlong, unsigned long long next_iter, double tol,
+                             bool set_l1, double* s_red) {
   double a = 0.0, b = 0.0;
-  for (uint32_t i = threadIdx.x; i < ncta; i += kPrThreads) {
+  for (uint32_t i = threadIdx.x; i < ncta; i += blockDim.x) {
     a += __ldcg(cta_part + 2 * i);
     b += __ldcg(cta_part + 2 * i + 1);
   }
-  for (uint32_t i = threadIdx.x; i < nlong; i += kPrThreads) {
-    a += __ldcg(long_part + 2 * i);
-    b += __ldcg(long_part + 2 * i + 1);
+  for (uint32_t i = threadIdx.x; i < nlong; i += blockDim.x) {
+    const uint32_t f = long_first[i];
+    a += __ldcg(long_part + 2 * (size_t)f);
+    b += __ldcg(long_part + 2 * (size_t)f + 1);
   }
   cta_sum2(a, b, s_red);
   if (threadIdx.x == 0) {
@@ -156,15 +240,36 @@ __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta,
   }
 }
 
+// Publishes a CTA's partials and runs the final reduction in the last CTA.
+__device__ __forceinline__ void cta_publish(PrState* st, double* cta_part, const double* long_part,
+                                            const uint32_t* long_first, uint32_t nlong, double l1, double dsum,
+                                            unsigned long long next_iter, double tol, bool set_l1, double* s_red,
+                                            int* s_flag) {
+  cta_sum2(l1, dsum, s_red);
+  if (threadIdx.x == 0) {
+    cta_part[2 * blockIdx.x] = l1;
+    cta_part[2 * blockIdx.x + 1] = dsum;
+    __threadfence();
+    const unsigned int t = atomicAdd(&st->done_ctas, 1u);
+    *s_flag = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (*s_flag) {
+    __threadfence();
+    final_reduce(st, cta_part, gridDim.x, long_part, long_first, nlong, next_iter, tol, set_l1, s_red);
+  }
+}
+
 // x0 / c0 from the start vector; sink of x0.  `given` = x0 already holds a
-// caller's start vector (warm start), else the uniform 1/n of :912-918.
+// caller's start vector in ranked order (warm start), else the uniform 1/n of
+// centrality.zig:912-918.
 template <typename OffT, typename CT>
-__global__ void __launch_bounds__(kPrThreads) pr_init_kernel(PrArgs<OffT, CT> A, uint32_t V, int given) {
-  __shared__ double s_red[2 * (kPrThreads / 32)];
-  __shared__ int s_last;
-  double dsum = 0.0, unused = 0.0;
+__global__ void __launch_bounds__(256) pr_init_kernel(PrArgs<OffT, CT> A, uint32_t V, int given) {
+  __shared__ double s_red[2 * 8];
+  __shared__ int s_flag;
+  double dsum = 0.0;
   const double init = 1.0 / A.n_f;
-  for (uint64_t v = blockIdx.x * (uint64_t)kPrThreads + threadIdx.x; v < V; v += (uint64_t)gridDim.x * kPrThreads) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t deg = A.deg[v];
     double x = 0.0;
     if (deg != kDeletedDegree) {
@@ -175,26 +280,14 @@ __global__ void __launch_bounds__(kPrThreads) pr_init_kernel(PrArgs<OffT, CT> A,
     A.x0[v] = x;
     A.x1[v] = 0.0;
   }
-  cta_sum2(unused, dsum, s_red);
-  if (threadIdx.x == 0) {
-    A.cta_part[2 * blockIdx.x] = 0.0;
-    A.cta_part[2 * blockIdx.x + 1] = dsum;
-    __threadfence();
-    unsigned int t = atomicAdd(&A.st->done_ctas, 1u);
-    s_last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    final_reduce(A.st, A.cta_part, gridDim.x, A.long_part, 0, 0ull, A.tol, false, s_red);
-  }
+  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, 0, 0.0, dsum, 0ull, A.tol, false, s_red, &s_flag);
 }
 
 template <typename OffT, typename CT>
-__global__ void __launch_bounds__(kPrThreads, 4) pr_iter_kernel(PrArgs<OffT, CT> A) {
-  __shared__ __align__(16) double s_val[kBlockNnz];
-  __shared__ uint32_t s_off[kRowCap + 1];
-  __shared__ double s_red[2 * (kPrThreads / 32)];
+__global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT> A) {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  __shared__ __align__(16) double s_val[kPrWarps][kWarpNnz];
+  __shared__ double s_red[2 * kPrWarps];
   __shared__ int s_flag;
 
   const PrState* st = A.st;
@@ -210,40 +303,65 @@ __global__ void __launch_bounds__(kPrThreads, 4) pr_iter_kernel(PrArgs<OffT, CT>
   CT* __restrict__ cnxt = par ? A.c0 : A.c1;
   const double tele_u = (1.0 - A.damping) / A.n_f;
 
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // ---- stage the hot prefix of c in shared memory --------------------------
+  CT* hub = reinterpret_cast<CT*>(s_dyn);
+  const uint32_t nhub = A.hub;
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(ccur);
+    uint4* dst = reinterpret_cast<uint4*>(hub);
+    const uint32_t n16 = (uint32_t)(((size_t)nhub * sizeof(CT)) >> 4);
+    for (uint32_t i = threadIdx.x; i < n16; i += kPrThreads) dst[i] = __ldcg(src + i);
+  }
+  __syncthreads();
+
+  const uint64_t pol_arc = policy_evict_first();
+  const uint64_t pol_c = policy_evict_last();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* sv = s_val[warp];
   double l1 = 0.0, dsum = 0.0;
 
-  for (uint32_t ti = blockIdx.x; ti < A.ntasks; ti += gridDim.x) {
-    const PrTask t = A.tasks[ti];
-    if ((t.kind & 0xFFFFu) == 0) {
-      // ---- block of rows [r0, r1) --------------------------------------
-      const uint32_t r0 = t.a, r1 = t.b, nrows = r1 - r0;
+  const uint32_t nwarps = gridDim.x * kPrWarps;
+  uint32_t ti = blockIdx.x * kPrWarps + warp;
+  PrTask t = ti < A.ntasks ? A.tasks[ti] : PrTask{0, 0};
+  while (ti < A.ntasks) {
+    const uint32_t tn = ti + nwarps;
+    const PrTask nx = tn < A.ntasks ? A.tasks[tn] : PrTask{0, 0};  // prefetch
+    const uint32_t kind = t.b >> 30;
+    if (kind == kTaskBlock) {
+      // ---- rows [r0, r1): <= kWarpNnz arcs, <= kWarpRows rows ------------
+      const uint32_t r0 = t.a, r1 = t.b & 0x3FFFFFFFu, nrows = r1 - r0;
       const OffT e0 = __ldg(A.off + r0), e1 = __ldg(A.off + r1);
-      for (uint32_t i = tid; i <= nrows; i += kPrThreads) s_off[i] = (uint32_t)(__ldg(A.off + r0 + i) - e0);
       const OffT base = e0 & ~(OffT)3;
       const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
       const uint4* cv = reinterpret_cast<const uint4*>(A.col + base);
-      for (uint32_t j = tid; j < nvec; j += kPrThreads) {
-        const uint4 q = ld_stream_u4(cv + j);
+      for (uint32_t j = lane; j < nvec; j += 32) {
+        const uint4 q = ld_arcs(cv + j, pol_arc);
         const OffT e = base + 4 * (OffT)j;
-        if (e >= e0 && e < e1) s_val[e - e0] = to_d(__ldg(ccur + q.x));
-        if (e + 1 >= e0 && e + 1 < e1) s_val[e + 1 - e0] = to_d(__ldg(ccur + q.y));
-        if (e + 2 >= e0 && e + 2 < e1) s_val[e + 2 - e0] = to_d(__ldg(ccur + q.z));
-        if (e + 3 >= e0 && e + 3 < e1) s_val[e + 3 - e0] = to_d(__ldg(ccur + q.w));
+        if (e >= e0 && e < e1) sv[e - e0] = gather(q.x, hub, nhub, ccur, pol_c);
+        if (e + 1 >= e0 && e + 1 < e1) sv[e + 1 - e0] = gather(q.y, hub, nhub, ccur, pol_c);
+        if (e + 2 >= e0 && e + 2 < e1) sv[e + 2 - e0] = gather(q.z, hub, nhub, ccur, pol_c);
+        if (e + 3 >= e0 && e + 3 < e1) sv[e + 3 - e0] = gather(q.w, hub, nhub, ccur, pol_c);
       }
-      __syncthreads();
-      for (uint32_t wb = (uint32_t)warp * 32; wb < nrows; wb += kPrThreads) {
-        const uint32_t i = wb + lane;
+      // row bounds (relative to e0) of rows lane and lane+32
+      uint32_t b0 = 0, n0 = 0, b1 = 0, n1 = 0;
+      if ((uint32_t)lane < nrows) {
+        b0 = (uint32_t)(__ldg(A.off + r0 + lane) - e0);
+        n0 = (uint32_t)(__ldg(A.off + r0 + lane + 1) - e0);
+      }
+      if ((uint32_t)lane + 32 < nrows) {
+        b1 = (uint32_t)(__ldg(A.off + r0 + lane + 32) - e0);
+        n1 = (uint32_t)(__ldg(A.off + r0 + lane + 33) - e0);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        const uint32_t i = lane + 32 * half;
         const bool valid = i < nrows;
-        uint32_t b = 0, en = 0;
-        if (valid) {
-          b = s_off[i];
-          en = s_off[i + 1];
-        }
+        const uint32_t b = half ? b1 : b0, en = half ? n1 : n0;
         const bool is_short = valid && (en - b) <= (uint32_t)kShortLen;
         if (is_short) {
           double s = 0.0;
-          for (uint32_t k = b; k < en; ++k) s += s_val[k];  // ascending source order
+          for (uint32_t k = b; k < en; ++k) s += sv[k];  // ascending source order
           pr_row_epilogue(A, r0 + i, s, xcur, xnxt, cnxt, tele_u, sink, l1, dsum);
         }
         unsigned med = __ballot_sync(0xffffffffu, valid && !is_short);
@@ -252,177 +370,282 @@ __global__ void __launch_bounds__(kPrThreads, 4) pr_iter_kernel(PrArgs<OffT, CT>
           med &= med - 1;
           const uint32_t bk = __shfl_sync(0xffffffffu, b, k), ek = __shfl_sync(0xffffffffu, en, k);
           double s = 0.0;
-          for (uint32_t j = bk + lane; j < ek; j += 32) s += s_val[j];
+          for (uint32_t j = bk + lane; j < ek; j += 32) s += sv[j];
           s = warp_sum(s);
           if (lane == k) pr_row_epilogue(A, r0 + i, s, xcur, xnxt, cnxt, tele_u, sink, l1, dsum);
         }
       }
-      __syncthreads();
+      __syncwarp();
+    } else if (kind == kTaskRow) {
+      // ---- one row of kWarpNnz < in-degree <= kLongChunk ---------------------
+      const uint32_t row = t.a;
+      const double s = warp_range_sum(A.col, ccur, hub, nhub, __ldg(A.off + row), __ldg(A.off + row + 1), lane,
+                                      pol_arc, pol_c);
+      if (lane == 0) pr_row_epilogue(A, row, s, xcur, xnxt, cnxt, tele_u, sink, l1, dsum);
     } else {
-      // ---- chunk c of nch of long row `row` ------------------------------
-      const uint32_t row = t.a, c = t.b, nch = t.kind >> 16, slot = t.slot;
+      // ---- chunk c of a long row ---------------------------------------------
+      const uint32_t row = t.a, c = t.b & 0xFFFFu;
       const OffT rs = __ldg(A.off + row), re = __ldg(A.off + row + 1);
-      const OffT e0 = rs + (OffT)c * kBlockNnz;
-      const OffT e1 = min(e0 + (OffT)kBlockNnz, re);
-      const OffT base = e0 & ~(OffT)3;
-      const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
-      const uint4* cv = reinterpret_cast<const uint4*>(A.col + base);
-      double s = 0.0;
-      for (uint32_t j = tid; j < nvec; j += kPrThreads) {
-        const uint4 q = ld_stream_u4(cv + j);
-        const OffT e = base + 4 * (OffT)j;
-        if (e >= e0 && e < e1) s += to_d(__ldg(ccur + q.x));
-        if (e + 1 >= e0 && e + 1 < e1) s += to_d(__ldg(ccur + q.y));
-        if (e + 2 >= e0 && e + 2 < e1) s += to_d(__ldg(ccur + q.z));
-        if (e + 3 >= e0 && e + 3 < e1) s += to_d(__ldg(ccur + q.w));
-      }
-      double unused = 0.0;
-      cta_sum2(unused, s, s_red);
-      if (tid == 0) {
+      const uint32_t nch = (uint32_t)((re - rs + kLongChunk - 1) / kLongChunk);
+      const OffT e0 = rs + (OffT)c * kLongChunk;
+      const OffT e1 = min(e0 + (OffT)kLongChunk, re);
+      const double s = warp_range_sum(A.col, ccur, hub, nhub, e0, e1, lane, pol_arc, pol_c);
+      const uint32_t first = ti - c;
+      unsigned int last = 0;
+      if (lane == 0) {
         A.chunk_part[ti] = s;
         __threadfence();
-        const unsigned int old = atomicAdd(A.long_cnt + slot, 1u);
-        s_flag = (old == nch - 1);
+        last = (atomicAdd(A.long_cnt + first, 1u) == nch - 1) ? 1u : 0u;
       }
-      __syncthreads();
-      if (s_flag && tid == 0) {
+      last = __shfl_sync(0xffffffffu, last, 0);
+      if (last && lane == 0) {
         __threadfence();
         double tot = 0.0;
-        for (uint32_t k = 0; k < nch; ++k) tot += __ldcg(A.chunk_part + (ti - c + k));
+        for (uint32_t k = 0; k < nch; ++k) tot += __ldcg(A.chunk_part + (first + k));
         double rl1 = 0.0, rds = 0.0;
         pr_row_epilogue(A, row, tot, xcur, xnxt, cnxt, tele_u, sink, rl1, rds);
-        A.long_part[2 * slot] = rl1;
-        A.long_part[2 * slot + 1] = rds;
-        A.long_cnt[slot] = 0;
+        A.long_part[2 * (size_t)first] = rl1;
+        A.long_part[2 * (size_t)first + 1] = rds;
+        A.long_cnt[first] = 0;
       }
-      __syncthreads();
     }
+    t = nx;
+    ti = tn;
   }
-
-  // ---- publish this CTA's residual / dangling partials ---------------------
-  cta_sum2(l1, dsum, s_red);
-  if (tid == 0) {
-    A.cta_part[2 * blockIdx.x] = l1;
-    A.cta_part[2 * blockIdx.x + 1] = dsum;
-    __threadfence();
-    const unsigned int t = atomicAdd(&A.st->done_ctas, 1u);
-    s_flag = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (s_flag) {
-    __threadfence();
-    final_reduce(A.st, A.cta_part, gridDim.x, A.long_part, A.nlong, iter + 1, A.tol, true, s_red);
-  }
+  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol, true, s_red,
+              &s_flag);
 }
 
 // ---------------------------------------------------------------------------
-// Schedule: greedy packing of rows into blocks, long rows into chunks.
+// PageRank view: degree ranking, re-laid in-CSR, schedule
 // ---------------------------------------------------------------------------
+__global__ void k_rank_keys(const uint32_t* __restrict__ deg, uint32_t V, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ ids) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = deg[v];
+    key[v] = (d == kDeletedDegree) ? 0xFFFFFFFFu : 0xFFFFFFFEu - d;  // descending degree, deleted last
+    ids[v] = (uint32_t)v;
+  }
+}
+
+__global__ void k_rank_invert(const uint32_t* __restrict__ perm, uint32_t V, uint32_t* __restrict__ rank,
+                              const uint32_t* __restrict__ deg, uint32_t* __restrict__ pdeg,
+                              const uint64_t* __restrict__ in_off, unsigned long long* __restrict__ pcnt) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < V; p += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = perm[p];
+    rank[v] = (uint32_t)p;
+    pdeg[p] = deg[v];
+    pcnt[p] = in_off[v + 1] - in_off[v];
+  }
+}
+
+// Row p of the ranked in-CSR = row perm[p] of the in-CSR with every source
+// replaced by its rank; the order inside the row is kept.
+__global__ void k_rank_rows(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ rank, uint32_t V,
+                            const uint64_t* __restrict__ in_off, const uint32_t* __restrict__ in_col,
+                            const uint64_t* __restrict__ poff, uint32_t* __restrict__ pcol) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t p = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; p < V; p += nw) {
+    const uint32_t v = perm[p];
+    const uint64_t s = in_off[v], e = in_off[v + 1], d = poff[p];
+    for (uint64_t k = s + lane; k < e; k += 32) pcol[d + (k - s)] = rank[in_col[k]];
+  }
+}
+
+__global__ void k_permute_in(const double* __restrict__ src, const uint32_t* __restrict__ perm, uint32_t V,
+                             double* __restrict__ dst) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < V; p += (uint64_t)gridDim.x * blockDim.x)
+    dst[p] = src[perm[p]];
+}
+
+__global__ void k_permute_out(const double* __restrict__ src, const uint32_t* __restrict__ rank, uint32_t V,
+                              double* __restrict__ dst) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+    dst[v] = src[rank[v]];
+}
+
+__global__ void k_off_narrow(const uint64_t* __restrict__ a, uint32_t* __restrict__ b, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = (uint32_t)a[i];
+}
+
+static unsigned grid_1d(uint64_t n) {
+  uint64_t g = (n + 255) / 256;
+  const uint64_t cap = (uint64_t)sm_count() * 16;
+  if (g > cap) g = cap;
+  return (unsigned)std::max<uint64_t>(g, 1);
+}
+
 int ensure_pr_schedule(Graph* g, cudaStream_t s) {
   std::lock_guard<std::mutex> lk(g->mu);
-  if (g->pr.built) return ZOGCU_OK;
+  PrSchedule& P = g->pr;
+  if (P.built) return ZOGCU_OK;
   const uint32_t V = g->V;
+  if (V >= (1u << 30)) return fail(ZOGCU_ERR_TOO_LARGE, "PageRank schedule supports fewer than 2^30 nodes");
+  // ---- ranking by out-degree ---------------------------------------------
+  ZOGCU_TRY(P.rank.alloc((size_t)V * 4));
+  ZOGCU_TRY(P.perm.alloc((size_t)V * 4));
+  ZOGCU_TRY(P.deg.alloc((size_t)V * 4));
+  {
+    DevBuf key, key2, ids, tmp;
+    ZOGCU_TRY(key.alloc((size_t)V * 4, s));
+    ZOGCU_TRY(key2.alloc((size_t)V * 4, s));
+    ZOGCU_TRY(ids.alloc((size_t)V * 4, s));
+    k_rank_keys<<<grid_1d(V), 256, 0, s>>>(g->out_deg.as<uint32_t>(), V, key.as<uint32_t>(), ids.as<uint32_t>());
+    ZOGCU_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.as<uint32_t>(), key2.as<uint32_t>(),
+                                               ids.as<uint32_t>(), P.perm.as<uint32_t>(), (int64_t)V, 0, 32, s));
+    ZOGCU_TRY(tmp.alloc(tb, s));
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, key.as<uint32_t>(), key2.as<uint32_t>(),
+                                               ids.as<uint32_t>(), P.perm.as<uint32_t>(), (int64_t)V, 0, 32, s));
+  }
+  // ---- ranked in-CSR ---------------------------------------------------------
+  DevBuf cnt, poff64;
+  ZOGCU_TRY(cnt.alloc(((size_t)V + 1) * 8, s));
+  ZOGCU_TRY(poff64.alloc(((size_t)V + 1) * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, ((size_t)V + 1) * 8, s));
+  k_rank_invert<<<grid_1d(V), 256, 0, s>>>(P.perm.as<uint32_t>(), V, P.rank.as<uint32_t>(),
+                                           g->out_deg.as<uint32_t>(), P.deg.as<uint32_t>(),
+                                           g->in_off64.as<uint64_t>(), cnt.as<unsigned long long>());
+  ZOGCU_CUDA(cudaGetLastError());
+  {
+    size_t tb = 0;
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.as<unsigned long long>(),
+                                             poff64.as<unsigned long long>(), (int64_t)V + 1, s));
+    DevBuf tmp;
+    ZOGCU_TRY(tmp.alloc(tb, s));
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, cnt.as<unsigned long long>(),
+                                             poff64.as<unsigned long long>(), (int64_t)V + 1, s));
+  }
+  ZOGCU_TRY(P.col.alloc((g->E + 4) * 4));
+  ZOGCU_CUDA(cudaMemsetAsync(P.col.ptr, 0, (g->E + 4) * 4, s));
+  k_rank_rows<<<grid_1d((uint64_t)V * 32), 256, 0, s>>>(P.perm.as<uint32_t>(), P.rank.as<uint32_t>(), V,
+                                                         g->in_off64.as<uint64_t>(), g->in_col.as<uint32_t>(),
+                                                         poff64.as<uint64_t>(), P.col.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  if (g->offsets32) {
+    ZOGCU_TRY(P.off.alloc(((size_t)V + 1) * 4));
+    k_off_narrow<<<grid_1d(V + 1), 256, 0, s>>>(poff64.as<uint64_t>(), P.off.as<uint32_t>(), (uint64_t)V + 1);
+    ZOGCU_CUDA(cudaGetLastError());
+  } else {
+    ZOGCU_TRY(P.off.alloc(((size_t)V + 1) * 8));
+    ZOGCU_CUDA(cudaMemcpyAsync(P.off.ptr, poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToDevice, s));
+  }
+  // ---- schedule (host greedy pass over the ranked offsets) -------------------
   std::vector<uint64_t> off((size_t)V + 1);
-  ZOGCU_CUDA(cudaMemcpyAsync(off.data(), g->in_off64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(off.data(), poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   std::vector<PrTask> tasks;
-  tasks.reserve(g->E / kBlockNnz + V / kRowCap + 16);
-  uint32_t nlong = 0, maxch = 0;
+  std::vector<uint32_t> long_first;
+  tasks.reserve(g->E / (kWarpNnz / 2) + V / kWarpRows + 16);
   uint32_t r = 0;
   while (r < V) {
     uint64_t len = off[r + 1] - off[r];
-    if (len > (uint64_t)kBlockNnz) {
-      const uint32_t nch = (uint32_t)((len + kBlockNnz - 1) / kBlockNnz);
-      if (nch > 0xFFFFu) return fail(ZOGCU_ERR_TOO_LARGE, "row in-degree too large for the chunk schedule");
-      for (uint32_t c = 0; c < nch; ++c) tasks.push_back(PrTask{r, c, 1u | (nch << 16), nlong});
-      maxch = std::max(maxch, nch);
-      ++nlong;
+    if (len > (uint64_t)kWarpNnz) {
+      if (len <= (uint64_t)kLongChunk) {
+        tasks.push_back(PrTask{r, (kTaskRow << 30) | (r + 1)});
+      } else {
+        const uint64_t nch = (len + kLongChunk - 1) / kLongChunk;
+        if (nch > 0xFFFFu) return fail(ZOGCU_ERR_TOO_LARGE, "row in-degree too large for the chunk schedule");
+        long_first.push_back((uint32_t)tasks.size());
+        for (uint32_t c = 0; c < (uint32_t)nch; ++c) tasks.push_back(PrTask{r, (kTaskChunk << 30) | c});
+      }
       ++r;
       continue;
     }
     const uint32_t r0 = r;
     uint64_t nnz = 0;
-    while (r < V && (r - r0) < (uint32_t)kRowCap) {
+    while (r < V && (r - r0) < (uint32_t)kWarpRows) {
       len = off[r + 1] - off[r];
-      if (len > (uint64_t)kBlockNnz || nnz + len > (uint64_t)kBlockNnz) break;
+      if (len > (uint64_t)kWarpNnz || nnz + len > (uint64_t)kWarpNnz) break;
       nnz += len;
       ++r;
     }
-    tasks.push_back(PrTask{r0, r, 0u, 0u});
+    tasks.push_back(PrTask{r0, (kTaskBlock << 30) | r});
   }
-  g->pr.num_tasks = (uint32_t)tasks.size();
-  g->pr.num_long = nlong;
-  g->pr.max_chunks = maxch;
-  if (!tasks.empty()) {
-    ZOGCU_TRY(g->pr.tasks.alloc(tasks.size() * sizeof(PrTask)));
-    ZOGCU_CUDA(cudaMemcpyAsync(g->pr.tasks.ptr, tasks.data(), tasks.size() * sizeof(PrTask),
-                               cudaMemcpyHostToDevice, s));
-    ZOGCU_CUDA(cudaStreamSynchronize(s));
-  }
-  g->pr.built = true;
+  if (tasks.size() >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "too many PageRank work items");
+  P.num_tasks = (uint32_t)tasks.size();
+  P.num_long = (uint32_t)long_first.size();
+  ZOGCU_TRY(P.tasks.alloc(std::max<size_t>(tasks.size(), 1) * sizeof(PrTask)));
+  ZOGCU_TRY(P.long_first.alloc(std::max<size_t>(long_first.size(), 1) * 4));
+  if (!tasks.empty())
+    ZOGCU_CUDA(cudaMemcpyAsync(P.tasks.ptr, tasks.data(), tasks.size() * sizeof(PrTask), cudaMemcpyHostToDevice, s));
+  if (!long_first.empty())
+    ZOGCU_CUDA(cudaMemcpyAsync(P.long_first.ptr, long_first.data(), long_first.size() * 4, cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  P.built = true;
   return ZOGCU_OK;
 }
 
 template <typename OffT, typename CT>
-static int pr_grid() {
-  static int grid = 0;
-  if (grid == 0) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_iter_kernel<OffT, CT>, kPrThreads, 0);
-    if (per_sm <= 0) per_sm = 1;
-    grid = per_sm * sm_count();
+static int pr_prepare_kernel() {
+  static bool done = false;
+  if (!done) {
+    ZOGCU_CUDA(cudaFuncSetAttribute(pr_iter_kernel<OffT, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kHubBytes));
+    done = true;
   }
-  return grid;
+  return ZOGCU_OK;
 }
 
 template <typename OffT>
-static int run_pagerank_fp64(Graph* g, const OffT* off, double damping, uint64_t max_iter, double tol,
-                             const zogcu_pr_opts* o, double* out, zogcu_stats* stats, cudaStream_t s) {
+static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double tol, const zogcu_pr_opts* o,
+                             double* out, zogcu_stats* stats, cudaStream_t s) {
+  const PrSchedule& P = g->pr;
   const uint32_t V = g->V;
-  const uint32_t ntasks = g->pr.num_tasks, nlong = g->pr.num_long;
-  int grid = pr_grid<OffT, double>();
-  if (ntasks > 0 && (uint32_t)grid > ntasks) grid = (int)ntasks;
+  const uint32_t ntasks = P.num_tasks, nlong = P.num_long;
+  ZOGCU_TRY((pr_prepare_kernel<OffT, double>()));
+  int grid = sm_count();
+  const uint32_t need = (ntasks + kPrWarps - 1) / kPrWarps;
+  if (need > 0 && (uint32_t)grid > need) grid = (int)need;
   if (grid < 1) grid = 1;
+  const uint32_t hub = std::min<uint32_t>((uint32_t)(kHubBytes / sizeof(double)), V & ~1u);
   const bool dev_ptrs = o && o->device_pointers;
 
-  DevBuf x0, x1, c0, c1, part, chunk, lcnt, lpart, stb, tele;
+  DevBuf x0, x1, c0, c1, part, chunk, lcnt, lpart, stb, tele, tmp;
   ZOGCU_TRY(x0.alloc((size_t)V * 8, s));
   ZOGCU_TRY(x1.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(c0.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(c1.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(part.alloc((size_t)grid * 16, s));
+  ZOGCU_TRY(c0.alloc((size_t)V * 8 + 16, s));
+  ZOGCU_TRY(c1.alloc((size_t)V * 8 + 16, s));
+  const unsigned init_grid = std::min(grid_1d(V), 148u * 4);
+  ZOGCU_TRY(part.alloc((size_t)std::max<unsigned>((unsigned)grid, init_grid) * 16, s));
   ZOGCU_TRY(chunk.alloc((size_t)std::max<uint32_t>(ntasks, 1) * 8, s));
-  ZOGCU_TRY(lcnt.alloc((size_t)std::max<uint32_t>(nlong, 1) * 4, s));
-  ZOGCU_TRY(lpart.alloc((size_t)std::max<uint32_t>(nlong, 1) * 16, s));
+  ZOGCU_TRY(lcnt.alloc((size_t)std::max<uint32_t>(ntasks, 1) * 4, s));
+  ZOGCU_TRY(lpart.alloc((size_t)std::max<uint32_t>(ntasks, 1) * 16, s));
   ZOGCU_TRY(stb.alloc(sizeof(PrState), s));
   ZOGCU_CUDA(cudaMemsetAsync(lcnt.ptr, 0, lcnt.bytes, s));
-  ZOGCU_CUDA(cudaMemsetAsync(lpart.ptr, 0, lpart.bytes, s));
   ZOGCU_CUDA(cudaMemsetAsync(stb.ptr, 0, sizeof(PrState), s));
   ZOGCU_CUDA(cudaMemsetAsync(c0.ptr, 0, c0.bytes, s));
   ZOGCU_CUDA(cudaMemsetAsync(c1.ptr, 0, c1.bytes, s));
   int given = 0;
-  if (o && o->x0) {
-    ZOGCU_CUDA(cudaMemcpyAsync(x0.ptr, o->x0, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  if (o && o->x0) {  // caller order -> ranked order
+    ZOGCU_TRY(tmp.alloc((size_t)V * 8, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(tmp.ptr, o->x0, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    k_permute_in<<<grid_1d(V), 256, 0, s>>>(tmp.as<double>(), P.perm.as<uint32_t>(), V, x0.as<double>());
+    ZOGCU_CUDA(cudaGetLastError());
     given = 1;
   }
   const double* tele_ptr = nullptr;
   if (o && o->teleport) {
-    if (dev_ptrs) {
-      tele_ptr = o->teleport;
-    } else {
-      ZOGCU_TRY(tele.alloc((size_t)V * 8, s));
-      ZOGCU_CUDA(cudaMemcpyAsync(tele.ptr, o->teleport, (size_t)V * 8, cudaMemcpyHostToDevice, s));
-      tele_ptr = tele.as<double>();
-    }
+    ZOGCU_TRY(tele.alloc((size_t)V * 8, s));
+    if (!tmp.ptr) ZOGCU_TRY(tmp.alloc((size_t)V * 8, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(tmp.ptr, o->teleport, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    k_permute_in<<<grid_1d(V), 256, 0, s>>>(tmp.as<double>(), P.perm.as<uint32_t>(), V, tele.as<double>());
+    ZOGCU_CUDA(cudaGetLastError());
+    tele_ptr = tele.as<double>();
   }
 
   PrArgs<OffT, double> A;
-  A.off = off;
-  A.col = g->in_col.as<uint32_t>();
-  A.deg = g->out_deg.as<uint32_t>();
-  A.tasks = g->pr.tasks.as<PrTask>();
+  A.off = P.off.as<OffT>();
+  A.col = P.col.as<uint32_t>();
+  A.deg = P.deg.as<uint32_t>();
+  A.tasks = P.tasks.as<PrTask>();
+  A.long_first = P.long_first.as<uint32_t>();
   A.ntasks = ntasks;
   A.nlong = nlong;
+  A.hub = hub;
   A.x0 = x0.as<double>();
   A.x1 = x1.as<double>();
   A.c0 = c0.as<double>();
@@ -438,13 +661,14 @@ static int run_pagerank_fp64(Graph* g, const OffT* off, double damping, uint64_t
   A.tol = tol;
   A.max_iter = max_iter;
 
+  const size_t dyn = (size_t)hub * sizeof(double);
   EventTimer tm;
   ZOGCU_TRY(tm.start(s));
-  pr_init_kernel<OffT, double><<<grid, kPrThreads, 0, s>>>(A, V, given);
+  pr_init_kernel<OffT, double><<<init_grid, 256, 0, s>>>(A, V, given);
   ZOGCU_CUDA(cudaGetLastError());
   uint64_t launches = 1;
   for (uint64_t k = 0; k < max_iter; ++k) {
-    pr_iter_kernel<OffT, double><<<grid, kPrThreads, 0, s>>>(A);
+    pr_iter_kernel<OffT, double><<<grid, kPrThreads, dyn, s>>>(A);
     ++launches;
   }
   ZOGCU_CUDA(cudaGetLastError());
@@ -453,7 +677,11 @@ static int run_pagerank_fp64(Graph* g, const OffT* off, double damping, uint64_t
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   const double* result = (hs.iter & 1ull) ? A.x1 : A.x0;
-  ZOGCU_CUDA(cudaMemcpyAsync(out, result, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  double* unperm = (hs.iter & 1ull) ? A.x0 : A.x1;  // the other buffer is free now
+  k_permute_out<<<grid_1d(V), 256, 0, s>>>(result, P.rank.as<uint32_t>(), V, unperm);
+  ZOGCU_CUDA(cudaGetLastError());
+  ++launches;
+  ZOGCU_CUDA(cudaMemcpyAsync(out, unperm, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   if (stats) {
     stats->iterations = hs.iter;
@@ -503,10 +731,8 @@ int zogcu_pagerank_ex(zogcu_graph* G, double damping, uint64_t max_iterations, d
   ZOGCU_TRY(sg.init(opts ? opts->stream : nullptr));
   ZOGCU_TRY(ensure_pr_schedule(g, sg.s));
   if (g->offsets32)
-    return run_pagerank_fp64<uint32_t>(g, g->in_off32.as<uint32_t>(), damping, max_iterations, tolerance, opts,
-                                       out_scores, stats, sg.s);
-  return run_pagerank_fp64<uint64_t>(g, g->in_off64.as<uint64_t>(), damping, max_iterations, tolerance, opts,
-                                     out_scores, stats, sg.s);
+    return run_pagerank_fp64<uint32_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
+  return run_pagerank_fp64<uint64_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
 }
 
 int zogcu_pagerank(zogcu_graph* G, double damping, uint64_t max_iterations, double tolerance, double* out_scores,
