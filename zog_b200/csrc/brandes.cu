@@ -9,20 +9,25 @@
 // over predecessors and adds delta[v] to the score of every v != s (:769-787).
 //
 // B200 design: a batch of 64 sources advances level by level in lock-step.
-// Per vertex the batch keeps 64-bit masks (visited, frontier of the current
-// level) and, per (vertex, source) pair, dist (u32), sigma (u64) and
-// q = (1+delta)/sigma (f64) in vertex-major rows of 64, so one warp owns one
-// vertex and each lane owns sources lane and lane+32.
+// Per vertex the batch keeps 64-bit masks -- visited, and the frontier of
+// every level (kept for the backward sweep) -- and, per (vertex, source) pair,
+// dist (u32), sigma (u64) and q = (1+delta)/sigma (f64) in vertex-major rows
+// of 64, so one warp owns one vertex and each lane owns sources lane and
+// lane+32.
 //   forward (pull): a vertex w with unvisited sources scans its in-neighbours
-//     32 at a time (one coalesced index load, one mask gather per lane), keeps
-//     only neighbours whose frontier mask meets w's unvisited mask, and lanes
-//     add the matching sigma[v][b] -- no atomics, deterministic, and the sums
-//     are exact integers (wrapping modulo 2^64 like the reference's usize);
+//     32 at a time (one coalesced index load, one frontier-mask gather per
+//     lane), keeps only neighbours whose mask meets w's unvisited mask, and the
+//     lanes add the matching sigma[v][b], four neighbour rows in flight at a
+//     time -- no atomics, deterministic, exact integer sums that wrap modulo
+//     2^64 like the reference's usize;
 //   backward (pull over successors): at level l a vertex v with sources at
-//     depth l gathers q[w][b] of successors w at depth l+1 (mask test first),
-//     so delta[v][b] = sigma[v][b] * sum q[w][b] -- the reference's
-//     sum of sigma_v/sigma_w * (1+delta_w), reassociated -- and the warp adds
-//     sum_b delta[v][b] to BC[v] (only v's own warp touches BC[v]).
+//     depth l (its level-l mask) gathers q[w][b] of successors w whose level-l+1
+//     mask has bit b, so delta[v][b] = sigma[v][b] * sum q[w][b] -- the
+//     reference's sum of sigma_v/sigma_w * (1+delta_w), reassociated -- and
+//     the warp adds sum_b delta[v][b] to BC[v] (only v's warp touches BC[v]);
+//   level loop on the device: forward launches are enqueued in chunks and a
+//     launch returns at once when the previous level discovered nothing, so
+//     the host synchronises once per chunk of levels, not once per level.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -33,9 +38,32 @@ namespace zogcu {
 
 constexpr int kBcBatch = 64;
 constexpr int kBcThreads = 256;
+constexpr int kLevelChunk = 8;     // forward levels enqueued between host checks
+constexpr int kMaxStoredLevels = 64;  // frontier masks kept for the backward sweep
+constexpr int kOverflowFlag = kMaxStoredLevels + 8;
 
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
   return __shfl_sync(0xffffffffu, v, src);
+}
+
+// One neighbour of the inner loops: its id and the mask of the batch's sources
+// for which it matters (0 = none).
+struct Nb {
+  uint32_t v;
+  unsigned long long m;
+};
+
+// Pops up to four set lanes of `bal` and broadcasts their (v, m) pairs.
+__device__ __forceinline__ void pop4(unsigned& bal, uint32_t v, unsigned long long m, Nb (&out)[4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int k = bal ? __ffs(bal) - 1 : 0;
+    const bool any = bal != 0;
+    bal &= bal - 1;
+    out[i].v = __shfl_sync(0xffffffffu, v, k);
+    const unsigned long long mk = shfl_u64(m, k);
+    out[i].m = any ? mk : 0ull;
+  }
 }
 
 template <typename OffT>
@@ -44,9 +72,12 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
     const unsigned long long* __restrict__ front_cur, unsigned long long* __restrict__ front_nxt,
     unsigned long long* __restrict__ visited, unsigned long long* __restrict__ sigma, uint32_t* __restrict__ dist,
     unsigned long long full, uint32_t level, unsigned int* __restrict__ flags) {
+  // flags[l % kMaxStoredLevels] = 1 when level l discovered a vertex;
+  // flags[kOverflowFlag] = some path count wrapped
+  if (level > 0 && *(volatile unsigned int*)(flags + (level - 1) % kMaxStoredLevels) == 0u) return;
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = (uint64_t)gridDim.x * (kBcThreads / 32);
-  bool any_ovf = false;
+  bool any_ovf = false, any_new = false;
   for (uint64_t w = blockIdx.x * (uint64_t)(kBcThreads / 32) + (threadIdx.x >> 5); w < V; w += nwarps) {
     const unsigned long long vis = visited[w];
     const unsigned long long cand = full & ~vis;
@@ -65,23 +96,25 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
         }
         unsigned bal = __ballot_sync(0xffffffffu, m != 0);
         while (bal) {
-          const int k = __ffs(bal) - 1;
-          bal &= bal - 1;
-          const uint32_t vk = __shfl_sync(0xffffffffu, v, k);
-          const unsigned long long mk = shfl_u64(m, k);
-          if ((mk >> lane) & 1ull) {
-            const unsigned long long s = sigma[(uint64_t)vk * kBcBatch + lane];
-            const unsigned long long n = acc0 + s;
+          Nb nb[4];
+          pop4(bal, v, m, nb);
+          unsigned long long s0[4], s1[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const uint64_t row = (uint64_t)nb[i].v * kBcBatch;
+            s0[i] = ((nb[i].m >> lane) & 1ull) ? sigma[row + lane] : 0ull;
+            s1[i] = ((nb[i].m >> (lane + 32)) & 1ull) ? sigma[row + lane + 32] : 0ull;
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            got0 |= ((nb[i].m >> lane) & 1ull) != 0;
+            got1 |= ((nb[i].m >> (lane + 32)) & 1ull) != 0;
+            unsigned long long n = acc0 + s0[i];
             any_ovf |= n < acc0;
             acc0 = n;
-            got0 = true;
-          }
-          if ((mk >> (lane + 32)) & 1ull) {
-            const unsigned long long s = sigma[(uint64_t)vk * kBcBatch + lane + 32];
-            const unsigned long long n = acc1 + s;
+            n = acc1 + s1[i];
             any_ovf |= n < acc1;
             acc1 = n;
-            got1 = true;
           }
         }
       }
@@ -100,28 +133,42 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
       front_nxt[w] = newmask;
       if (newmask) {
         visited[w] = vis | newmask;
-        flags[0] = 1u;
+        any_new = true;
       }
     }
   }
-  if (__any_sync(0xffffffffu, any_ovf) && lane == 0) flags[1] = 1u;
+  if (__any_sync(0xffffffffu, any_new) && lane == 0) flags[level % kMaxStoredLevels] = 1u;
+  if (__any_sync(0xffffffffu, any_ovf) && lane == 0) flags[kOverflowFlag] = 1u;
+}
+
+// Level-l mask of v: stored frontier masks when the BFS was shallow enough,
+// else recomputed from dist.
+__device__ __forceinline__ unsigned long long level_mask(const unsigned long long* __restrict__ mask_l,
+                                                         const uint32_t* __restrict__ dist, uint64_t v,
+                                                         uint32_t level, int lane) {
+  if (mask_l) return mask_l[v];
+  const bool a0 = dist[v * kBcBatch + lane] == level;
+  const bool a1 = dist[v * kBcBatch + lane + 32] == level;
+  return (unsigned long long)__ballot_sync(0xffffffffu, a0) | ((unsigned long long)__ballot_sync(0xffffffffu, a1) << 32);
 }
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBcThreads) bc_backward_kernel(
     uint32_t V, const OffT* __restrict__ off, const uint32_t* __restrict__ col,
-    const unsigned long long* __restrict__ mask_nxt, unsigned long long* __restrict__ mask_cur,
-    const uint32_t* __restrict__ dist, const unsigned long long* __restrict__ sigma, double* __restrict__ q,
-    double* __restrict__ bc, uint32_t level, int last_level) {
+    const unsigned long long* __restrict__ mask_l, const unsigned long long* __restrict__ mask_next,
+    unsigned long long* __restrict__ mask_out, const uint32_t* __restrict__ dist,
+    const unsigned long long* __restrict__ sigma, double* __restrict__ q, double* __restrict__ bc, uint32_t level,
+    int last_level) {
+  // mask_l / mask_next: stored masks of levels l and l+1 (null: derive level l
+  // from dist, and read level l+1 from mask_next written by the previous launch
+  // into its mask_out).
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = (uint64_t)gridDim.x * (kBcThreads / 32);
   for (uint64_t v = blockIdx.x * (uint64_t)(kBcThreads / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
-    const bool a0 = dist[v * kBcBatch + lane] == level;
-    const bool a1 = dist[v * kBcBatch + lane + 32] == level;
-    const unsigned long long act =
-        (unsigned long long)__ballot_sync(0xffffffffu, a0) | ((unsigned long long)__ballot_sync(0xffffffffu, a1) << 32);
-    if (lane == 0) mask_cur[v] = act;
+    const unsigned long long act = mask_l ? __ldg(mask_l + v) : level_mask(nullptr, dist, v, level, lane);
+    if (mask_out && lane == 0) mask_out[v] = act;
     if (!act) continue;
+    const bool a0 = (act >> lane) & 1ull, a1 = (act >> (lane + 32)) & 1ull;
     double acc0 = 0.0, acc1 = 0.0;
     if (!last_level) {
       const OffT b = __ldg(off + v), e = __ldg(off + v + 1);
@@ -131,16 +178,24 @@ __global__ void __launch_bounds__(kBcThreads) bc_backward_kernel(
         unsigned long long g = 0;
         if (j < e) {
           w = __ldg(col + j);
-          g = __ldg(mask_nxt + w) & act;
+          g = __ldg(mask_next + w) & act;
         }
         unsigned bal = __ballot_sync(0xffffffffu, g != 0);
         while (bal) {
-          const int k = __ffs(bal) - 1;
-          bal &= bal - 1;
-          const uint32_t wk = __shfl_sync(0xffffffffu, w, k);
-          const unsigned long long gk = shfl_u64(g, k);
-          if ((gk >> lane) & 1ull) acc0 += q[(uint64_t)wk * kBcBatch + lane];
-          if ((gk >> (lane + 32)) & 1ull) acc1 += q[(uint64_t)wk * kBcBatch + lane + 32];
+          Nb nb[4];
+          pop4(bal, w, g, nb);
+          double t0[4], t1[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const uint64_t row = (uint64_t)nb[i].v * kBcBatch;
+            t0[i] = ((nb[i].m >> lane) & 1ull) ? q[row + lane] : 0.0;
+            t1[i] = ((nb[i].m >> (lane + 32)) & 1ull) ? q[row + lane + 32] : 0.0;
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            acc0 += t0[i];
+            acc1 += t1[i];
+          }
         }
       }
     }
@@ -184,23 +239,37 @@ static int bc_grid(uint32_t V) {
   return (int)blocks;
 }
 
+constexpr int kFlagWords = kMaxStoredLevels + 16;
+
 struct BcWork {
-  DevBuf visited, fa, fb, sigma, dist, q, flags, src;
+  // masks: kMaxStoredLevels + 1 frontier arrays (level l at masks + l*V); when
+  // the BFS is deeper, levels wrap around and the backward sweep derives its
+  // masks from dist instead.
+  DevBuf visited, masks, mbuf_a, mbuf_b, sigma, dist, q, flags, src;
   int alloc(uint32_t V, uint64_t ns, cudaStream_t s, bool need_q) {
     const size_t Vs = std::max<uint32_t>(V, 1);
     ZOGCU_TRY(visited.alloc(Vs * 8, s));
-    ZOGCU_TRY(fa.alloc(Vs * 8, s));
-    ZOGCU_TRY(fb.alloc(Vs * 8, s));
+    ZOGCU_TRY(masks.alloc(Vs * 8 * (kMaxStoredLevels + 1), s));
     ZOGCU_TRY(sigma.alloc(Vs * 8 * kBcBatch, s));
     ZOGCU_TRY(dist.alloc(Vs * 4 * kBcBatch, s));
-    if (need_q) ZOGCU_TRY(q.alloc(Vs * 8 * kBcBatch, s));
-    ZOGCU_TRY(flags.alloc(16, s));
+    if (need_q) {
+      ZOGCU_TRY(q.alloc(Vs * 8 * kBcBatch, s));
+      ZOGCU_TRY(mbuf_a.alloc(Vs * 8, s));
+      ZOGCU_TRY(mbuf_b.alloc(Vs * 8, s));
+    }
+    ZOGCU_TRY(flags.alloc(kFlagWords * 4, s));
     ZOGCU_TRY(src.alloc(std::max<uint64_t>(ns, 1) * 4, s));
     return ZOGCU_OK;
+  }
+  unsigned long long* level(uint32_t l, uint32_t V) const {
+    return masks.as<unsigned long long>() + (size_t)(l % (kMaxStoredLevels + 1)) * std::max<uint32_t>(V, 1);
   }
 };
 
 // Forward phase of one batch; returns the deepest level reached in *depth.
+// Levels are enqueued kLevelChunk at a time (never across a multiple of
+// kMaxStoredLevels, where the per-level flag words are reused) and the host
+// reads the flags once per chunk.
 template <typename OffT>
 static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint64_t first, int nb,
                             cudaStream_t s, uint32_t* depth, bool* overflow, uint64_t* launches,
@@ -209,34 +278,40 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
   const int grid = bc_grid(V);
   const unsigned long long full = nb == 64 ? ~0ull : ((1ull << nb) - 1);
   ZOGCU_CUDA(cudaMemsetAsync(W.visited.ptr, 0, (size_t)V * 8, s));
-  ZOGCU_CUDA(cudaMemsetAsync(W.fa.ptr, 0, (size_t)V * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.level(0, V), 0, (size_t)V * 8, s));
   ZOGCU_CUDA(cudaMemsetAsync(W.dist.ptr, 0xFF, (size_t)V * 4 * kBcBatch, s));
-  ZOGCU_CUDA(cudaMemsetAsync(W.flags.ptr, 0, 16, s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.flags.ptr, 0, kFlagWords * 4, s));
   bc_seed_kernel<<<1, 64, 0, s>>>(W.src.as<uint32_t>() + first, nb, W.visited.as<unsigned long long>(),
-                                  W.fa.as<unsigned long long>(), W.sigma.as<unsigned long long>(),
-                                  W.dist.as<uint32_t>());
+                                  W.level(0, V), W.sigma.as<unsigned long long>(), W.dist.as<uint32_t>());
   ZOGCU_CUDA(cudaGetLastError());
   *launches += 1;
-  unsigned long long* cur = W.fa.as<unsigned long long>();
-  unsigned long long* nxt = W.fb.as<unsigned long long>();
   uint32_t level = 0;
   for (;;) {
-    ZOGCU_CUDA(cudaMemsetAsync(W.flags.ptr, 0, 4, s));
-    bc_forward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(V, in_off, g->in_col.as<uint32_t>(), cur, nxt,
-                                                        W.visited.as<unsigned long long>(),
-                                                        W.sigma.as<unsigned long long>(), W.dist.as<uint32_t>(),
-                                                        full, level, W.flags.as<unsigned int>());
-    ZOGCU_CUDA(cudaGetLastError());
-    *launches += 1;
-    ZOGCU_CUDA(cudaMemcpyAsync(h_flags, W.flags.ptr, 8, cudaMemcpyDeviceToHost, s));
+    const uint32_t lo = level;
+    // flag words of levels lo-64 .. lo-2 are all set; clear them for reuse
+    // (the word of level lo-1, which level lo checks, stays set)
+    if (lo > 0 && lo % kMaxStoredLevels == 0)
+      ZOGCU_CUDA(cudaMemsetAsync(W.flags.ptr, 0, (kMaxStoredLevels - 1) * 4, s));
+    const uint32_t hi = std::min<uint32_t>(lo + kLevelChunk, (lo / kMaxStoredLevels + 1) * kMaxStoredLevels);
+    for (uint32_t l = lo; l < hi; ++l) {
+      bc_forward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(V, in_off, g->in_col.as<uint32_t>(), W.level(l, V),
+                                                          W.level(l + 1, V), W.visited.as<unsigned long long>(),
+                                                          W.sigma.as<unsigned long long>(), W.dist.as<uint32_t>(),
+                                                          full, l, W.flags.as<unsigned int>());
+      ZOGCU_CUDA(cudaGetLastError());
+      *launches += 1;
+    }
+    level = hi;
+    ZOGCU_CUDA(cudaMemcpyAsync(h_flags, W.flags.ptr, kFlagWords * 4, cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
-    if (h_flags[1]) *overflow = true;
-    if (!h_flags[0]) break;
-    ++level;
-    std::swap(cur, nxt);
+    if (h_flags[kOverflowFlag]) *overflow = true;
+    for (uint32_t l = lo; l < hi; ++l) {
+      if (!h_flags[l % kMaxStoredLevels]) {  // level l found nothing: depth l
+        *depth = l;
+        return ZOGCU_OK;
+      }
+    }
   }
-  *depth = level;
-  return ZOGCU_OK;
 }
 
 template <typename OffT>
@@ -248,7 +323,7 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   ZOGCU_TRY(W.alloc(V, ns, s, true));
   if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W.src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, s));
   unsigned int* h_flags = nullptr;
-  ZOGCU_CUDA(cudaMallocHost(&h_flags, 16));
+  ZOGCU_CUDA(cudaMallocHost(&h_flags, kFlagWords * 4));
   struct HostFree {
     unsigned int* p;
     ~HostFree() { cudaFreeHost(p); }
@@ -263,16 +338,23 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
     ZOGCU_TRY(bc_forward_batch<OffT>(g, in_off, W, first, nb, s, &depth, &overflow, &launches, h_flags));
     max_depth = std::max(max_depth, depth);
     // backward: levels depth .. 1 (the sources sit at level 0 and are excluded)
-    unsigned long long* mnxt = W.fa.as<unsigned long long>();
-    unsigned long long* mcur = W.fb.as<unsigned long long>();
-    ZOGCU_CUDA(cudaMemsetAsync(mnxt, 0, (size_t)V * 8, s));
+    const bool stored = depth < (uint32_t)kMaxStoredLevels;
+    unsigned long long* mnxt = W.mbuf_a.as<unsigned long long>();
+    unsigned long long* mcur = W.mbuf_b.as<unsigned long long>();
+    if (!stored) ZOGCU_CUDA(cudaMemsetAsync(mnxt, 0, (size_t)V * 8, s));
     for (uint32_t l = depth; l >= 1; --l) {
-      bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(V, out_off, g->out_col.as<uint32_t>(), mnxt, mcur,
-                                                           W.dist.as<uint32_t>(), W.sigma.as<unsigned long long>(),
-                                                           W.q.as<double>(), d_bc, l, l == depth ? 1 : 0);
+      if (stored) {
+        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(
+            V, out_off, g->out_col.as<uint32_t>(), W.level(l, V), W.level(l + 1, V), nullptr,
+            W.dist.as<uint32_t>(), W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0);
+      } else {
+        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(
+            V, out_off, g->out_col.as<uint32_t>(), nullptr, mnxt, mcur, W.dist.as<uint32_t>(),
+            W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0);
+        std::swap(mnxt, mcur);
+      }
       ZOGCU_CUDA(cudaGetLastError());
       ++launches;
-      std::swap(mnxt, mcur);
     }
   }
   if (stats) {
@@ -366,7 +448,7 @@ int zogcu_bfs_sigma(zogcu_graph* G, const uint32_t* sources, uint64_t num_source
   ZOGCU_TRY(W.alloc(V, num_sources, sg.s, false));
   if (num_sources) ZOGCU_CUDA(cudaMemcpyAsync(W.src.ptr, sources, num_sources * 4, cudaMemcpyHostToDevice, sg.s));
   unsigned int* h_flags = nullptr;
-  ZOGCU_CUDA(cudaMallocHost(&h_flags, 16));
+  ZOGCU_CUDA(cudaMallocHost(&h_flags, kFlagWords * 4));
   std::vector<uint32_t> hd((size_t)V * kBcBatch);
   std::vector<unsigned long long> hs((size_t)V * kBcBatch);
   bool ovf = false;

@@ -137,27 +137,27 @@ __device__ __forceinline__ T warp_sum(T v) {
 // Epilogue of one row: the reference's update (centrality.zig:943) evaluated
 // with explicit round-to-nearest operations (no FMA contraction), then the
 // residual / dangling bookkeeping and the next contribution c' = x'/deg.
-template <typename OffT, typename CT>
-__device__ __forceinline__ void pr_row_epilogue(const PrArgs<OffT, CT>& A, uint32_t v, double rank_sum,
-                                                const double* __restrict__ xcur, double* __restrict__ xnxt,
-                                                CT* __restrict__ cnxt, double tele_u, double sink, double& l1,
-                                                double& dsum) {
-  const uint32_t deg = __ldg(A.deg + v);
+// `deg`, `xo` and `tp` (teleport, when personalised) were loaded earlier.
+template <typename CT>
+__device__ __forceinline__ void pr_row_epilogue(uint32_t v, double rank_sum, uint32_t deg, double xo, double tp,
+                                                bool personalised, double damping, double n_f,
+                                                double* __restrict__ xnxt, CT* __restrict__ cnxt, double tele_u,
+                                                double sink, double& l1, double& dsum) {
   if (deg == kDeletedDegree) return;
-  const double tele = A.teleport ? __dmul_rn(1.0 - A.damping, __ldg(A.teleport + v)) : tele_u;
-  const double xn = __dadd_rn(tele, __dmul_rn(A.damping, __dadd_rn(sink, rank_sum)));
-  const double xo = __ldg(xcur + v);
+  const double tele = personalised ? __dmul_rn(1.0 - damping, tp) : tele_u;
+  const double xn = __dadd_rn(tele, __dmul_rn(damping, __dadd_rn(sink, rank_sum)));
   l1 += fabs(xn - xo);
   xnxt[v] = xn;
   if (deg == 0) {
-    dsum += __ddiv_rn(xn, A.n_f);
+    dsum += __ddiv_rn(xn, n_f);
   } else {
     cnxt[v] = (CT)__ddiv_rn(xn, (double)deg);
   }
 }
 
 // Sum of c[col[e]] over e in [e0, e1) by one warp (lane partials, then a fixed
-// shuffle tree), two 16-byte index vectors per lane per step.
+// shuffle tree).  Index vectors for the next step are loaded before the
+// gathers of the current one, so two round trips overlap.
 template <typename OffT, typename CT>
 __device__ __forceinline__ double warp_range_sum(const uint32_t* __restrict__ col, const CT* __restrict__ c,
                                                  const CT* __restrict__ hub, uint32_t nhub, OffT e0, OffT e1,
@@ -166,11 +166,15 @@ __device__ __forceinline__ double warp_range_sum(const uint32_t* __restrict__ co
   const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
   const uint4* cv = reinterpret_cast<const uint4*>(col + base);
   double s = 0.0;
-  for (uint32_t j = lane; j < nvec; j += 64) {
-    const uint4 q0 = ld_arcs(cv + j, pol_arc);
-    uint4 q1 = make_uint4(0, 0, 0, 0);
+  uint32_t j = lane;
+  uint4 q0 = make_uint4(0, 0, 0, 0), q1 = make_uint4(0, 0, 0, 0);
+  if (j < nvec) q0 = ld_arcs(cv + j, pol_arc);
+  if (j + 32 < nvec) q1 = ld_arcs(cv + j + 32, pol_arc);
+  for (; j < nvec; j += 64) {
+    uint4 n0 = make_uint4(0, 0, 0, 0), n1 = make_uint4(0, 0, 0, 0);
+    if (j + 64 < nvec) n0 = ld_arcs(cv + j + 64, pol_arc);
+    if (j + 96 < nvec) n1 = ld_arcs(cv + j + 96, pol_arc);
     const bool two = j + 32 < nvec;
-    if (two) q1 = ld_arcs(cv + j + 32, pol_arc);
     const OffT ea = base + 4 * (OffT)j, eb = ea + 128;
     double v[8];
     v[0] = (ea >= e0 && ea < e1) ? gather(q0.x, hub, nhub, c, pol_c) : 0.0;
@@ -182,6 +186,8 @@ __device__ __forceinline__ double warp_range_sum(const uint32_t* __restrict__ co
     v[6] = (two && eb + 2 < e1) ? gather(q1.z, hub, nhub, c, pol_c) : 0.0;
     v[7] = (two && eb + 3 < e1) ? gather(q1.w, hub, nhub, c, pol_c) : 0.0;
     s += ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+    q0 = n0;
+    q1 = n1;
   }
   return warp_sum(s);
 }
@@ -302,6 +308,8 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
   const CT* __restrict__ ccur = par ? A.c1 : A.c0;
   CT* __restrict__ cnxt = par ? A.c0 : A.c1;
   const double tele_u = (1.0 - A.damping) / A.n_f;
+  const bool personalised = A.teleport != nullptr;
+  const double damping = A.damping, n_f = A.n_f;
 
   // ---- stage the hot prefix of c in shared memory --------------------------
   CT* hub = reinterpret_cast<CT*>(s_dyn);
@@ -320,37 +328,69 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
   double* sv = s_val[warp];
   double l1 = 0.0, dsum = 0.0;
 
+  // Software pipeline over this warp's work items: descriptors are loaded two
+  // items ahead and their arc ranges one item ahead, so a block needs two
+  // dependent round trips (index vectors with row data, then gathers).
   const uint32_t nwarps = gridDim.x * kPrWarps;
+  const PrTask none{0, 0};
+  auto range_of = [&](const PrTask& tk, OffT& lo, OffT& hi) {
+    const uint32_t kind = tk.b >> 30;
+    const uint32_t end = (kind == kTaskBlock) ? (tk.b & 0x3FFFFFFFu) : tk.a + 1;
+    lo = __ldg(A.off + tk.a);
+    hi = __ldg(A.off + end);
+  };
   uint32_t ti = blockIdx.x * kPrWarps + warp;
-  PrTask t = ti < A.ntasks ? A.tasks[ti] : PrTask{0, 0};
+  PrTask t = ti < A.ntasks ? A.tasks[ti] : none;
+  PrTask t1 = ti + nwarps < A.ntasks ? A.tasks[ti + nwarps] : none;
+  OffT ra = 0, rb = 0;
+  if (ti < A.ntasks) range_of(t, ra, rb);
   while (ti < A.ntasks) {
     const uint32_t tn = ti + nwarps;
-    const PrTask nx = tn < A.ntasks ? A.tasks[tn] : PrTask{0, 0};  // prefetch
+    const PrTask t2 = tn + nwarps < A.ntasks ? A.tasks[tn + nwarps] : none;  // two ahead
+    OffT na = 0, nb = 0;
+    if (tn < A.ntasks) range_of(t1, na, nb);  // one ahead
     const uint32_t kind = t.b >> 30;
     if (kind == kTaskBlock) {
       // ---- rows [r0, r1): <= kWarpNnz arcs, <= kWarpRows rows ------------
-      const uint32_t r0 = t.a, r1 = t.b & 0x3FFFFFFFu, nrows = r1 - r0;
-      const OffT e0 = __ldg(A.off + r0), e1 = __ldg(A.off + r1);
+      const uint32_t r0 = t.a, nrows = (t.b & 0x3FFFFFFFu) - t.a;
+      const OffT e0 = ra, e1 = rb;
       const OffT base = e0 & ~(OffT)3;
       const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
       const uint4* cv = reinterpret_cast<const uint4*>(A.col + base);
-      for (uint32_t j = lane; j < nvec; j += 32) {
-        const uint4 q = ld_arcs(cv + j, pol_arc);
-        const OffT e = base + 4 * (OffT)j;
-        if (e >= e0 && e < e1) sv[e - e0] = gather(q.x, hub, nhub, ccur, pol_c);
-        if (e + 1 >= e0 && e + 1 < e1) sv[e + 1 - e0] = gather(q.y, hub, nhub, ccur, pol_c);
-        if (e + 2 >= e0 && e + 2 < e1) sv[e + 2 - e0] = gather(q.z, hub, nhub, ccur, pol_c);
-        if (e + 3 >= e0 && e + 3 < e1) sv[e + 3 - e0] = gather(q.w, hub, nhub, ccur, pol_c);
-      }
-      // row bounds (relative to e0) of rows lane and lane+32
-      uint32_t b0 = 0, n0 = 0, b1 = 0, n1 = 0;
+      // round trip 1: index vectors, row bounds, row data for the epilogue
+      uint4 qa = make_uint4(0, 0, 0, 0), qb = make_uint4(0, 0, 0, 0);
+      if ((uint32_t)lane < nvec) qa = ld_arcs(cv + lane, pol_arc);
+      if ((uint32_t)lane + 32 < nvec) qb = ld_arcs(cv + lane + 32, pol_arc);
+      uint32_t b0 = 0, n0 = 0, b1 = 0, n1 = 0, d0 = kDeletedDegree, d1 = kDeletedDegree;
+      double xo0 = 0.0, xo1 = 0.0, tp0 = 0.0, tp1 = 0.0;
       if ((uint32_t)lane < nrows) {
-        b0 = (uint32_t)(__ldg(A.off + r0 + lane) - e0);
-        n0 = (uint32_t)(__ldg(A.off + r0 + lane + 1) - e0);
+        const uint32_t r = r0 + lane;
+        b0 = (uint32_t)(__ldg(A.off + r) - e0);
+        n0 = (uint32_t)(__ldg(A.off + r + 1) - e0);
+        d0 = __ldg(A.deg + r);
+        xo0 = __ldg(xcur + r);
+        if (personalised) tp0 = __ldg(A.teleport + r);
       }
       if ((uint32_t)lane + 32 < nrows) {
-        b1 = (uint32_t)(__ldg(A.off + r0 + lane + 32) - e0);
-        n1 = (uint32_t)(__ldg(A.off + r0 + lane + 33) - e0);
+        const uint32_t r = r0 + lane + 32;
+        b1 = (uint32_t)(__ldg(A.off + r) - e0);
+        n1 = (uint32_t)(__ldg(A.off + r + 1) - e0);
+        d1 = __ldg(A.deg + r);
+        xo1 = __ldg(xcur + r);
+        if (personalised) tp1 = __ldg(A.teleport + r);
+      }
+      // round trip 2: gathers into this warp's staging slice
+      {
+        const OffT e = base + 4 * (OffT)lane;
+        if (e >= e0 && e < e1) sv[e - e0] = gather(qa.x, hub, nhub, ccur, pol_c);
+        if (e + 1 >= e0 && e + 1 < e1) sv[e + 1 - e0] = gather(qa.y, hub, nhub, ccur, pol_c);
+        if (e + 2 >= e0 && e + 2 < e1) sv[e + 2 - e0] = gather(qa.z, hub, nhub, ccur, pol_c);
+        if (e + 3 >= e0 && e + 3 < e1) sv[e + 3 - e0] = gather(qa.w, hub, nhub, ccur, pol_c);
+        const OffT f = e + 128;
+        if (f < e1) sv[f - e0] = gather(qb.x, hub, nhub, ccur, pol_c);
+        if (f + 1 < e1) sv[f + 1 - e0] = gather(qb.y, hub, nhub, ccur, pol_c);
+        if (f + 2 < e1) sv[f + 2 - e0] = gather(qb.z, hub, nhub, ccur, pol_c);
+        if (f + 3 < e1) sv[f + 3 - e0] = gather(qb.w, hub, nhub, ccur, pol_c);
       }
       __syncwarp();
 #pragma unroll
@@ -358,11 +398,13 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
         const uint32_t i = lane + 32 * half;
         const bool valid = i < nrows;
         const uint32_t b = half ? b1 : b0, en = half ? n1 : n0;
+        const uint32_t dg = half ? d1 : d0;
+        const double xo = half ? xo1 : xo0, tp = half ? tp1 : tp0;
         const bool is_short = valid && (en - b) <= (uint32_t)kShortLen;
         if (is_short) {
           double s = 0.0;
           for (uint32_t k = b; k < en; ++k) s += sv[k];  // ascending source order
-          pr_row_epilogue(A, r0 + i, s, xcur, xnxt, cnxt, tele_u, sink, l1, dsum);
+          pr_row_epilogue(r0 + i, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
         }
         unsigned med = __ballot_sync(0xffffffffu, valid && !is_short);
         while (med) {
@@ -372,44 +414,55 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
           double s = 0.0;
           for (uint32_t j = bk + lane; j < ek; j += 32) s += sv[j];
           s = warp_sum(s);
-          if (lane == k) pr_row_epilogue(A, r0 + i, s, xcur, xnxt, cnxt, tele_u, sink, l1, dsum);
+          if (lane == k)
+            pr_row_epilogue(r0 + i, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
         }
       }
       __syncwarp();
-    } else if (kind == kTaskRow) {
-      // ---- one row of kWarpNnz < in-degree <= kLongChunk ---------------------
-      const uint32_t row = t.a;
-      const double s = warp_range_sum(A.col, ccur, hub, nhub, __ldg(A.off + row), __ldg(A.off + row + 1), lane,
-                                      pol_arc, pol_c);
-      if (lane == 0) pr_row_epilogue(A, row, s, xcur, xnxt, cnxt, tele_u, sink, l1, dsum);
     } else {
-      // ---- chunk c of a long row ---------------------------------------------
-      const uint32_t row = t.a, c = t.b & 0xFFFFu;
-      const OffT rs = __ldg(A.off + row), re = __ldg(A.off + row + 1);
-      const uint32_t nch = (uint32_t)((re - rs + kLongChunk - 1) / kLongChunk);
-      const OffT e0 = rs + (OffT)c * kLongChunk;
-      const OffT e1 = min(e0 + (OffT)kLongChunk, re);
-      const double s = warp_range_sum(A.col, ccur, hub, nhub, e0, e1, lane, pol_arc, pol_c);
-      const uint32_t first = ti - c;
-      unsigned int last = 0;
+      // ---- one heavy row (B) or one chunk of a long row (C) -----------------
+      const uint32_t row = t.a;
+      uint32_t dg = 0;
+      double xo = 0.0, tp = 0.0;
       if (lane == 0) {
-        A.chunk_part[ti] = s;
-        __threadfence();
-        last = (atomicAdd(A.long_cnt + first, 1u) == nch - 1) ? 1u : 0u;
+        dg = __ldg(A.deg + row);
+        xo = __ldg(xcur + row);
+        if (personalised) tp = __ldg(A.teleport + row);
       }
-      last = __shfl_sync(0xffffffffu, last, 0);
-      if (last && lane == 0) {
-        __threadfence();
-        double tot = 0.0;
-        for (uint32_t k = 0; k < nch; ++k) tot += __ldcg(A.chunk_part + (first + k));
-        double rl1 = 0.0, rds = 0.0;
-        pr_row_epilogue(A, row, tot, xcur, xnxt, cnxt, tele_u, sink, rl1, rds);
-        A.long_part[2 * (size_t)first] = rl1;
-        A.long_part[2 * (size_t)first + 1] = rds;
-        A.long_cnt[first] = 0;
+      if (kind == kTaskRow) {
+        const double s = warp_range_sum(A.col, ccur, hub, nhub, ra, rb, lane, pol_arc, pol_c);
+        if (lane == 0)
+          pr_row_epilogue(row, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
+      } else {
+        const uint32_t c = t.b & 0xFFFFu;
+        const uint32_t nch = (uint32_t)((rb - ra + kLongChunk - 1) / kLongChunk);
+        const OffT e0 = ra + (OffT)c * kLongChunk;
+        const OffT e1 = min(e0 + (OffT)kLongChunk, rb);
+        const double s = warp_range_sum(A.col, ccur, hub, nhub, e0, e1, lane, pol_arc, pol_c);
+        const uint32_t first = ti - c;
+        unsigned int last = 0;
+        if (lane == 0) {
+          A.chunk_part[ti] = s;
+          __threadfence();
+          last = (atomicAdd(A.long_cnt + first, 1u) == nch - 1) ? 1u : 0u;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && lane == 0) {
+          __threadfence();
+          double tot = 0.0;
+          for (uint32_t k = 0; k < nch; ++k) tot += __ldcg(A.chunk_part + (first + k));
+          double rl1 = 0.0, rds = 0.0;
+          pr_row_epilogue(row, tot, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, rl1, rds);
+          A.long_part[2 * (size_t)first] = rl1;
+          A.long_part[2 * (size_t)first + 1] = rds;
+          A.long_cnt[first] = 0;
+        }
       }
     }
-    t = nx;
+    t = t1;
+    t1 = t2;
+    ra = na;
+    rb = nb;
     ti = tn;
   }
   cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol, true, s_red,
