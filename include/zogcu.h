@@ -181,6 +181,25 @@ ZOGCU_API int zogcu_pagerank_ex(zogcu_graph* g, double damping, uint64_t max_ite
                       double tolerance, const zogcu_pr_opts* opts, double* out_scores,
                       zogcu_stats* stats);
 
+/* PageRank that allocates nothing, for callers that cannot call cudaMalloc
+ * (a process whose device memory is owned by another runtime, or code that
+ * must not allocate while it runs).  No counterpart in the reference: it is an
+ * addition of this library.  The caller passes device arrays it owns -- the
+ * in-CSR (in_off[V+1], in_col[E], sources ascending per row), out-degrees
+ * (out_degree[V]) and the output (out_scores[V]) -- and every node counts as
+ * live.  Scratch comes from one fixed device array reserved when the library
+ * loads (about 8 MiB, kept until exit), so V is limited to 262,144 nodes;
+ * larger graphs return ZOGCU_ERR_TOO_LARGE.  The first call on a device looks
+ * up that array's address (do it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race, so serialise them.  Runs on
+ * `stream` (NULL = the default stream) and returns when the scores are
+ * written.  Same options and result as zogcu_pagerank. */
+ZOGCU_API int zogcu_pagerank_noalloc(const uint32_t* d_in_off, const uint32_t* d_in_col,
+                                     const uint32_t* d_out_degree, uint32_t num_nodes,
+                                     uint64_t num_arcs, double damping, uint64_t max_iterations,
+                                     double tolerance, double* d_out_scores, zogcu_stats* stats,
+                                     void* stream);
+
 /* ---- Brandes betweenness -------------------------------------------------- */
 
 /* Replaces nif_betweenness_unweighted (.zig:112-121 ->

@@ -30,7 +30,7 @@ EXPORTS = (
     "zogcu_graph_create_from_arraygraph", "zogcu_graph_generate_rmat", "zogcu_rmat_raw_device",
     "zogcu_read_edgelist", "zogcu_graph_destroy", "zogcu_graph_info", "zogcu_graph_export_csr",
     "zogcu_free", "zogcu_pagerank", "zogcu_pagerank_ex", "zogcu_betweenness_unweighted",
-    "zogcu_betweenness_unweighted_ex", "zogcu_bfs_sigma",
+    "zogcu_betweenness_unweighted_ex", "zogcu_bfs_sigma", "zogcu_pagerank_noalloc",
 )
 
 
@@ -107,6 +107,7 @@ def load(path: str | None = None):
         L.zogcu_betweenness_unweighted.argtypes = [vp, vp, C.POINTER(Stats)]
         L.zogcu_betweenness_unweighted_ex.argtypes = [vp, C.POINTER(BcOpts), vp, C.POINTER(Stats)]
         L.zogcu_bfs_sigma.argtypes = [vp, vp, u64, vp, vp, C.POINTER(u32)]
+        L.zogcu_pagerank_noalloc.argtypes = [vp, vp, vp, u32, u64, dbl, u64, dbl, vp, C.POINTER(Stats), vp]
         for name in EXPORTS:  # every other entry point returns a zogcu_status
             if name not in ("zogcu_status_string", "zogcu_last_error", "zogcu_free"):
                 getattr(L, name).restype = C.c_int
