@@ -398,7 +398,8 @@ def run_zog(args):
                        "parallelism": "replicas" if ws > 1 else "single"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "pr_iter_kernel", "ms_per_launch": t_iter_ms,
+                         "kernel": "pr_iter_kernel", "kernel_config": int(st["kernel_config"]),
+                         "ms_per_launch": t_iter_ms,
                          "algorithmic_bytes_per_launch": bytes_per_iter},
             "clocks": clk,
             "gpu_launches": int(launches + (bc_line["launches"] if bc_line else 0)),

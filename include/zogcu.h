@@ -67,6 +67,8 @@ typedef struct zogcu_stats {
   uint32_t sigma_overflow;/* Brandes: some path count wrapped modulo 2^64        */
   uint64_t launches;      /* kernels launched by the call                        */
   uint64_t polish_iterations; /* mixed precision: FP64 iterations at the end     */
+  uint32_t kernel_config; /* PageRank: kernel configuration the autotuner chose  */
+  uint32_t reserved;
 } zogcu_stats;
 
 /* PageRank precision forms. */

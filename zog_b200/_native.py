@@ -47,6 +47,7 @@ class Stats(C.Structure):
         ("iterations", C.c_uint64), ("residual", C.c_double), ("elapsed_ms", C.c_double),
         ("bytes_moved", C.c_double), ("sources", C.c_uint64), ("max_depth", C.c_uint32),
         ("sigma_overflow", C.c_uint32), ("launches", C.c_uint64), ("polish_iterations", C.c_uint64),
+        ("kernel_config", C.c_uint32), ("reserved", C.c_uint32),
     ]
 
     def as_dict(self):

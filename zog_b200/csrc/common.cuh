@@ -81,18 +81,25 @@ struct PrTask {
 // by out-degree (descending; deleted slots last), so the most gathered
 // contributions form a contiguous prefix that fits in shared memory, with the
 // in-CSR re-laid in that order (each row keeps the reference's ascending
-// source order) and the schedule of warp work items.
-struct PrSchedule {
+// source order), plus one schedule of warp work items per work-item size.
+struct PrTaskList {
   bool built = false;
   uint32_t num_tasks = 0;
   uint32_t num_long = 0;      // rows split into chunks
+  DevArray tasks;             // PrTask[num_tasks]
+  DevArray long_first;        // uint32_t[num_long]: first chunk task of each long row
+};
+
+struct PrSchedule {
+  bool built = false;
   DevArray rank;              // uint32_t[V]: rank of node v
   DevArray perm;              // uint32_t[V]: node of rank p
   DevArray off;               // uint32_t[V+1] (or uint64_t when E >= 2^32)
   DevArray col;               // uint32_t[E+4]: ranks of the sources
   DevArray deg;               // uint32_t[V]: out-degree of rank p
-  DevArray tasks;             // PrTask[num_tasks]
-  DevArray long_first;        // uint32_t[num_long]: first chunk task of each long row
+  std::vector<uint64_t> host_off;  // ranked offsets on the host (schedule builds)
+  PrTaskList lists[2];        // work items of 128 and of 256 arcs
+  int config = -1;            // kernel configuration chosen by the autotuner
 };
 
 // Device-resident graph (one per NIF resource).

@@ -13,21 +13,24 @@
 //     c[u] = x[u]/deg(u), the reference's per-term quotient bit for bit -- form
 //     a contiguous prefix; each row keeps the reference's ascending-source
 //     order.  Random 8-byte gathers are limited by the L1 tag stage (about one
-//     128-byte line per SM clock); the prefix of c (the "hub" part, 192 KB) is
-//     copied into shared memory at the start of every iteration and gathered
-//     from there instead;
+//     128-byte line per SM clock); a prefix of c (the "hub") is copied into
+//     shared memory at the start of every iteration and gathered from there;
 //   * degree-binned schedule, one warp per work item:
-//       A  a block of consecutive rows, each of in-degree <= kWarpNnz, with
-//          <= kWarpNnz arcs and <= kWarpRows rows in total: 16-byte index loads,
-//          gathers staged in the warp's shared-memory slice, rows of in-degree
-//          <= kShortLen summed by one lane each in the reference's order,
-//          longer ones by the warp;
-//       B  one row with kWarpNnz < in-degree <= kLongChunk, reduced by a warp;
+//       A  a block of consecutive rows, each of in-degree <= NNZ, with <= NNZ
+//          arcs and <= kWarpRows rows in total: 16-byte index loads, gathers
+//          staged in the warp's shared-memory slice, rows of in-degree <=
+//          kShortLen summed by one lane each in the reference's order, longer
+//          ones by the warp;
+//       B  one row with NNZ < in-degree <= kLongChunk, reduced by a warp;
 //       C  one kLongChunk-arc chunk of a longer row; the last warp to finish a
 //          row (arrival counter) adds the chunk partials in chunk order and
 //          runs the row's epilogue;
-//     warps never wait on each other inside the pass and prefetch their next
-//     work item;
+//     each warp runs a software pipeline over its items (descriptors two
+//     ahead, arc ranges one ahead), so an item costs two dependent round
+//     trips, and warps never wait on each other inside the pass;
+//   * the kernel is a template over (CTA size, arcs per item, hub size); an
+//     autotuner times the candidate configurations on the graph at its first
+//     PageRank call and keeps the fastest (ZOGCU_PR_CONFIG forces one);
 //   * arc indices stream with an L2 evict-first policy, bypassing L1; gathered
 //     contributions use an L2 evict-last policy;
 //   * the epilogue writes x', c' = x'/deg and accumulates |x'-x| and the
@@ -40,6 +43,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -47,15 +51,27 @@
 
 namespace zogcu {
 
-constexpr int kPrThreads = 1024;         // one CTA per SM
-constexpr int kPrWarps = kPrThreads / 32;
-constexpr int kWarpNnz = 128;            // arcs per row block (4 per lane)
 constexpr int kWarpRows = 64;            // rows per row block (2 per lane)
 constexpr int kShortLen = 32;            // in-degree summed by a single lane
 constexpr int kLongChunk = 4096;         // arcs per chunk of a long row
-constexpr int kHubBytes = 192 * 1024;    // shared-memory copy of the hottest contributions
 
 enum : uint32_t { kTaskBlock = 0, kTaskRow = 1, kTaskChunk = 2 };
+
+// Kernel configurations the autotuner chooses from.
+struct PrConfig {
+  int threads;      // CTA size
+  int nnz;          // arcs per row-block work item
+  int hub_bytes;    // shared-memory hub per CTA
+};
+constexpr PrConfig kPrConfigs[] = {
+    {1024, 128, 192 * 1024},  // 0: one CTA per SM, biggest hub
+    {1024, 256, 160 * 1024},  // 1: one CTA per SM, bigger items
+    {512, 256, 64 * 1024},    // 2: two CTAs per SM
+    {256, 256, 0},            // 3: four CTAs per SM, no hub
+    {256, 128, 0},            // 4: four CTAs per SM, no hub, small items
+};
+constexpr int kNumPrConfigs = sizeof(kPrConfigs) / sizeof(kPrConfigs[0]);
+constexpr int kDefaultPrConfig = 0;
 
 struct PrState {
   unsigned long long iter;  // iterations completed
@@ -289,11 +305,14 @@ __global__ void __launch_bounds__(256) pr_init_kernel(PrArgs<OffT, CT> A, uint32
   cta_publish(A.st, A.cta_part, A.long_part, A.long_first, 0, 0.0, dsum, 0ull, A.tol, false, s_red, &s_flag);
 }
 
-template <typename OffT, typename CT>
-__global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT> A) {
+constexpr int pr_min_blocks(int threads) { return threads >= 1024 ? 1 : (threads >= 512 ? 2 : 4); }
+
+template <typename OffT, typename CT, int THREADS, int NNZ>
+__global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kernel(PrArgs<OffT, CT> A) {
+  constexpr int WARPS = THREADS / 32;
+  constexpr int VPL = (NNZ / 4 + 1 + 31) / 32;  // 16-byte index vectors per lane in a row block
   extern __shared__ __align__(16) unsigned char s_dyn[];
-  __shared__ __align__(16) double s_val[kPrWarps][kWarpNnz];
-  __shared__ double s_red[2 * kPrWarps];
+  __shared__ double s_red[2 * WARPS];
   __shared__ int s_flag;
 
   const PrState* st = A.st;
@@ -311,27 +330,29 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
   const bool personalised = A.teleport != nullptr;
   const double damping = A.damping, n_f = A.n_f;
 
-  // ---- stage the hot prefix of c in shared memory --------------------------
-  CT* hub = reinterpret_cast<CT*>(s_dyn);
+  // ---- dynamic shared memory: [hub | per-warp staging] ----------------------
   const uint32_t nhub = A.hub;
-  {
+  const size_t hub_bytes = ((size_t)nhub * sizeof(CT) + 15) & ~(size_t)15;
+  CT* hub = reinterpret_cast<CT*>(s_dyn);
+  double* staging = reinterpret_cast<double*>(s_dyn + hub_bytes);
+  if (nhub) {
     const uint4* src = reinterpret_cast<const uint4*>(ccur);
     uint4* dst = reinterpret_cast<uint4*>(hub);
     const uint32_t n16 = (uint32_t)(((size_t)nhub * sizeof(CT)) >> 4);
-    for (uint32_t i = threadIdx.x; i < n16; i += kPrThreads) dst[i] = __ldcg(src + i);
+    for (uint32_t i = threadIdx.x; i < n16; i += THREADS) dst[i] = __ldcg(src + i);
+    __syncthreads();
   }
-  __syncthreads();
 
   const uint64_t pol_arc = policy_evict_first();
   const uint64_t pol_c = policy_evict_last();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* sv = s_val[warp];
+  double* sv = staging + (size_t)warp * NNZ;
   double l1 = 0.0, dsum = 0.0;
 
   // Software pipeline over this warp's work items: descriptors are loaded two
   // items ahead and their arc ranges one item ahead, so a block needs two
   // dependent round trips (index vectors with row data, then gathers).
-  const uint32_t nwarps = gridDim.x * kPrWarps;
+  const uint32_t nwarps = gridDim.x * WARPS;
   const PrTask none{0, 0};
   auto range_of = [&](const PrTask& tk, OffT& lo, OffT& hi) {
     const uint32_t kind = tk.b >> 30;
@@ -339,7 +360,7 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
     lo = __ldg(A.off + tk.a);
     hi = __ldg(A.off + end);
   };
-  uint32_t ti = blockIdx.x * kPrWarps + warp;
+  uint32_t ti = blockIdx.x * WARPS + warp;
   PrTask t = ti < A.ntasks ? A.tasks[ti] : none;
   PrTask t1 = ti + nwarps < A.ntasks ? A.tasks[ti + nwarps] : none;
   OffT ra = 0, rb = 0;
@@ -351,16 +372,17 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
     if (tn < A.ntasks) range_of(t1, na, nb);  // one ahead
     const uint32_t kind = t.b >> 30;
     if (kind == kTaskBlock) {
-      // ---- rows [r0, r1): <= kWarpNnz arcs, <= kWarpRows rows ------------
+      // ---- rows [r0, r1): <= NNZ arcs, <= kWarpRows rows ------------------
       const uint32_t r0 = t.a, nrows = (t.b & 0x3FFFFFFFu) - t.a;
       const OffT e0 = ra, e1 = rb;
       const OffT base = e0 & ~(OffT)3;
       const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
       const uint4* cv = reinterpret_cast<const uint4*>(A.col + base);
       // round trip 1: index vectors, row bounds, row data for the epilogue
-      uint4 qa = make_uint4(0, 0, 0, 0), qb = make_uint4(0, 0, 0, 0);
-      if ((uint32_t)lane < nvec) qa = ld_arcs(cv + lane, pol_arc);
-      if ((uint32_t)lane + 32 < nvec) qb = ld_arcs(cv + lane + 32, pol_arc);
+      uint4 q[VPL];
+#pragma unroll
+      for (int k = 0; k < VPL; ++k)
+        q[k] = ((uint32_t)lane + 32 * k < nvec) ? ld_arcs(cv + lane + 32 * k, pol_arc) : make_uint4(0, 0, 0, 0);
       uint32_t b0 = 0, n0 = 0, b1 = 0, n1 = 0, d0 = kDeletedDegree, d1 = kDeletedDegree;
       double xo0 = 0.0, xo1 = 0.0, tp0 = 0.0, tp1 = 0.0;
       if ((uint32_t)lane < nrows) {
@@ -380,17 +402,13 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
         if (personalised) tp1 = __ldg(A.teleport + r);
       }
       // round trip 2: gathers into this warp's staging slice
-      {
-        const OffT e = base + 4 * (OffT)lane;
-        if (e >= e0 && e < e1) sv[e - e0] = gather(qa.x, hub, nhub, ccur, pol_c);
-        if (e + 1 >= e0 && e + 1 < e1) sv[e + 1 - e0] = gather(qa.y, hub, nhub, ccur, pol_c);
-        if (e + 2 >= e0 && e + 2 < e1) sv[e + 2 - e0] = gather(qa.z, hub, nhub, ccur, pol_c);
-        if (e + 3 >= e0 && e + 3 < e1) sv[e + 3 - e0] = gather(qa.w, hub, nhub, ccur, pol_c);
-        const OffT f = e + 128;
-        if (f < e1) sv[f - e0] = gather(qb.x, hub, nhub, ccur, pol_c);
-        if (f + 1 < e1) sv[f + 1 - e0] = gather(qb.y, hub, nhub, ccur, pol_c);
-        if (f + 2 < e1) sv[f + 2 - e0] = gather(qb.z, hub, nhub, ccur, pol_c);
-        if (f + 3 < e1) sv[f + 3 - e0] = gather(qb.w, hub, nhub, ccur, pol_c);
+#pragma unroll
+      for (int k = 0; k < VPL; ++k) {
+        const OffT e = base + 4 * (OffT)(lane + 32 * k);
+        if (e >= e0 && e < e1) sv[e - e0] = gather(q[k].x, hub, nhub, ccur, pol_c);
+        if (e + 1 >= e0 && e + 1 < e1) sv[e + 1 - e0] = gather(q[k].y, hub, nhub, ccur, pol_c);
+        if (e + 2 >= e0 && e + 2 < e1) sv[e + 2 - e0] = gather(q[k].z, hub, nhub, ccur, pol_c);
+        if (e + 3 >= e0 && e + 3 < e1) sv[e + 3 - e0] = gather(q[k].w, hub, nhub, ccur, pol_c);
       }
       __syncwarp();
 #pragma unroll
@@ -470,7 +488,7 @@ __global__ void __launch_bounds__(kPrThreads, 1) pr_iter_kernel(PrArgs<OffT, CT>
 }
 
 // ---------------------------------------------------------------------------
-// PageRank view: degree ranking, re-laid in-CSR, schedule
+// PageRank view: degree ranking, re-laid in-CSR, schedules
 // ---------------------------------------------------------------------------
 __global__ void k_rank_keys(const uint32_t* __restrict__ deg, uint32_t V, uint32_t* __restrict__ key,
                             uint32_t* __restrict__ ids) {
@@ -530,13 +548,10 @@ static unsigned grid_1d(uint64_t n) {
   return (unsigned)std::max<uint64_t>(g, 1);
 }
 
-int ensure_pr_schedule(Graph* g, cudaStream_t s) {
-  std::lock_guard<std::mutex> lk(g->mu);
+// Ranking and re-laid in-CSR (once per graph; caller holds g->mu).
+static int build_ranked_view(Graph* g, cudaStream_t s) {
   PrSchedule& P = g->pr;
-  if (P.built) return ZOGCU_OK;
   const uint32_t V = g->V;
-  if (V >= (1u << 30)) return fail(ZOGCU_ERR_TOO_LARGE, "PageRank schedule supports fewer than 2^30 nodes");
-  // ---- ranking by out-degree ---------------------------------------------
   ZOGCU_TRY(P.rank.alloc((size_t)V * 4));
   ZOGCU_TRY(P.perm.alloc((size_t)V * 4));
   ZOGCU_TRY(P.deg.alloc((size_t)V * 4));
@@ -554,7 +569,6 @@ int ensure_pr_schedule(Graph* g, cudaStream_t s) {
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, key.as<uint32_t>(), key2.as<uint32_t>(),
                                                ids.as<uint32_t>(), P.perm.as<uint32_t>(), (int64_t)V, 0, 32, s));
   }
-  // ---- ranked in-CSR ---------------------------------------------------------
   DevBuf cnt, poff64;
   ZOGCU_TRY(cnt.alloc(((size_t)V + 1) * 8, s));
   ZOGCU_TRY(poff64.alloc(((size_t)V + 1) * 8, s));
@@ -586,17 +600,24 @@ int ensure_pr_schedule(Graph* g, cudaStream_t s) {
     ZOGCU_TRY(P.off.alloc(((size_t)V + 1) * 8));
     ZOGCU_CUDA(cudaMemcpyAsync(P.off.ptr, poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToDevice, s));
   }
-  // ---- schedule (host greedy pass over the ranked offsets) -------------------
-  std::vector<uint64_t> off((size_t)V + 1);
-  ZOGCU_CUDA(cudaMemcpyAsync(off.data(), poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToHost, s));
+  P.host_off.resize((size_t)V + 1);
+  ZOGCU_CUDA(cudaMemcpyAsync(P.host_off.data(), poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  return ZOGCU_OK;
+}
+
+// Work items for row blocks of at most `nnz` arcs (host greedy pass over the
+// ranked offsets; caller holds g->mu).
+static int build_task_list(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
+  const uint32_t V = g->V;
+  const std::vector<uint64_t>& off = g->pr.host_off;
   std::vector<PrTask> tasks;
   std::vector<uint32_t> long_first;
-  tasks.reserve(g->E / (kWarpNnz / 2) + V / kWarpRows + 16);
+  tasks.reserve(g->E / (nnz / 2) + V / kWarpRows + 16);
   uint32_t r = 0;
   while (r < V) {
     uint64_t len = off[r + 1] - off[r];
-    if (len > (uint64_t)kWarpNnz) {
+    if (len > (uint64_t)nnz) {
       if (len <= (uint64_t)kLongChunk) {
         tasks.push_back(PrTask{r, (kTaskRow << 30) | (r + 1)});
       } else {
@@ -609,37 +630,153 @@ int ensure_pr_schedule(Graph* g, cudaStream_t s) {
       continue;
     }
     const uint32_t r0 = r;
-    uint64_t nnz = 0;
+    uint64_t tot = 0;
     while (r < V && (r - r0) < (uint32_t)kWarpRows) {
       len = off[r + 1] - off[r];
-      if (len > (uint64_t)kWarpNnz || nnz + len > (uint64_t)kWarpNnz) break;
-      nnz += len;
+      if (len > (uint64_t)nnz || tot + len > (uint64_t)nnz) break;
+      tot += len;
       ++r;
     }
     tasks.push_back(PrTask{r0, (kTaskBlock << 30) | r});
   }
   if (tasks.size() >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "too many PageRank work items");
-  P.num_tasks = (uint32_t)tasks.size();
-  P.num_long = (uint32_t)long_first.size();
-  ZOGCU_TRY(P.tasks.alloc(std::max<size_t>(tasks.size(), 1) * sizeof(PrTask)));
-  ZOGCU_TRY(P.long_first.alloc(std::max<size_t>(long_first.size(), 1) * 4));
+  L.num_tasks = (uint32_t)tasks.size();
+  L.num_long = (uint32_t)long_first.size();
+  ZOGCU_TRY(L.tasks.alloc(std::max<size_t>(tasks.size(), 1) * sizeof(PrTask)));
+  ZOGCU_TRY(L.long_first.alloc(std::max<size_t>(long_first.size(), 1) * 4));
   if (!tasks.empty())
-    ZOGCU_CUDA(cudaMemcpyAsync(P.tasks.ptr, tasks.data(), tasks.size() * sizeof(PrTask), cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(L.tasks.ptr, tasks.data(), tasks.size() * sizeof(PrTask), cudaMemcpyHostToDevice, s));
   if (!long_first.empty())
-    ZOGCU_CUDA(cudaMemcpyAsync(P.long_first.ptr, long_first.data(), long_first.size() * 4, cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(L.long_first.ptr, long_first.data(), long_first.size() * 4, cudaMemcpyHostToDevice, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  L.built = true;
+  return ZOGCU_OK;
+}
+
+static int list_index(int nnz) { return nnz == 128 ? 0 : 1; }
+
+int ensure_pr_schedule(Graph* g, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g->mu);
+  PrSchedule& P = g->pr;
+  if (P.built) return ZOGCU_OK;
+  if (g->V >= (1u << 30)) return fail(ZOGCU_ERR_TOO_LARGE, "PageRank schedule supports fewer than 2^30 nodes");
+  ZOGCU_TRY(build_ranked_view(g, s));
   P.built = true;
   return ZOGCU_OK;
 }
 
+static int ensure_task_list(Graph* g, int nnz, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g->mu);
+  PrTaskList& L = g->pr.lists[list_index(nnz)];
+  if (L.built) return ZOGCU_OK;
+  return build_task_list(g, nnz, L, s);
+}
+
+// ---------------------------------------------------------------------------
+// Launching a configuration
+// ---------------------------------------------------------------------------
 template <typename OffT, typename CT>
-static int pr_prepare_kernel() {
-  static bool done = false;
-  if (!done) {
-    ZOGCU_CUDA(cudaFuncSetAttribute(pr_iter_kernel<OffT, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    kHubBytes));
-    done = true;
+struct PrLauncher {
+  using Fn = void (*)(PrArgs<OffT, CT>);
+  static Fn fn(int cfg) {
+    switch (cfg) {
+      case 0: return pr_iter_kernel<OffT, CT, 1024, 128>;
+      case 1: return pr_iter_kernel<OffT, CT, 1024, 256>;
+      case 2: return pr_iter_kernel<OffT, CT, 512, 256>;
+      case 3: return pr_iter_kernel<OffT, CT, 256, 256>;
+      default: return pr_iter_kernel<OffT, CT, 256, 128>;
+    }
   }
+  static size_t staging_bytes(int cfg) { return (size_t)(kPrConfigs[cfg].threads / 32) * kPrConfigs[cfg].nnz * 8; }
+  // hub entries and dynamic shared memory of configuration `cfg` for V nodes
+  static uint32_t hub_entries(int cfg, uint32_t V) {
+    const uint32_t cap = (uint32_t)(kPrConfigs[cfg].hub_bytes / sizeof(CT));
+    return std::min<uint32_t>(cap, V & ~3u);
+  }
+  static int grid(int cfg, size_t dyn) {
+    static int cache[kNumPrConfigs] = {};
+    if (!cache[cfg]) {
+      Fn f = fn(cfg);
+      const size_t maxdyn = (size_t)kPrConfigs[cfg].hub_bytes + staging_bytes(cfg);
+      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxdyn) != cudaSuccess) return 0;
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kPrConfigs[cfg].threads, maxdyn) != cudaSuccess)
+        return 0;
+      cache[cfg] = std::max(per_sm, 1) * sm_count();
+    }
+    (void)dyn;
+    return cache[cfg];
+  }
+};
+
+// Per-call workspace, sized for the largest schedule a call may launch.
+struct PrWork {
+  DevBuf x0, x1, c0, c1, part, chunk, lcnt, lpart, stb, tele, tmp;
+};
+
+template <typename OffT, typename CT>
+static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, int given, uint64_t max_iter,
+                           cudaStream_t s, uint64_t* launches) {
+  const PrTaskList& L = g->pr.lists[list_index(kPrConfigs[cfg].nnz)];
+  A.tasks = L.tasks.as<PrTask>();
+  A.long_first = L.long_first.as<uint32_t>();
+  A.ntasks = L.num_tasks;
+  A.nlong = L.num_long;
+  A.hub = PrLauncher<OffT, CT>::hub_entries(cfg, V);
+  A.max_iter = max_iter;
+  const size_t dyn = (((size_t)A.hub * sizeof(CT) + 15) & ~(size_t)15) + PrLauncher<OffT, CT>::staging_bytes(cfg);
+  int grid = PrLauncher<OffT, CT>::grid(cfg, dyn);
+  if (grid <= 0) return fail(ZOGCU_ERR_CUDA, "PageRank kernel configuration could not be set up");
+  const uint32_t warps = kPrConfigs[cfg].threads / 32;
+  const uint32_t need = (A.ntasks + warps - 1) / warps;
+  if (need > 0 && (uint32_t)grid > need) grid = (int)need;
+  ZOGCU_CUDA(cudaMemsetAsync(A.st, 0, sizeof(PrState), s));
+  const unsigned init_grid = std::min(grid_1d(V), 148u * 4);
+  pr_init_kernel<OffT, CT><<<init_grid, 256, 0, s>>>(A, V, given);
+  ZOGCU_CUDA(cudaGetLastError());
+  auto fn = PrLauncher<OffT, CT>::fn(cfg);
+  for (uint64_t k = 0; k < max_iter; ++k) fn<<<grid, kPrConfigs[cfg].threads, dyn, s>>>(A);
+  ZOGCU_CUDA(cudaGetLastError());
+  *launches += 1 + max_iter;
+  return ZOGCU_OK;
+}
+
+// Times each configuration on this graph (a few iterations from the uniform
+// start, tolerance 0) and keeps the fastest.  Small graphs keep the default.
+template <typename OffT, typename CT>
+static int pr_autotune(Graph* g, const PrArgs<OffT, CT>& A0, uint32_t V, cudaStream_t s) {
+  PrSchedule& P = g->pr;
+  if (P.config >= 0) return ZOGCU_OK;
+  if (const char* e = std::getenv("ZOGCU_PR_CONFIG")) {
+    const int c = std::atoi(e);
+    if (c >= 0 && c < kNumPrConfigs) {
+      ZOGCU_TRY(ensure_task_list(g, kPrConfigs[c].nnz, s));
+      P.config = c;
+      return ZOGCU_OK;
+    }
+  }
+  if (g->E < (1ull << 22)) {
+    ZOGCU_TRY(ensure_task_list(g, kPrConfigs[kDefaultPrConfig].nnz, s));
+    P.config = kDefaultPrConfig;
+    return ZOGCU_OK;
+  }
+  EventTimer tm;
+  float best = 1e30f;
+  int best_cfg = kDefaultPrConfig;
+  for (int c = 0; c < kNumPrConfigs; ++c) {
+    ZOGCU_TRY(ensure_task_list(g, kPrConfigs[c].nnz, s));
+    uint64_t launches = 0;
+    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A0, V, 0, 1, s, &launches)));  // warm-up
+    ZOGCU_TRY(tm.start(s));
+    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A0, V, 0, 4, s, &launches)));
+    ZOGCU_TRY(tm.stop(s));
+    const float ms = tm.ms();
+    if (ms > 0.f && ms < best) {
+      best = ms;
+      best_cfg = c;
+    }
+  }
+  P.config = best_cfg;
   return ZOGCU_OK;
 }
 
@@ -648,86 +785,74 @@ static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double
                              double* out, zogcu_stats* stats, cudaStream_t s) {
   const PrSchedule& P = g->pr;
   const uint32_t V = g->V;
-  const uint32_t ntasks = P.num_tasks, nlong = P.num_long;
-  ZOGCU_TRY((pr_prepare_kernel<OffT, double>()));
-  int grid = sm_count();
-  const uint32_t need = (ntasks + kPrWarps - 1) / kPrWarps;
-  if (need > 0 && (uint32_t)grid > need) grid = (int)need;
-  if (grid < 1) grid = 1;
-  const uint32_t hub = std::min<uint32_t>((uint32_t)(kHubBytes / sizeof(double)), V & ~1u);
   const bool dev_ptrs = o && o->device_pointers;
+  // workspace sized for every configuration's schedule
+  ZOGCU_TRY(ensure_task_list(g, 128, s));
+  ZOGCU_TRY(ensure_task_list(g, 256, s));
+  const uint32_t max_tasks = std::max(P.lists[0].num_tasks, P.lists[1].num_tasks);
+  PrWork W;
+  ZOGCU_TRY(W.x0.alloc((size_t)V * 8, s));
+  ZOGCU_TRY(W.x1.alloc((size_t)V * 8, s));
+  ZOGCU_TRY(W.c0.alloc((size_t)V * 8 + 16, s));
+  ZOGCU_TRY(W.c1.alloc((size_t)V * 8 + 16, s));
+  ZOGCU_TRY(W.part.alloc((size_t)std::max<int>(sm_count() * 8, 148 * 4) * 16, s));
+  ZOGCU_TRY(W.chunk.alloc((size_t)std::max<uint32_t>(max_tasks, 1) * 8, s));
+  ZOGCU_TRY(W.lcnt.alloc((size_t)std::max<uint32_t>(max_tasks, 1) * 4, s));
+  ZOGCU_TRY(W.lpart.alloc((size_t)std::max<uint32_t>(max_tasks, 1) * 16, s));
+  ZOGCU_TRY(W.stb.alloc(sizeof(PrState), s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.lcnt.ptr, 0, W.lcnt.bytes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.c0.ptr, 0, W.c0.bytes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.c1.ptr, 0, W.c1.bytes, s));
 
-  DevBuf x0, x1, c0, c1, part, chunk, lcnt, lpart, stb, tele, tmp;
-  ZOGCU_TRY(x0.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(x1.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(c0.alloc((size_t)V * 8 + 16, s));
-  ZOGCU_TRY(c1.alloc((size_t)V * 8 + 16, s));
-  const unsigned init_grid = std::min(grid_1d(V), 148u * 4);
-  ZOGCU_TRY(part.alloc((size_t)std::max<unsigned>((unsigned)grid, init_grid) * 16, s));
-  ZOGCU_TRY(chunk.alloc((size_t)std::max<uint32_t>(ntasks, 1) * 8, s));
-  ZOGCU_TRY(lcnt.alloc((size_t)std::max<uint32_t>(ntasks, 1) * 4, s));
-  ZOGCU_TRY(lpart.alloc((size_t)std::max<uint32_t>(ntasks, 1) * 16, s));
-  ZOGCU_TRY(stb.alloc(sizeof(PrState), s));
-  ZOGCU_CUDA(cudaMemsetAsync(lcnt.ptr, 0, lcnt.bytes, s));
-  ZOGCU_CUDA(cudaMemsetAsync(stb.ptr, 0, sizeof(PrState), s));
-  ZOGCU_CUDA(cudaMemsetAsync(c0.ptr, 0, c0.bytes, s));
-  ZOGCU_CUDA(cudaMemsetAsync(c1.ptr, 0, c1.bytes, s));
-  int given = 0;
-  if (o && o->x0) {  // caller order -> ranked order
-    ZOGCU_TRY(tmp.alloc((size_t)V * 8, s));
-    ZOGCU_CUDA(cudaMemcpyAsync(tmp.ptr, o->x0, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-    k_permute_in<<<grid_1d(V), 256, 0, s>>>(tmp.as<double>(), P.perm.as<uint32_t>(), V, x0.as<double>());
-    ZOGCU_CUDA(cudaGetLastError());
-    given = 1;
-  }
-  const double* tele_ptr = nullptr;
-  if (o && o->teleport) {
-    ZOGCU_TRY(tele.alloc((size_t)V * 8, s));
-    if (!tmp.ptr) ZOGCU_TRY(tmp.alloc((size_t)V * 8, s));
-    ZOGCU_CUDA(cudaMemcpyAsync(tmp.ptr, o->teleport, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
-    k_permute_in<<<grid_1d(V), 256, 0, s>>>(tmp.as<double>(), P.perm.as<uint32_t>(), V, tele.as<double>());
-    ZOGCU_CUDA(cudaGetLastError());
-    tele_ptr = tele.as<double>();
-  }
-
-  PrArgs<OffT, double> A;
+  PrArgs<OffT, double> A{};
   A.off = P.off.as<OffT>();
   A.col = P.col.as<uint32_t>();
   A.deg = P.deg.as<uint32_t>();
-  A.tasks = P.tasks.as<PrTask>();
-  A.long_first = P.long_first.as<uint32_t>();
-  A.ntasks = ntasks;
-  A.nlong = nlong;
-  A.hub = hub;
-  A.x0 = x0.as<double>();
-  A.x1 = x1.as<double>();
-  A.c0 = c0.as<double>();
-  A.c1 = c1.as<double>();
-  A.cta_part = part.as<double>();
-  A.chunk_part = chunk.as<double>();
-  A.long_cnt = lcnt.as<unsigned int>();
-  A.long_part = lpart.as<double>();
-  A.st = stb.as<PrState>();
-  A.teleport = tele_ptr;
+  A.x0 = W.x0.as<double>();
+  A.x1 = W.x1.as<double>();
+  A.c0 = W.c0.as<double>();
+  A.c1 = W.c1.as<double>();
+  A.cta_part = W.part.as<double>();
+  A.chunk_part = W.chunk.as<double>();
+  A.long_cnt = W.lcnt.as<unsigned int>();
+  A.long_part = W.lpart.as<double>();
+  A.st = W.stb.as<PrState>();
+  A.teleport = nullptr;
   A.damping = damping;
   A.n_f = (double)g->n_live;
   A.tol = tol;
-  A.max_iter = max_iter;
 
-  const size_t dyn = (size_t)hub * sizeof(double);
-  EventTimer tm;
-  ZOGCU_TRY(tm.start(s));
-  pr_init_kernel<OffT, double><<<init_grid, 256, 0, s>>>(A, V, given);
-  ZOGCU_CUDA(cudaGetLastError());
-  uint64_t launches = 1;
-  for (uint64_t k = 0; k < max_iter; ++k) {
-    pr_iter_kernel<OffT, double><<<grid, kPrThreads, dyn, s>>>(A);
-    ++launches;
+  {
+    PrArgs<OffT, double> At = A;
+    At.tol = 0.0;
+    ZOGCU_TRY((pr_autotune<OffT, double>(g, At, V, s)));
   }
-  ZOGCU_CUDA(cudaGetLastError());
+  const int cfg = g->pr.config;
+
+  int given = 0;
+  if (o && o->x0) {  // caller order -> ranked order
+    ZOGCU_TRY(W.tmp.alloc((size_t)V * 8, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(W.tmp.ptr, o->x0, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    k_permute_in<<<grid_1d(V), 256, 0, s>>>(W.tmp.as<double>(), P.perm.as<uint32_t>(), V, W.x0.as<double>());
+    ZOGCU_CUDA(cudaGetLastError());
+    given = 1;
+  }
+  if (o && o->teleport) {
+    ZOGCU_TRY(W.tele.alloc((size_t)V * 8, s));
+    if (!W.tmp.ptr) ZOGCU_TRY(W.tmp.alloc((size_t)V * 8, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(W.tmp.ptr, o->teleport, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    k_permute_in<<<grid_1d(V), 256, 0, s>>>(W.tmp.as<double>(), P.perm.as<uint32_t>(), V, W.tele.as<double>());
+    ZOGCU_CUDA(cudaGetLastError());
+    A.teleport = W.tele.as<double>();
+  }
+
+  EventTimer tm;
+  uint64_t launches = 0;
+  ZOGCU_TRY(tm.start(s));
+  ZOGCU_TRY((pr_launch_chain<OffT, double>(g, cfg, A, V, given, max_iter, s, &launches)));
   ZOGCU_TRY(tm.stop(s));
   PrState hs;
-  ZOGCU_CUDA(cudaMemcpyAsync(&hs, stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   const double* result = (hs.iter & 1ull) ? A.x1 : A.x0;
   double* unperm = (hs.iter & 1ull) ? A.x0 : A.x1;  // the other buffer is free now
@@ -744,6 +869,7 @@ static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double
     stats->bytes_moved = per_iter * (double)hs.iter;
     stats->launches = launches;
     stats->polish_iterations = 0;
+    stats->kernel_config = (uint32_t)cfg;
   }
   return ZOGCU_OK;
 }
