@@ -41,6 +41,7 @@ constexpr int kBcThreads = 256;
 constexpr int kLevelChunk = 8;     // forward levels enqueued between host checks
 constexpr int kMaxStoredLevels = 64;  // frontier masks kept for the backward sweep
 constexpr int kOverflowFlag = kMaxStoredLevels + 8;
+constexpr int kHeavyDegree = 512;  // vertices above this degree get a whole CTA
 
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
   return __shfl_sync(0xffffffffu, v, src);
@@ -66,74 +67,137 @@ __device__ __forceinline__ void pop4(unsigned& bal, uint32_t v, unsigned long lo
   }
 }
 
+// Work of one vertex's adjacency slice for the forward step: neighbours
+// [j0, e) in steps of `stride`, 32 at a time; lanes accumulate sigma of their
+// two sources over neighbours in the frontier for those sources.
+template <typename OffT>
+__device__ __forceinline__ void fwd_scan(const uint32_t* __restrict__ col, const unsigned long long* __restrict__ front_cur,
+                                         const unsigned long long* __restrict__ sigma, unsigned long long cand, OffT j0,
+                                         OffT e, OffT stride, int lane, unsigned long long& acc0,
+                                         unsigned long long& acc1, bool& got0, bool& got1, bool& ovf) {
+  for (; j0 < e; j0 += stride) {
+    const OffT j = j0 + lane;
+    uint32_t v = 0;
+    unsigned long long m = 0;
+    if (j < e) {
+      v = __ldg(col + j);
+      m = __ldg(front_cur + v) & cand;
+    }
+    unsigned bal = __ballot_sync(0xffffffffu, m != 0);
+    while (bal) {
+      Nb nb[4];
+      pop4(bal, v, m, nb);
+      unsigned long long s0[4], s1[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint64_t row = (uint64_t)nb[i].v * kBcBatch;
+        s0[i] = ((nb[i].m >> lane) & 1ull) ? sigma[row + lane] : 0ull;
+        s1[i] = ((nb[i].m >> (lane + 32)) & 1ull) ? sigma[row + lane + 32] : 0ull;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        got0 |= ((nb[i].m >> lane) & 1ull) != 0;
+        got1 |= ((nb[i].m >> (lane + 32)) & 1ull) != 0;
+        unsigned long long n = acc0 + s0[i];
+        ovf |= n < acc0;
+        acc0 = n;
+        n = acc1 + s1[i];
+        ovf |= n < acc1;
+        acc1 = n;
+      }
+    }
+  }
+}
+
+// Publishes the level-(l+1) result of vertex w (one warp).
+__device__ __forceinline__ void fwd_commit(uint64_t w, unsigned long long vis, unsigned long long newmask,
+                                           unsigned long long acc0, unsigned long long acc1, uint32_t level, int lane,
+                                           unsigned long long* __restrict__ front_nxt,
+                                           unsigned long long* __restrict__ visited,
+                                           unsigned long long* __restrict__ sigma, uint32_t* __restrict__ dist,
+                                           bool& any_new) {
+  if ((newmask >> lane) & 1ull) {
+    sigma[w * kBcBatch + lane] = acc0;
+    dist[w * kBcBatch + lane] = level + 1;
+  }
+  if ((newmask >> (lane + 32)) & 1ull) {
+    sigma[w * kBcBatch + lane + 32] = acc1;
+    dist[w * kBcBatch + lane + 32] = level + 1;
+  }
+  if (lane == 0) {
+    front_nxt[w] = newmask;
+    if (newmask) {
+      visited[w] = vis | newmask;
+      any_new = true;
+    }
+  }
+}
+
+// Forward step of level `level`: the CTA first takes the heavy vertices (a
+// whole CTA per vertex, its 8 warps splitting the adjacency, partial sums
+// added in shared memory), then blocks of 8 light vertices (a warp each).
 template <typename OffT>
 __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
     uint32_t V, const OffT* __restrict__ off, const uint32_t* __restrict__ col,
     const unsigned long long* __restrict__ front_cur, unsigned long long* __restrict__ front_nxt,
     unsigned long long* __restrict__ visited, unsigned long long* __restrict__ sigma, uint32_t* __restrict__ dist,
-    unsigned long long full, uint32_t level, unsigned int* __restrict__ flags) {
+    unsigned long long full, uint32_t level, unsigned int* __restrict__ flags, const uint32_t* __restrict__ heavy,
+    uint32_t nheavy) {
   // flags[l % kMaxStoredLevels] = 1 when level l discovered a vertex;
   // flags[kOverflowFlag] = some path count wrapped
   if (level > 0 && *(volatile unsigned int*)(flags + (level - 1) % kMaxStoredLevels) == 0u) return;
-  const int lane = threadIdx.x & 31;
-  const uint64_t nwarps = (uint64_t)gridDim.x * (kBcThreads / 32);
+  constexpr int W = kBcThreads / 32;
+  __shared__ unsigned long long s_acc[W][kBcBatch];
+  __shared__ unsigned long long s_got[W];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   bool any_ovf = false, any_new = false;
-  for (uint64_t w = blockIdx.x * (uint64_t)(kBcThreads / 32) + (threadIdx.x >> 5); w < V; w += nwarps) {
-    const unsigned long long vis = visited[w];
-    const unsigned long long cand = full & ~vis;
-    unsigned long long newmask = 0;
-    if (cand) {
-      const OffT b = __ldg(off + w), e = __ldg(off + w + 1);
+  const uint64_t ntasks = (uint64_t)nheavy + ((uint64_t)V + W - 1) / W;
+  for (uint64_t t = blockIdx.x; t < ntasks; t += gridDim.x) {
+    if (t < nheavy) {
+      const uint64_t w = heavy[t];
+      const unsigned long long vis = visited[w];
+      const unsigned long long cand = full & ~vis;
       unsigned long long acc0 = 0, acc1 = 0;
       bool got0 = false, got1 = false;
-      for (OffT j0 = b; j0 < e; j0 += 32) {
-        const OffT j = j0 + lane;
-        uint32_t v = 0;
-        unsigned long long m = 0;
-        if (j < e) {
-          v = __ldg(col + j);
-          m = __ldg(front_cur + v) & cand;
+      if (cand) {
+        const OffT b = __ldg(off + w), e = __ldg(off + w + 1);
+        fwd_scan<OffT>(col, front_cur, sigma, cand, b + (OffT)(32 * warp), e, (OffT)(32 * W), lane, acc0, acc1, got0,
+                       got1, any_ovf);
+      }
+      s_acc[warp][lane] = acc0;
+      s_acc[warp][lane + 32] = acc1;
+      const unsigned long long gm = (unsigned long long)__ballot_sync(0xffffffffu, got0) |
+                                    ((unsigned long long)__ballot_sync(0xffffffffu, got1) << 32);
+      if (lane == 0) s_got[warp] = gm;
+      __syncthreads();
+      if (warp == 0) {
+        unsigned long long t0 = 0, t1 = 0, newmask = 0;
+        for (int k = 0; k < W; ++k) {
+          unsigned long long n = t0 + s_acc[k][lane];
+          any_ovf |= n < t0;
+          t0 = n;
+          n = t1 + s_acc[k][lane + 32];
+          any_ovf |= n < t1;
+          t1 = n;
+          newmask |= s_got[k];
         }
-        unsigned bal = __ballot_sync(0xffffffffu, m != 0);
-        while (bal) {
-          Nb nb[4];
-          pop4(bal, v, m, nb);
-          unsigned long long s0[4], s1[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const uint64_t row = (uint64_t)nb[i].v * kBcBatch;
-            s0[i] = ((nb[i].m >> lane) & 1ull) ? sigma[row + lane] : 0ull;
-            s1[i] = ((nb[i].m >> (lane + 32)) & 1ull) ? sigma[row + lane + 32] : 0ull;
-          }
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            got0 |= ((nb[i].m >> lane) & 1ull) != 0;
-            got1 |= ((nb[i].m >> (lane + 32)) & 1ull) != 0;
-            unsigned long long n = acc0 + s0[i];
-            any_ovf |= n < acc0;
-            acc0 = n;
-            n = acc1 + s1[i];
-            any_ovf |= n < acc1;
-            acc1 = n;
-          }
+        fwd_commit(w, vis, newmask, t0, t1, level, lane, front_nxt, visited, sigma, dist, any_new);
+      }
+      __syncthreads();
+    } else {
+      const uint64_t w = (t - nheavy) * W + warp;
+      if (w < V) {
+        const OffT b = __ldg(off + w), e = __ldg(off + w + 1);
+        if ((uint64_t)(e - b) <= (uint64_t)kHeavyDegree) {  // heavy vertices were done above
+          const unsigned long long vis = visited[w];
+          const unsigned long long cand = full & ~vis;
+          unsigned long long acc0 = 0, acc1 = 0;
+          bool got0 = false, got1 = false;
+          if (cand) fwd_scan<OffT>(col, front_cur, sigma, cand, b, e, (OffT)32, lane, acc0, acc1, got0, got1, any_ovf);
+          const unsigned long long newmask = (unsigned long long)__ballot_sync(0xffffffffu, got0) |
+                                             ((unsigned long long)__ballot_sync(0xffffffffu, got1) << 32);
+          fwd_commit(w, vis, newmask, acc0, acc1, level, lane, front_nxt, visited, sigma, dist, any_new);
         }
-      }
-      newmask = (unsigned long long)__ballot_sync(0xffffffffu, got0) |
-                ((unsigned long long)__ballot_sync(0xffffffffu, got1) << 32);
-      if (got0) {
-        sigma[w * kBcBatch + lane] = acc0;
-        dist[w * kBcBatch + lane] = level + 1;
-      }
-      if (got1) {
-        sigma[w * kBcBatch + lane + 32] = acc1;
-        dist[w * kBcBatch + lane + 32] = level + 1;
-      }
-    }
-    if (lane == 0) {
-      front_nxt[w] = newmask;
-      if (newmask) {
-        visited[w] = vis | newmask;
-        any_new = true;
       }
     }
   }
@@ -141,80 +205,122 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
   if (__any_sync(0xffffffffu, any_ovf) && lane == 0) flags[kOverflowFlag] = 1u;
 }
 
-// Level-l mask of v: stored frontier masks when the BFS was shallow enough,
-// else recomputed from dist.
-__device__ __forceinline__ unsigned long long level_mask(const unsigned long long* __restrict__ mask_l,
-                                                         const uint32_t* __restrict__ dist, uint64_t v,
-                                                         uint32_t level, int lane) {
-  if (mask_l) return mask_l[v];
+// Level-l mask of v recomputed from dist (deep BFS, masks not stored).
+__device__ __forceinline__ unsigned long long dist_mask(const uint32_t* __restrict__ dist, uint64_t v, uint32_t level,
+                                                        int lane) {
   const bool a0 = dist[v * kBcBatch + lane] == level;
   const bool a1 = dist[v * kBcBatch + lane + 32] == level;
   return (unsigned long long)__ballot_sync(0xffffffffu, a0) | ((unsigned long long)__ballot_sync(0xffffffffu, a1) << 32);
 }
 
+// Sum of q[w][b] over successors w in [j0, e) (stride `stride`) whose
+// level-(l+1) mask has bit b.
+template <typename OffT>
+__device__ __forceinline__ void bwd_scan(const uint32_t* __restrict__ col, const unsigned long long* __restrict__ mask_next,
+                                         const double* __restrict__ q, unsigned long long act, OffT j0, OffT e,
+                                         OffT stride, int lane, double& acc0, double& acc1) {
+  for (; j0 < e; j0 += stride) {
+    const OffT j = j0 + lane;
+    uint32_t w = 0;
+    unsigned long long g = 0;
+    if (j < e) {
+      w = __ldg(col + j);
+      g = __ldg(mask_next + w) & act;
+    }
+    unsigned bal = __ballot_sync(0xffffffffu, g != 0);
+    while (bal) {
+      Nb nb[4];
+      pop4(bal, w, g, nb);
+      double t0[4], t1[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint64_t row = (uint64_t)nb[i].v * kBcBatch;
+        t0[i] = ((nb[i].m >> lane) & 1ull) ? q[row + lane] : 0.0;
+        t1[i] = ((nb[i].m >> (lane + 32)) & 1ull) ? q[row + lane + 32] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        acc0 += t0[i];
+        acc1 += t1[i];
+      }
+    }
+  }
+}
+
+// delta, q and the BC contribution of vertex v at this level (one warp).
+__device__ __forceinline__ void bwd_commit(uint64_t v, unsigned long long act, double acc0, double acc1, int lane,
+                                           const unsigned long long* __restrict__ sigma, double* __restrict__ q,
+                                           double* __restrict__ bc) {
+  double dsum = 0.0;
+  if ((act >> lane) & 1ull) {
+    const double sv = (double)sigma[v * kBcBatch + lane];
+    const double d = __dmul_rn(sv, acc0);
+    q[v * kBcBatch + lane] = __ddiv_rn(1.0 + d, sv);
+    dsum += d;
+  }
+  if ((act >> (lane + 32)) & 1ull) {
+    const double sv = (double)sigma[v * kBcBatch + lane + 32];
+    const double d = __dmul_rn(sv, acc1);
+    q[v * kBcBatch + lane + 32] = __ddiv_rn(1.0 + d, sv);
+    dsum += d;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
+  if (lane == 0) bc[v] += dsum;
+}
+
+// Backward step of level `level`.  mask_l / mask_next: stored masks of levels
+// l and l+1; when null, level l is derived from dist and written to mask_out
+// for the next (shallower) launch, which reads it as its mask_next.
 template <typename OffT>
 __global__ void __launch_bounds__(kBcThreads) bc_backward_kernel(
     uint32_t V, const OffT* __restrict__ off, const uint32_t* __restrict__ col,
     const unsigned long long* __restrict__ mask_l, const unsigned long long* __restrict__ mask_next,
     unsigned long long* __restrict__ mask_out, const uint32_t* __restrict__ dist,
     const unsigned long long* __restrict__ sigma, double* __restrict__ q, double* __restrict__ bc, uint32_t level,
-    int last_level) {
-  // mask_l / mask_next: stored masks of levels l and l+1 (null: derive level l
-  // from dist, and read level l+1 from mask_next written by the previous launch
-  // into its mask_out).
-  const int lane = threadIdx.x & 31;
-  const uint64_t nwarps = (uint64_t)gridDim.x * (kBcThreads / 32);
-  for (uint64_t v = blockIdx.x * (uint64_t)(kBcThreads / 32) + (threadIdx.x >> 5); v < V; v += nwarps) {
-    const unsigned long long act = mask_l ? __ldg(mask_l + v) : level_mask(nullptr, dist, v, level, lane);
-    if (mask_out && lane == 0) mask_out[v] = act;
-    if (!act) continue;
-    const bool a0 = (act >> lane) & 1ull, a1 = (act >> (lane + 32)) & 1ull;
-    double acc0 = 0.0, acc1 = 0.0;
-    if (!last_level) {
-      const OffT b = __ldg(off + v), e = __ldg(off + v + 1);
-      for (OffT j0 = b; j0 < e; j0 += 32) {
-        const OffT j = j0 + lane;
-        uint32_t w = 0;
-        unsigned long long g = 0;
-        if (j < e) {
-          w = __ldg(col + j);
-          g = __ldg(mask_next + w) & act;
+    int last_level, const uint32_t* __restrict__ heavy, uint32_t nheavy) {
+  constexpr int W = kBcThreads / 32;
+  __shared__ double s_acc[W][kBcBatch];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t ntasks = (uint64_t)nheavy + ((uint64_t)V + W - 1) / W;
+  for (uint64_t t = blockIdx.x; t < ntasks; t += gridDim.x) {
+    if (t < nheavy) {
+      const uint64_t v = heavy[t];
+      const unsigned long long act = mask_l ? __ldg(mask_l + v) : dist_mask(dist, v, level, lane);
+      if (mask_out && warp == 0 && lane == 0) mask_out[v] = act;
+      if (!act) continue;  // the whole CTA sees the same mask
+      double acc0 = 0.0, acc1 = 0.0;
+      if (!last_level) {
+        const OffT b = __ldg(off + v), e = __ldg(off + v + 1);
+        bwd_scan<OffT>(col, mask_next, q, act, b + (OffT)(32 * warp), e, (OffT)(32 * W), lane, acc0, acc1);
+      }
+      s_acc[warp][lane] = acc0;
+      s_acc[warp][lane + 32] = acc1;
+      __syncthreads();
+      if (warp == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int k = 0; k < W; ++k) {  // fixed order: deterministic
+          t0 += s_acc[k][lane];
+          t1 += s_acc[k][lane + 32];
         }
-        unsigned bal = __ballot_sync(0xffffffffu, g != 0);
-        while (bal) {
-          Nb nb[4];
-          pop4(bal, w, g, nb);
-          double t0[4], t1[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const uint64_t row = (uint64_t)nb[i].v * kBcBatch;
-            t0[i] = ((nb[i].m >> lane) & 1ull) ? q[row + lane] : 0.0;
-            t1[i] = ((nb[i].m >> (lane + 32)) & 1ull) ? q[row + lane + 32] : 0.0;
-          }
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            acc0 += t0[i];
-            acc1 += t1[i];
+        bwd_commit(v, act, t0, t1, lane, sigma, q, bc);
+      }
+      __syncthreads();
+    } else {
+      const uint64_t v = (t - nheavy) * W + warp;
+      if (v < V) {
+        const OffT b = __ldg(off + v), e = __ldg(off + v + 1);
+        if ((uint64_t)(e - b) <= (uint64_t)kHeavyDegree) {
+          const unsigned long long act = mask_l ? __ldg(mask_l + v) : dist_mask(dist, v, level, lane);
+          if (mask_out && lane == 0) mask_out[v] = act;
+          if (act) {
+            double acc0 = 0.0, acc1 = 0.0;
+            if (!last_level) bwd_scan<OffT>(col, mask_next, q, act, b, e, (OffT)32, lane, acc0, acc1);
+            bwd_commit(v, act, acc0, acc1, lane, sigma, q, bc);
           }
         }
       }
     }
-    double dsum = 0.0;
-    if (a0) {
-      const double sv = (double)sigma[v * kBcBatch + lane];
-      const double d = __dmul_rn(sv, acc0);
-      q[v * kBcBatch + lane] = __ddiv_rn(1.0 + d, sv);
-      dsum += d;
-    }
-    if (a1) {
-      const double sv = (double)sigma[v * kBcBatch + lane + 32];
-      const double d = __dmul_rn(sv, acc1);
-      q[v * kBcBatch + lane + 32] = __ddiv_rn(1.0 + d, sv);
-      dsum += d;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
-    if (lane == 0) bc[v] += dsum;
   }
 }
 
@@ -233,10 +339,39 @@ __global__ void bc_seed_kernel(const uint32_t* __restrict__ sources, int nb, uns
 static int bc_grid(uint32_t V) {
   const uint64_t warps = V;
   uint64_t blocks = (warps + (kBcThreads / 32) - 1) / (kBcThreads / 32);
-  const uint64_t cap = (uint64_t)sm_count() * (2048 / kBcThreads) * 4;
+  const uint64_t cap = (uint64_t)sm_count() * (2048 / kBcThreads);
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   return (int)blocks;
+}
+
+// Vertices of in- (forward) and out-degree (backward) above kHeavyDegree, by
+// degree descending, so the biggest get their CTAs first.
+static int ensure_heavy_lists(Graph* g, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g->mu);
+  if (g->bc_built) return ZOGCU_OK;
+  const uint32_t V = g->V;
+  for (int dir = 0; dir < 2; ++dir) {
+    std::vector<uint64_t> off((size_t)V + 1);
+    const DevArray& o = dir == 0 ? g->in_off64 : g->out_off64;
+    ZOGCU_CUDA(cudaMemcpyAsync(off.data(), o.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    std::vector<std::pair<uint64_t, uint32_t>> hv;
+    for (uint32_t v = 0; v < V; ++v) {
+      const uint64_t d = off[v + 1] - off[v];
+      if (d > (uint64_t)kHeavyDegree) hv.emplace_back(d, v);
+    }
+    std::sort(hv.begin(), hv.end(), [](const auto& a, const auto& b) { return a.first != b.first ? a.first > b.first : a.second < b.second; });
+    std::vector<uint32_t> ids(hv.size());
+    for (size_t i = 0; i < hv.size(); ++i) ids[i] = hv[i].second;
+    DevArray& dst = dir == 0 ? g->heavy_in : g->heavy_out;
+    ZOGCU_TRY(dst.alloc(std::max<size_t>(ids.size(), 1) * 4));
+    if (!ids.empty()) ZOGCU_CUDA(cudaMemcpyAsync(dst.ptr, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    (dir == 0 ? g->n_heavy_in : g->n_heavy_out) = (uint32_t)ids.size();
+  }
+  g->bc_built = true;
+  return ZOGCU_OK;
 }
 
 constexpr int kFlagWords = kMaxStoredLevels + 16;
@@ -297,7 +432,8 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
       bc_forward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(V, in_off, g->in_col.as<uint32_t>(), W.level(l, V),
                                                           W.level(l + 1, V), W.visited.as<unsigned long long>(),
                                                           W.sigma.as<unsigned long long>(), W.dist.as<uint32_t>(),
-                                                          full, l, W.flags.as<unsigned int>());
+                                                          full, l, W.flags.as<unsigned int>(),
+                                                          g->heavy_in.as<uint32_t>(), g->n_heavy_in);
       ZOGCU_CUDA(cudaGetLastError());
       *launches += 1;
     }
@@ -319,6 +455,7 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {
   const uint32_t V = g->V;
   const uint64_t ns = sources.size();
+  ZOGCU_TRY(ensure_heavy_lists(g, s));
   BcWork W;
   ZOGCU_TRY(W.alloc(V, ns, s, true));
   if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W.src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, s));
@@ -346,11 +483,13 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
       if (stored) {
         bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(
             V, out_off, g->out_col.as<uint32_t>(), W.level(l, V), W.level(l + 1, V), nullptr,
-            W.dist.as<uint32_t>(), W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0);
+            W.dist.as<uint32_t>(), W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0,
+            g->heavy_out.as<uint32_t>(), g->n_heavy_out);
       } else {
         bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(
             V, out_off, g->out_col.as<uint32_t>(), nullptr, mnxt, mcur, W.dist.as<uint32_t>(),
-            W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0);
+            W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0,
+            g->heavy_out.as<uint32_t>(), g->n_heavy_out);
         std::swap(mnxt, mcur);
       }
       ZOGCU_CUDA(cudaGetLastError());
@@ -444,6 +583,7 @@ int zogcu_bfs_sigma(zogcu_graph* G, const uint32_t* sources, uint64_t num_source
   ZOGCU_CUDA(cudaSetDevice(g->device));
   StreamGuard sg;
   ZOGCU_TRY(sg.init(nullptr));
+  ZOGCU_TRY(ensure_heavy_lists(g, sg.s));
   BcWork W;
   ZOGCU_TRY(W.alloc(V, num_sources, sg.s, false));
   if (num_sources) ZOGCU_CUDA(cudaMemcpyAsync(W.src.ptr, sources, num_sources * 4, cudaMemcpyHostToDevice, sg.s));

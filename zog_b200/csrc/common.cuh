@@ -117,6 +117,11 @@ struct Graph {
   DevArray live;                  // uint8_t[V] (when has_deleted)
   std::mutex mu;                  // guards lazy schedule builds
   PrSchedule pr;                  // PageRank schedule (built on first call)
+  // Brandes: vertices whose in- / out-degree exceeds the heavy threshold,
+  // by degree descending (built on the first betweenness call)
+  bool bc_built = false;
+  uint32_t n_heavy_in = 0, n_heavy_out = 0;
+  DevArray heavy_in, heavy_out;
 };
 
 int ensure_device(int* dev);
