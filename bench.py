@@ -294,6 +294,28 @@ def run_zog(args):
     hbm_peak, peak_kind = peaks()
     achieved = bytes_per_iter / (t_iter_ms * 1e-3) / 1e9
 
+    # ---------------- precision form: FP32 SpMV + FP64 polish ----------------
+    mixed = None
+    if not args.no_mixed:
+        x64 = out.clone()
+        outm = torch.empty_like(out)
+        for _ in range(args.warmup):
+            stm = G.pagerank_device(outm.data_ptr(), DAMPING, MAX_ITER, TOL, precision=N.PREC_MIXED, stream=sp)
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True); m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            stm = G.pagerank_device(outm.data_ptr(), DAMPING, MAX_ITER, TOL, precision=N.PREC_MIXED, stream=sp)
+            launches += stm["launches"]
+        m1.record(stream)
+        torch.cuda.synchronize()
+        mms = max_over_ranks(m0.elapsed_time(m1) / args.steps, ws)
+        err = float((outm - x64).abs().sum() / x64.abs().sum())
+        mixed = {"ms": mms, "speedup_vs_fp64": ms / mms, "iterations": int(stm["iterations"]),
+                 "fp64_polish_iterations": int(stm["polish_iterations"]), "residual": float(stm["residual"]),
+                 "rel_l1_vs_fp64": err, "bound": "rel L1 <= 2*d/(1-d)*tol = %.2e" % (2 * DAMPING / (1 - DAMPING) * TOL)}
+        del x64, outm
+
     # ---------------- e2e through the C ABI with host buffers ----------------
     e2e = None
     if not args.no_e2e:
@@ -405,6 +427,7 @@ def run_zog(args):
             "gpu_launches": int(launches + (bc_line["launches"] if bc_line else 0)),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "precision_mixed": mixed,
             "brandes": bc_line,
         }
         print(json.dumps(line), flush=True)
@@ -427,6 +450,7 @@ def main():
     ap.add_argument("--bc-steps", type=int, default=0, help="Brandes steps of 4,096 sources (0 = all sources)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-brandes", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP32/FP64 precision form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)

@@ -169,3 +169,24 @@ def test_large_graph_properties(native, oracle):
         assert st["residual"] < 1e-9 and st["iterations"] < 200
     finally:
         G.destroy()
+
+
+@pytest.mark.parametrize("scale", [13, 16])
+def test_mixed_precision_bound(native, oracle, scale):
+    """Precision form: FP32 contributions, FP64 sums / residual / dangling,
+    then an FP64 polish to the same L1 step.  Both results satisfy
+    ||x - x*||_1 <= d/(1-d) * tol (Sigma x = 1), so they differ from the FP64
+    oracle's by at most 2 * d/(1-d) * tol < 12 * tol."""
+    V, f, t = oracle.rmat(scale, 16, 500 + scale, directed=True)
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        tol = 1e-10
+        x, st = G.pagerank(0.85, 200, tol, precision=native.PREC_MIXED, stats=True)
+        ref, it, _ = oracle.ArrayGraph(V, f, t).pagerank(0.85, 200, tol)
+        assert rel_l1(x, ref) <= 12 * tol
+        assert st["residual"] < tol and st["polish_iterations"] >= 1
+        assert st["iterations"] > st["polish_iterations"]
+        x64 = G.pagerank(0.85, 200, tol)
+        assert rel_l1(x64, ref) <= TOL
+    finally:
+        G.destroy()

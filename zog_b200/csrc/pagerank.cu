@@ -105,6 +105,7 @@ struct PrArgs {
   double damping;
   double n_f;
   double tol;
+  double stall;          // > 0: also stop once l1 > stall * previous l1
   unsigned long long max_iter;
 };
 
@@ -235,7 +236,7 @@ __device__ __forceinline__ void cta_sum2(double& a, double& b, double* s_red) {
 // order, then publication of the iteration's result.
 __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta, const double* long_part,
                              const uint32_t* long_first, uint32_t nlong, unsigned long long next_iter, double tol,
-                             bool set_l1, double* s_red) {
+                             double stall, bool set_l1, double* s_red) {
   double a = 0.0, b = 0.0;
   for (uint32_t i = threadIdx.x; i < ncta; i += blockDim.x) {
     a += __ldcg(cta_part + 2 * i);
@@ -250,8 +251,9 @@ __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta,
   if (threadIdx.x == 0) {
     st->sink = b;
     if (set_l1) {
+      const bool stalled = stall > 0.0 && next_iter > 2 && a > stall * st->l1;
       st->l1 = a;
-      st->converged = (a < tol) ? 1 : 0;
+      st->converged = (a < tol || stalled) ? 1 : 0;
     } else {
       st->l1 = 0.0;
       st->converged = 0;
@@ -265,8 +267,8 @@ __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta,
 // Publishes a CTA's partials and runs the final reduction in the last CTA.
 __device__ __forceinline__ void cta_publish(PrState* st, double* cta_part, const double* long_part,
                                             const uint32_t* long_first, uint32_t nlong, double l1, double dsum,
-                                            unsigned long long next_iter, double tol, bool set_l1, double* s_red,
-                                            int* s_flag) {
+                                            unsigned long long next_iter, double tol, double stall, bool set_l1,
+                                            double* s_red, int* s_flag) {
   cta_sum2(l1, dsum, s_red);
   if (threadIdx.x == 0) {
     cta_part[2 * blockIdx.x] = l1;
@@ -278,7 +280,7 @@ __device__ __forceinline__ void cta_publish(PrState* st, double* cta_part, const
   __syncthreads();
   if (*s_flag) {
     __threadfence();
-    final_reduce(st, cta_part, gridDim.x, long_part, long_first, nlong, next_iter, tol, set_l1, s_red);
+    final_reduce(st, cta_part, gridDim.x, long_part, long_first, nlong, next_iter, tol, stall, set_l1, s_red);
   }
 }
 
@@ -302,7 +304,7 @@ __global__ void __launch_bounds__(256) pr_init_kernel(PrArgs<OffT, CT> A, uint32
     A.x0[v] = x;
     A.x1[v] = 0.0;
   }
-  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, 0, 0.0, dsum, 0ull, A.tol, false, s_red, &s_flag);
+  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, 0, 0.0, dsum, 0ull, A.tol, 0.0, false, s_red, &s_flag);
 }
 
 constexpr int pr_min_blocks(int threads) { return threads >= 1024 ? 1 : (threads >= 512 ? 2 : 4); }
@@ -483,8 +485,8 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
     rb = nb;
     ti = tn;
   }
-  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol, true, s_red,
-              &s_flag);
+  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol, A.stall, true,
+              s_red, &s_flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -780,17 +782,26 @@ static int pr_autotune(Graph* g, const PrArgs<OffT, CT>& A0, uint32_t V, cudaStr
   return ZOGCU_OK;
 }
 
+// FP32-phase switch: the FP32 contributions carry relative rounding ~6e-8, so
+// the L1 step of the FP32 iterates floors near 1e-7; the FP32 phase stops at
+// kMixedSwitchTol or when the step stops shrinking (kMixedStall), and the FP64
+// polish continues from its vector to the caller's tolerance.
+constexpr double kMixedSwitchTol = 1e-6;
+constexpr double kMixedStall = 0.97;
+
 template <typename OffT>
-static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double tol, const zogcu_pr_opts* o,
-                             double* out, zogcu_stats* stats, cudaStream_t s) {
+static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol, const zogcu_pr_opts* o, double* out,
+                        zogcu_stats* stats, cudaStream_t s) {
   const PrSchedule& P = g->pr;
   const uint32_t V = g->V;
   const bool dev_ptrs = o && o->device_pointers;
+  const bool mixed = o && o->precision == ZOGCU_PREC_MIXED;
   // workspace sized for every configuration's schedule
   ZOGCU_TRY(ensure_task_list(g, 128, s));
   ZOGCU_TRY(ensure_task_list(g, 256, s));
   const uint32_t max_tasks = std::max(P.lists[0].num_tasks, P.lists[1].num_tasks);
   PrWork W;
+  DevBuf cf0, cf1;
   ZOGCU_TRY(W.x0.alloc((size_t)V * 8, s));
   ZOGCU_TRY(W.x1.alloc((size_t)V * 8, s));
   ZOGCU_TRY(W.c0.alloc((size_t)V * 8 + 16, s));
@@ -803,6 +814,12 @@ static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double
   ZOGCU_CUDA(cudaMemsetAsync(W.lcnt.ptr, 0, W.lcnt.bytes, s));
   ZOGCU_CUDA(cudaMemsetAsync(W.c0.ptr, 0, W.c0.bytes, s));
   ZOGCU_CUDA(cudaMemsetAsync(W.c1.ptr, 0, W.c1.bytes, s));
+  if (mixed) {
+    ZOGCU_TRY(cf0.alloc((size_t)V * 4 + 16, s));
+    ZOGCU_TRY(cf1.alloc((size_t)V * 4 + 16, s));
+    ZOGCU_CUDA(cudaMemsetAsync(cf0.ptr, 0, cf0.bytes, s));
+    ZOGCU_CUDA(cudaMemsetAsync(cf1.ptr, 0, cf1.bytes, s));
+  }
 
   PrArgs<OffT, double> A{};
   A.off = P.off.as<OffT>();
@@ -821,6 +838,7 @@ static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double
   A.damping = damping;
   A.n_f = (double)g->n_live;
   A.tol = tol;
+  A.stall = 0.0;
 
   {
     PrArgs<OffT, double> At = A;
@@ -847,11 +865,27 @@ static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double
   }
 
   EventTimer tm;
-  uint64_t launches = 0;
-  ZOGCU_TRY(tm.start(s));
-  ZOGCU_TRY((pr_launch_chain<OffT, double>(g, cfg, A, V, given, max_iter, s, &launches)));
-  ZOGCU_TRY(tm.stop(s));
+  uint64_t launches = 0, it32 = 0;
   PrState hs;
+  ZOGCU_TRY(tm.start(s));
+  if (mixed && max_iter > 0) {
+    // ---- FP32 phase: x in FP64, contributions in FP32 -----------------------
+    PrArgs<OffT, float> Af{};
+    std::memcpy(&Af, &A, sizeof(Af));  // same layout; only the contribution pointers differ in type
+    Af.c0 = cf0.as<float>();
+    Af.c1 = cf1.as<float>();
+    Af.tol = std::max(tol, kMixedSwitchTol);
+    Af.stall = kMixedStall;
+    ZOGCU_TRY((pr_launch_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches)));
+    ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    it32 = hs.iter;
+    // ---- FP64 polish from the FP32 phase's last vector ----------------------
+    if (it32 & 1ull) std::swap(A.x0, A.x1);
+    given = 1;
+  }
+  ZOGCU_TRY((pr_launch_chain<OffT, double>(g, cfg, A, V, given, max_iter - it32, s, &launches)));
+  ZOGCU_TRY(tm.stop(s));
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   const double* result = (hs.iter & 1ull) ? A.x1 : A.x0;
@@ -862,19 +896,21 @@ static int run_pagerank_fp64(Graph* g, double damping, uint64_t max_iter, double
   ZOGCU_CUDA(cudaMemcpyAsync(out, unperm, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   if (stats) {
-    stats->iterations = hs.iter;
+    stats->iterations = it32 + hs.iter;
     stats->residual = hs.l1;
     stats->elapsed_ms = tm.ms();
-    const double per_iter = 4.0 * (double)g->E + (double)sizeof(OffT) * ((double)V + 1) + 36.0 * (double)V;
-    stats->bytes_moved = per_iter * (double)hs.iter;
+    const double per_iter64 = 4.0 * (double)g->E + (double)sizeof(OffT) * ((double)V + 1) + 36.0 * (double)V;
+    const double per_iter32 = per_iter64 - 8.0 * (double)V;  // c read and written as 4 bytes
+    stats->bytes_moved = per_iter64 * (double)hs.iter + per_iter32 * (double)it32;
     stats->launches = launches;
-    stats->polish_iterations = 0;
+    stats->polish_iterations = mixed ? hs.iter : 0;
     stats->kernel_config = (uint32_t)cfg;
   }
   return ZOGCU_OK;
 }
 
 }  // namespace zogcu
+
 
 using namespace zogcu;
 
@@ -910,8 +946,8 @@ int zogcu_pagerank_ex(zogcu_graph* G, double damping, uint64_t max_iterations, d
   ZOGCU_TRY(sg.init(opts ? opts->stream : nullptr));
   ZOGCU_TRY(ensure_pr_schedule(g, sg.s));
   if (g->offsets32)
-    return run_pagerank_fp64<uint32_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
-  return run_pagerank_fp64<uint64_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
+    return run_pagerank<uint32_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
+  return run_pagerank<uint64_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
 }
 
 int zogcu_pagerank(zogcu_graph* G, double damping, uint64_t max_iterations, double tolerance, double* out_scores,
