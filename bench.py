@@ -297,7 +297,8 @@ def run_zog(args):
     # ---------------- precision form: FP32 SpMV + FP64 polish ----------------
     mixed = None
     if not args.no_mixed:
-        x64 = out.clone()
+        x64 = torch.empty_like(out)
+        G.pagerank_device(x64.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)  # the FP64 result
         outm = torch.empty_like(out)
         for _ in range(args.warmup):
             stm = G.pagerank_device(outm.data_ptr(), DAMPING, MAX_ITER, TOL, precision=N.PREC_MIXED, stream=sp)
@@ -456,8 +457,9 @@ def main():
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--bc-scale", type=int, default=BC_SCALE, help="R-MAT scale of the Brandes graph")
-    ap.add_argument("--ref-pr-iterations", type=int, default=128,
-                    help="iterations the full solve takes (the GPU arm reports the measured count)")
+    ap.add_argument("--ref-pr-iterations", type=int, default=28,
+                    help="iterations the full solve takes on the benchmark graph: 28 for the seeded scale-24 "
+                         "R-MAT (the GPU arm measures the same count, since both follow the reference iteration)")
     args = ap.parse_args()
     if args.pr_scale != PR_SCALE:
         PR_SCALE, PR_SEED = args.pr_scale, 1000 + args.pr_scale
