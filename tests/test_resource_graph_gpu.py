@@ -138,3 +138,32 @@ def test_node_not_found_error(native):
     with pytest.raises(zog._native.ZogCudaError) as ei:
         zog._native.Graph.from_edges(3, [0, 5], [1, 2])
     assert ei.value.status == 2
+
+
+# ---- copy-in/copy-out API (lib/zog/centrality.ex), test/centrality_test.exs --
+
+def test_centrality_betweenness_known_answers(native):
+    """centrality_test.exs:11-51."""
+    C = zog.Centrality
+    s = C.betweenness_unweighted(zog.directed().add_edge("A", "B", 1.0).add_edge("B", "C", 1.0))
+    assert s["B"] > s["A"] and s["B"] > s["C"] and s["A"] == 0.0 and s["C"] == 0.0
+    b = zog.undirected()
+    for leaf in "abc":
+        b.add_edge("center", leaf, 1.0)
+    s = C.betweenness_unweighted(b)
+    assert s["center"] > 0.0 and all(s[x] == 0.0 for x in "abc")
+    assert C.betweenness_unweighted(zog.directed()) == {}
+    assert C.betweenness_unweighted(zog.directed().add_node("A")) == {"A": 0.0}
+
+
+def test_centrality_pagerank_known_answers(native, oracle):
+    """centrality_test.exs:137-163, and equality with the resource API."""
+    C = zog.Centrality
+    s = C.pagerank(zog.directed().add_edge("A", "B", 1.0).add_edge("C", "B", 1.0))
+    assert s["B"] > s["A"] and s["B"] > s["C"]
+    chain = zog.directed().add_edge("A", "B", 1.0).add_edge("B", "C", 1.0)
+    for d in (0.85, 0.99):
+        assert C.pagerank(chain, damping=d)["A"] > 0.0
+    g = RG.new(chain)
+    assert RG.pagerank(g, damping=0.99) == C.pagerank(chain, damping=0.99)
+    RG.destroy(g)

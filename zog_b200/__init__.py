@@ -13,7 +13,8 @@ zog_b200.build``); this package is the host-side mirror of the reference's
 Elixir API and holds no CPU implementation of either algorithm.
 """
 from . import _native
+from . import centrality as Centrality
 from . import resource_graph as ResourceGraph
 from .soa import SoA, directed, undirected
 
-__all__ = ["ResourceGraph", "SoA", "directed", "undirected", "_native"]
+__all__ = ["Centrality", "ResourceGraph", "SoA", "directed", "undirected", "_native"]

@@ -1,0 +1,52 @@
+"""Host-side mirror of ``Zog.Centrality`` (``lib/zog/centrality.ex``), the
+copy-in/copy-out API: every call builds the device graph from the builder's
+edge arrays, runs the GPU kernel and frees the graph again -- the resource
+pattern of ``Zog.ResourceGraph`` without keeping the resource.
+
+=====================================  =========================================
+this module                            reference
+=====================================  =========================================
+``pagerank(builder, ...)``             ``pagerank/2``                centrality.ex:237-247
+``betweenness_unweighted(builder)``    ``betweenness_unweighted/1``  centrality.ex:191-197
+=====================================  =========================================
+
+Scores map labels in insertion order to values (``map_scores``,
+centrality.ex:319-324); betweenness of undirected builders is halved first
+(centrality.ex:326-330).
+"""
+from __future__ import annotations
+
+from . import _native
+from .soa import SoA
+
+
+def _map_scores(builder: SoA, scores):
+    """centrality.ex:319-324: all_labels zipped with the scores."""
+    return {lbl: float(s) for lbl, s in zip(builder.all_labels(), scores)}
+
+
+def _graph(builder: SoA) -> _native.Graph:
+    frm, to, w = builder.to_edge_arrays()
+    return _native.Graph.from_edges(builder.node_count(), frm, to, w)
+
+
+def pagerank(builder: SoA, damping: float = 0.85, max_iterations: int = 100, tolerance: float = 0.0001):
+    """centrality.ex:237-247 (defaults 0.85 / 100 / 1e-4)."""
+    g = _graph(builder)
+    try:
+        scores = g.pagerank(damping, max_iterations, tolerance)
+    finally:
+        g.destroy()
+    return _map_scores(builder, scores)
+
+
+def betweenness_unweighted(builder: SoA):
+    """centrality.ex:191-197: unnormalised; halved for undirected builders."""
+    g = _graph(builder)
+    try:
+        scores = g.betweenness_unweighted()
+    finally:
+        g.destroy()
+    if builder.kind == "undirected":
+        scores = scores * 0.5
+    return _map_scores(builder, scores)
