@@ -183,6 +183,30 @@ ZOGCU_API int zogcu_pagerank_ex(zogcu_graph* g, double damping, uint64_t max_ite
                       double tolerance, const zogcu_pr_opts* opts, double* out_scores,
                       zogcu_stats* stats);
 
+/* ---- SpMV centralities (the same schedule and gather path) ------------- */
+
+/* Replaces the NIF `katz(res, alpha, beta, max_iterations, tolerance)`
+ * (.zig:183-192 -> centrality.zig:1190-1251): start beta, x' = alpha * sum of
+ * in-neighbours + beta, stop when the L1 step < tolerance. */
+ZOGCU_API int zogcu_katz(zogcu_graph* g, double alpha, double beta, uint64_t max_iterations,
+                         double tolerance, double* out_scores, zogcu_stats* stats);
+
+/* Replaces the NIF `alpha_centrality(res, alpha, initial, max_iterations,
+ * tolerance)` (.zig:194-203 -> centrality.zig:1262-1321): start `initial`,
+ * x' = alpha * sum of in-neighbours, L1 stopping rule. */
+ZOGCU_API int zogcu_alpha_centrality(zogcu_graph* g, double alpha, double initial,
+                                     uint64_t max_iterations, double tolerance, double* out_scores,
+                                     zogcu_stats* stats);
+
+/* Replaces the NIF `eigenvector(res, max_iterations, tolerance)` (.zig:172-181
+ * -> centrality.zig:1050-1180): start 1 + i/1000, in-neighbour sums, L2
+ * normalisation, zero-vector fallback 1/sqrt(n), oscillation exit with the
+ * normalised average, L2 stopping rule.  stats->reserved receives how it
+ * ended (0 max iterations, 1 converged, 2 zero vector, 3 oscillation).
+ * Graphs with deleted nodes are not supported (ZOGCU_ERR_INVALID_ARGUMENT). */
+ZOGCU_API int zogcu_eigenvector(zogcu_graph* g, uint64_t max_iterations, double tolerance,
+                                double* out_scores, zogcu_stats* stats);
+
 /* PageRank that allocates nothing, for callers that cannot call cudaMalloc
  * (a process whose device memory is owned by another runtime, or code that
  * must not allocate while it runs).  No counterpart in the reference: it is an

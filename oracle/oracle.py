@@ -58,6 +58,12 @@ def lib():
     L.og_pagerank.argtypes = [vp, C.c_double, C.c_uint64, C.c_double, _f64p,
                               C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
     L.og_betweenness_unweighted.argtypes = [vp, _f64p, C.POINTER(C.c_uint32)]
+    L.og_katz.argtypes = [vp, C.c_double, C.c_double, C.c_uint64, C.c_double, _f64p,
+                          C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    L.og_alpha_centrality.argtypes = [vp, C.c_double, C.c_double, C.c_uint64, C.c_double, _f64p,
+                                      C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    L.og_eigenvector.argtypes = [vp, C.c_uint64, C.c_double, _f64p, C.POINTER(C.c_uint64),
+                                 C.POINTER(C.c_int)]
     L.og_betweenness_sources.argtypes = [vp, _u32p, C.c_uint64, _f64p, C.POINTER(C.c_uint32)]
     L.og_bfs.argtypes = [vp, C.c_uint32, _u32p, _u64p, C.POINTER(C.c_uint32)]
     L.og_pagerank_csr.restype = C.c_uint64
@@ -160,6 +166,28 @@ class ArrayGraph:
         it = C.c_uint64(0); l1 = C.c_double(0)
         lib().og_pagerank(self._h, damping, max_iterations, tolerance, out, C.byref(it), C.byref(l1))
         return out[: self.node_capacity], int(it.value), float(l1.value)
+
+    def katz(self, alpha=0.1, beta=1.0, max_iterations=100, tolerance=1e-4):
+        """centrality.zig:1190-1251."""
+        out = np.zeros(max(self.node_capacity, 1), np.float64)
+        it = C.c_uint64(0); l1 = C.c_double(0)
+        lib().og_katz(self._h, alpha, beta, max_iterations, tolerance, out, C.byref(it), C.byref(l1))
+        return out[: self.node_capacity], int(it.value), float(l1.value)
+
+    def alpha_centrality(self, alpha=0.5, initial=1.0, max_iterations=100, tolerance=1e-4):
+        """centrality.zig:1262-1321."""
+        out = np.zeros(max(self.node_capacity, 1), np.float64)
+        it = C.c_uint64(0); l1 = C.c_double(0)
+        lib().og_alpha_centrality(self._h, alpha, initial, max_iterations, tolerance, out, C.byref(it),
+                                  C.byref(l1))
+        return out[: self.node_capacity], int(it.value), float(l1.value)
+
+    def eigenvector(self, max_iterations=100, tolerance=1e-4):
+        """centrality.zig:1050-1180; returns (scores, iterations, how)."""
+        out = np.zeros(max(self.node_capacity, 1), np.float64)
+        it = C.c_uint64(0); how = C.c_int(0)
+        lib().og_eigenvector(self._h, max_iterations, tolerance, out, C.byref(it), C.byref(how))
+        return out[: self.node_capacity], int(it.value), int(how.value)
 
     def betweenness_unweighted(self):
         out = np.zeros(max(self.node_capacity, 1), np.float64)

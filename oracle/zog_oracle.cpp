@@ -200,6 +200,122 @@ void pagerank_arraygraph(const ArrayGraph& g, double damping, uint64_t max_iter,
 }
 
 // ---------------------------------------------------------------------------
+// katz (centrality.zig:1190-1251) and alphaCentrality (:1262-1321): plain
+// in-neighbour sums (buildInNeighbors order, utils.zig:52-74: sources
+// ascending), L1 step, swap, stop when the step < tol.
+// ---------------------------------------------------------------------------
+void linear_centrality(const ArrayGraph& g, double alpha, double beta, double start, uint64_t max_iter,
+                       double tol, double* out, uint64_t* iters_out, double* l1_out) {
+  const size_t V = g.node_capacity();
+  std::vector<uint32_t> nodes = g.collect_nodes();
+  for (size_t i = 0; i < V; ++i) out[i] = 0.0;
+  *iters_out = 0;
+  *l1_out = 0.0;
+  if (nodes.empty()) return;
+  std::vector<std::vector<uint32_t>> in_nb(V);
+  for (uint32_t from : nodes) g.for_each_successor(from, [&](uint32_t t) { in_nb[t].push_back(from); });
+  std::vector<double> curr(V, 0.0), next(V, 0.0);
+  for (uint32_t v : nodes) curr[v] = start;
+  uint64_t it = 0;
+  double l1 = 0.0;
+  while (it < max_iter) {
+    for (uint32_t v : nodes) {
+      double sum = 0.0;
+      for (uint32_t u : in_nb[v]) sum += curr[u];
+      next[v] = alpha * sum + beta;  // beta = 0 for alpha centrality
+    }
+    l1 = 0.0;
+    for (uint32_t v : nodes) l1 += std::fabs(next[v] - curr[v]);
+    std::swap(curr, next);
+    it += 1;
+    if (l1 < tol) break;
+  }
+  for (uint32_t v : nodes) out[v] = curr[v];
+  *iters_out = it;
+  *l1_out = l1;
+}
+
+// eigenvector (centrality.zig:1050-1180): start 1 + i/1000 (i = position in
+// the ascending live-node list), new = sum of in-neighbours, L2-normalise,
+// degenerate zero vector -> uniform 1/sqrt(n), oscillation test against the
+// vector two steps back (-> normalised average), stop when the L2 step < tol,
+// else rotate; after max_iterations return the last vector.  The reference
+// sums the squared norm in hash-map order; this restatement sums in node
+// order.  *how: 0 = converged or max_iterations, 1 = oscillation, 2 = zero.
+void eigenvector_arraygraph(const ArrayGraph& g, uint64_t max_iter, double tol, double* out,
+                            uint64_t* iters_out, int* how) {
+  const size_t V = g.node_capacity();
+  std::vector<uint32_t> nodes = g.collect_nodes();
+  const size_t n = nodes.size();
+  for (size_t i = 0; i < V; ++i) out[i] = 0.0;
+  *iters_out = 0;
+  *how = 0;
+  if (n <= 1) {
+    for (uint32_t v : nodes) out[v] = 1.0;
+    return;
+  }
+  std::vector<std::vector<uint32_t>> in_nb(V);
+  for (uint32_t from : nodes) g.for_each_successor(from, [&](uint32_t t) { in_nb[t].push_back(from); });
+  std::vector<double> curr(V, 0.0), pp(V, 0.0), nw(V, 0.0);
+  bool have_pp = false;
+  for (size_t i = 0; i < n; ++i) curr[nodes[i]] = 1.0 + (double)i / 1000.0;
+  uint64_t it = 0;
+  while (it < max_iter) {
+    for (uint32_t v : nodes) {
+      double sum = 0.0;
+      for (uint32_t u : in_nb[v]) sum += curr[u];
+      nw[v] = sum;
+    }
+    double l2 = 0.0;
+    for (uint32_t v : nodes) l2 += nw[v] * nw[v];
+    if (l2 > 0.0) {
+      const double norm = std::sqrt(l2);
+      for (uint32_t v : nodes) nw[v] /= norm;
+    }
+    if (l2 == 0.0) {
+      const double u = 1.0 / std::sqrt((double)n);
+      for (uint32_t v : nodes) out[v] = u;
+      *iters_out = it + 1;
+      *how = 2;
+      return;
+    }
+    double d = 0.0;
+    for (uint32_t v : nodes) d += (nw[v] - curr[v]) * (nw[v] - curr[v]);
+    if (d > 0.0) d = std::sqrt(d);
+    if (have_pp) {
+      double d2 = 0.0;
+      for (uint32_t v : nodes) d2 += (nw[v] - pp[v]) * (nw[v] - pp[v]);
+      if (d2 > 0.0) d2 = std::sqrt(d2);
+      if (d2 < tol) {
+        double a2 = 0.0;
+        for (uint32_t v : nodes) {
+          out[v] = (nw[v] + curr[v]) / 2.0;
+          a2 += out[v] * out[v];
+        }
+        if (a2 > 0.0) {
+          const double an = std::sqrt(a2);
+          for (uint32_t v : nodes) out[v] /= an;
+        }
+        *iters_out = it + 1;
+        *how = 1;
+        return;
+      }
+    }
+    if (d < tol) {
+      for (uint32_t v : nodes) out[v] = nw[v];
+      *iters_out = it + 1;
+      return;
+    }
+    std::swap(pp, curr);  // prev_prev <- curr
+    std::swap(curr, nw);  // curr <- new
+    have_pp = true;
+    it += 1;
+  }
+  for (uint32_t v : nodes) out[v] = curr[v];
+  *iters_out = it;
+}
+
+// ---------------------------------------------------------------------------
 // betweennessUnweighted, ArrayGraph branch   centrality.zig:687-798
 // Runs the per-source body for the given sources (all live nodes ascending
 // for the reference call).
@@ -369,6 +485,18 @@ void og_successor_csr(void* h, uint64_t* off, uint32_t* col) {
 void og_pagerank(void* h, double damping, uint64_t max_iter, double tol, double* out,
                  uint64_t* iters, double* l1) {
   pagerank_arraygraph(*(ArrayGraph*)h, damping, max_iter, tol, out, iters, l1);
+}
+
+void og_katz(void* h, double alpha, double beta, uint64_t max_iter, double tol, double* out, uint64_t* iters,
+             double* l1) {
+  linear_centrality(*(ArrayGraph*)h, alpha, beta, beta, max_iter, tol, out, iters, l1);
+}
+void og_alpha_centrality(void* h, double alpha, double initial, uint64_t max_iter, double tol, double* out,
+                         uint64_t* iters, double* l1) {
+  linear_centrality(*(ArrayGraph*)h, alpha, 0.0, initial, max_iter, tol, out, iters, l1);
+}
+void og_eigenvector(void* h, uint64_t max_iter, double tol, double* out, uint64_t* iters, int* how) {
+  eigenvector_arraygraph(*(ArrayGraph*)h, max_iter, tol, out, iters, how);
 }
 
 void og_betweenness_unweighted(void* h, double* out, uint32_t* overflow) {

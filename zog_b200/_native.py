@@ -31,6 +31,7 @@ EXPORTS = (
     "zogcu_read_edgelist", "zogcu_graph_destroy", "zogcu_graph_info", "zogcu_graph_export_csr",
     "zogcu_free", "zogcu_pagerank", "zogcu_pagerank_ex", "zogcu_betweenness_unweighted",
     "zogcu_betweenness_unweighted_ex", "zogcu_bfs_sigma", "zogcu_pagerank_noalloc",
+    "zogcu_katz", "zogcu_alpha_centrality", "zogcu_eigenvector",
 )
 
 
@@ -109,6 +110,9 @@ def load(path: str | None = None):
         L.zogcu_betweenness_unweighted_ex.argtypes = [vp, C.POINTER(BcOpts), vp, C.POINTER(Stats)]
         L.zogcu_bfs_sigma.argtypes = [vp, vp, u64, vp, vp, C.POINTER(u32)]
         L.zogcu_pagerank_noalloc.argtypes = [vp, vp, vp, u32, u64, dbl, u64, dbl, vp, C.POINTER(Stats), vp]
+        L.zogcu_katz.argtypes = [vp, dbl, dbl, u64, dbl, vp, C.POINTER(Stats)]
+        L.zogcu_alpha_centrality.argtypes = [vp, dbl, dbl, u64, dbl, vp, C.POINTER(Stats)]
+        L.zogcu_eigenvector.argtypes = [vp, u64, dbl, vp, C.POINTER(Stats)]
         for name in EXPORTS:  # every other entry point returns a zogcu_status
             if name not in ("zogcu_status_string", "zogcu_last_error", "zogcu_free"):
                 getattr(L, name).restype = C.c_int
@@ -278,6 +282,29 @@ class Graph:
         o = BcOpts(C.sizeof(BcOpts), 0, _ptr(src), 0 if src is None else src.size, 1, 0, stream)
         check(load().zogcu_betweenness_unweighted_ex(self.handle, C.byref(o), out_ptr, C.byref(st)))
         return st.as_dict()
+
+    def katz(self, alpha=0.1, beta=1.0, max_iterations=100, tolerance=1e-4, stats=False):
+        V, _, _ = self.info()
+        res = np.zeros(max(V, 1), np.float64)
+        st = Stats()
+        check(load().zogcu_katz(self.handle, float(alpha), float(beta), int(max_iterations), float(tolerance),
+                                _ptr(res), C.byref(st)))
+        return (res[:V], st.as_dict()) if stats else res[:V]
+
+    def alpha_centrality(self, alpha=0.5, initial=1.0, max_iterations=100, tolerance=1e-4, stats=False):
+        V, _, _ = self.info()
+        res = np.zeros(max(V, 1), np.float64)
+        st = Stats()
+        check(load().zogcu_alpha_centrality(self.handle, float(alpha), float(initial), int(max_iterations),
+                                            float(tolerance), _ptr(res), C.byref(st)))
+        return (res[:V], st.as_dict()) if stats else res[:V]
+
+    def eigenvector(self, max_iterations=100, tolerance=1e-4, stats=False):
+        V, _, _ = self.info()
+        res = np.zeros(max(V, 1), np.float64)
+        st = Stats()
+        check(load().zogcu_eigenvector(self.handle, int(max_iterations), float(tolerance), _ptr(res), C.byref(st)))
+        return (res[:V], st.as_dict()) if stats else res[:V]
 
     def bfs_sigma(self, sources):
         V, _, _ = self.info()

@@ -8,6 +8,9 @@ this module                            reference
 =====================================  =========================================
 ``pagerank(builder, ...)``             ``pagerank/2``                centrality.ex:237-247
 ``betweenness_unweighted(builder)``    ``betweenness_unweighted/1``  centrality.ex:191-197
+``eigenvector(builder, ...)``          ``eigenvector/2``             centrality.ex:253-275
+``katz(builder, ...)``                 ``katz/2``                    centrality.ex:281-293
+``alpha_centrality(builder, ...)``     ``alpha_centrality/2``        centrality.ex:300-313
 =====================================  =========================================
 
 Scores map labels in insertion order to values (``map_scores``,
@@ -49,4 +52,42 @@ def betweenness_unweighted(builder: SoA):
         g.destroy()
     if builder.kind == "undirected":
         scores = scores * 0.5
+    return _map_scores(builder, scores)
+
+
+def eigenvector(builder: SoA, max_iterations: int = 100, tolerance: float = 0.0001):
+    """centrality.ex:253-275, including the zero-vector fallback to a uniform
+    1/sqrt(n) when every score is 0.0 and there is more than one node."""
+    g = _graph(builder)
+    try:
+        scores = g.eigenvector(max_iterations, tolerance)
+    finally:
+        g.destroy()
+    mapped = _map_scores(builder, scores)
+    n = builder.node_count()
+    if n > 1 and all(v == 0.0 for v in mapped.values()):
+        u = 1.0 / (n ** 0.5)
+        mapped = {k: u for k in mapped}
+    return mapped
+
+
+def katz(builder: SoA, alpha: float = 0.1, beta: float = 1.0, max_iterations: int = 100,
+         tolerance: float = 0.0001):
+    """centrality.ex:281-293."""
+    g = _graph(builder)
+    try:
+        scores = g.katz(alpha, beta, max_iterations, tolerance)
+    finally:
+        g.destroy()
+    return _map_scores(builder, scores)
+
+
+def alpha_centrality(builder: SoA, alpha: float = 0.5, initial: float = 1.0, max_iterations: int = 100,
+                     tolerance: float = 0.0001):
+    """centrality.ex:300-313."""
+    g = _graph(builder)
+    try:
+        scores = g.alpha_centrality(alpha, initial, max_iterations, tolerance)
+    finally:
+        g.destroy()
     return _map_scores(builder, scores)

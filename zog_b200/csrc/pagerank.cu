@@ -107,7 +107,13 @@ struct PrArgs {
   double tol;
   double stall;          // > 0: also stop once l1 > stall * previous l1
   unsigned long long max_iter;
+  double ka, kb;         // katz: alpha, beta; alpha centrality: alpha
+  double* x2;            // eigenvector: third rotating buffer
 };
+
+// Epilogue modes of the iteration kernel (all share the schedule and the
+// gather path; the non-PageRank modes gather x itself).
+enum : int { kModePageRank = 0, kModeKatz = 1, kModeAlpha = 2, kModeEigen = 3 };
 
 // ---- cache-policy loads ------------------------------------------------------
 __device__ __forceinline__ uint64_t policy_evict_last() {
@@ -250,6 +256,11 @@ __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta,
   cta_sum2(a, b, s_red);
   if (threadIdx.x == 0) {
     st->sink = b;
+    if (stall < 0.0) {  // sum-only publication (eigenvector SpMV: b = sum of squares)
+      __threadfence();
+      st->done_ctas = 0;
+      return;
+    }
     if (set_l1) {
       const bool stalled = stall > 0.0 && next_iter > 2 && a > stall * st->l1;
       st->l1 = a;
@@ -309,7 +320,27 @@ __global__ void __launch_bounds__(256) pr_init_kernel(PrArgs<OffT, CT> A, uint32
 
 constexpr int pr_min_blocks(int threads) { return threads >= 1024 ? 1 : (threads >= 512 ? 2 : 4); }
 
-template <typename OffT, typename CT, int THREADS, int NNZ>
+// Row epilogue of the non-PageRank modes (katz: alpha*sum + beta,
+// centrality.zig:1215; alpha centrality: alpha*sum, :1287; eigenvector: the raw
+// sum, with its square added to the norm accumulator).
+template <int MODE>
+__device__ __forceinline__ void lin_row_epilogue(uint32_t v, double sum, uint32_t deg, double xo, double ka, double kb,
+                                                 double* __restrict__ xnxt, double& l1, double& acc) {
+  if (deg == kDeletedDegree) return;
+  double xn;
+  if constexpr (MODE == kModeKatz) {
+    xn = __dadd_rn(__dmul_rn(ka, sum), kb);
+  } else if constexpr (MODE == kModeAlpha) {
+    xn = __dmul_rn(ka, sum);
+  } else {
+    xn = sum;
+    acc += xn * xn;
+  }
+  if constexpr (MODE != kModeEigen) l1 += fabs(xn - xo);
+  xnxt[v] = xn;
+}
+
+template <typename OffT, typename CT, int THREADS, int NNZ, int MODE = kModePageRank>
 __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kernel(PrArgs<OffT, CT> A) {
   constexpr int WARPS = THREADS / 32;
   constexpr int VPL = (NNZ / 4 + 1 + 31) / 32;  // 16-byte index vectors per lane in a row block
@@ -324,13 +355,37 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
   const double sink = *(volatile const double*)&st->sink;
 
   const int par = (int)(iter & 1ull);
-  const double* __restrict__ xcur = par ? A.x1 : A.x0;
-  double* __restrict__ xnxt = par ? A.x0 : A.x1;
-  const CT* __restrict__ ccur = par ? A.c1 : A.c0;
-  CT* __restrict__ cnxt = par ? A.c0 : A.c1;
+  const double* __restrict__ xcur;
+  double* __restrict__ xnxt;
+  const CT* __restrict__ ccur;
+  CT* __restrict__ cnxt;
+  if constexpr (MODE == kModeEigen) {
+    const int k3 = (int)(iter % 3ull);
+    xcur = k3 == 0 ? A.x0 : (k3 == 1 ? A.x1 : A.x2);
+    xnxt = k3 == 0 ? A.x1 : (k3 == 1 ? A.x2 : A.x0);
+    ccur = reinterpret_cast<const CT*>(xcur);
+    cnxt = nullptr;
+  } else if constexpr (MODE != kModePageRank) {
+    xcur = par ? A.x1 : A.x0;
+    xnxt = par ? A.x0 : A.x1;
+    ccur = reinterpret_cast<const CT*>(xcur);
+    cnxt = nullptr;
+  } else {
+    xcur = par ? A.x1 : A.x0;
+    xnxt = par ? A.x0 : A.x1;
+    ccur = par ? A.c1 : A.c0;
+    cnxt = par ? A.c0 : A.c1;
+  }
   const double tele_u = (1.0 - A.damping) / A.n_f;
   const bool personalised = A.teleport != nullptr;
   const double damping = A.damping, n_f = A.n_f;
+  const double ka = A.ka, kb = A.kb;
+  auto epilogue = [&](uint32_t v, double s, uint32_t dg, double xo, double tp, double& el1, double& eacc) {
+    if constexpr (MODE == kModePageRank)
+      pr_row_epilogue(v, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, el1, eacc);
+    else
+      lin_row_epilogue<MODE>(v, s, dg, xo, ka, kb, xnxt, el1, eacc);
+  };
 
   // ---- dynamic shared memory: [hub | per-warp staging] ----------------------
   const uint32_t nhub = A.hub;
@@ -424,7 +479,7 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
         if (is_short) {
           double s = 0.0;
           for (uint32_t k = b; k < en; ++k) s += sv[k];  // ascending source order
-          pr_row_epilogue(r0 + i, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
+          epilogue(r0 + i, s, dg, xo, tp, l1, dsum);
         }
         unsigned med = __ballot_sync(0xffffffffu, valid && !is_short);
         while (med) {
@@ -434,8 +489,7 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
           double s = 0.0;
           for (uint32_t j = bk + lane; j < ek; j += 32) s += sv[j];
           s = warp_sum(s);
-          if (lane == k)
-            pr_row_epilogue(r0 + i, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
+          if (lane == k) epilogue(r0 + i, s, dg, xo, tp, l1, dsum);
         }
       }
       __syncwarp();
@@ -451,8 +505,7 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
       }
       if (kind == kTaskRow) {
         const double s = warp_range_sum(A.col, ccur, hub, nhub, ra, rb, lane, pol_arc, pol_c);
-        if (lane == 0)
-          pr_row_epilogue(row, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
+        if (lane == 0) epilogue(row, s, dg, xo, tp, l1, dsum);
       } else {
         const uint32_t c = t.b & 0xFFFFu;
         const uint32_t nch = (uint32_t)((rb - ra + kLongChunk - 1) / kLongChunk);
@@ -472,7 +525,7 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
           double tot = 0.0;
           for (uint32_t k = 0; k < nch; ++k) tot += __ldcg(A.chunk_part + (first + k));
           double rl1 = 0.0, rds = 0.0;
-          pr_row_epilogue(row, tot, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, rl1, rds);
+          epilogue(row, tot, dg, xo, tp, rl1, rds);
           A.long_part[2 * (size_t)first] = rl1;
           A.long_part[2 * (size_t)first + 1] = rds;
           A.long_cnt[first] = 0;
@@ -485,8 +538,8 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
     rb = nb;
     ti = tn;
   }
-  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol, A.stall, true,
-              s_red, &s_flag);
+  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol,
+              MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag);
 }
 
 // ---------------------------------------------------------------------------
@@ -909,7 +962,262 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   return ZOGCU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Katz, alpha and eigenvector centrality (centrality.zig:1050-1321): the same
+// schedule and gather path as PageRank, gathering x itself.
+// ---------------------------------------------------------------------------
+__global__ void k_fill_start(const uint32_t* __restrict__ deg, const uint32_t* __restrict__ perm, uint32_t V,
+                             int eigen, double start, double* __restrict__ x) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < V; p += (uint64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (deg[p] != kDeletedDegree) v = eigen ? 1.0 + (double)perm[p] / 1000.0 : start;  // :1076-1078
+    x[p] = v;
+  }
+}
+
+// Eigenvector step 2: normalise the raw sums by their L2 norm, measure the
+// L2 step against the current vector and the one two steps back, and decide
+// (converged = 1 step < tol, 2 zero vector, 3 oscillation) on the device.
+__global__ void __launch_bounds__(256) k_eigen_normalise(PrArgs<uint32_t, double> A, const uint32_t* __restrict__ deg,
+                                                         uint32_t V) {
+  __shared__ double s_red[16];
+  __shared__ int s_flag;
+  PrState* st = A.st;
+  const unsigned long long iter = *(volatile unsigned long long*)&st->iter;
+  if (*(volatile int*)&st->converged || iter >= A.max_iter) return;
+  const double norm2 = *(volatile double*)&st->sink;
+  if (norm2 == 0.0) {  // degenerate: every CTA returns, block 0 records it
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->converged = 2;
+      st->iter = iter + 1;
+    }
+    return;
+  }
+  const int k3 = (int)(iter % 3ull);
+  const double* cur = k3 == 0 ? A.x0 : (k3 == 1 ? A.x1 : A.x2);
+  double* nw = k3 == 0 ? A.x1 : (k3 == 1 ? A.x2 : A.x0);
+  const double* pp = k3 == 0 ? A.x2 : (k3 == 1 ? A.x0 : A.x1);
+  const double norm = sqrt(norm2);
+  double d1 = 0.0, d2 = 0.0;
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < V; p += (uint64_t)gridDim.x * blockDim.x) {
+    if (deg[p] == kDeletedDegree) continue;
+    const double xn = nw[p] / norm;
+    nw[p] = xn;
+    const double a = xn - cur[p];
+    d1 += a * a;
+    if (iter >= 1) {
+      const double b = xn - pp[p];
+      d2 += b * b;
+    }
+  }
+  cta_sum2(d1, d2, s_red);
+  if (threadIdx.x == 0) {
+    A.cta_part[2 * blockIdx.x] = d1;
+    A.cta_part[2 * blockIdx.x + 1] = d2;
+    __threadfence();
+    s_flag = (atomicAdd(&st->done_ctas, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_flag) return;
+  __threadfence();
+  double D1 = 0.0, D2 = 0.0;
+  for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+    D1 += __ldcg(A.cta_part + 2 * i);
+    D2 += __ldcg(A.cta_part + 2 * i + 1);
+  }
+  cta_sum2(D1, D2, s_red);
+  if (threadIdx.x == 0) {
+    const double step = D1 > 0.0 ? sqrt(D1) : 0.0;
+    const double step2 = D2 > 0.0 ? sqrt(D2) : 0.0;
+    const bool osc = iter >= 1 && step2 < A.tol;  // :1136-1150
+    st->l1 = step;
+    st->converged = osc ? 3 : (step < A.tol ? 1 : 0);
+    st->iter = iter + 1;
+    __threadfence();
+    st->done_ctas = 0;
+  }
+}
+
+// Normalised average of two vectors (the oscillation exit, :1152-1172), in
+// two passes: squares into CTA partials, then one CTA folds them and scales.
+__global__ void __launch_bounds__(256) k_avg_squares(const double* __restrict__ a, const double* __restrict__ b,
+                                                     const uint32_t* __restrict__ deg, uint32_t V,
+                                                     double* __restrict__ avg, double* __restrict__ part) {
+  __shared__ double s_red[16];
+  double s = 0.0, unused = 0.0;
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < V; p += (uint64_t)gridDim.x * blockDim.x) {
+    const double v = deg[p] == kDeletedDegree ? 0.0 : (a[p] + b[p]) / 2.0;
+    avg[p] = v;
+    s += v * v;
+  }
+  cta_sum2(s, unused, s_red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+__global__ void __launch_bounds__(256) k_avg_scale(double* __restrict__ avg, uint32_t V, const double* __restrict__ part,
+                                                   uint32_t nparts) {
+  __shared__ double s_red[16];
+  __shared__ double s_norm;
+  double s = 0.0, unused = 0.0;
+  for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) s += part[i];
+  cta_sum2(s, unused, s_red);
+  if (threadIdx.x == 0) s_norm = s > 0.0 ? sqrt(s) : 1.0;
+  __syncthreads();
+  const double n = s_norm;
+  for (uint64_t p = threadIdx.x; p < V; p += blockDim.x) avg[p] /= n;
+}
+
+template <typename OffT, int MODE>
+static int run_linear(Graph* g, double ka, double kb, double start, uint64_t max_iter, double tol, double* out,
+                      bool dev_out, zogcu_stats* stats, cudaStream_t s) {
+  const uint32_t V = g->V;
+  ZOGCU_TRY(ensure_pr_schedule(g, s));
+  ZOGCU_TRY(ensure_task_list(g, 256, s));
+  const PrSchedule& P = g->pr;
+  const PrTaskList& L = P.lists[list_index(256)];
+  PrWork W;
+  DevBuf x2;
+  ZOGCU_TRY(W.x0.alloc((size_t)V * 8 + 16, s));
+  ZOGCU_TRY(W.x1.alloc((size_t)V * 8 + 16, s));
+  ZOGCU_TRY(x2.alloc((size_t)V * 8 + 16, s));
+  ZOGCU_TRY(W.part.alloc((size_t)std::max<int>(sm_count() * 8, 148 * 4) * 16, s));
+  ZOGCU_TRY(W.chunk.alloc((size_t)std::max<uint32_t>(L.num_tasks, 1) * 8, s));
+  ZOGCU_TRY(W.lcnt.alloc((size_t)std::max<uint32_t>(L.num_tasks, 1) * 4, s));
+  ZOGCU_TRY(W.lpart.alloc((size_t)std::max<uint32_t>(L.num_tasks, 1) * 16, s));
+  ZOGCU_TRY(W.stb.alloc(sizeof(PrState), s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.lcnt.ptr, 0, W.lcnt.bytes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.stb.ptr, 0, sizeof(PrState), s));
+  ZOGCU_CUDA(cudaMemsetAsync(W.x1.ptr, 0, W.x1.bytes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(x2.ptr, 0, x2.bytes, s));
+  k_fill_start<<<grid_1d(V), 256, 0, s>>>(P.deg.as<uint32_t>(), P.perm.as<uint32_t>(), V, MODE == kModeEigen ? 1 : 0,
+                                          start, W.x0.as<double>());
+  ZOGCU_CUDA(cudaGetLastError());
+  PrArgs<OffT, double> A{};
+  A.off = P.off.as<OffT>();
+  A.col = P.col.as<uint32_t>();
+  A.deg = P.deg.as<uint32_t>();
+  A.tasks = L.tasks.as<PrTask>();
+  A.long_first = L.long_first.as<uint32_t>();
+  A.ntasks = L.num_tasks;
+  A.nlong = L.num_long;
+  A.hub = 0;
+  A.x0 = W.x0.as<double>();
+  A.x1 = W.x1.as<double>();
+  A.x2 = x2.as<double>();
+  A.c0 = A.x0;
+  A.c1 = A.x1;
+  A.cta_part = W.part.as<double>();
+  A.chunk_part = W.chunk.as<double>();
+  A.long_cnt = W.lcnt.as<unsigned int>();
+  A.long_part = W.lpart.as<double>();
+  A.st = W.stb.as<PrState>();
+  A.n_f = (double)g->n_live;
+  A.tol = tol;
+  A.max_iter = max_iter;
+  A.ka = ka;
+  A.kb = kb;
+  auto fn = pr_iter_kernel<OffT, double, 256, 256, MODE>;
+  constexpr int cfg = 3;
+  const size_t dyn = PrLauncher<OffT, double>::staging_bytes(cfg);
+  static int grid = 0;
+  if (!grid) {
+    int per_sm = 0;
+    ZOGCU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, dyn));
+    grid = std::max(per_sm, 1) * sm_count();
+  }
+  int gr = grid;
+  const uint32_t need = (A.ntasks + 7) / 8;
+  if (need > 0 && (uint32_t)gr > need) gr = (int)need;
+  const unsigned gn = std::min(grid_1d(V), 148u * 4);
+  EventTimer tm;
+  ZOGCU_TRY(tm.start(s));
+  uint64_t launches = 1;
+  for (uint64_t k = 0; k < max_iter; ++k) {
+    fn<<<gr, 256, dyn, s>>>(A);
+    ++launches;
+    if constexpr (MODE == kModeEigen) {
+      if constexpr (sizeof(OffT) == 4) {
+        k_eigen_normalise<<<gn, 256, 0, s>>>(A, A.deg, V);
+        ++launches;
+      }
+    }
+  }
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_TRY(tm.stop(s));
+  PrState hs;
+  ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  double* X[3] = {A.x0, A.x1, A.x2};
+  double* result;
+  double* spare;
+  if (MODE == kModeEigen) {
+    result = X[hs.iter % 3];
+    spare = X[(hs.iter + 1) % 3];
+    if (hs.converged == 2) {  // zero vector: uniform 1/sqrt(n) (:1101-1112)
+      k_fill_start<<<grid_1d(V), 256, 0, s>>>(P.deg.as<uint32_t>(), P.perm.as<uint32_t>(), V, 0,
+                                              1.0 / std::sqrt((double)g->n_live), spare);
+      result = spare;
+      spare = X[(hs.iter + 2) % 3];
+    } else if (hs.converged == 3) {  // oscillation: normalised average of the last two
+      const double* prev = X[(hs.iter + 2) % 3];
+      k_avg_squares<<<gn, 256, 0, s>>>(result, prev, P.deg.as<uint32_t>(), V, spare, A.cta_part);
+      k_avg_scale<<<1, 256, 0, s>>>(spare, V, A.cta_part, gn);
+      launches += 2;
+      result = spare;
+      spare = const_cast<double*>(prev);
+    }
+  } else {
+    result = (hs.iter & 1ull) ? A.x1 : A.x0;
+    spare = x2.as<double>();
+  }
+  k_permute_out<<<grid_1d(V), 256, 0, s>>>(result, P.rank.as<uint32_t>(), V, spare);
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_CUDA(cudaMemcpyAsync(out, spare, (size_t)V * 8, dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (stats) {
+    stats->iterations = hs.iter;
+    stats->residual = hs.l1;
+    stats->elapsed_ms = tm.ms();
+    stats->launches = launches + 1;
+    stats->kernel_config = cfg;
+    stats->reserved = (uint32_t)hs.converged;
+  }
+  return ZOGCU_OK;
+}
+
+// Common entry: argument checks, n <= 1 shortcuts, offset-width dispatch.
+template <int MODE>
+static int linear_entry(zogcu_graph* G, double ka, double kb, double start, uint64_t max_iter, double tol, double* out,
+                        zogcu_stats* stats) {
+  if (!G) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "graph is null");
+  Graph* g = &G->g;
+  if (!out && g->V) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out_scores is null");
+  ZOGCU_CUDA(cudaSetDevice(g->device));
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  const uint32_t V = g->V;
+  if (g->n_live == 0 || (MODE == kModeEigen && g->n_live == 1)) {
+    // empty graph: every slot 0.0; eigenvector with one node: 1.0 (:1069-1072)
+    std::vector<double> h(V, 0.0);
+    if (g->n_live == 1) {
+      std::vector<uint32_t> deg(V);
+      ZOGCU_CUDA(cudaMemcpy(deg.data(), g->out_deg.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost));
+      for (uint32_t v = 0; v < V; ++v)
+        if (deg[v] != kDeletedDegree) h[v] = 1.0;
+    }
+    if (V) std::memcpy(out, h.data(), (size_t)V * 8);
+    return ZOGCU_OK;
+  }
+  if (MODE == kModeEigen && g->has_deleted)
+    return fail(ZOGCU_ERR_INVALID_ARGUMENT, "eigenvector on graphs with deleted nodes is not supported");
+  if (MODE == kModeEigen && !g->offsets32)
+    return fail(ZOGCU_ERR_TOO_LARGE, "eigenvector needs fewer than 2^32 arcs");
+  StreamGuard sg;
+  ZOGCU_TRY(sg.init(nullptr));
+  if (g->offsets32) return run_linear<uint32_t, MODE>(g, ka, kb, start, max_iter, tol, out, false, stats, sg.s);
+  return run_linear<uint64_t, MODE>(g, ka, kb, start, max_iter, tol, out, false, stats, sg.s);
+}
+
 }  // namespace zogcu
+
 
 
 using namespace zogcu;
@@ -953,6 +1261,21 @@ int zogcu_pagerank_ex(zogcu_graph* G, double damping, uint64_t max_iterations, d
 int zogcu_pagerank(zogcu_graph* G, double damping, uint64_t max_iterations, double tolerance, double* out_scores,
                    zogcu_stats* stats) {
   return zogcu_pagerank_ex(G, damping, max_iterations, tolerance, nullptr, out_scores, stats);
+}
+
+int zogcu_katz(zogcu_graph* G, double alpha, double beta, uint64_t max_iterations, double tolerance,
+               double* out_scores, zogcu_stats* stats) {
+  return linear_entry<kModeKatz>(G, alpha, beta, beta, max_iterations, tolerance, out_scores, stats);
+}
+
+int zogcu_alpha_centrality(zogcu_graph* G, double alpha, double initial, uint64_t max_iterations, double tolerance,
+                           double* out_scores, zogcu_stats* stats) {
+  return linear_entry<kModeAlpha>(G, alpha, 0.0, initial, max_iterations, tolerance, out_scores, stats);
+}
+
+int zogcu_eigenvector(zogcu_graph* G, uint64_t max_iterations, double tolerance, double* out_scores,
+                      zogcu_stats* stats) {
+  return linear_entry<kModeEigen>(G, 0.0, 0.0, 0.0, max_iterations, tolerance, out_scores, stats);
 }
 
 }  // extern "C"

@@ -121,6 +121,26 @@ def betweenness_unweighted(g: ResourceGraph, raw: bool = False, sources=None):
     return _map_scores(g.builder, scores)
 
 
+def eigenvector(g: ResourceGraph, max_iterations: int = 100, tolerance: float = 0.0001, raw: bool = False):
+    """resource_graph.ex:1697-1709 (defaults 100 / 1e-4)."""
+    scores = g.resource.eigenvector(max_iterations, tolerance)
+    return [float(x) for x in scores] if raw else _map_scores(g.builder, scores)
+
+
+def katz(g: ResourceGraph, alpha: float = 0.1, beta: float = 1.0, max_iterations: int = 100,
+         tolerance: float = 0.0001, raw: bool = False):
+    """resource_graph.ex:1723-1737 (defaults 0.1 / 1.0 / 100 / 1e-4)."""
+    scores = g.resource.katz(alpha, beta, max_iterations, tolerance)
+    return [float(x) for x in scores] if raw else _map_scores(g.builder, scores)
+
+
+def alpha_centrality(g: ResourceGraph, alpha: float = 0.5, initial: float = 1.0, max_iterations: int = 100,
+                     tolerance: float = 0.0001, raw: bool = False):
+    """resource_graph.ex:1751-1765 (defaults 0.5 / 1.0 / 100 / 1e-4)."""
+    scores = g.resource.alpha_centrality(alpha, initial, max_iterations, tolerance)
+    return [float(x) for x in scores] if raw else _map_scores(g.builder, scores)
+
+
 #: The name used for this path in the project's goal statement; the reference
 #: only exports ``betweenness_unweighted/2``.
 betweenness_centrality = betweenness_unweighted
