@@ -369,8 +369,10 @@ def run_zog(args):
         Vb, Eb, _ = B.info()
         bc = torch.zeros(Vb, dtype=torch.float64, device="cuda")
         part = torch.empty(Vb, dtype=torch.float64, device="cuda")
+        from zog_b200.distributed import shard_sources
+
         all_src = np.arange(Vb, dtype=np.uint32)
-        mine = all_src[rank::ws]
+        mine = shard_sources(all_src, rank, ws)
         chunks = [mine[i:i + BC_STEP_SOURCES] for i in range(0, mine.size, BC_STEP_SOURCES)]
         steps = len(chunks) if args.bc_steps <= 0 else min(args.bc_steps, len(chunks))
         with torch.cuda.stream(stream):
