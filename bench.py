@@ -37,6 +37,10 @@ PR_SCALE, PR_EF, PR_SEED = 24, 16, 1024
 BC_SCALE, BC_EF, BC_SEED = 16, 16, 1016
 BC_STEP_SOURCES = 4096
 DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
+# DRAM bytes (read + write) of one pr_iter_kernel launch on the default
+# workload (scale 24, kernel configuration 3), from one ncu capture of this
+# command; see profiles/pagerank_rmat24_launches_and_traffic.md.
+PROFILED_TRAFFIC = {(24, 3): 1.54e9 + 0.1762e9}
 
 
 # --------------------------------------------------------------------------
@@ -422,7 +426,9 @@ def run_zog(args):
                        "iterations": iterations, "residual": residual, "l2": "inputs larger than L2",
                        "parallelism": "replicas" if ws > 1 else "single"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / hbm_peak,
+                         "traffic": PROFILED_TRAFFIC.get((PR_SCALE, int(st["kernel_config"]))),
+                         "peak_kind": peak_kind,
                          "kernel": "pr_iter_kernel", "kernel_config": int(st["kernel_config"]),
                          "ms_per_launch": t_iter_ms,
                          "algorithmic_bytes_per_launch": bytes_per_iter},
