@@ -79,6 +79,10 @@ def lib():
     L.og_rmat.restype = vp
     L.og_rmat.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_int]
     L.og_edges_count.restype = C.c_uint64
+    L.og_ba.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_int]
+    L.og_ba.restype = vp
+    L.og_ws.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, C.c_int]
+    L.og_ws.restype = vp
     L.og_edges_count.argtypes = [vp]
     L.og_edges_nodes.restype = C.c_uint32
     L.og_edges_nodes.argtypes = [vp]
@@ -223,6 +227,28 @@ def rmat(scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, c=0.19, direct
     finally:
         L.og_edges_free(h)
     return V, frm[:m], to[:m]
+
+
+def _edges(h):
+    L = lib()
+    try:
+        m = int(L.og_edges_count(h))
+        V = int(L.og_edges_nodes(h))
+        frm = np.zeros(max(m, 1), np.uint32); to = np.zeros(max(m, 1), np.uint32)
+        L.og_edges_copy(h, frm, to)
+    finally:
+        L.og_edges_free(h)
+    return V, frm[:m], to[:m]
+
+
+def barabasi_albert(n: int, m: int, seed: int, directed=True):
+    """Seeded Barabasi-Albert edge list (V, from, to) in insertion order."""
+    return _edges(lib().og_ba(n, m, seed, 1 if directed else 0))
+
+
+def watts_strogatz(n: int, k: int, beta: float, seed: int, directed=False):
+    """Seeded Watts-Strogatz edge list (V, from, to) in insertion order."""
+    return _edges(lib().og_ws(n, k, beta, seed, 1 if directed else 0))
 
 
 def rmat_raw(scale, seed, i0, m, a=0.57, b=0.19, c=0.19):

@@ -31,7 +31,9 @@
 //   * og_pagerank_ext: the generalised iteration with a start vector and a
 //     teleport vector (personalised PageRank), uniform dangling mass;
 //   * og_rmat: the seeded R-MAT generator whose definition the CUDA generator
-//     shares (counter-based SplitMix64; see rmat_edge below).
+//     shares (counter-based SplitMix64; see rmat_edge below);
+//   * og_ba / og_ws: the seeded Barabasi-Albert and Watts-Strogatz generators
+//     (generator.ex:132-253 models), written independently of the library's.
 
 #include <algorithm>
 #include <chrono>
@@ -41,6 +43,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -733,6 +736,98 @@ void* og_rmat(int scale, int edge_factor, uint64_t seed, double a, double b, dou
   }
   return el;
 }
+// ---- Barabasi-Albert and Watts-Strogatz (benchmark / training inputs) --------
+// The model definitions of generator.ex:132-198 and :210-253 with a seeded
+// SplitMix64 stream (state advanced by the golden gamma, output mixed) in
+// place of :rand.  below(n) = high 64 bits of next() * n; uniform() =
+// (next() >> 11) * 2^-53.
+//   BA: clique on 0..m-1 (pairs u < v in order); the degree list holds each
+//       clique node m-1 times (node 0 once when m = 1).  Node u = m..n-1 draws
+//       list entries until it has m distinct targets, adds u->v for them in
+//       ascending order, then appends u, the targets, and u m-1 more times.
+//   WS: ring lattice u -- u+j mod n (j = 1..k/2); each lattice slot (u, j)
+//       draws one uniform; below beta, and if (u, u+j) is still joined, it is
+//       rewired to (u, w) with w drawn until w != u and not joined to u
+//       (skipped when u is joined to every other node).  Edges in sorted
+//       (lo, hi) order.
+// Undirected: both arcs per edge, forward first.
+namespace {
+struct Sm64Stream {
+  uint64_t s;
+  uint64_t next() {
+    const uint64_t r = splitmix64(s);
+    s += 0x9E3779B97F4A7C15ull;
+    return r;
+  }
+  uint64_t below(uint64_t n) { return (uint64_t)(((unsigned __int128)next() * n) >> 64); }
+  double uniform() { return (double)(next() >> 11) * 0x1p-53; }
+};
+void el_push(EdgeList* el, uint32_t u, uint32_t v, bool directed) {
+  el->from.push_back(u);
+  el->to.push_back(v);
+  if (!directed) {
+    el->from.push_back(v);
+    el->to.push_back(u);
+  }
+}
+}  // namespace
+
+void* og_ba(uint32_t n, uint32_t m, uint64_t seed, int directed) {
+  auto* el = new EdgeList();
+  el->V = n;
+  Sm64Stream rng{seed};
+  for (uint32_t u = 0; u < m; ++u)
+    for (uint32_t v = u + 1; v < m; ++v) el_push(el, u, v, directed != 0);
+  std::vector<uint32_t> pool;
+  for (uint32_t u = 0; u < m; ++u)
+    for (uint32_t c = 1; c < m; ++c) pool.push_back(u);
+  if (m == 1) pool.push_back(0);
+  for (uint32_t u = m; u < n; ++u) {
+    std::vector<uint32_t> chosen;
+    while (chosen.size() < m) {
+      const uint32_t v = pool[rng.below(pool.size())];
+      bool dup = false;
+      for (uint32_t x : chosen) dup |= x == v;
+      if (!dup) chosen.push_back(v);
+    }
+    std::sort(chosen.begin(), chosen.end());
+    for (uint32_t v : chosen) el_push(el, u, v, directed != 0);
+    pool.push_back(u);
+    pool.insert(pool.end(), chosen.begin(), chosen.end());
+    for (uint32_t c = 1; c < m; ++c) pool.push_back(u);
+  }
+  return el;
+}
+
+void* og_ws(uint32_t n, uint32_t k, double beta, uint64_t seed, int directed) {
+  auto* el = new EdgeList();
+  el->V = n;
+  Sm64Stream rng{seed};
+  std::vector<std::set<uint32_t>> adj(n);
+  for (uint32_t u = 0; u < n; ++u)
+    for (uint32_t j = 1; j <= k / 2; ++j) {
+      const uint32_t v = (u + j) % n;
+      adj[u].insert(v);
+      adj[v].insert(u);
+    }
+  for (uint32_t u = 0; u < n; ++u)
+    for (uint32_t j = 1; j <= k / 2; ++j) {
+      const uint32_t v = (u + j) % n;
+      const double r = rng.uniform();
+      if (!(r < beta) || !adj[u].count(v) || adj[u].size() + 1 >= n) continue;
+      uint32_t w = (uint32_t)rng.below(n);
+      while (w == u || adj[u].count(w)) w = (uint32_t)rng.below(n);
+      adj[u].erase(v);
+      adj[v].erase(u);
+      adj[u].insert(w);
+      adj[w].insert(u);
+    }
+  for (uint32_t u = 0; u < n; ++u)
+    for (uint32_t v : adj[u])
+      if (u < v) el_push(el, u, v, directed != 0);
+  return el;
+}
+
 uint64_t og_edges_count(void* h) { return ((EdgeList*)h)->from.size(); }
 uint32_t og_edges_nodes(void* h) { return ((EdgeList*)h)->V; }
 void og_edges_copy(void* h, uint32_t* from, uint32_t* to) {
