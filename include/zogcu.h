@@ -135,6 +135,18 @@ ZOGCU_API int zogcu_graph_create_from_arraygraph(uint32_t node_capacity, const u
 ZOGCU_API int zogcu_graph_generate_rmat(int scale, int edge_factor, uint64_t seed, double a, double b,
                               double c, int directed, zogcu_graph** out);
 
+/* Seeded Barabasi-Albert graph (lib/zog/generator.ex:132-198 model): clique
+ * on m nodes, then each new node attaches to m distinct existing nodes chosen
+ * with probability proportional to degree.  directed != 0 stores only the
+ * new->old arcs (heavy-tailed in-degree); else both arcs. */
+ZOGCU_API int zogcu_graph_generate_ba(uint32_t n, uint32_t m, uint64_t seed, int directed,
+                                      zogcu_graph** out);
+
+/* Seeded Watts-Strogatz graph (lib/zog/generator.ex:210-253 model): ring
+ * lattice of k nearest neighbours, each edge rewired with probability beta. */
+ZOGCU_API int zogcu_graph_generate_ws(uint32_t n, uint32_t k, double beta, uint64_t seed,
+                                      int directed, zogcu_graph** out);
+
 /* Raw (pre-dedupe) endpoints of R-MAT edges [i0, i0+m) of the generator above,
  * written to device arrays -- lets a test compare the generator element by
  * element with an independent CPU implementation of the same definition. */
@@ -244,6 +256,44 @@ ZOGCU_API int zogcu_betweenness_unweighted_ex(zogcu_graph* g, const zogcu_bc_opt
  * count wrapped. */
 ZOGCU_API int zogcu_bfs_sigma(zogcu_graph* g, const uint32_t* sources, uint64_t num_sources,
                     uint32_t* dist_out, uint64_t* sigma_out, uint32_t* overflow);
+
+/* ---- Learned PageRank warm start -------------------------------------------
+ * No counterpart in the reference, whose start is always uniform
+ * (centrality.zig:912-918).  A 3-layer message-passing network (hidden 64,
+ * FP32 master weights, BF16 weights in the forward pass, FP32 accumulation)
+ * maps degree features to a predicted log(n * pagerank); its softmax is a
+ * start vector for zogcu_pagerank_ex (opts.x0), and power iteration still runs
+ * to the caller's tolerance.  Training, prediction and the weight file all run
+ * through the entry points below. */
+typedef struct zogcu_gnn zogcu_gnn;
+
+/* Number of FP32 parameters (the length of get/set_params buffers). */
+ZOGCU_API int zogcu_gnn_num_params(void);
+/* New network with seeded Glorot-uniform weights and zero Adam state. */
+ZOGCU_API int zogcu_gnn_create(uint64_t seed, zogcu_gnn** out);
+ZOGCU_API int zogcu_gnn_destroy(zogcu_gnn* net);
+ZOGCU_API int zogcu_gnn_get_params(const zogcu_gnn* net, float* out_params);
+ZOGCU_API int zogcu_gnn_set_params(zogcu_gnn* net, const float* params);
+/* Training losses against a PageRank vector pr (sums to 1 over live nodes). */
+enum {
+  ZOGCU_GNN_LOSS_LOG_MSE = 0, /* mean over live nodes of (y - log(n pr))^2          */
+  ZOGCU_GNN_LOSS_KL = 1       /* KL(pr || softmax(y)): errors weighted by rank mass */
+};
+/* Loss and its gradient with respect to the parameters, for one graph and its
+ * PageRank vector target_pr[V] (host).  Either output may be NULL. */
+ZOGCU_API int zogcu_gnn_loss_grad(zogcu_gnn* net, zogcu_graph* g, const double* target_pr,
+                                  int loss_kind, float* loss, float* grad_out);
+/* One Adam step (beta 0.9 / 0.999) on one graph; d_target_pr is a device array. */
+ZOGCU_API int zogcu_gnn_train_step(zogcu_gnn* net, zogcu_graph* g, const double* d_target_pr,
+                                   int loss_kind, float learning_rate, float* loss);
+/* Start vector x0[V] (sums to 1 over live nodes; 0 on deleted slots), into a
+ * device array when device_out != 0; raw_out[V] (host, may be NULL) receives
+ * the network output y.  Runs on `stream` (NULL = a private stream). */
+ZOGCU_API int zogcu_gnn_predict(const zogcu_gnn* net, zogcu_graph* g, double* x0, int device_out,
+                                void* stream, float* raw_out);
+/* Weight file: magic "ZOGN", version 1, parameter count, BF16 weights. */
+ZOGCU_API int zogcu_gnn_save(const zogcu_gnn* net, const char* path);
+ZOGCU_API int zogcu_gnn_load(const char* path, zogcu_gnn** out);
 
 #ifdef __cplusplus
 }

@@ -22,6 +22,8 @@ STATUS_NAMES = {
 }
 PREC_FP64 = 0
 PREC_MIXED = 1
+LOSS_LOG_MSE = 0
+LOSS_KL = 1
 
 #: every entry point declared in include/zogcu.h
 EXPORTS = (
@@ -32,6 +34,10 @@ EXPORTS = (
     "zogcu_free", "zogcu_pagerank", "zogcu_pagerank_ex", "zogcu_betweenness_unweighted",
     "zogcu_betweenness_unweighted_ex", "zogcu_bfs_sigma", "zogcu_pagerank_noalloc",
     "zogcu_katz", "zogcu_alpha_centrality", "zogcu_eigenvector",
+    "zogcu_graph_generate_ba", "zogcu_graph_generate_ws",
+    "zogcu_gnn_num_params", "zogcu_gnn_create", "zogcu_gnn_destroy", "zogcu_gnn_get_params",
+    "zogcu_gnn_set_params", "zogcu_gnn_loss_grad", "zogcu_gnn_train_step", "zogcu_gnn_predict",
+    "zogcu_gnn_save", "zogcu_gnn_load",
 )
 
 
@@ -111,8 +117,21 @@ def load(path: str | None = None):
         L.zogcu_bfs_sigma.argtypes = [vp, vp, u64, vp, vp, C.POINTER(u32)]
         L.zogcu_pagerank_noalloc.argtypes = [vp, vp, vp, u32, u64, dbl, u64, dbl, vp, C.POINTER(Stats), vp]
         L.zogcu_katz.argtypes = [vp, dbl, dbl, u64, dbl, vp, C.POINTER(Stats)]
+        L.zogcu_graph_generate_ba.argtypes = [u32, u32, u64, i32, pp]
+        L.zogcu_graph_generate_ws.argtypes = [u32, u32, dbl, u64, i32, pp]
         L.zogcu_alpha_centrality.argtypes = [vp, dbl, dbl, u64, dbl, vp, C.POINTER(Stats)]
         L.zogcu_eigenvector.argtypes = [vp, u64, dbl, vp, C.POINTER(Stats)]
+        fp = C.POINTER(C.c_float)
+        L.zogcu_gnn_num_params.argtypes = []
+        L.zogcu_gnn_create.argtypes = [u64, pp]
+        L.zogcu_gnn_destroy.argtypes = [vp]
+        L.zogcu_gnn_get_params.argtypes = [vp, vp]
+        L.zogcu_gnn_set_params.argtypes = [vp, vp]
+        L.zogcu_gnn_loss_grad.argtypes = [vp, vp, vp, i32, fp, vp]
+        L.zogcu_gnn_train_step.argtypes = [vp, vp, vp, i32, C.c_float, fp]
+        L.zogcu_gnn_predict.argtypes = [vp, vp, vp, i32, vp, vp]
+        L.zogcu_gnn_save.argtypes = [vp, C.c_char_p]
+        L.zogcu_gnn_load.argtypes = [C.c_char_p, pp]
         for name in EXPORTS:  # every other entry point returns a zogcu_status
             if name not in ("zogcu_status_string", "zogcu_last_error", "zogcu_free"):
                 getattr(L, name).restype = C.c_int
@@ -185,6 +204,18 @@ class Graph:
         L = load()
         h = C.c_void_p()
         check(L.zogcu_graph_generate_rmat(scale, edge_factor, seed, a, b, c, 1 if directed else 0, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def barabasi_albert(cls, n: int, m: int, seed: int, directed=True) -> "Graph":
+        h = C.c_void_p()
+        check(load().zogcu_graph_generate_ba(n, m, seed, 1 if directed else 0, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def watts_strogatz(cls, n: int, k: int, beta: float, seed: int, directed=False) -> "Graph":
+        h = C.c_void_p()
+        check(load().zogcu_graph_generate_ws(n, k, beta, seed, 1 if directed else 0, C.byref(h)))
         return cls(h)
 
     @classmethod
@@ -324,3 +355,84 @@ def rmat_raw_device(scale, seed, i0, m, a=0.57, b=0.19, c=0.19):
     d = torch.empty(m, dtype=torch.int32, device="cuda")
     check(load().zogcu_rmat_raw_device(scale, seed, a, b, c, i0, m, s.data_ptr(), d.data_ptr()))
     return s.cpu().numpy().view(np.uint32), d.cpu().numpy().view(np.uint32)
+
+
+class WarmStart:
+    """Owning wrapper of a ``zogcu_gnn*``: the learned PageRank start vector.
+
+    The network predicts y = log(n * pagerank) from degree features; its
+    softmax is handed to ``Graph.pagerank(x0=...)``, which still iterates to
+    the caller's tolerance.
+    """
+
+    def __init__(self, handle):
+        self._h = handle if isinstance(handle, C.c_void_p) else C.c_void_p(handle)
+
+    @classmethod
+    def create(cls, seed: int = 0) -> "WarmStart":
+        h = C.c_void_p()
+        check(load().zogcu_gnn_create(int(seed), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load_file(cls, path: str) -> "WarmStart":
+        h = C.c_void_p()
+        check(load().zogcu_gnn_load(os.fsencode(path), C.byref(h)))
+        return cls(h)
+
+    @staticmethod
+    def num_params() -> int:
+        return int(load().zogcu_gnn_num_params())
+
+    def destroy(self):
+        if self._h:
+            check(load().zogcu_gnn_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def save(self, path: str):
+        check(load().zogcu_gnn_save(self._h, os.fsencode(path)))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params(), np.float32)
+        check(load().zogcu_gnn_get_params(self._h, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.num_params():
+            raise ValueError("parameter vector has the wrong length")
+        check(load().zogcu_gnn_set_params(self._h, _ptr(p)))
+
+    def loss_grad(self, g: Graph, target_pr, loss_kind: int = LOSS_KL):
+        V, _, _ = g.info()
+        t = np.ascontiguousarray(target_pr, dtype=np.float64)
+        if t.size != V:
+            raise ValueError("target must have node-capacity length")
+        loss = C.c_float(0)
+        grad = np.zeros(self.num_params(), np.float32)
+        check(load().zogcu_gnn_loss_grad(self._h, g.handle, _ptr(t), int(loss_kind), C.byref(loss), _ptr(grad)))
+        return float(loss.value), grad
+
+    def train_step(self, g: Graph, d_target_ptr: int, lr: float, loss_kind: int = LOSS_KL) -> float:
+        loss = C.c_float(0)
+        check(load().zogcu_gnn_train_step(self._h, g.handle, d_target_ptr, int(loss_kind), float(lr),
+                                          C.byref(loss)))
+        return float(loss.value)
+
+    def predict(self, g: Graph, raw=False):
+        """Start vector x0 (host, length V); with raw=True also the output y."""
+        V, _, _ = g.info()
+        x0 = np.zeros(max(V, 1), np.float64)
+        y = np.zeros(max(V, 1), np.float32) if raw else None
+        check(load().zogcu_gnn_predict(self._h, g.handle, _ptr(x0), 0, None, _ptr(y)))
+        return (x0[:V], y[:V]) if raw else x0[:V]
+
+    def predict_device(self, g: Graph, x0_ptr: int, stream=None):
+        """Start vector into a device buffer (length V, f64) on a caller stream."""
+        check(load().zogcu_gnn_predict(self._h, g.handle, x0_ptr, 1, stream, None))
