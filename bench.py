@@ -11,6 +11,12 @@ Workload (the scale configuration, synthetic and seeded):
   * Brandes, exact, unweighted: undirected R-MAT scale 16, edge factor 16
     (seed 1016), every source.  One step = 4,096 consecutive sources; the timed
     steps cover all 65,536 sources.  Reported as GTEPS = sources * arcs / time.
+  * Learned start (object "learned_start"): the same scale-24 solve started
+    from the shipped warm-start network's prediction; one step = inference +
+    power iteration to the same tolerance.
+  * Barabasi-Albert (object "barabasi_albert"): directed BA n = 4,194,304,
+    m = 8 (seed 4096), solved in FP64, in the mixed form and from the learned
+    start.
 
 The graph inputs (~1 GB of arc indices at scale 24) exceed the 126 MB L2, so no
 L2 flush is needed between steps.  N > 1 (torchrun): PageRank runs as
@@ -36,7 +42,11 @@ METRIC = "PageRank ms to L1 res 1e-9 (learned vs uniform start); Brandes GTEPS"
 PR_SCALE, PR_EF, PR_SEED = 24, 16, 1024
 BC_SCALE, BC_EF, BC_SEED = 16, 16, 1016
 BC_STEP_SOURCES = 4096
+BA_N, BA_M, BA_SEED = 1 << 22, 8, 4096
 DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
+# kernels one zogcu_gnn_predict launches: features, chunk rows, 3 x (SpMM,
+# dense), head, and the 4 softmax kernels
+GNN_PREDICT_LAUNCHES = 13
 # DRAM bytes (read + write) of one pr_iter_kernel launch on the default
 # workload (scale 24, kernel configuration 3), from one ncu capture of this
 # command; see profiles/pagerank_rmat24_launches_and_traffic.md.
@@ -234,6 +244,115 @@ def _successor_csr_undirected(V, f, t):
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
+def _timed(stream, steps, fn):
+    """Mean device ms of `steps` calls of fn() on `stream` (CUDA events)."""
+    import torch
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = [fn() for _ in range(steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / max(steps, 1), res
+
+
+def learned_start_block(N, G, like, ms_uniform, it_uniform, args, stream, ws):
+    """Solve from the shipped network's start and compare with the FP64
+    uniform-start solve of the same graph (timed before: ms_uniform)."""
+    import torch
+
+    from zog_b200 import warm_start as W
+
+    sp = stream.cuda_stream
+    net = W.load_default()
+    x_uniform = torch.empty_like(like)
+    G.pagerank_device(x_uniform.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+    x0 = torch.empty_like(x_uniform)
+    xl = torch.empty_like(x_uniform)
+
+    def solve():
+        net.predict_device(G, x0.data_ptr(), stream=sp)
+        return G.pagerank_device(xl.data_ptr(), DAMPING, MAX_ITER, TOL, x0_ptr=x0.data_ptr(), stream=sp)
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    barrier(ws)
+    lms, sts = _timed(stream, args.steps, solve)
+    lms = max_over_ranks(lms, ws)
+    ims, _ = _timed(stream, args.steps, lambda: net.predict_device(G, x0.data_ptr(), stream=sp))
+    V = x_uniform.numel()
+    n_live = G.info()[2]
+    den = float(x_uniform.abs().sum())
+    res = {"ms": lms, "speedup_vs_uniform": ms_uniform / lms, "iterations": int(sts[-1]["iterations"]),
+           "uniform_iterations": int(it_uniform), "inference_ms": ims,
+           "rel_l1_vs_uniform_result": float((xl - x_uniform).abs().sum()) / den,
+           "start_l1_error_learned": float((x0 - x_uniform).abs().sum()),
+           "start_l1_error_uniform": float((x_uniform - 1.0 / max(n_live, 1)).abs().sum()),
+           "weights": "zog_b200/data/warm_start.zogn"}
+    nl = args.steps * (GNN_PREDICT_LAUNCHES + int(sts[-1]["launches"])) + args.steps * GNN_PREDICT_LAUNCHES
+    net.destroy()
+    del x0, xl, x_uniform
+    return res, nl
+
+
+def ba_block(N, args, stream, ws):
+    """Directed Barabasi-Albert graph: FP64 uniform start, the mixed form and
+    the learned start, each to the same tolerance."""
+    import torch
+
+    from zog_b200 import warm_start as W
+
+    sp = stream.cuda_stream
+    t0 = time.perf_counter()
+    B = N.Graph.barabasi_albert(BA_N, BA_M, BA_SEED, directed=True)
+    gen_s = time.perf_counter() - t0
+    V, E, _ = B.info()
+    x64 = torch.empty(V, dtype=torch.float64, device="cuda")
+    xm = torch.empty_like(x64)
+    xl = torch.empty_like(x64)
+    x0 = torch.empty_like(x64)
+    net = W.load_default()
+    launches = 0
+
+    def fp64():
+        return B.pagerank_device(x64.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+
+    def mixed():
+        return B.pagerank_device(xm.data_ptr(), DAMPING, MAX_ITER, TOL, precision=N.PREC_MIXED, stream=sp)
+
+    def learned():
+        net.predict_device(B, x0.data_ptr(), stream=sp)
+        return B.pagerank_device(xl.data_ptr(), DAMPING, MAX_ITER, TOL, x0_ptr=x0.data_ptr(), stream=sp)
+
+    out = {}
+    for name, fn in (("fp64", fp64), ("mixed", mixed), ("learned", learned)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(ws)
+        t, sts = _timed(stream, args.steps, fn)
+        out[name] = (max_over_ranks(t, ws), sts[-1])
+        launches += sum(int(st["launches"]) for st in sts) + (args.steps * GNN_PREDICT_LAUNCHES if name == "learned" else 0)
+    den = float(x64.abs().sum())
+    res = {"workload": f"directed barabasi-albert n={BA_N} m={BA_M} seed={BA_SEED}", "vertices": V, "arcs": E,
+           "generate_s": gen_s,
+           "fp64": {"ms": out["fp64"][0], "iterations": int(out["fp64"][1]["iterations"])},
+           "mixed": {"ms": out["mixed"][0], "iterations": int(out["mixed"][1]["iterations"]),
+                     "fp64_polish_iterations": int(out["mixed"][1]["polish_iterations"]),
+                     "speedup_vs_fp64": out["fp64"][0] / out["mixed"][0],
+                     "rel_l1_vs_fp64": float((xm - x64).abs().sum()) / den},
+           "learned": {"ms": out["learned"][0], "iterations": int(out["learned"][1]["iterations"]),
+                       "speedup_vs_fp64_uniform": out["fp64"][0] / out["learned"][0],
+                       "rel_l1_vs_fp64": float((xl - x64).abs().sum()) / den,
+                       "start_l1_error_learned": float((x0 - x64).abs().sum()),
+                       "start_l1_error_uniform": float((x64 - 1.0 / V).abs().sum())}}
+    net.destroy()
+    B.destroy()
+    return res, launches
+
+
 def run_zog(args):
     import torch
 
@@ -321,6 +440,12 @@ def run_zog(args):
                  "rel_l1_vs_fp64": err, "bound": "rel L1 <= 2*d/(1-d)*tol = %.2e" % (2 * DAMPING / (1 - DAMPING) * TOL)}
         del x64, outm
 
+    # ---------------- learned warm start on the same graph ----------------
+    learned = None
+    if not args.no_learned:
+        learned, nl = learned_start_block(N, G, out, ms, iterations, args, stream, ws)
+        launches += nl
+
     # ---------------- e2e through the C ABI with host buffers ----------------
     e2e = None
     if not args.no_e2e:
@@ -365,6 +490,13 @@ def run_zog(args):
         del ih, ic
     G.destroy()
     torch.cuda.empty_cache()
+
+    # ---------------- Barabasi-Albert: FP64, mixed, learned ----------------
+    ba = None
+    if not args.no_ba:
+        ba, nl = ba_block(N, args, stream, ws)
+        launches += nl
+        torch.cuda.empty_cache()
 
     # ---------------- Brandes, all sources, sharded over ranks ----------------
     bc_line = None
@@ -437,6 +569,8 @@ def run_zog(args):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "precision_mixed": mixed,
+            "learned_start": learned,
+            "barabasi_albert": ba,
             "brandes": bc_line,
         }
         print(json.dumps(line), flush=True)
@@ -461,6 +595,8 @@ def main():
     ap.add_argument("--no-brandes", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32/FP64 precision form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm start")
+    ap.add_argument("--no-ba", action="store_true", help="skip the Barabasi-Albert graph")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")

@@ -257,6 +257,37 @@ ZOGCU_API int zogcu_betweenness_unweighted_ex(zogcu_graph* g, const zogcu_bc_opt
 ZOGCU_API int zogcu_bfs_sigma(zogcu_graph* g, const uint32_t* sources, uint64_t num_sources,
                     uint32_t* dist_out, uint64_t* sigma_out, uint32_t* overflow);
 
+/* ---- Batched PageRank: many graphs in one persistent launch ------------------
+ * No counterpart in the reference (one graph per NIF call).  A batch holds
+ * copies of several graphs' device CSRs; one call solves every graph exactly
+ * as zogcu_pagerank solves it alone (uniform start, FP64), in a single
+ * persistent kernel launch replayed from a CUDA graph.  The kernel
+ * configuration (CTA size, cluster size, degree bin) is chosen by an
+ * autotuner on the first call. */
+typedef struct zogcu_batch zogcu_batch;
+
+typedef struct zogcu_batch_opts {
+  uint32_t struct_size;   /* sizeof(zogcu_batch_opts)                            */
+  int32_t config;         /* kernel configuration, -1 = autotuned                */
+  int32_t device_pointers;/* out_scores is a device pointer                      */
+  int32_t reserved;
+  void* stream;           /* cudaStream_t to run on, or NULL = a private stream  */
+} zogcu_batch_opts;
+
+/* Copies the graphs (all on one device; each with fewer than 2^32 arcs) into
+ * a new batch; the graphs stay owned by the caller. */
+ZOGCU_API int zogcu_batch_create(zogcu_graph* const* graphs, uint32_t count, zogcu_batch** out);
+ZOGCU_API int zogcu_batch_destroy(zogcu_batch* batch);
+/* Graph count, total node slots and arcs; node_offsets[count + 1] (may be
+ * NULL) receives where each graph's scores start in the output. */
+ZOGCU_API int zogcu_batch_info(const zogcu_batch* batch, uint32_t* count, uint64_t* total_nodes,
+                               uint64_t* total_arcs, uint64_t* node_offsets);
+/* PageRank of every graph: out_scores[total_nodes] (graph g at
+ * node_offsets[g]), iterations[count] (may be NULL). */
+ZOGCU_API int zogcu_batch_pagerank(zogcu_batch* batch, double damping, uint64_t max_iterations,
+                                   double tolerance, const zogcu_batch_opts* opts, double* out_scores,
+                                   uint64_t* iterations, zogcu_stats* stats);
+
 /* ---- Learned PageRank warm start -------------------------------------------
  * No counterpart in the reference, whose start is always uniform
  * (centrality.zig:912-918).  A 3-layer message-passing network (hidden 64,

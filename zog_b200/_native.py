@@ -38,6 +38,7 @@ EXPORTS = (
     "zogcu_gnn_num_params", "zogcu_gnn_create", "zogcu_gnn_destroy", "zogcu_gnn_get_params",
     "zogcu_gnn_set_params", "zogcu_gnn_loss_grad", "zogcu_gnn_train_step", "zogcu_gnn_predict",
     "zogcu_gnn_save", "zogcu_gnn_load",
+    "zogcu_batch_create", "zogcu_batch_destroy", "zogcu_batch_info", "zogcu_batch_pagerank",
 )
 
 
@@ -66,6 +67,13 @@ class PrOpts(C.Structure):
         ("struct_size", C.c_uint32), ("precision", C.c_int32), ("x0", C.c_void_p),
         ("teleport", C.c_void_p), ("device_pointers", C.c_int32), ("reserved", C.c_int32),
         ("stream", C.c_void_p),
+    ]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("config", C.c_int32), ("device_pointers", C.c_int32),
+        ("reserved", C.c_int32), ("stream", C.c_void_p),
     ]
 
 
@@ -132,6 +140,10 @@ def load(path: str | None = None):
         L.zogcu_gnn_predict.argtypes = [vp, vp, vp, i32, vp, vp]
         L.zogcu_gnn_save.argtypes = [vp, C.c_char_p]
         L.zogcu_gnn_load.argtypes = [C.c_char_p, pp]
+        L.zogcu_batch_create.argtypes = [vp, u32, pp]
+        L.zogcu_batch_destroy.argtypes = [vp]
+        L.zogcu_batch_info.argtypes = [vp, C.POINTER(u32), C.POINTER(u64), C.POINTER(u64), vp]
+        L.zogcu_batch_pagerank.argtypes = [vp, dbl, u64, dbl, C.POINTER(BatchOpts), vp, vp, C.POINTER(Stats)]
         for name in EXPORTS:  # every other entry point returns a zogcu_status
             if name not in ("zogcu_status_string", "zogcu_last_error", "zogcu_free"):
                 getattr(L, name).restype = C.c_int
@@ -436,3 +448,56 @@ class WarmStart:
     def predict_device(self, g: Graph, x0_ptr: int, stream=None):
         """Start vector into a device buffer (length V, f64) on a caller stream."""
         check(load().zogcu_gnn_predict(self._h, g.handle, x0_ptr, 1, stream, None))
+
+
+class Batch:
+    """Owning wrapper of a ``zogcu_batch*``: copies of several graphs solved
+    together in one persistent launch."""
+
+    def __init__(self, graphs):
+        arr = (C.c_void_p * max(len(graphs), 1))(*[g.handle.value for g in graphs])
+        self._h = C.c_void_p()
+        check(load().zogcu_batch_create(arr, len(graphs), C.byref(self._h)))
+
+    def destroy(self):
+        if self._h:
+            check(load().zogcu_batch_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def info(self):
+        n = C.c_uint32(0); V = C.c_uint64(0); E = C.c_uint64(0)
+        check(load().zogcu_batch_info(self._h, C.byref(n), C.byref(V), C.byref(E), None))
+        offs = np.zeros(n.value + 1, np.uint64)
+        check(load().zogcu_batch_info(self._h, None, None, None, _ptr(offs)))
+        return int(n.value), int(V.value), int(E.value), offs
+
+    def pagerank(self, damping=0.85, max_iterations=100, tolerance=1e-4, config=-1, stats=False):
+        """Scores of every graph (a list of arrays) and their iteration counts."""
+        n, V, _, offs = self.info()
+        out = np.zeros(max(V, 1), np.float64)
+        its = np.zeros(max(n, 1), np.uint64)
+        st = Stats()
+        o = BatchOpts(C.sizeof(BatchOpts), int(config), 0, 0, None)
+        check(load().zogcu_batch_pagerank(self._h, float(damping), int(max_iterations), float(tolerance),
+                                          C.byref(o), _ptr(out), _ptr(its), C.byref(st)))
+        res = [out[int(offs[i]):int(offs[i + 1])] for i in range(n)]
+        return (res, its[:n], st.as_dict()) if stats else (res, its[:n])
+
+    def pagerank_device(self, out_ptr: int, damping=0.85, max_iterations=100, tolerance=1e-4, config=-1,
+                        stream=None):
+        """Scores into a device buffer (total node slots, f64); returns stats."""
+        n, _, _, _ = self.info()
+        its = np.zeros(max(n, 1), np.uint64)
+        st = Stats()
+        o = BatchOpts(C.sizeof(BatchOpts), int(config), 1, 0, stream)
+        check(load().zogcu_batch_pagerank(self._h, float(damping), int(max_iterations), float(tolerance),
+                                          C.byref(o), out_ptr, _ptr(its), C.byref(st)))
+        d = st.as_dict()
+        d["per_graph_iterations"] = its[:n]
+        return d
