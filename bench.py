@@ -17,6 +17,11 @@ Workload (the scale configuration, synthetic and seeded):
   * Barabasi-Albert (object "barabasi_albert"): directed BA n = 4,194,304,
     m = 8 (seed 4096), solved in FP64, in the mixed form and from the learned
     start.
+  * Batched forms (object "batched"), each against a loop of single launches:
+    1,024 directed R-MAT graphs (scales 8-16, edge factors 4-16, seeded) in
+    one persistent CUDA-graph launch; 256 personalised-PageRank seeds
+    (seeded one-hot) as one SpMM on directed R-MAT scale 22; Brandes over
+    4,096 seeded sources of undirected R-MAT scale 18.
 
 The graph inputs (~1 GB of arc indices at scale 24) exceed the 126 MB L2, so no
 L2 flush is needed between steps.  N > 1 (torchrun): PageRank runs as
@@ -43,6 +48,10 @@ PR_SCALE, PR_EF, PR_SEED = 24, 16, 1024
 BC_SCALE, BC_EF, BC_SEED = 16, 16, 1016
 BC_STEP_SOURCES = 4096
 BA_N, BA_M, BA_SEED = 1 << 22, 8, 4096
+# batched forms
+BATCH_GRAPHS, BATCH_SEED = 1024, 8016          # R-MAT scales 8-16, edge factors 4-16
+PPR_SCALE, PPR_EF, PPR_SEED, PPR_SEEDS = 22, 16, 1022, 256
+BCB_SCALE, BCB_EF, BCB_SEED, BCB_SOURCES = 18, 16, 1018, 4096
 DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
 # kernels one zogcu_gnn_predict launches: features, chunk rows, 3 x (SpMM,
 # dense), head, and the 4 softmax kernels
@@ -353,6 +362,114 @@ def ba_block(N, args, stream, ws):
     return res, launches
 
 
+def batched_block(N, args, stream, ws):
+    """The three batched forms, each timed against a loop of single launches."""
+    import torch
+
+    sp = stream.cuda_stream
+    res = {}
+    launches = 0
+    # ---- 1,024 uneven graphs in one persistent launch ----
+    rng = np.random.default_rng(BATCH_SEED)
+    specs = [(int(rng.integers(8, 17)), int(rng.integers(4, 17))) for _ in range(BATCH_GRAPHS)]
+    graphs = [N.Graph.rmat(sc, ef, BATCH_SEED + i) for i, (sc, ef) in enumerate(specs)]
+    B = N.Batch(graphs)
+    n, Vt, Et, offs = B.info()
+    out = torch.empty(Vt, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        st = B.pagerank_device(out.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+    torch.cuda.synchronize()
+    barrier(ws)
+    bms, sts = _timed(stream, args.steps, lambda: B.pagerank_device(out.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp))
+    bms = max_over_ranks(bms, ws)
+    launches += args.steps
+    xs = [torch.empty(g.info()[0], dtype=torch.float64, device="cuda") for g in graphs]
+    loop = lambda: [g.pagerank_device(x.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp) for g, x in zip(graphs, xs)]
+    loop()
+    torch.cuda.synchronize()
+    lms, lsts = _timed(stream, 1, loop)
+    launches += sum(int(s2["launches"]) for s2 in lsts[0])
+    its = sts[-1]["per_graph_iterations"]
+    diff = 0.0
+    o = out.cpu().numpy()
+    for i in range(n):
+        r = xs[i].cpu().numpy()
+        diff = max(diff, float(np.abs(o[int(offs[i]):int(offs[i + 1])] - r).sum() / max(np.abs(r).sum(), 1e-300)))
+    res["graphs"] = {"workload": f"{n} directed rmat graphs, scales 8-16, edge factors 4-16, seed {BATCH_SEED}",
+                     "vertices": Vt, "arcs": Et, "ms": bms, "loop_of_single_launches_ms": lms,
+                     "speedup_vs_loop": lms / bms, "kernel_config": int(sts[-1]["kernel_config"]),
+                     "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
+                     "achieved_gbs": sts[-1]["bytes_moved"] / (bms * 1e-3) / 1e9,
+                     "max_rel_l1_vs_single": diff, "launches_per_step": 1}
+    B.destroy()
+    for g in graphs:
+        g.destroy()
+    del out, xs
+    torch.cuda.empty_cache()
+    # ---- 256 personalised seeds as one SpMM ----
+    G = N.Graph.rmat(PPR_SCALE, PPR_EF, PPR_SEED, directed=True)
+    V, E, _ = G.info()
+    seeds = np.random.default_rng(PPR_SEED).choice(V, PPR_SEEDS, replace=False).astype(np.uint32)
+    pout = torch.empty(PPR_SEEDS * V, dtype=torch.float64, device="cuda")
+    for _ in range(max(1, args.warmup - 2)):
+        st = G.ppr_device(seeds, pout.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+    torch.cuda.synchronize()
+    barrier(ws)
+    psteps = max(1, args.steps // 2)
+    pms, psts = _timed(stream, psteps, lambda: G.ppr_device(seeds, pout.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp))
+    pms = max_over_ranks(pms, ws)
+    launches += sum(int(s2["launches"]) for s2 in psts)
+    # loop of single-seed solves (the teleport form of the single-vector kernel), on a sample of seeds
+    k = 16
+    x1 = torch.empty(V, dtype=torch.float64, device="cuda")
+    tp = torch.zeros(V, dtype=torch.float64, device="cuda")
+
+    def single(sd):
+        tp.zero_()
+        tp[int(sd)] = 1.0
+        return G.pagerank_device(x1.data_ptr(), DAMPING, MAX_ITER, TOL, teleport_ptr=tp.data_ptr(), stream=sp)
+
+    with torch.cuda.stream(stream):
+        single(seeds[0])
+        torch.cuda.synchronize()
+        sms, ssts = _timed(stream, 1, lambda: [single(sd) for sd in seeds[:k]])
+    launches += sum(int(s2["launches"]) for s2 in ssts[0])
+    err = float((pout[(k - 1) * V:k * V] - x1).abs().sum() / x1.abs().sum())
+    pit = psts[-1]["per_seed_iterations"]
+    res["ppr"] = {"workload": f"directed rmat{PPR_SCALE} ef{PPR_EF} seed {PPR_SEED}, {PPR_SEEDS} one-hot seeds",
+                  "vertices": V, "arcs": E, "ms": pms, "loop_of_single_launches_ms": sms * PPR_SEEDS / k,
+                  "loop_sample": f"{k} single-seed solves timed, scaled to {PPR_SEEDS}",
+                  "speedup_vs_loop": sms * PPR_SEEDS / k / pms, "iterations_max": int(pit.max()),
+                  "iterations_mean": float(pit.mean()),
+                  "achieved_gbs": psts[-1]["bytes_moved"] / (pms * 1e-3) / 1e9,
+                  "rel_l1_vs_single_seed_solve": err}
+    G.destroy()
+    del pout, x1, tp
+    torch.cuda.empty_cache()
+    # ---- Brandes over 4,096 seeded sources, and one source per launch ----
+    Bg = N.Graph.rmat(BCB_SCALE, BCB_EF, BCB_SEED, directed=False)
+    Vb, Eb, _ = Bg.info()
+    src = np.random.default_rng(BCB_SEED).choice(Vb, BCB_SOURCES, replace=False).astype(np.uint32)
+    part = torch.empty(Vb, dtype=torch.float64, device="cuda")
+    Bg.betweenness_device(part.data_ptr(), sources=src[:256], stream=sp)
+    torch.cuda.synchronize()
+    barrier(ws)
+    cms, csts = _timed(stream, 1, lambda: Bg.betweenness_device(part.data_ptr(), sources=src, stream=sp))
+    cms = max_over_ranks(cms, ws)
+    launches += int(csts[0]["launches"])
+    k1 = 64
+    one_ms, osts = _timed(stream, 1, lambda: [Bg.betweenness_device(part.data_ptr(), sources=src[i:i + 1], stream=sp)
+                                              for i in range(k1)])
+    launches += sum(int(s2["launches"]) for s2 in osts[0])
+    res["brandes"] = {"workload": f"undirected rmat{BCB_SCALE} ef{BCB_EF} seed {BCB_SEED}, {BCB_SOURCES} seeded sources",
+                      "vertices": Vb, "arcs": Eb, "ms": cms, "gteps": BCB_SOURCES * Eb / (cms * 1e-3) / 1e9,
+                      "loop_of_single_launches_ms": one_ms * BCB_SOURCES / k1,
+                      "loop_sample": f"{k1} one-source launches timed, scaled to {BCB_SOURCES}",
+                      "speedup_vs_loop": one_ms * BCB_SOURCES / k1 / cms, "max_depth": int(csts[0]["max_depth"])}
+    Bg.destroy()
+    return res, launches
+
+
 def run_zog(args):
     import torch
 
@@ -498,6 +615,13 @@ def run_zog(args):
         launches += nl
         torch.cuda.empty_cache()
 
+    # ---------------- batched forms ----------------
+    batched = None
+    if not args.no_batched:
+        batched, nl = batched_block(N, args, stream, ws)
+        launches += nl
+        torch.cuda.empty_cache()
+
     # ---------------- Brandes, all sources, sharded over ranks ----------------
     bc_line = None
     if not args.no_brandes:
@@ -571,6 +695,7 @@ def run_zog(args):
             "precision_mixed": mixed,
             "learned_start": learned,
             "barabasi_albert": ba,
+            "batched": batched,
             "brandes": bc_line,
         }
         print(json.dumps(line), flush=True)
@@ -597,6 +722,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm start")
     ap.add_argument("--no-ba", action="store_true", help="skip the Barabasi-Albert graph")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched forms")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")

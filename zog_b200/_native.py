@@ -39,6 +39,7 @@ EXPORTS = (
     "zogcu_gnn_set_params", "zogcu_gnn_loss_grad", "zogcu_gnn_train_step", "zogcu_gnn_predict",
     "zogcu_gnn_save", "zogcu_gnn_load",
     "zogcu_batch_create", "zogcu_batch_destroy", "zogcu_batch_info", "zogcu_batch_pagerank",
+    "zogcu_ppr",
 )
 
 
@@ -140,6 +141,7 @@ def load(path: str | None = None):
         L.zogcu_gnn_predict.argtypes = [vp, vp, vp, i32, vp, vp]
         L.zogcu_gnn_save.argtypes = [vp, C.c_char_p]
         L.zogcu_gnn_load.argtypes = [C.c_char_p, pp]
+        L.zogcu_ppr.argtypes = [vp, vp, u32, dbl, u64, dbl, C.POINTER(PrOpts), vp, vp, C.POINTER(Stats)]
         L.zogcu_batch_create.argtypes = [vp, u32, pp]
         L.zogcu_batch_destroy.argtypes = [vp]
         L.zogcu_batch_info.argtypes = [vp, C.POINTER(u32), C.POINTER(u64), C.POINTER(u64), vp]
@@ -348,6 +350,31 @@ class Graph:
         st = Stats()
         check(load().zogcu_eigenvector(self.handle, int(max_iterations), float(tolerance), _ptr(res), C.byref(st)))
         return (res[:V], st.as_dict()) if stats else res[:V]
+
+    def ppr(self, seeds, damping=0.85, max_iterations=100, tolerance=1e-4, stats=False):
+        """Personalised PageRank of every seed: (num_seeds, V) array and the
+        per-seed iteration counts."""
+        V, _, _ = self.info()
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        res = np.zeros((max(sd.size, 1), max(V, 1)), np.float64)
+        its = np.zeros(max(sd.size, 1), np.uint64)
+        st = Stats()
+        check(load().zogcu_ppr(self.handle, _ptr(sd), sd.size, float(damping), int(max_iterations),
+                               float(tolerance), None, _ptr(res), _ptr(its), C.byref(st)))
+        r = (res[:sd.size, :V], its[:sd.size])
+        return (*r, st.as_dict()) if stats else r
+
+    def ppr_device(self, seeds, out_ptr: int, damping=0.85, max_iterations=100, tolerance=1e-4, stream=None):
+        """Personalised PageRank into a device buffer (num_seeds * V, f64, seed-major)."""
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        its = np.zeros(max(sd.size, 1), np.uint64)
+        st = Stats()
+        o = PrOpts(C.sizeof(PrOpts), PREC_FP64, None, None, 1, 0, stream)
+        check(load().zogcu_ppr(self.handle, _ptr(sd), sd.size, float(damping), int(max_iterations),
+                               float(tolerance), C.byref(o), out_ptr, _ptr(its), C.byref(st)))
+        d = st.as_dict()
+        d["per_seed_iterations"] = its[:sd.size]
+        return d
 
     def bfs_sigma(self, sources):
         V, _, _ = self.info()

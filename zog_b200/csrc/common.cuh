@@ -68,6 +68,13 @@ struct DevArray {
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// PageRank work-item schedule (shared by the single-vector kernel and the
+// personalised SpMM): row blocks hold at most kWarpRows rows, long rows are
+// cut into chunks of kLongChunk arcs.
+constexpr int kWarpRows = 64;
+constexpr int kLongChunk = 4096;
+enum : uint32_t { kTaskBlock = 0, kTaskRow = 1, kTaskChunk = 2 };
+
 // One PageRank work item (8 bytes): kind = b >> 30.
 //   kind 0: rows [a, b & 0x3FFFFFFF) of the degree-ranked in-CSR
 //   kind 1: the single row a
@@ -133,8 +140,10 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src,
                                   const uint32_t* d_dst, uint64_t E, bool reverse_within_source,
                                   const uint8_t* h_node_deleted, cudaStream_t stream);
 
-// PageRank schedule (pagerank.cu).
+// PageRank schedule (pagerank.cu): the degree-ranked view, and the work-item
+// list of row blocks of at most nnz (128 or 256) arcs.
 int ensure_pr_schedule(Graph* g, cudaStream_t stream);
+int ensure_task_list(Graph* g, int nnz, cudaStream_t stream);
 
 // Small helper: number of SMs of the current device.
 int sm_count();

@@ -51,11 +51,7 @@
 
 namespace zogcu {
 
-constexpr int kWarpRows = 64;            // rows per row block (2 per lane)
 constexpr int kShortLen = 32;            // in-degree summed by a single lane
-constexpr int kLongChunk = 4096;         // arcs per chunk of a long row
-
-enum : uint32_t { kTaskBlock = 0, kTaskRow = 1, kTaskChunk = 2 };
 
 // Kernel configurations the autotuner chooses from.
 struct PrConfig {
@@ -720,7 +716,7 @@ int ensure_pr_schedule(Graph* g, cudaStream_t s) {
   return ZOGCU_OK;
 }
 
-static int ensure_task_list(Graph* g, int nnz, cudaStream_t s) {
+int ensure_task_list(Graph* g, int nnz, cudaStream_t s) {
   std::lock_guard<std::mutex> lk(g->mu);
   PrTaskList& L = g->pr.lists[list_index(nnz)];
   if (L.built) return ZOGCU_OK;
