@@ -420,7 +420,7 @@ def batched_block(N, args, stream, ws):
     pms = max_over_ranks(pms, ws)
     launches += sum(int(s2["launches"]) for s2 in psts)
     # loop of single-seed solves (the teleport form of the single-vector kernel), on a sample of seeds
-    k = 16
+    k = min(16, PPR_SEEDS)
     x1 = torch.empty(V, dtype=torch.float64, device="cuda")
     tp = torch.zeros(V, dtype=torch.float64, device="cuda")
 
@@ -707,7 +707,7 @@ def run_zog(args):
 
 
 def main():
-    global PR_SCALE, PR_SEED, BC_SCALE, BC_SEED
+    global PR_SCALE, PR_SEED, BC_SCALE, BC_SEED, BATCH_GRAPHS, PPR_SCALE, PPR_SEED, PPR_SEEDS, BCB_SCALE, BCB_SEED, BA_N
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -727,6 +727,11 @@ def main():
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--bc-scale", type=int, default=BC_SCALE, help="R-MAT scale of the Brandes graph")
+    ap.add_argument("--batch-graphs", type=int, default=BATCH_GRAPHS, help="graphs of the batched form")
+    ap.add_argument("--ppr-scale", type=int, default=PPR_SCALE, help="R-MAT scale of the personalised form")
+    ap.add_argument("--ppr-seeds", type=int, default=PPR_SEEDS, help="seeds of the personalised form")
+    ap.add_argument("--bcb-scale", type=int, default=BCB_SCALE, help="R-MAT scale of the batched Brandes form")
+    ap.add_argument("--ba-n", type=int, default=BA_N, help="nodes of the Barabasi-Albert graph")
     ap.add_argument("--ref-pr-iterations", type=int, default=28,
                     help="iterations the full solve takes on the benchmark graph: 28 for the seeded scale-24 "
                          "R-MAT (the GPU arm measures the same count, since both follow the reference iteration)")
@@ -735,6 +740,11 @@ def main():
         PR_SCALE, PR_SEED = args.pr_scale, 1000 + args.pr_scale
     if args.bc_scale != BC_SCALE:
         BC_SCALE, BC_SEED = args.bc_scale, 1000 + args.bc_scale
+    BATCH_GRAPHS, PPR_SEEDS, BA_N = args.batch_graphs, args.ppr_seeds, args.ba_n
+    if args.ppr_scale != PPR_SCALE:
+        PPR_SCALE, PPR_SEED = args.ppr_scale, 1000 + args.ppr_scale
+    if args.bcb_scale != BCB_SCALE:
+        BCB_SCALE, BCB_SEED = args.bcb_scale, 1000 + args.bcb_scale
     if args.impl == "reference":
         return run_reference(args)
     return run_zog(args)
