@@ -109,7 +109,8 @@ ZOGCU_API int zogcu_abi_version(void);
  * (lib/zog/.Elixir.Zog.ResourceGraph.zig:94-106 with buildGraph :26-35): node
  * ids 0..node_count-1, edges added in list order (head insertion, so each
  * node's successors iterate in reverse list order, array_graph.zig:88-108).
- * `weight` may be NULL (all 1.0).  Duplicate arcs and self-loops are kept. */
+ * `weight` may be NULL (all 1.0); PageRank and unweighted betweenness ignore
+ * it, weighted betweenness reads it.  Duplicate arcs and self-loops are kept. */
 ZOGCU_API int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from,
                                   const uint32_t* to, const double* weight,
                                   uint64_t num_edges, zogcu_graph** out);
@@ -123,11 +124,20 @@ ZOGCU_API int zogcu_graph_create_from_device_edges(uint32_t node_count, const ui
  * (array_graph.zig:21-38), as a NIF holding a GraphRes can pass them:
  * first_edge / next_edge use 0xFFFFFFFF for null; deleted nodes and edges are
  * skipped exactly like SuccessorIterator.next (array_graph.zig:164-180).
- * node_deleted / edge_deleted / data may be NULL (none deleted / unit). */
+ * node_deleted / edge_deleted may be NULL (none deleted).  Arc weights are
+ * not read (every weight is 1.0); the _weighted form below keeps them. */
 ZOGCU_API int zogcu_graph_create_from_arraygraph(uint32_t node_capacity, const uint32_t* first_edge,
                                        const uint8_t* node_deleted, uint64_t edge_capacity,
                                        const uint32_t* to, const uint32_t* next_edge,
                                        const uint8_t* edge_deleted, zogcu_graph** out);
+
+/* As above, also keeping the edges' f64 weights (the ArrayGraph's `data`
+ * slice, one per edge slot) for weighted betweenness. */
+ZOGCU_API int zogcu_graph_create_from_arraygraph_weighted(uint32_t node_capacity, const uint32_t* first_edge,
+                                                          const uint8_t* node_deleted, uint64_t edge_capacity,
+                                                          const uint32_t* to, const uint32_t* next_edge,
+                                                          const uint8_t* edge_deleted, const double* data,
+                                                          zogcu_graph** out);
 
 /* Seeded R-MAT graph generated on the device (benchmark input): ef * 2^scale
  * raw edges, self-loops and duplicates removed, inserted in (src,dst) order;
@@ -248,6 +258,21 @@ ZOGCU_API int zogcu_betweenness_unweighted(zogcu_graph* g, double* out_scores, z
 /* As above with options (source subset, batch size, device output, stream). */
 ZOGCU_API int zogcu_betweenness_unweighted_ex(zogcu_graph* g, const zogcu_bc_opts* opts,
                                     double* out_scores, zogcu_stats* stats);
+
+/* Replaces nif_betweenness_f64 (.zig:123-132 -> centrality.betweennessF64
+ * :1355-1357 -> betweenness, ArrayGraph branch, centrality.zig:528-682):
+ * Dijkstra-based Brandes over the arc weights (1.0 where none were given),
+ * unnormalised, every live source ascending or opts->sources (opts may be
+ * NULL; its batch field is ignored).  Weights must be positive and finite; a
+ * shortest path through an arc of effective length zero (fl(d + w) == d) is
+ * reported as ZOGCU_ERR_INVALID_ARGUMENT, since the reference's counts would
+ * then depend on its heap's tie order. */
+ZOGCU_API int zogcu_betweenness_weighted(zogcu_graph* g, const zogcu_bc_opts* opts, double* out_scores,
+                                         zogcu_stats* stats);
+
+/* The arc weights in out-CSR (successor) order, out_weights[E] (1.0 each when
+ * the graph was built without weights). */
+ZOGCU_API int zogcu_graph_export_weights(const zogcu_graph* g, double* out_weights);
 
 /* BFS intermediates of the Brandes forward phase (centrality.zig:741-767) for
  * `num_sources` sources: dist_out[i*V + v] (0xFFFFFFFF = unreached) and

@@ -79,6 +79,7 @@ def lib():
     L.og_rmat.restype = vp
     L.og_rmat.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_int]
     L.og_edges_count.restype = C.c_uint64
+    L.og_betweenness_weighted.argtypes = [vp, C.c_void_p, C.c_uint64, _f64p, C.POINTER(C.c_uint32)]
     L.og_ba.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.c_int]
     L.og_ba.restype = vp
     L.og_ws.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, C.c_int]
@@ -204,6 +205,18 @@ class ArrayGraph:
         out = np.zeros(max(self.node_capacity, 1), np.float64)
         ovf = C.c_uint32(0)
         lib().og_betweenness_sources(self._h, src, len(src), out, C.byref(ovf))
+        return out[: self.node_capacity], bool(ovf.value)
+
+    def betweenness_weighted(self, sources=None):
+        """nif_betweenness_f64 restated (centrality.zig:528-682): every live
+        source ascending, or `sources`."""
+        out = np.zeros(max(self.node_capacity, 1), np.float64)
+        ovf = C.c_uint32(0)
+        if sources is None:
+            lib().og_betweenness_weighted(self._h, None, 0, out, C.byref(ovf))
+        else:
+            src = np.ascontiguousarray(sources, dtype=np.uint32)
+            lib().og_betweenness_weighted(self._h, src.ctypes.data, len(src), out, C.byref(ovf))
         return out[: self.node_capacity], bool(ovf.value)
 
     def bfs(self, s):

@@ -32,6 +32,8 @@
 //     teleport vector (personalised PageRank), uniform dangling mass;
 //   * og_rmat: the seeded R-MAT generator whose definition the CUDA generator
 //     shares (counter-based SplitMix64; see rmat_edge below);
+//   * og_betweenness_weighted: the weighted (Dijkstra) Brandes of
+//     centrality.zig:528-682, restated loop for loop like the unweighted one;
 //   * og_ba / og_ws: the seeded Barabasi-Albert and Watts-Strogatz generators
 //     (generator.ex:132-253 models), written independently of the library's.
 
@@ -134,6 +136,19 @@ struct ArrayGraph {
       if (!edge_deleted[idx]) {
         uint32_t dest = to[idx];
         if (!node_deleted[dest]) f(dest);
+      }
+      idx = nxt;
+    }
+  }
+  // the same walk, also handing over the edge's f64 data (the weight)
+  template <class F>
+  void for_each_successor_edge(uint32_t id, F&& f) const {
+    uint32_t idx = first_edge[id];
+    while (idx != kNull) {
+      uint32_t nxt = next_edge[idx];
+      if (!edge_deleted[idx]) {
+        uint32_t dest = to[idx];
+        if (!node_deleted[dest]) f(dest, data[idx]);
       }
       idx = nxt;
     }
@@ -316,6 +331,94 @@ void eigenvector_arraygraph(const ArrayGraph& g, uint64_t max_iter, double tol, 
   }
   for (uint32_t v : nodes) out[v] = curr[v];
   *iters_out = it;
+}
+
+// ---------------------------------------------------------------------------
+// betweenness (weighted, f64), ArrayGraph branch   centrality.zig:528-682
+// (betweennessF64 :1355-1357: Weight = f64, zero = 0.0, add = a + b,
+// compare = std.math.order).  The heap is a binary min-heap on the distance;
+// the reference's std.PriorityQueue pops equal distances in its own order,
+// which with positive weights changes only the summation order of delta.
+// ---------------------------------------------------------------------------
+void betweenness_weighted_arraygraph(const ArrayGraph& g, const uint32_t* sources, size_t ns, double* out,
+                                     uint32_t* overflow_out) {
+  const size_t V = g.node_capacity();
+  std::vector<double> dist(V);
+  std::vector<uint8_t> has_dist(V);  // ?f64: 0 = null
+  std::vector<uint64_t> sigma(V);
+  std::vector<double> delta(V);
+  std::vector<std::vector<uint32_t>> preds(V);
+  std::vector<std::pair<double, uint32_t>> heap;  // (d, node)
+  std::vector<uint32_t> stack;
+  std::vector<double> scores(V, 0.0);
+  uint32_t overflow = 0;
+  auto cmp = [](const std::pair<double, uint32_t>& a, const std::pair<double, uint32_t>& b) {
+    return a.first > b.first;  // min-heap on d
+  };
+  for (size_t si = 0; si < ns; ++si) {
+    const uint32_t s = sources[si];
+    std::fill(has_dist.begin(), has_dist.end(), 0);  // :592-599
+    std::fill(sigma.begin(), sigma.end(), 0);
+    std::fill(delta.begin(), delta.end(), 0.0);
+    for (auto& p : preds) p.clear();
+    heap.clear();
+    stack.clear();
+    dist[s] = 0.0;  // :602-605
+    has_dist[s] = 1;
+    sigma[s] = 1;
+    heap.push_back({0.0, s});
+    std::push_heap(heap.begin(), heap.end(), cmp);
+    while (!heap.empty()) {  // :607-642
+      std::pop_heap(heap.begin(), heap.end(), cmp);
+      const double d_v = heap.back().first;
+      const uint32_t v = heap.back().second;
+      heap.pop_back();
+      const double current_best = has_dist[v] ? dist[v] : d_v;
+      if (d_v > current_best) continue;  // compare(d_v, current_best) == .gt
+      stack.push_back(v);
+      g.for_each_successor_edge(v, [&](uint32_t w, double weight) {
+        const double new_dist = d_v + weight;
+        if (has_dist[w]) {
+          const double old_dist = dist[w];
+          if (new_dist < old_dist) {
+            dist[w] = new_dist;
+            sigma[w] = sigma[v];
+            preds[w].clear();
+            preds[w].push_back(v);
+            heap.push_back({new_dist, w});
+            std::push_heap(heap.begin(), heap.end(), cmp);
+          } else if (new_dist == old_dist) {
+            const uint64_t before = sigma[w];
+            sigma[w] += sigma[v];  // usize add; wraps like a ReleaseFast build
+            if (sigma[w] < before) overflow = 1;
+            preds[w].push_back(v);
+          }
+        } else {
+          dist[w] = new_dist;
+          has_dist[w] = 1;
+          sigma[w] = sigma[v];
+          preds[w].push_back(v);
+          heap.push_back({new_dist, w});
+          std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+      });
+    }
+    size_t i = stack.size();  // :645-662
+    while (i > 0) {
+      i -= 1;
+      const uint32_t v = stack[i];
+      const double sigma_v_f = (double)sigma[v];
+      const double delta_v = delta[v];
+      for (uint32_t u : preds[v]) {
+        const double sigma_u_f = (double)sigma[u];
+        const double c = (sigma_u_f / sigma_v_f) * (1.0 + delta_v);
+        delta[u] += c;
+      }
+      if (v != s) scores[v] += delta_v;
+    }
+  }
+  for (size_t v = 0; v < V; ++v) out[v] = g.has_node((uint32_t)v) ? scores[v] : 0.0;  // :664-671, extractScores
+  if (overflow_out) *overflow_out = overflow;
 }
 
 // ---------------------------------------------------------------------------
@@ -511,6 +614,17 @@ void og_betweenness_unweighted(void* h, double* out, uint32_t* overflow) {
 void og_betweenness_sources(void* h, const uint32_t* sources, uint64_t ns, double* out,
                             uint32_t* overflow) {
   betweenness_arraygraph(*(ArrayGraph*)h, sources, ns, out, overflow);
+}
+
+// nif_betweenness_f64 (.zig:123-132): every live node ascending, or a subset.
+void og_betweenness_weighted(void* h, const uint32_t* sources, uint64_t ns, double* out, uint32_t* overflow) {
+  auto* g = (ArrayGraph*)h;
+  if (sources) {
+    betweenness_weighted_arraygraph(*g, sources, ns, out, overflow);
+  } else {
+    std::vector<uint32_t> nodes = g->collect_nodes();
+    betweenness_weighted_arraygraph(*g, nodes.data(), nodes.size(), out, overflow);
+  }
 }
 
 // BFS intermediates of one source (centrality.zig:741-767): dist (0xFFFFFFFF =

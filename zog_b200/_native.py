@@ -39,7 +39,8 @@ EXPORTS = (
     "zogcu_gnn_set_params", "zogcu_gnn_loss_grad", "zogcu_gnn_train_step", "zogcu_gnn_predict",
     "zogcu_gnn_save", "zogcu_gnn_load",
     "zogcu_batch_create", "zogcu_batch_destroy", "zogcu_batch_info", "zogcu_batch_pagerank",
-    "zogcu_ppr",
+    "zogcu_ppr", "zogcu_betweenness_weighted", "zogcu_graph_export_weights",
+    "zogcu_graph_create_from_arraygraph_weighted",
 )
 
 
@@ -141,6 +142,9 @@ def load(path: str | None = None):
         L.zogcu_gnn_predict.argtypes = [vp, vp, vp, i32, vp, vp]
         L.zogcu_gnn_save.argtypes = [vp, C.c_char_p]
         L.zogcu_gnn_load.argtypes = [C.c_char_p, pp]
+        L.zogcu_betweenness_weighted.argtypes = [vp, C.POINTER(BcOpts), vp, C.POINTER(Stats)]
+        L.zogcu_graph_export_weights.argtypes = [vp, vp]
+        L.zogcu_graph_create_from_arraygraph_weighted.argtypes = [u32, vp, vp, u64, vp, vp, vp, vp, pp]
         L.zogcu_ppr.argtypes = [vp, vp, u32, dbl, u64, dbl, C.POINTER(PrOpts), vp, vp, C.POINTER(Stats)]
         L.zogcu_batch_create.argtypes = [vp, u32, pp]
         L.zogcu_batch_destroy.argtypes = [vp]
@@ -201,7 +205,7 @@ class Graph:
         return cls(h)
 
     @classmethod
-    def from_arraygraph(cls, first_edge, node_deleted, to, next_edge, edge_deleted) -> "Graph":
+    def from_arraygraph(cls, first_edge, node_deleted, to, next_edge, edge_deleted, data=None) -> "Graph":
         L = load()
         fe = np.ascontiguousarray(first_edge, dtype=np.uint32)
         nd = None if node_deleted is None else np.ascontiguousarray(node_deleted, dtype=np.uint8)
@@ -209,8 +213,13 @@ class Graph:
         ne = np.ascontiguousarray(next_edge, dtype=np.uint32)
         ed = None if edge_deleted is None else np.ascontiguousarray(edge_deleted, dtype=np.uint8)
         h = C.c_void_p()
-        check(L.zogcu_graph_create_from_arraygraph(fe.size, _ptr(fe), _ptr(nd), to_.size, _ptr(to_), _ptr(ne),
-                                                   _ptr(ed), C.byref(h)))
+        if data is None:
+            check(L.zogcu_graph_create_from_arraygraph(fe.size, _ptr(fe), _ptr(nd), to_.size, _ptr(to_), _ptr(ne),
+                                                       _ptr(ed), C.byref(h)))
+        else:
+            dt = np.ascontiguousarray(data, dtype=np.float64)
+            check(L.zogcu_graph_create_from_arraygraph_weighted(fe.size, _ptr(fe), _ptr(nd), to_.size, _ptr(to_),
+                                                                _ptr(ne), _ptr(ed), _ptr(dt), C.byref(h)))
         return cls(h)
 
     @classmethod
@@ -310,6 +319,32 @@ class Graph:
             check(load().zogcu_betweenness_unweighted_ex(self.handle, C.byref(o), _ptr(res), C.byref(st)))
         r = res[:V]
         return (r, st.as_dict()) if stats else r
+
+    def betweenness_weighted(self, sources=None, stats=False):
+        """Weighted (Dijkstra) betweenness over the arc weights."""
+        V, _, _ = self.info()
+        res = np.zeros(max(V, 1), np.float64)
+        st = Stats()
+        src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+        o = BcOpts(C.sizeof(BcOpts), 0, _ptr(src), 0 if src is None else src.size, 0, 0, None)
+        check(load().zogcu_betweenness_weighted(self.handle, C.byref(o), _ptr(res), C.byref(st)))
+        r = res[:V]
+        return (r, st.as_dict()) if stats else r
+
+    def betweenness_weighted_device(self, out_ptr: int, sources=None, stream=None) -> dict:
+        """Weighted betweenness into a device buffer (length V, f64)."""
+        st = Stats()
+        src = None if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+        o = BcOpts(C.sizeof(BcOpts), 0, _ptr(src), 0 if src is None else src.size, 1, 0, stream)
+        check(load().zogcu_betweenness_weighted(self.handle, C.byref(o), out_ptr, C.byref(st)))
+        return st.as_dict()
+
+    def export_weights(self):
+        """Arc weights in successor (out-CSR) order."""
+        _, E, _ = self.info()
+        w = np.zeros(max(E, 1), np.float64)
+        check(load().zogcu_graph_export_weights(self.handle, _ptr(w)))
+        return w[:E]
 
     def pagerank_device(self, out_ptr: int, damping=0.85, max_iterations=100, tolerance=1e-4, *,
                         precision=PREC_FP64, x0_ptr=None, teleport_ptr=None, stream=None) -> dict:

@@ -55,6 +55,19 @@ def betweenness_unweighted(builder: SoA):
     return _map_scores(builder, scores)
 
 
+def betweenness_f64(builder: SoA):
+    """centrality.ex:203-209: weighted (Dijkstra) betweenness over the
+    builder's f64 weights, unnormalised; halved for undirected builders."""
+    g = _graph(builder)
+    try:
+        scores = g.betweenness_weighted()
+    finally:
+        g.destroy()
+    if builder.kind == "undirected":
+        scores = scores * 0.5
+    return _map_scores(builder, scores)
+
+
 def eigenvector(builder: SoA, max_iterations: int = 100, tolerance: float = 0.0001):
     """centrality.ex:253-275, including the zero-vector fallback to a uniform
     1/sqrt(n) when every score is 0.0 and there is more than one node."""

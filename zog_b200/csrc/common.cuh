@@ -121,6 +121,8 @@ struct Graph {
   DevArray in_off32, out_off32;   // uint32_t[V+1] (when offsets32)
   DevArray in_col, out_col;       // uint32_t[E + 4] (padded for 16-byte loads)
   DevArray out_deg;               // uint32_t[V], kDeletedDegree for deleted slots
+  bool weighted = false;          // arc weights were given (else every weight is 1.0)
+  DevArray out_w;                 // double[E]: weight of each out-CSR arc (when weighted)
   DevArray live;                  // uint8_t[V] (when has_deleted)
   std::mutex mu;                  // guards lazy schedule builds
   PrSchedule pr;                  // PageRank schedule (built on first call)
@@ -136,9 +138,11 @@ int ensure_device(int* dev);
 // Builds a Graph from device edge arrays (src,dst) in ArrayGraph insertion
 // order (reverse_within_source = true) or already in successor order (false).
 // All endpoints must be < V and refer to live nodes.
+// d_w (may be null) holds one weight per edge in the same order as d_src / d_dst.
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src,
                                   const uint32_t* d_dst, uint64_t E, bool reverse_within_source,
-                                  const uint8_t* h_node_deleted, cudaStream_t stream);
+                                  const uint8_t* h_node_deleted, cudaStream_t stream,
+                                  const double* d_w = nullptr);
 
 // PageRank schedule (pagerank.cu): the degree-ranked view, and the work-item
 // list of row blocks of at most nnz (128 or 256) arcs.

@@ -159,6 +159,13 @@ __global__ void k_reverse_copy(const uint32_t* __restrict__ src, const uint32_t*
   }
 }
 
+__global__ void k_reverse_copy_u64(const unsigned long long* __restrict__ w, unsigned long long* __restrict__ out,
+                                   uint64_t E, int reverse) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = w[reverse ? (E - 1 - i) : i];
+}
+
 __global__ void k_validate(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t E,
                            uint32_t V, unsigned int* bad) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E;
@@ -211,7 +218,7 @@ static int counts_to_offsets(unsigned long long* d_cnt, uint64_t* d_off, uint32_
 
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, const uint32_t* d_dst,
                                   uint64_t E, bool reverse_within_source, const uint8_t* h_node_deleted,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, const double* d_w) {
   ZOGCU_TRY(ensure_device(&g->device));
   g->V = V;
   g->E = E;
@@ -264,6 +271,26 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
                                                vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
                                                0, bits, s));
+    if (d_w) {
+      // the same stable sort of the same keys carries the weights along
+      DevBuf wr, kd;
+      ZOGCU_TRY(wr.alloc(E * 8, s));
+      ZOGCU_TRY(kd.alloc(E * 4, s));
+      ZOGCU_TRY(g->out_w.alloc(E * 8));
+      k_reverse_copy_u64<<<grid_for(E), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(d_w),
+                                                     wr.as<unsigned long long>(), E, reverse_within_source ? 1 : 0);
+      ZOGCU_CUDA(cudaGetLastError());
+      size_t tmpw = 0;
+      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpw, ks.as<uint32_t>(), kd.as<uint32_t>(),
+                                                 wr.as<unsigned long long>(), g->out_w.as<unsigned long long>(),
+                                                 (int64_t)E, 0, bits, s));
+      DevBuf tw;
+      ZOGCU_TRY(tw.alloc(tmpw, s));
+      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tw.ptr, tmpw, ks.as<uint32_t>(), kd.as<uint32_t>(),
+                                                 wr.as<unsigned long long>(), g->out_w.as<unsigned long long>(),
+                                                 (int64_t)E, 0, bits, s));
+      g->weighted = true;
+    }
     // out offsets
     ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
     k_histogram<<<grid_for(E), 256, 0, s>>>(ks2.as<uint32_t>(), E, cnt.as<unsigned long long>());
@@ -383,7 +410,8 @@ static void rmat_thresholds(double a, double b, double c, uint64_t* ta, uint64_t
 // Validates device edge arrays (addEdge's hasNode check, array_graph.zig:88-89)
 // and builds the graph on stream s.
 static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_from, const uint32_t* d_to,
-                                       uint64_t num_edges, cudaStream_t s, zogcu_graph** out) {
+                                       uint64_t num_edges, cudaStream_t s, zogcu_graph** out,
+                                       const double* d_w = nullptr) {
   if (num_edges) {
     DevBuf bad;
     ZOGCU_TRY(bad.alloc(4, s));
@@ -397,7 +425,7 @@ static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_fr
   }
   std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
   if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
-  ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s));
+  ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s, d_w));
   *out = G.release();
   return ZOGCU_OK;
 }
@@ -446,7 +474,8 @@ int zogcu_graph_create_from_device_edges(uint32_t node_count, const uint32_t* d_
 
 int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, const uint32_t* to,
                                   const double* weight, uint64_t num_edges, zogcu_graph** out) {
-  (void)weight;  // PageRank and unweighted Brandes ignore weights (centrality.zig:936-941)
+  // PageRank and unweighted Brandes ignore the weights (centrality.zig:936-941);
+  // weighted betweenness reads them (centrality.zig:528-682)
   if (!out) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out is null");
   *out = nullptr;
   if (num_edges && (!from || !to)) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "edge arrays are null");
@@ -458,24 +487,32 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
   DevBuf df, dt;
   ZOGCU_TRY(df.alloc(num_edges * 4, sg.s));
   ZOGCU_TRY(dt.alloc(num_edges * 4, sg.s));
+  DevBuf dw;
   if (num_edges) {
     ZOGCU_CUDA(cudaMemcpyAsync(df.ptr, from, num_edges * 4, cudaMemcpyHostToDevice, sg.s));
     ZOGCU_CUDA(cudaMemcpyAsync(dt.ptr, to, num_edges * 4, cudaMemcpyHostToDevice, sg.s));
+    if (weight) {
+      ZOGCU_TRY(dw.alloc(num_edges * 8, sg.s));
+      ZOGCU_CUDA(cudaMemcpyAsync(dw.ptr, weight, num_edges * 8, cudaMemcpyHostToDevice, sg.s));
+    }
   }
-  return create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out);
+  return create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out,
+                                     weight ? dw.as<double>() : nullptr);
 }
 
-int zogcu_graph_create_from_arraygraph(uint32_t V, const uint32_t* first_edge, const uint8_t* node_deleted,
-                                       uint64_t edge_capacity, const uint32_t* to, const uint32_t* next_edge,
-                                       const uint8_t* edge_deleted, zogcu_graph** out) {
+static int create_from_arraygraph(uint32_t V, const uint32_t* first_edge, const uint8_t* node_deleted,
+                                  uint64_t edge_capacity, const uint32_t* to, const uint32_t* next_edge,
+                                  const uint8_t* edge_deleted, const double* data, zogcu_graph** out) {
   if (!out) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out is null");
   *out = nullptr;
   if (V && !first_edge) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "first_edge is null");
   if (edge_capacity && (!to || !next_edge)) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "edge slices are null");
   // Walk every live node's list like SuccessorIterator.next (array_graph.zig:164-180).
   std::vector<uint32_t> src, dst;
+  std::vector<double> wts;
   src.reserve(edge_capacity);
   dst.reserve(edge_capacity);
+  if (data) wts.reserve(edge_capacity);
   for (uint32_t v = 0; v < V; ++v) {
     if (node_deleted && node_deleted[v]) continue;
     uint32_t idx = first_edge[v];
@@ -490,6 +527,7 @@ int zogcu_graph_create_from_arraygraph(uint32_t V, const uint32_t* first_edge, c
         if (!(node_deleted && node_deleted[d])) {
           src.push_back(v);
           dst.push_back(d);
+          if (data) wts.push_back(data[idx]);
         }
       }
       idx = nxt;
@@ -500,19 +538,40 @@ int zogcu_graph_create_from_arraygraph(uint32_t V, const uint32_t* first_edge, c
   StreamGuard sg;
   ZOGCU_TRY(sg.init(nullptr));
   uint64_t E = src.size();
-  DevBuf df, dt;
+  DevBuf df, dt, dw;
   ZOGCU_TRY(df.alloc(E * 4, sg.s));
   ZOGCU_TRY(dt.alloc(E * 4, sg.s));
   if (E) {
     ZOGCU_CUDA(cudaMemcpyAsync(df.ptr, src.data(), E * 4, cudaMemcpyHostToDevice, sg.s));
     ZOGCU_CUDA(cudaMemcpyAsync(dt.ptr, dst.data(), E * 4, cudaMemcpyHostToDevice, sg.s));
+    if (data) {
+      ZOGCU_TRY(dw.alloc(E * 8, sg.s));
+      ZOGCU_CUDA(cudaMemcpyAsync(dw.ptr, wts.data(), E * 8, cudaMemcpyHostToDevice, sg.s));
+    }
   }
   std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
   if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
   ZOGCU_TRY(build_graph_from_device_edges(&G->g, V, df.as<uint32_t>(), dt.as<uint32_t>(), E,
-                                          /*already successor order*/ false, node_deleted, sg.s));
+                                          /*already successor order*/ false, node_deleted, sg.s,
+                                          data && E ? dw.as<double>() : nullptr));
+  if (data) G->g.weighted = true;
   *out = G.release();
   return ZOGCU_OK;
+}
+
+int zogcu_graph_create_from_arraygraph(uint32_t V, const uint32_t* first_edge, const uint8_t* node_deleted,
+                                       uint64_t edge_capacity, const uint32_t* to, const uint32_t* next_edge,
+                                       const uint8_t* edge_deleted, zogcu_graph** out) {
+  return create_from_arraygraph(V, first_edge, node_deleted, edge_capacity, to, next_edge, edge_deleted, nullptr,
+                                out);
+}
+
+int zogcu_graph_create_from_arraygraph_weighted(uint32_t V, const uint32_t* first_edge, const uint8_t* node_deleted,
+                                                uint64_t edge_capacity, const uint32_t* to,
+                                                const uint32_t* next_edge, const uint8_t* edge_deleted,
+                                                const double* data, zogcu_graph** out) {
+  if (edge_capacity && !data) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "data is null");
+  return create_from_arraygraph(V, first_edge, node_deleted, edge_capacity, to, next_edge, edge_deleted, data, out);
 }
 
 int zogcu_graph_generate_rmat(int scale, int edge_factor, uint64_t seed, double a, double b, double c,

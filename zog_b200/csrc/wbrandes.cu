@@ -1,0 +1,419 @@
+// wbrandes.cu -- weighted Brandes betweenness on the device.
+//
+// Reference: priv/zog/src/centrality.zig:528-682 (`betweenness`, ArrayGraph
+// branch, called through betweennessF64 :1355-1357 by nif_betweenness_f64).
+// Per source s, in ascending id order, a Dijkstra pass with a lazy-deletion
+// binary heap computes f64 distances (new = d_v + w, compared with
+// std.math.order: exact equality is a tie), shortest-path counts sigma
+// (usize; a tie adds, a strict improvement resets) and predecessor lists; the
+// reverse settle order then accumulates delta[u] += (sigma_u/sigma_v)(1+delta_v)
+// over predecessors and adds delta_v to the score of every v != s.
+//
+// With positive weights every predecessor of v on a shortest path has a
+// strictly smaller distance, so the distances are the fixed point
+// D(w) = min over arcs v->w of fl(D(v) + w), sigma(w) is the sum of sigma(v)
+// over the arcs with fl(D(v) + w) == D(w) (multi-arcs counted), and neither
+// depends on the order in which the heap pops ties -- which lets a parallel
+// algorithm reproduce them exactly:
+//   1. distances: Bellman-Ford rounds over a per-node frontier mask with a
+//      64-bit atomic min on the bit pattern of non-negative doubles (ordered
+//      like the values);
+//   2. sigma: the shortest-path DAG is swept in topological rounds (each node
+//      counts its DAG in-arcs; the last predecessor to add its sigma makes the
+//      node ready for the next round), which also numbers the rounds;
+//   3. delta: rounds in reverse, each node pulling (sigma_v / sigma_w)(1 +
+//      delta_w) from its DAG successors -- the reference's per-term value.
+// 32 sources run side by side: node-major rows of 32 (distance, sigma, delta,
+// round, in-count), one warp per node, lane b = source b.  Rounds are chained
+// launches with device flags (a launch whose round has no work returns at
+// once); the host checks the flags every 32 launches.  No kernel waits on
+// another.
+//
+// An arc of effective length zero on a shortest path (fl(D + w) == D, for
+// w <= 0 or w below half an ulp of D) would make the reference's sigma depend
+// on its heap's tie order; weights must be positive and finite, and such an
+// arc is reported as an error instead of guessed at.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace zogcu {
+namespace {
+
+constexpr int kWb = 32;                                     // sources per batch
+constexpr unsigned long long kInf = 0x7FF0000000000000ull;  // +inf
+constexpr uint32_t kNoRound = 0xFFFFFFFFu;
+constexpr int kWbChain = 32;                                // launches between host checks
+
+enum : int { kFlagZeroArc = 0, kFlagOverflow = 1, kFlagBadWeight = 2, kFlagMaxRound = 3, kFlags = 4 };
+
+__device__ __forceinline__ double wt_of(const double* __restrict__ w, uint32_t j) { return w ? __ldg(w + j) : 1.0; }
+
+__global__ void k_wb_check_weights(const double* __restrict__ w, uint64_t E, uint32_t* __restrict__ flags) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < E; j += (uint64_t)gridDim.x * blockDim.x) {
+    const double x = w[j];
+    if (!(x > 0.0) || !(x <= 1.7976931348623157e308)) atomicOr(flags + kFlagBadWeight, 1u);
+  }
+}
+
+__global__ void k_wb_init(uint32_t V, unsigned long long* __restrict__ dist, unsigned long long* __restrict__ sigma,
+                          double* __restrict__ delta, uint32_t* __restrict__ round, uint32_t* __restrict__ cnt,
+                          uint32_t* __restrict__ mask0, uint32_t* __restrict__ mask1) {
+  const uint64_t n = (uint64_t)V * kWb;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    dist[i] = kInf;
+    sigma[i] = 0;
+    delta[i] = 0.0;
+    round[i] = kNoRound;
+    cnt[i] = 0;
+    if (i < V) {
+      mask0[i] = 0;
+      mask1[i] = 0;
+    }
+  }
+}
+
+// Lane b < ns: distance 0, sigma 1 and round 0 at its source, which joins the
+// first frontier / ready set.
+__global__ void k_wb_seed(const uint32_t* __restrict__ src, uint32_t ns, unsigned long long* __restrict__ dist,
+                          unsigned long long* __restrict__ sigma, uint32_t* __restrict__ round,
+                          uint32_t* __restrict__ mask0) {
+  const uint32_t b = threadIdx.x;
+  if (b < ns) {
+    const uint32_t s = src[b];
+    dist[(size_t)s * kWb + b] = 0ull;  // +0.0
+    sigma[(size_t)s * kWb + b] = 1ull;
+    round[(size_t)s * kWb + b] = 0;
+    atomicOr(mask0 + s, 1u << b);
+  }
+}
+
+// Phase 1, round k: relax the out-arcs of every (node, source) in the frontier.
+__global__ void __launch_bounds__(256) k_wb_relax(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                  const double* __restrict__ w, uint32_t V,
+                                                  unsigned long long* __restrict__ dist, uint32_t* __restrict__ mcur,
+                                                  uint32_t* __restrict__ mnext, uint32_t* __restrict__ work,
+                                                  uint32_t k) {
+  if (*(volatile uint32_t*)(work + k) == 0) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  bool any = false;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+    const uint32_t m = mcur[v];
+    if (m == 0) continue;
+    const bool on = (m >> lane) & 1u;
+    const double dv = on ? __longlong_as_double((long long)dist[(size_t)v * kWb + lane]) : 0.0;
+    __syncwarp();
+    if (lane == 0) mcur[v] = 0;
+    const uint32_t b = off[v], e = off[v + 1];
+    for (uint32_t j = b; j < e; ++j) {
+      const uint32_t u = __ldg(col + j);
+      const double wt = wt_of(w, j);
+      if (on) {
+        const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(dv, wt));
+        const unsigned long long old = atomicMin(dist + (size_t)u * kWb + lane, nd);
+        if (nd < old) {
+          atomicOr(mnext + u, 1u << lane);
+          any = true;
+        }
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, any) && lane == 0) work[k + 1] = 1u;
+}
+
+// Phase 2a: DAG in-arc counts (and the zero-length check).
+__global__ void __launch_bounds__(256) k_wb_dagcount(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                     const double* __restrict__ w, uint32_t V,
+                                                     const unsigned long long* __restrict__ dist,
+                                                     uint32_t* __restrict__ cnt, uint32_t* __restrict__ flags) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+    const unsigned long long dvb = dist[(size_t)v * kWb + lane];
+    const bool on = dvb != kInf;
+    if (!__any_sync(0xffffffffu, on)) continue;
+    const double dv = __longlong_as_double((long long)dvb);
+    const uint32_t b = off[v], e = off[v + 1];
+    for (uint32_t j = b; j < e; ++j) {
+      const uint32_t u = __ldg(col + j);
+      const double wt = wt_of(w, j);
+      if (on) {
+        const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(dv, wt));
+        const unsigned long long du = dist[(size_t)u * kWb + lane];
+        if (nd == du) {
+          atomicAdd(cnt + (size_t)u * kWb + lane, 1u);
+          if (du == dvb) atomicOr(flags + kFlagZeroArc, 1u);
+        }
+      }
+    }
+  }
+}
+
+// Phase 2b, round k: ready nodes add their sigma along DAG arcs; a node whose
+// last DAG predecessor has added becomes ready in round k + 1.
+__global__ void __launch_bounds__(256) k_wb_sigma(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                  const double* __restrict__ w, uint32_t V,
+                                                  const unsigned long long* __restrict__ dist,
+                                                  unsigned long long* __restrict__ sigma, uint32_t* __restrict__ cnt,
+                                                  uint32_t* __restrict__ round, uint32_t* __restrict__ mcur,
+                                                  uint32_t* __restrict__ mnext, uint32_t* __restrict__ work,
+                                                  uint32_t* __restrict__ flags, uint32_t k) {
+  if (*(volatile uint32_t*)(work + k) == 0) return;
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  bool any = false;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+    const uint32_t m = mcur[v];
+    if (m == 0) continue;
+    const bool on = (m >> lane) & 1u;
+    const unsigned long long sv = on ? sigma[(size_t)v * kWb + lane] : 0ull;
+    const double dv = on ? __longlong_as_double((long long)dist[(size_t)v * kWb + lane]) : 0.0;
+    __syncwarp();
+    if (lane == 0) mcur[v] = 0;
+    const uint32_t b = off[v], e = off[v + 1];
+    for (uint32_t j = b; j < e; ++j) {
+      const uint32_t u = __ldg(col + j);
+      const double wt = wt_of(w, j);
+      if (on) {
+        const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(dv, wt));
+        const size_t iu = (size_t)u * kWb + lane;
+        if (nd == dist[iu]) {
+          const unsigned long long old = atomicAdd(sigma + iu, sv);  // wraps modulo 2^64 like usize
+          if (old + sv < old) atomicOr(flags + kFlagOverflow, 1u);
+          if (atomicSub(cnt + iu, 1u) == 1u) {
+            round[iu] = k + 1;
+            atomicOr(mnext + u, 1u << lane);
+            atomicMax(flags + kFlagMaxRound, k + 1);
+            any = true;
+          }
+        }
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, any) && lane == 0) work[k + 1] = 1u;
+}
+
+// Phase 3, round r (descending): delta_v = sum over DAG successors w of
+// (sigma_v / sigma_w)(1 + delta_w); the score of v gains delta_v for v != s.
+__global__ void __launch_bounds__(256) k_wb_delta(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                  const double* __restrict__ w, uint32_t V,
+                                                  const unsigned long long* __restrict__ dist,
+                                                  const unsigned long long* __restrict__ sigma,
+                                                  double* __restrict__ delta, const uint32_t* __restrict__ round,
+                                                  const uint32_t* __restrict__ src, uint32_t ns,
+                                                  double* __restrict__ bc, uint32_t r) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  const uint32_t my_src = (uint32_t)lane < ns ? src[lane] : 0xFFFFFFFFu;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+    const size_t iv = (size_t)v * kWb + lane;
+    const bool on = round[iv] == r;
+    if (!__any_sync(0xffffffffu, on)) continue;
+    const double dv = on ? __longlong_as_double((long long)dist[iv]) : 0.0;
+    const double sv = on ? __ull2double_rn(sigma[iv]) : 0.0;
+    double acc = 0.0;
+    const uint32_t b = off[v], e = off[v + 1];
+    for (uint32_t j = b; j < e; ++j) {
+      const uint32_t u = __ldg(col + j);
+      const double wt = wt_of(w, j);
+      if (on) {
+        const unsigned long long nd = (unsigned long long)__double_as_longlong(__dadd_rn(dv, wt));
+        const size_t iu = (size_t)u * kWb + lane;
+        if (nd == dist[iu]) {
+          const double c = __dmul_rn(__ddiv_rn(sv, __ull2double_rn(sigma[iu])), __dadd_rn(1.0, delta[iu]));
+          acc = __dadd_rn(acc, c);
+        }
+      }
+    }
+    if (on) delta[iv] = acc;
+    double add = (on && v != my_src) ? acc : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) add += __shfl_xor_sync(0xffffffffu, add, o);
+    if (lane == 0 && add != 0.0) bc[v] += add;
+  }
+}
+
+unsigned wb_grid(uint64_t warps) {
+  const uint64_t g = (warps * 32 + 255) / 256;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)sm_count() * 8));
+}
+
+// Runs launch(k) for k = 0, 1, ... in chains of kWbChain until round k has no
+// work (work[k] == 0).  Both sweeps have work in at most V + 1 rounds when the
+// weights are positive; `work` holds V + 3 + 2 kWbChain flags.
+template <class F>
+int run_rounds(uint32_t* work, uint32_t V, cudaStream_t s, F launch, uint32_t* rounds_out) {
+  uint32_t k = 0;
+  for (;;) {
+    if ((uint64_t)k > (uint64_t)V + 1) return fail(ZOGCU_ERR_INTERNAL, "weighted betweenness: round limit");
+    for (int i = 0; i < kWbChain; ++i) launch(k + (uint32_t)i);
+    ZOGCU_CUDA(cudaGetLastError());
+    k += kWbChain;
+    uint32_t more = 0;
+    ZOGCU_CUDA(cudaMemcpyAsync(&more, work + k, 4, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    if (!more) break;
+  }
+  if (rounds_out) *rounds_out = k;
+  return ZOGCU_OK;
+}
+
+int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bool dev_out, zogcu_stats* stats,
+                 cudaStream_t s) {
+  const uint32_t V = g->V;
+  const uint64_t E = g->E;
+  if (!g->offsets32) return fail(ZOGCU_ERR_TOO_LARGE, "weighted betweenness needs fewer than 2^32 arcs");
+  const uint32_t* off = g->out_off32.as<uint32_t>();
+  const uint32_t* col = g->out_col.as<uint32_t>();
+  const double* w = g->weighted ? g->out_w.as<double>() : nullptr;
+  const size_t n = (size_t)std::max<uint32_t>(V, 1) * kWb;
+  const size_t Vs = std::max<uint32_t>(V, 1);
+  DevBuf bdist, bsigma, bdelta, bround, bcnt, bm0, bm1, bwork, bflags, bsrc, bc;
+  ZOGCU_TRY(bdist.alloc(n * 8, s));
+  ZOGCU_TRY(bsigma.alloc(n * 8, s));
+  ZOGCU_TRY(bdelta.alloc(n * 8, s));
+  ZOGCU_TRY(bround.alloc(n * 4, s));
+  ZOGCU_TRY(bcnt.alloc(n * 4, s));
+  ZOGCU_TRY(bm0.alloc(Vs * 4, s));
+  ZOGCU_TRY(bm1.alloc(Vs * 4, s));
+  const size_t work_n = (size_t)V + 3 + 2 * kWbChain;
+  ZOGCU_TRY(bwork.alloc(work_n * 4, s));
+  ZOGCU_TRY(bflags.alloc(kFlags * 4, s));
+  ZOGCU_TRY(bsrc.alloc(kWb * 4, s));
+  ZOGCU_TRY(bc.alloc(Vs * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(bc.ptr, 0, Vs * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(bflags.ptr, 0, kFlags * 4, s));
+  uint32_t* flags = bflags.as<uint32_t>();
+  if (w && E) {
+    k_wb_check_weights<<<wb_grid(E / 32 + 1), 256, 0, s>>>(w, E, flags);
+    ZOGCU_CUDA(cudaGetLastError());
+    uint32_t bad = 0;
+    ZOGCU_CUDA(cudaMemcpyAsync(&bad, flags + kFlagBadWeight, 4, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    if (bad) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "weighted betweenness needs positive finite weights");
+  }
+  const unsigned grid = wb_grid(V);
+  unsigned long long* dist = bdist.as<unsigned long long>();
+  unsigned long long* sigma = bsigma.as<unsigned long long>();
+  double* delta = bdelta.as<double>();
+  uint32_t* round = bround.as<uint32_t>();
+  uint32_t* cnt = bcnt.as<uint32_t>();
+  uint32_t* masks[2] = {bm0.as<uint32_t>(), bm1.as<uint32_t>()};
+  uint32_t* work = bwork.as<uint32_t>();
+  const uint32_t* src = bsrc.as<uint32_t>();
+  EventTimer tm;
+  ZOGCU_TRY(tm.start(s));
+  uint64_t launches = 0;
+  uint32_t deepest = 0;
+  const uint32_t one = 1;
+  for (size_t b0 = 0; b0 < sources.size(); b0 += kWb) {
+    const uint32_t ns = (uint32_t)std::min<size_t>(kWb, sources.size() - b0);
+    ZOGCU_CUDA(cudaMemcpyAsync(bsrc.ptr, sources.data() + b0, ns * 4, cudaMemcpyHostToDevice, s));
+    k_wb_init<<<wb_grid(V), 256, 0, s>>>(V, dist, sigma, delta, round, cnt, masks[0], masks[1]);
+    k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_CUDA(cudaMemsetAsync(flags + kFlagMaxRound, 0, 4, s));
+    launches += 2;
+    // phase 1: distances
+    ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
+    uint32_t r1 = 0;
+    ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
+      k_wb_relax<<<grid, 256, 0, s>>>(off, col, w, V, dist, masks[k & 1], masks[(k + 1) & 1], work, k);
+    }, &r1));
+    launches += r1;
+    // phase 2: DAG in-counts, then sigma in topological rounds from the sources
+    k_wb_dagcount<<<grid, 256, 0, s>>>(off, col, w, V, dist, cnt, flags);
+    ZOGCU_CUDA(cudaMemsetAsync(masks[0], 0, Vs * 4, s));
+    ZOGCU_CUDA(cudaMemsetAsync(masks[1], 0, Vs * 4, s));
+    k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
+    uint32_t r2 = 0;
+    ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
+      k_wb_sigma<<<grid, 256, 0, s>>>(off, col, w, V, dist, sigma, cnt, round, masks[k & 1], masks[(k + 1) & 1], work,
+                                       flags, k);
+    }, &r2));
+    launches += r2 + 2;
+    uint32_t hf[kFlags];
+    ZOGCU_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    if (hf[kFlagZeroArc])
+      return fail(ZOGCU_ERR_INVALID_ARGUMENT,
+                  "weighted betweenness: a shortest path holds an arc of effective length zero (fl(d + w) == d)");
+    // phase 3: dependencies, rounds in reverse
+    const uint32_t maxr = hf[kFlagMaxRound];
+    deepest = std::max(deepest, maxr);
+    for (int64_t r = maxr; r >= 0; --r)
+      k_wb_delta<<<grid, 256, 0, s>>>(off, col, w, V, dist, sigma, delta, round, src, ns, bc.as<double>(),
+                                      (uint32_t)r);
+    ZOGCU_CUDA(cudaGetLastError());
+    launches += (uint64_t)maxr + 1;
+  }
+  ZOGCU_TRY(tm.stop(s));
+  uint32_t ovf = 0;
+  ZOGCU_CUDA(cudaMemcpyAsync(&ovf, flags + kFlagOverflow, 4, cudaMemcpyDeviceToHost, s));
+  if (V)
+    ZOGCU_CUDA(cudaMemcpyAsync(out, bc.ptr, (size_t)V * 8, dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (stats) {
+    stats->sources = sources.size();
+    stats->elapsed_ms = tm.ms();
+    stats->max_depth = deepest;
+    stats->sigma_overflow = ovf;
+    stats->launches = launches;
+  }
+  return ZOGCU_OK;
+}
+
+}  // namespace
+}  // namespace zogcu
+
+extern "C" {
+
+int zogcu_betweenness_weighted(zogcu_graph* G, const zogcu_bc_opts* opts, double* out_scores, zogcu_stats* stats) {
+  using namespace zogcu;
+  if (!G) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "graph is null");
+  if (!out_scores && G->g.V) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "out_scores is null");
+  if (opts && opts->struct_size != sizeof(zogcu_bc_opts))
+    return fail(ZOGCU_ERR_INVALID_ARGUMENT, "zogcu_bc_opts.struct_size mismatch");
+  Graph* g = &G->g;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  ZOGCU_CUDA(cudaSetDevice(g->device));
+  StreamGuard sg;
+  ZOGCU_TRY(sg.init(opts ? opts->stream : nullptr));
+  // sources: the subset given, or every live node ascending (centrality.zig:589)
+  std::vector<uint32_t> src;
+  if (opts && opts->sources) {
+    src.assign(opts->sources, opts->sources + opts->num_sources);
+    for (uint32_t x : src)
+      if (x >= g->V) return fail(ZOGCU_ERR_NODE_NOT_FOUND, "source is not a node of the graph");
+  } else {
+    std::vector<uint32_t> deg(g->V);
+    if (g->V) ZOGCU_CUDA(cudaMemcpy(deg.data(), g->out_deg.ptr, (size_t)g->V * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t v = 0; v < g->V; ++v)
+      if (deg[v] != kDeletedDegree) src.push_back(v);
+  }
+  return run_weighted(g, src, out_scores, opts && opts->device_pointers, stats, sg.s);
+}
+
+int zogcu_graph_export_weights(const zogcu_graph* G, double* out_weights) {
+  using namespace zogcu;
+  if (!G || (!out_weights && G->g.E)) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "null argument");
+  const Graph* g = &G->g;
+  if (!g->E) return ZOGCU_OK;
+  ZOGCU_CUDA(cudaSetDevice(g->device));
+  if (g->weighted) {
+    ZOGCU_CUDA(cudaMemcpy(out_weights, g->out_w.ptr, (size_t)g->E * 8, cudaMemcpyDeviceToHost));
+  } else {
+    for (uint64_t j = 0; j < g->E; ++j) out_weights[j] = 1.0;
+  }
+  return ZOGCU_OK;
+}
+
+}  // extern "C"

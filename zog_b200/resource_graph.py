@@ -12,6 +12,7 @@ this module                            reference
 ``destroy(g)``                         ``destroy/1``        resource_graph.ex:1578-1581
 ``pagerank(g, ...)``                   ``pagerank/2``       resource_graph.ex:1672-1685
 ``betweenness_unweighted(g, ...)``     ``betweenness_unweighted/2`` resource_graph.ex:1591-1601
+``betweenness_f64(g, ...)``            ``betweenness_f64/2`` resource_graph.ex:1611-1621
 ``betweenness_centrality``             alias of ``betweenness_unweighted``
 =====================================  =========================================
 
@@ -115,6 +116,17 @@ def betweenness_unweighted(g: ResourceGraph, raw: bool = False, sources=None):
     """resource_graph.ex:1591-1601.  ``sources`` (extension) restricts the
     outer Brandes loop to a subset of source ids."""
     scores = g.resource.betweenness_unweighted(sources=sources)
+    scores = _maybe_scale_undirected(g.builder, scores)
+    if raw:
+        return [float(x) for x in scores]
+    return _map_scores(g.builder, scores)
+
+
+def betweenness_f64(g: ResourceGraph, raw: bool = False, sources=None):
+    """resource_graph.ex:1611-1621: weighted (Dijkstra) betweenness over the
+    edges' f64 weights; halved for undirected builders like the unweighted
+    form.  ``sources`` (extension) restricts the outer loop."""
+    scores = g.resource.betweenness_weighted(sources=sources)
     scores = _maybe_scale_undirected(g.builder, scores)
     if raw:
         return [float(x) for x in scores]
