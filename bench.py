@@ -17,6 +17,9 @@ Workload (the scale configuration, synthetic and seeded):
   * Barabasi-Albert (object "barabasi_albert"): directed BA n = 4,194,304,
     m = 8 (seed 4096), solved in FP64, in the mixed form and from the learned
     start.
+  * Weighted Brandes (object "brandes_weighted"): the scale-16 Brandes graph
+    with seeded uniform weights in [1, 100) (one per edge, both arcs), the
+    first 1,024 sources; GTEPS with a CPU-oracle sample.
   * Batched forms (object "batched"), each against a loop of single launches:
     1,024 directed R-MAT graphs (scales 8-16, edge factors 4-16, seeded) in
     one persistent CUDA-graph launch; 256 personalised-PageRank seeds
@@ -52,6 +55,7 @@ BA_N, BA_M, BA_SEED = 1 << 22, 8, 4096
 BATCH_GRAPHS, BATCH_SEED = 1024, 8016          # R-MAT scales 8-16, edge factors 4-16
 PPR_SCALE, PPR_EF, PPR_SEED, PPR_SEEDS = 22, 16, 1022, 256
 BCB_SCALE, BCB_EF, BCB_SEED, BCB_SOURCES = 18, 16, 1018, 4096
+WBC_SOURCES, WBC_WSEED = 1024, 77                # weighted Brandes: sources timed, weight seed
 DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
 # kernels one zogcu_gnn_predict launches: features, chunk rows, 3 x (SpMM,
 # dense), head, and the 4 softmax kernels
@@ -79,8 +83,9 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, interval_ms: int = 25):
         self.gpu = gpu_index
+        self.interval = interval_ms
         self.proc = None
         self.lines = []
         self.t = None
@@ -89,7 +94,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.interval)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
@@ -470,6 +475,59 @@ def batched_block(N, args, stream, ws):
     return res, launches
 
 
+def edge_weights(f, t, seed):
+    """Seeded weights in [1, 100), one per undirected edge (both arcs of an
+    edge get the same value): a SplitMix64 hash of the (lo, hi) pair."""
+    lo = np.minimum(f, t).astype(np.uint64)
+    hi = np.maximum(f, t).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = (lo << np.uint64(32)) | hi
+        z = z ^ np.uint64(seed)
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return 1.0 + 99.0 * (z >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+
+
+def weighted_block(N, args, stream, ws, rank):
+    """Weighted (Dijkstra) Brandes on the scale-16 graph with seeded weights."""
+    import torch
+
+    sp = stream.cuda_stream
+    R = N.Graph.rmat(BC_SCALE, BC_EF, BC_SEED, directed=False)
+    V, _, _ = R.info()
+    _, _, oo, oc, _ = R.export_csr()
+    R.destroy()
+    f = np.repeat(np.arange(V, dtype=np.uint32), np.diff(oo).astype(np.int64))
+    t = oc.astype(np.uint32)
+    w = edge_weights(f, t, WBC_WSEED)
+    G = N.Graph.from_edges(V, f, t, w)
+    out = torch.empty(V, dtype=torch.float64, device="cuda")
+    src = np.arange(min(WBC_SOURCES, V), dtype=np.uint32)
+    G.betweenness_weighted_device(out.data_ptr(), sources=src[:64], stream=sp)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms, sts = _timed(stream, 1, lambda: G.betweenness_weighted_device(out.data_ptr(), sources=src, stream=sp))
+    ms = max_over_ranks(ms, ws)
+    res = {"workload": f"undirected rmat{BC_SCALE} ef{BC_EF}, weights in [1,100) hashed from the edge, seed "
+                       f"{WBC_WSEED}, {src.size} sources", "vertices": V, "arcs": int(f.size), "ms": ms,
+           "gteps": src.size * f.size / (ms * 1e-3) / 1e9, "max_rounds": int(sts[0]["max_depth"])}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O  # the CPU baseline only
+
+        O.build()
+        ag = O.ArrayGraph(V, f, t, w)
+        k = 16
+        t0 = time.perf_counter()
+        ag.betweenness_weighted(src[:k])
+        cs = time.perf_counter() - t0
+        res["cpu_baseline"] = {"gteps": k * f.size / cs / 1e9, "cores": 1, "kind": "port",
+                               "sample": f"{k} sources of the same graph, oracle restatement, 1 thread"}
+    G.destroy()
+    return res, int(sts[0]["launches"])
+
+
 def run_zog(args):
     import torch
 
@@ -672,6 +730,11 @@ def run_zog(args):
                                        "sample": f"{nsrc} sources of the same graph, oracle restatement, 1 thread"}
         B.destroy()
 
+    wbc_line = None
+    if not args.no_weighted:
+        wbc_line, nl = weighted_block(N, args, stream, ws, rank)
+        launches += nl
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": ws, "steps": args.steps,
@@ -697,6 +760,7 @@ def run_zog(args):
             "barabasi_albert": ba,
             "batched": batched,
             "brandes": bc_line,
+            "brandes_weighted": wbc_line,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -723,6 +787,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm start")
     ap.add_argument("--no-ba", action="store_true", help="skip the Barabasi-Albert graph")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched forms")
+    ap.add_argument("--no-weighted", action="store_true", help="skip weighted Brandes")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
