@@ -17,8 +17,9 @@
 //     shared memory at the start of every iteration and gathered from there;
 //   * degree-binned schedule, one warp per work item:
 //       A  a block of consecutive rows, each of in-degree <= NNZ, with <= NNZ
-//          arcs and <= kWarpRows rows in total: 16-byte index loads, gathers
-//          staged in the warp's shared-memory slice, rows of in-degree <=
+//          arcs and <= kWarpRows rows in total: lane l loads arcs l, l+32,
+//          ... (coalesced lines), gathers staged in the warp's shared-memory
+//          slice with conflict-free stores, rows of in-degree <=
 //          kShortLen summed by one lane each in the reference's order, longer
 //          ones by the warp;
 //       B  one row with NNZ < in-degree <= kLongChunk, reduced by a warp;
@@ -127,6 +128,11 @@ __device__ __forceinline__ uint4 ld_arcs(const uint4* a, uint64_t pol) {
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
       : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
       : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_arc(const uint32_t* a, uint64_t pol) {
+  uint32_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
   return v;
 }
 __device__ __forceinline__ double ld_contrib(const double* a, uint64_t pol) {
@@ -339,7 +345,7 @@ __device__ __forceinline__ void lin_row_epilogue(uint32_t v, double sum, uint32_
 template <typename OffT, typename CT, int THREADS, int NNZ, int MODE = kModePageRank>
 __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kernel(PrArgs<OffT, CT> A) {
   constexpr int WARPS = THREADS / 32;
-  constexpr int VPL = (NNZ / 4 + 1 + 31) / 32;  // 16-byte index vectors per lane in a row block
+  constexpr int NG = NNZ / 32;  // 32-arc groups of a row block: lane l holds arcs l, l+32, ...
   extern __shared__ __align__(16) unsigned char s_dyn[];
   __shared__ double s_red[2 * WARPS];
   __shared__ int s_flag;
@@ -428,14 +434,14 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
       // ---- rows [r0, r1): <= NNZ arcs, <= kWarpRows rows ------------------
       const uint32_t r0 = t.a, nrows = (t.b & 0x3FFFFFFFu) - t.a;
       const OffT e0 = ra, e1 = rb;
-      const OffT base = e0 & ~(OffT)3;
-      const uint32_t nvec = (uint32_t)((e1 - base + 3) >> 2);
-      const uint4* cv = reinterpret_cast<const uint4*>(A.col + base);
-      // round trip 1: index vectors, row bounds, row data for the epilogue
-      uint4 q[VPL];
+      const uint32_t na = (uint32_t)(e1 - e0);  // <= NNZ
+      // round trip 1: arc indices (lane l takes arcs l, l+32, ...: each load
+      // is one coalesced 128-byte line, and the staging stores below are
+      // conflict-free), row bounds, row data for the epilogue
+      uint32_t q[NG];
 #pragma unroll
-      for (int k = 0; k < VPL; ++k)
-        q[k] = ((uint32_t)lane + 32 * k < nvec) ? ld_arcs(cv + lane + 32 * k, pol_arc) : make_uint4(0, 0, 0, 0);
+      for (int k = 0; k < NG; ++k)
+        q[k] = ((uint32_t)lane + 32 * k < na) ? ld_arc(A.col + e0 + lane + 32 * k, pol_arc) : 0u;
       uint32_t b0 = 0, n0 = 0, b1 = 0, n1 = 0, d0 = kDeletedDegree, d1 = kDeletedDegree;
       double xo0 = 0.0, xo1 = 0.0, tp0 = 0.0, tp1 = 0.0;
       if ((uint32_t)lane < nrows) {
@@ -454,15 +460,10 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
         xo1 = __ldg(xcur + r);
         if (personalised) tp1 = __ldg(A.teleport + r);
       }
-      // round trip 2: gathers into this warp's staging slice
+      // round trip 2: gathers into this warp's staging slice, arc order
 #pragma unroll
-      for (int k = 0; k < VPL; ++k) {
-        const OffT e = base + 4 * (OffT)(lane + 32 * k);
-        if (e >= e0 && e < e1) sv[e - e0] = gather(q[k].x, hub, nhub, ccur, pol_c);
-        if (e + 1 >= e0 && e + 1 < e1) sv[e + 1 - e0] = gather(q[k].y, hub, nhub, ccur, pol_c);
-        if (e + 2 >= e0 && e + 2 < e1) sv[e + 2 - e0] = gather(q[k].z, hub, nhub, ccur, pol_c);
-        if (e + 3 >= e0 && e + 3 < e1) sv[e + 3 - e0] = gather(q[k].w, hub, nhub, ccur, pol_c);
-      }
+      for (int k = 0; k < NG; ++k)
+        if ((uint32_t)lane + 32 * k < na) sv[lane + 32 * k] = gather(q[k], hub, nhub, ccur, pol_c);
       __syncwarp();
 #pragma unroll
       for (int half = 0; half < 2; ++half) {
