@@ -772,6 +772,7 @@ def run_zog(args):
 
 def main():
     global PR_SCALE, PR_SEED, BC_SCALE, BC_SEED, BATCH_GRAPHS, PPR_SCALE, PPR_SEED, PPR_SEEDS, BCB_SCALE, BCB_SEED, BA_N
+    global WBC_SOURCES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -797,6 +798,7 @@ def main():
     ap.add_argument("--ppr-seeds", type=int, default=PPR_SEEDS, help="seeds of the personalised form")
     ap.add_argument("--bcb-scale", type=int, default=BCB_SCALE, help="R-MAT scale of the batched Brandes form")
     ap.add_argument("--ba-n", type=int, default=BA_N, help="nodes of the Barabasi-Albert graph")
+    ap.add_argument("--wbc-sources", type=int, default=WBC_SOURCES, help="sources of the weighted Brandes line")
     ap.add_argument("--ref-pr-iterations", type=int, default=28,
                     help="iterations the full solve takes on the benchmark graph: 28 for the seeded scale-24 "
                          "R-MAT (the GPU arm measures the same count, since both follow the reference iteration)")
@@ -805,7 +807,7 @@ def main():
         PR_SCALE, PR_SEED = args.pr_scale, 1000 + args.pr_scale
     if args.bc_scale != BC_SCALE:
         BC_SCALE, BC_SEED = args.bc_scale, 1000 + args.bc_scale
-    BATCH_GRAPHS, PPR_SEEDS, BA_N = args.batch_graphs, args.ppr_seeds, args.ba_n
+    BATCH_GRAPHS, PPR_SEEDS, BA_N, WBC_SOURCES = args.batch_graphs, args.ppr_seeds, args.ba_n, args.wbc_sources
     if args.ppr_scale != PPR_SCALE:
         PPR_SCALE, PPR_SEED = args.ppr_scale, 1000 + args.ppr_scale
     if args.bcb_scale != BCB_SCALE:

@@ -24,7 +24,11 @@
 //   3. delta: rounds in reverse, each node pulling (sigma_v / sigma_w)(1 +
 //      delta_w) from its DAG successors -- the reference's per-term value.
 // 32 sources run side by side: node-major rows of 32 (distance, sigma, delta,
-// round, in-count), one warp per node, lane b = source b.  Rounds are chained
+// round, in-count), lane b = source b.  Work items are (node, 256-arc chunk of
+// its out-arcs), one warp each, so a hub's arcs spread over many warps (R-MAT's
+// hubs are the low ids -- the first sources); chunk partials of delta and of
+// the scores are added atomically.  The frontier / ready masks rotate through
+// three buffers (read, write, clear for the next round).  Rounds are chained
 // launches with device flags (a launch whose round has no work returns at
 // once); the host checks the flags every 32 launches.  No kernel waits on
 // another.
@@ -46,6 +50,7 @@ constexpr int kWb = 32;                                     // sources per batch
 constexpr unsigned long long kInf = 0x7FF0000000000000ull;  // +inf
 constexpr uint32_t kNoRound = 0xFFFFFFFFu;
 constexpr int kWbChain = 32;                                // launches between host checks
+constexpr uint32_t kWbChunk = 256;                          // arcs per work item
 
 enum : int { kFlagZeroArc = 0, kFlagOverflow = 1, kFlagBadWeight = 2, kFlagMaxRound = 3, kFlags = 4 };
 
@@ -90,24 +95,29 @@ __global__ void k_wb_seed(const uint32_t* __restrict__ src, uint32_t ns, unsigne
   }
 }
 
+// Work item t: node tnode[t], arcs [tbeg[t], min(tbeg[t] + kWbChunk, off[node+1])).
+
 // Phase 1, round k: relax the out-arcs of every (node, source) in the frontier.
 __global__ void __launch_bounds__(256) k_wb_relax(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                  const double* __restrict__ w, uint32_t V,
-                                                  unsigned long long* __restrict__ dist, uint32_t* __restrict__ mcur,
-                                                  uint32_t* __restrict__ mnext, uint32_t* __restrict__ work,
-                                                  uint32_t k) {
+                                                  const double* __restrict__ w, const uint32_t* __restrict__ tnode,
+                                                  const uint32_t* __restrict__ tbeg, uint32_t ntasks,
+                                                  unsigned long long* __restrict__ dist,
+                                                  const uint32_t* __restrict__ mcur, uint32_t* __restrict__ mnext,
+                                                  uint32_t* __restrict__ mclear, uint32_t V,
+                                                  uint32_t* __restrict__ work, uint32_t k) {
   if (*(volatile uint32_t*)(work + k) == 0) return;
   const int lane = threadIdx.x & 31;
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) mclear[i] = 0;
   bool any = false;
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+  for (uint32_t t = gw; t < ntasks; t += nw) {
+    const uint32_t v = tnode[t];
     const uint32_t m = mcur[v];
     if (m == 0) continue;
     const bool on = (m >> lane) & 1u;
     const double dv = on ? __longlong_as_double((long long)dist[(size_t)v * kWb + lane]) : 0.0;
-    __syncwarp();
-    if (lane == 0) mcur[v] = 0;
-    const uint32_t b = off[v], e = off[v + 1];
+    const uint32_t b = tbeg[t], e = min(b + kWbChunk, off[v + 1]);
     for (uint32_t j = b; j < e; ++j) {
       const uint32_t u = __ldg(col + j);
       const double wt = wt_of(w, j);
@@ -126,17 +136,19 @@ __global__ void __launch_bounds__(256) k_wb_relax(const uint32_t* __restrict__ o
 
 // Phase 2a: DAG in-arc counts (and the zero-length check).
 __global__ void __launch_bounds__(256) k_wb_dagcount(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                     const double* __restrict__ w, uint32_t V,
+                                                     const double* __restrict__ w, const uint32_t* __restrict__ tnode,
+                                                     const uint32_t* __restrict__ tbeg, uint32_t ntasks,
                                                      const unsigned long long* __restrict__ dist,
                                                      uint32_t* __restrict__ cnt, uint32_t* __restrict__ flags) {
   const int lane = threadIdx.x & 31;
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nw) {
+    const uint32_t v = tnode[t];
     const unsigned long long dvb = dist[(size_t)v * kWb + lane];
     const bool on = dvb != kInf;
     if (!__any_sync(0xffffffffu, on)) continue;
     const double dv = __longlong_as_double((long long)dvb);
-    const uint32_t b = off[v], e = off[v + 1];
+    const uint32_t b = tbeg[t], e = min(b + kWbChunk, off[v + 1]);
     for (uint32_t j = b; j < e; ++j) {
       const uint32_t u = __ldg(col + j);
       const double wt = wt_of(w, j);
@@ -155,25 +167,27 @@ __global__ void __launch_bounds__(256) k_wb_dagcount(const uint32_t* __restrict_
 // Phase 2b, round k: ready nodes add their sigma along DAG arcs; a node whose
 // last DAG predecessor has added becomes ready in round k + 1.
 __global__ void __launch_bounds__(256) k_wb_sigma(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                  const double* __restrict__ w, uint32_t V,
+                                                  const double* __restrict__ w, const uint32_t* __restrict__ tnode,
+                                                  const uint32_t* __restrict__ tbeg, uint32_t ntasks,
                                                   const unsigned long long* __restrict__ dist,
                                                   unsigned long long* __restrict__ sigma, uint32_t* __restrict__ cnt,
-                                                  uint32_t* __restrict__ round, uint32_t* __restrict__ mcur,
-                                                  uint32_t* __restrict__ mnext, uint32_t* __restrict__ work,
+                                                  uint32_t* __restrict__ round, const uint32_t* __restrict__ mcur,
+                                                  uint32_t* __restrict__ mnext, uint32_t* __restrict__ mclear,
+                                                  uint32_t V, uint32_t* __restrict__ work,
                                                   uint32_t* __restrict__ flags, uint32_t k) {
   if (*(volatile uint32_t*)(work + k) == 0) return;
   const int lane = threadIdx.x & 31;
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) mclear[i] = 0;
   bool any = false;
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nw) {
+    const uint32_t v = tnode[t];
     const uint32_t m = mcur[v];
     if (m == 0) continue;
     const bool on = (m >> lane) & 1u;
     const unsigned long long sv = on ? sigma[(size_t)v * kWb + lane] : 0ull;
     const double dv = on ? __longlong_as_double((long long)dist[(size_t)v * kWb + lane]) : 0.0;
-    __syncwarp();
-    if (lane == 0) mcur[v] = 0;
-    const uint32_t b = off[v], e = off[v + 1];
+    const uint32_t b = tbeg[t], e = min(b + kWbChunk, off[v + 1]);
     for (uint32_t j = b; j < e; ++j) {
       const uint32_t u = __ldg(col + j);
       const double wt = wt_of(w, j);
@@ -198,8 +212,10 @@ __global__ void __launch_bounds__(256) k_wb_sigma(const uint32_t* __restrict__ o
 
 // Phase 3, round r (descending): delta_v = sum over DAG successors w of
 // (sigma_v / sigma_w)(1 + delta_w); the score of v gains delta_v for v != s.
+// A node's chunks add their partial sums atomically.
 __global__ void __launch_bounds__(256) k_wb_delta(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                  const double* __restrict__ w, uint32_t V,
+                                                  const double* __restrict__ w, const uint32_t* __restrict__ tnode,
+                                                  const uint32_t* __restrict__ tbeg, uint32_t ntasks,
                                                   const unsigned long long* __restrict__ dist,
                                                   const unsigned long long* __restrict__ sigma,
                                                   double* __restrict__ delta, const uint32_t* __restrict__ round,
@@ -208,14 +224,15 @@ __global__ void __launch_bounds__(256) k_wb_delta(const uint32_t* __restrict__ o
   const int lane = threadIdx.x & 31;
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
   const uint32_t my_src = (uint32_t)lane < ns ? src[lane] : 0xFFFFFFFFu;
-  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nw) {
+    const uint32_t v = tnode[t];
     const size_t iv = (size_t)v * kWb + lane;
     const bool on = round[iv] == r;
     if (!__any_sync(0xffffffffu, on)) continue;
     const double dv = on ? __longlong_as_double((long long)dist[iv]) : 0.0;
     const double sv = on ? __ull2double_rn(sigma[iv]) : 0.0;
     double acc = 0.0;
-    const uint32_t b = off[v], e = off[v + 1];
+    const uint32_t b = tbeg[t], e = min(b + kWbChunk, off[v + 1]);
     for (uint32_t j = b; j < e; ++j) {
       const uint32_t u = __ldg(col + j);
       const double wt = wt_of(w, j);
@@ -228,11 +245,11 @@ __global__ void __launch_bounds__(256) k_wb_delta(const uint32_t* __restrict__ o
         }
       }
     }
-    if (on) delta[iv] = acc;
+    if (on && acc != 0.0) atomicAdd(delta + iv, acc);
     double add = (on && v != my_src) ? acc : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) add += __shfl_xor_sync(0xffffffffu, add, o);
-    if (lane == 0 && add != 0.0) bc[v] += add;
+    if (lane == 0 && add != 0.0) atomicAdd(bc + v, add);
   }
 }
 
@@ -271,7 +288,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   const double* w = g->weighted ? g->out_w.as<double>() : nullptr;
   const size_t n = (size_t)std::max<uint32_t>(V, 1) * kWb;
   const size_t Vs = std::max<uint32_t>(V, 1);
-  DevBuf bdist, bsigma, bdelta, bround, bcnt, bm0, bm1, bwork, bflags, bsrc, bc;
+  DevBuf bdist, bsigma, bdelta, bround, bcnt, bm0, bm1, bm2, bwork, bflags, bsrc, bc, btn, btb;
   ZOGCU_TRY(bdist.alloc(n * 8, s));
   ZOGCU_TRY(bsigma.alloc(n * 8, s));
   ZOGCU_TRY(bdelta.alloc(n * 8, s));
@@ -279,6 +296,25 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   ZOGCU_TRY(bcnt.alloc(n * 4, s));
   ZOGCU_TRY(bm0.alloc(Vs * 4, s));
   ZOGCU_TRY(bm1.alloc(Vs * 4, s));
+  ZOGCU_TRY(bm2.alloc(Vs * 4, s));
+  // work items: (node, first arc) per kWbChunk arcs of every node's out-row
+  std::vector<uint32_t> h_off((size_t)V + 1), tn, tb;
+  if (V) ZOGCU_CUDA(cudaMemcpyAsync(h_off.data(), off, ((size_t)V + 1) * 4, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  for (uint32_t v = 0; v < V; ++v)
+    for (uint32_t j = h_off[v]; j < h_off[v + 1]; j += kWbChunk) {
+      tn.push_back(v);
+      tb.push_back(j);
+    }
+  const uint32_t ntasks = (uint32_t)tn.size();
+  ZOGCU_TRY(btn.alloc(std::max<size_t>(tn.size(), 1) * 4, s));
+  ZOGCU_TRY(btb.alloc(std::max<size_t>(tb.size(), 1) * 4, s));
+  if (ntasks) {
+    ZOGCU_CUDA(cudaMemcpyAsync(btn.ptr, tn.data(), tn.size() * 4, cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(btb.ptr, tb.data(), tb.size() * 4, cudaMemcpyHostToDevice, s));
+  }
+  const uint32_t* tnode = btn.as<uint32_t>();
+  const uint32_t* tbeg = btb.as<uint32_t>();
   const size_t work_n = (size_t)V + 3 + 2 * kWbChain;
   ZOGCU_TRY(bwork.alloc(work_n * 4, s));
   ZOGCU_TRY(bflags.alloc(kFlags * 4, s));
@@ -295,13 +331,13 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     if (bad) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "weighted betweenness needs positive finite weights");
   }
-  const unsigned grid = wb_grid(V);
+  const unsigned grid = wb_grid(std::max<uint32_t>(ntasks, V));
   unsigned long long* dist = bdist.as<unsigned long long>();
   unsigned long long* sigma = bsigma.as<unsigned long long>();
   double* delta = bdelta.as<double>();
   uint32_t* round = bround.as<uint32_t>();
   uint32_t* cnt = bcnt.as<uint32_t>();
-  uint32_t* masks[2] = {bm0.as<uint32_t>(), bm1.as<uint32_t>()};
+  uint32_t* masks[3] = {bm0.as<uint32_t>(), bm1.as<uint32_t>(), bm2.as<uint32_t>()};
   uint32_t* work = bwork.as<uint32_t>();
   const uint32_t* src = bsrc.as<uint32_t>();
   EventTimer tm;
@@ -313,6 +349,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     const uint32_t ns = (uint32_t)std::min<size_t>(kWb, sources.size() - b0);
     ZOGCU_CUDA(cudaMemcpyAsync(bsrc.ptr, sources.data() + b0, ns * 4, cudaMemcpyHostToDevice, s));
     k_wb_init<<<wb_grid(V), 256, 0, s>>>(V, dist, sigma, delta, round, cnt, masks[0], masks[1]);
+    ZOGCU_CUDA(cudaMemsetAsync(masks[2], 0, Vs * 4, s));
     k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
     ZOGCU_CUDA(cudaGetLastError());
     ZOGCU_CUDA(cudaMemsetAsync(flags + kFlagMaxRound, 0, 4, s));
@@ -322,21 +359,21 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
     uint32_t r1 = 0;
     ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
-      k_wb_relax<<<grid, 256, 0, s>>>(off, col, w, V, dist, masks[k & 1], masks[(k + 1) & 1], work, k);
+      k_wb_relax<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, masks[k % 3], masks[(k + 1) % 3],
+                                       masks[(k + 2) % 3], V, work, k);
     }, &r1));
     launches += r1;
     // phase 2: DAG in-counts, then sigma in topological rounds from the sources
-    k_wb_dagcount<<<grid, 256, 0, s>>>(off, col, w, V, dist, cnt, flags);
-    ZOGCU_CUDA(cudaMemsetAsync(masks[0], 0, Vs * 4, s));
-    ZOGCU_CUDA(cudaMemsetAsync(masks[1], 0, Vs * 4, s));
+    k_wb_dagcount<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, cnt, flags);
+    for (int i = 0; i < 3; ++i) ZOGCU_CUDA(cudaMemsetAsync(masks[i], 0, Vs * 4, s));
     k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
     ZOGCU_CUDA(cudaGetLastError());
     ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, s));
     ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
     uint32_t r2 = 0;
     ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
-      k_wb_sigma<<<grid, 256, 0, s>>>(off, col, w, V, dist, sigma, cnt, round, masks[k & 1], masks[(k + 1) & 1], work,
-                                       flags, k);
+      k_wb_sigma<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, cnt, round, masks[k % 3],
+                                       masks[(k + 1) % 3], masks[(k + 2) % 3], V, work, flags, k);
     }, &r2));
     launches += r2 + 2;
     uint32_t hf[kFlags];
@@ -349,8 +386,8 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     const uint32_t maxr = hf[kFlagMaxRound];
     deepest = std::max(deepest, maxr);
     for (int64_t r = maxr; r >= 0; --r)
-      k_wb_delta<<<grid, 256, 0, s>>>(off, col, w, V, dist, sigma, delta, round, src, ns, bc.as<double>(),
-                                      (uint32_t)r);
+      k_wb_delta<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, delta, round, src, ns,
+                                      bc.as<double>(), (uint32_t)r);
     ZOGCU_CUDA(cudaGetLastError());
     launches += (uint64_t)maxr + 1;
   }
