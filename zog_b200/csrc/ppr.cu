@@ -16,7 +16,8 @@
 // single-vector kernel are reused (row blocks, single rows, and 4096-arc
 // chunks of hub rows; chunk partials are added into a side matrix and the
 // last chunk to arrive runs the row's epilogue).  Each lane owns S/32
-// consecutive columns and sums a row's arcs in the reference's order.  A
+// consecutive columns, reads them with 32-byte loads that skip L1 allocation,
+// and sums a row's arcs in the reference's order.  A
 // seed that has converged is frozen (its column is carried over unchanged),
 // so every seed returns exactly the vector of its own stopping iteration.
 // Per-column L1 steps and dangling masses go lane -> warp -> CTA partials ->
@@ -69,6 +70,27 @@ struct PprArgs {
   unsigned long long max_iter;
 };
 
+// PL consecutive doubles of one contribution row, read with 32-byte loads
+// that skip L1 allocation (16-byte loads when PL is 2): the row is streamed,
+// never re-read by this warp.
+template <int PL>
+__device__ __forceinline__ void ld_row(const double* p, double (&v)[PL]) {
+  if constexpr (PL % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < PL / 4; ++q)
+      asm volatile("ld.global.nc.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];"
+                   : "=d"(v[4 * q]), "=d"(v[4 * q + 1]), "=d"(v[4 * q + 2]), "=d"(v[4 * q + 3])
+                   : "l"(p + 4 * q));
+  } else {
+#pragma unroll
+    for (int q = 0; q < PL / 2; ++q) {
+      const double2 x = __ldg(reinterpret_cast<const double2*>(p) + q);
+      v[2 * q] = x.x;
+      v[2 * q + 1] = x.y;
+    }
+  }
+}
+
 template <int S>
 __device__ __forceinline__ void ppr_row_sum(const PprArgs<S>& A, const double* __restrict__ Cc, uint32_t b, uint32_t e,
                                             int c0, double (&acc)[S / 32]) {
@@ -78,31 +100,21 @@ __device__ __forceinline__ void ppr_row_sum(const PprArgs<S>& A, const double* _
   uint32_t j = b;
   for (; j + 2 <= e; j += 2) {
     const uint32_t u0 = __ldg(A.col + j), u1 = __ldg(A.col + j + 1);
-    const double2* p0 = reinterpret_cast<const double2*>(Cc + (size_t)u0 * S + c0);
-    const double2* p1 = reinterpret_cast<const double2*>(Cc + (size_t)u1 * S + c0);
-    double2 v0[PL / 2], v1[PL / 2];
+    double v0[PL], v1[PL];
+    ld_row<PL>(Cc + (size_t)u0 * S + c0, v0);
+    ld_row<PL>(Cc + (size_t)u1 * S + c0, v1);
 #pragma unroll
-    for (int q = 0; q < PL / 2; ++q) {
-      v0[q] = __ldg(p0 + q);
-      v1[q] = __ldg(p1 + q);
-    }
-#pragma unroll
-    for (int q = 0; q < PL / 2; ++q) {  // arc j, then arc j+1: the reference's order per column
-      acc[2 * q] = __dadd_rn(acc[2 * q], v0[q].x);
-      acc[2 * q + 1] = __dadd_rn(acc[2 * q + 1], v0[q].y);
-      acc[2 * q] = __dadd_rn(acc[2 * q], v1[q].x);
-      acc[2 * q + 1] = __dadd_rn(acc[2 * q + 1], v1[q].y);
+    for (int i = 0; i < PL; ++i) {  // arc j, then arc j+1: the reference's order per column
+      acc[i] = __dadd_rn(acc[i], v0[i]);
+      acc[i] = __dadd_rn(acc[i], v1[i]);
     }
   }
   if (j < e) {
     const uint32_t u = __ldg(A.col + j);
-    const double2* p = reinterpret_cast<const double2*>(Cc + (size_t)u * S + c0);
+    double v[PL];
+    ld_row<PL>(Cc + (size_t)u * S + c0, v);
 #pragma unroll
-    for (int q = 0; q < PL / 2; ++q) {
-      const double2 v = __ldg(p + q);
-      acc[2 * q] = __dadd_rn(acc[2 * q], v.x);
-      acc[2 * q + 1] = __dadd_rn(acc[2 * q + 1], v.y);
-    }
+    for (int i = 0; i < PL; ++i) acc[i] = __dadd_rn(acc[i], v[i]);
   }
 }
 
