@@ -61,9 +61,10 @@ DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
 # dense), head, and the 4 softmax kernels
 GNN_PREDICT_LAUNCHES = 13
 # DRAM bytes (read + write) of one pr_iter_kernel launch on the default
-# workload (scale 24, kernel configuration 3), from one ncu capture of this
-# command; see profiles/pagerank_rmat24_launches_and_traffic.md.
-PROFILED_TRAFFIC = {(24, 3): 1.54e9 + 0.1762e9}
+# workload (scale 24), dram__bytes_read.sum + dram__bytes_write.sum from one
+# ncu capture of this command with only the PageRank block enabled (kernel
+# configuration 4; configurations 3 and 4 move the same bytes).
+PROFILED_TRAFFIC = {24: 1.53e9 + 0.1763e9}
 
 
 # --------------------------------------------------------------------------
@@ -746,7 +747,7 @@ def run_zog(args):
                        "parallelism": "replicas" if ws > 1 else "single"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak,
-                         "traffic": PROFILED_TRAFFIC.get((PR_SCALE, int(st["kernel_config"]))),
+                         "traffic": PROFILED_TRAFFIC.get(PR_SCALE),
                          "peak_kind": peak_kind,
                          "kernel": "pr_iter_kernel", "kernel_config": int(st["kernel_config"]),
                          "ms_per_launch": t_iter_ms,
