@@ -190,3 +190,34 @@ def test_mixed_precision_bound(native, oracle, scale):
         assert rel_l1(x64, ref) <= TOL
     finally:
         G.destroy()
+
+
+@pytest.mark.slow
+def test_in_solve_tuning_matches_each_configuration(native):
+    """Directed R-MAT scale 19 (ef 16, > 2^22 arcs): the first solve on a graph
+    times each kernel configuration on its own early iterations and finishes
+    with the fastest.  Its result agrees with a solve forced to any one
+    configuration, and later solves reuse the choice and repeat bit for bit."""
+    G = native.Graph.rmat(19, 16, 1919, directed=True)
+    try:
+        V, E, _ = G.info()
+        assert E >= 1 << 22
+        x, st = G.pagerank(0.85, 200, 1e-10, stats=True)
+        x2, st2 = G.pagerank(0.85, 200, 1e-10, stats=True)
+        assert st2["kernel_config"] == st["kernel_config"]
+        assert np.array_equal(x2, G.pagerank(0.85, 200, 1e-10))
+        in_off, in_col, out_off, out_col, deg = G.export_csr()
+    finally:
+        G.destroy()
+    src = np.repeat(np.arange(V, dtype=np.uint32), np.diff(out_off).astype(np.int64))
+    for cfg in range(5):
+        os.environ["ZOGCU_PR_CONFIG"] = str(cfg)
+        try:
+            H = native.Graph.from_edges(V, src, out_col)
+            y, sty = H.pagerank(0.85, 200, 1e-10, stats=True)
+            H.destroy()
+        finally:
+            del os.environ["ZOGCU_PR_CONFIG"]
+        assert sty["kernel_config"] == cfg
+        assert rel_l1(x, y) <= 1e-12
+        assert abs(sty["iterations"] - st["iterations"]) <= 1

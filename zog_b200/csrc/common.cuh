@@ -104,7 +104,6 @@ struct PrSchedule {
   DevArray off;               // uint32_t[V+1] (or uint64_t when E >= 2^32)
   DevArray col;               // uint32_t[E+4]: ranks of the sources
   DevArray deg;               // uint32_t[V]: out-degree of rank p
-  std::vector<uint64_t> host_off;  // ranked offsets on the host (schedule builds)
   PrTaskList lists[2];        // work items of 128 and of 256 arcs
   int config = -1;            // kernel configuration chosen by the autotuner
 };

@@ -29,9 +29,10 @@
 //     each warp runs a software pipeline over its items (descriptors two
 //     ahead, arc ranges one ahead), so an item costs two dependent round
 //     trips, and warps never wait on each other inside the pass;
-//   * the kernel is a template over (CTA size, arcs per item, hub size); an
-//     autotuner times the candidate configurations on the graph at its first
-//     PageRank call and keeps the fastest (ZOGCU_PR_CONFIG forces one);
+//   * the kernel is a template over (CTA size, arcs per item, hub size); the
+//     first PageRank solve on a graph times each configuration on its own
+//     early iterations and keeps the fastest (ZOGCU_PR_CONFIG forces one);
+//   * the work-item lists are built on the device (segmented greedy pass);
 //   * arc indices stream with an L2 evict-first policy, bypassing L1; gathered
 //     contributions use an L2 evict-last policy;
 //   * the epilogue writes x', c' = x'/deg and accumulates |x'-x| and the
@@ -652,57 +653,125 @@ static int build_ranked_view(Graph* g, cudaStream_t s) {
     ZOGCU_TRY(P.off.alloc(((size_t)V + 1) * 8));
     ZOGCU_CUDA(cudaMemcpyAsync(P.off.ptr, poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToDevice, s));
   }
-  P.host_off.resize((size_t)V + 1);
-  ZOGCU_CUDA(cudaMemcpyAsync(P.host_off.data(), poff64.ptr, ((size_t)V + 1) * 8, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   return ZOGCU_OK;
 }
 
-// Work items for row blocks of at most `nnz` arcs (host greedy pass over the
-// ranked offsets; caller holds g->mu).
-static int build_task_list(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
-  const uint32_t V = g->V;
-  const std::vector<uint64_t>& off = g->pr.host_off;
-  std::vector<PrTask> tasks;
-  std::vector<uint32_t> long_first;
-  tasks.reserve(g->E / (nnz / 2) + V / kWarpRows + 16);
-  uint32_t r = 0;
-  while (r < V) {
-    uint64_t len = off[r + 1] - off[r];
-    if (len > (uint64_t)nnz) {
-      if (len <= (uint64_t)kLongChunk) {
-        tasks.push_back(PrTask{r, (kTaskRow << 30) | (r + 1)});
-      } else {
-        const uint64_t nch = (len + kLongChunk - 1) / kLongChunk;
-        if (nch > 0xFFFFu) return fail(ZOGCU_ERR_TOO_LARGE, "row in-degree too large for the chunk schedule");
-        long_first.push_back((uint32_t)tasks.size());
-        for (uint32_t c = 0; c < (uint32_t)nch; ++c) tasks.push_back(PrTask{r, (kTaskChunk << 30) | c});
+// Work items for row blocks of at most `nnz` arcs, built on the device.  The
+// ranked rows are cut into segments of kTaskSegRows rows and one thread walks
+// each segment with the greedy rule: a row longer than nnz becomes one row
+// item (<= kLongChunk arcs) or its run of chunk items; otherwise consecutive
+// rows of <= nnz arcs join a block while the block stays within nnz arcs and
+// kWarpRows rows.  Blocks never cross a segment boundary, so the segments are
+// independent: a counting pass, a scan over the segments, and a writing pass
+// that repeats the walk.  Which rows share a block does not change any row's
+// sum: a row's summation order depends only on its own arcs.
+constexpr uint32_t kTaskSegRows = 1024;
+
+template <typename OffT>
+__global__ void k_task_segments(const OffT* __restrict__ off, uint32_t V, uint32_t nnz, uint32_t nseg,
+                                unsigned long long* __restrict__ seg_tasks, unsigned long long* __restrict__ seg_long,
+                                PrTask* __restrict__ tasks, uint32_t* __restrict__ long_first, int write,
+                                unsigned int* __restrict__ err) {
+  for (uint32_t sg = blockIdx.x * blockDim.x + threadIdx.x; sg < nseg; sg += gridDim.x * blockDim.x) {
+    uint32_t r = sg * kTaskSegRows;
+    const uint32_t rend = min(V, r + kTaskSegRows);  // V < 2^30
+    unsigned long long nt = write ? seg_tasks[sg] : 0ull, nl = write ? seg_long[sg] : 0ull;
+    OffT o_r = off[r];
+    while (r < rend) {
+      OffT o_n = off[r + 1];
+      uint64_t len = (uint64_t)(o_n - o_r);
+      if (len > nnz) {
+        if (len <= (uint64_t)kLongChunk) {
+          if (write) tasks[nt] = PrTask{r, (kTaskRow << 30) | (r + 1)};
+          ++nt;
+        } else {
+          uint64_t nch = (len + kLongChunk - 1) / kLongChunk;
+          if (nch > 0xFFFFull) {
+            atomicOr(err, 1u);
+            nch = 0;
+          }
+          if (write) {
+            long_first[nl] = (uint32_t)nt;
+            for (uint32_t c = 0; c < (uint32_t)nch; ++c) tasks[nt + c] = PrTask{r, (kTaskChunk << 30) | c};
+          }
+          ++nl;
+          nt += nch;
+        }
+        ++r;
+        o_r = o_n;
+        continue;
       }
-      ++r;
-      continue;
+      const uint32_t r0 = r;
+      uint64_t tot = 0;
+      while (r < rend && r - r0 < (uint32_t)kWarpRows) {
+        o_n = off[r + 1];
+        len = (uint64_t)(o_n - o_r);
+        if (len > nnz || tot + len > nnz) break;
+        tot += len;
+        ++r;
+        o_r = o_n;
+      }
+      if (write) tasks[nt] = PrTask{r0, (kTaskBlock << 30) | r};
+      ++nt;
     }
-    const uint32_t r0 = r;
-    uint64_t tot = 0;
-    while (r < V && (r - r0) < (uint32_t)kWarpRows) {
-      len = off[r + 1] - off[r];
-      if (len > (uint64_t)nnz || tot + len > (uint64_t)nnz) break;
-      tot += len;
-      ++r;
+    if (!write) {
+      seg_tasks[sg] = nt;
+      seg_long[sg] = nl;
     }
-    tasks.push_back(PrTask{r0, (kTaskBlock << 30) | r});
   }
-  if (tasks.size() >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "too many PageRank work items");
-  L.num_tasks = (uint32_t)tasks.size();
-  L.num_long = (uint32_t)long_first.size();
-  ZOGCU_TRY(L.tasks.alloc(std::max<size_t>(tasks.size(), 1) * sizeof(PrTask)));
-  ZOGCU_TRY(L.long_first.alloc(std::max<size_t>(long_first.size(), 1) * 4));
-  if (!tasks.empty())
-    ZOGCU_CUDA(cudaMemcpyAsync(L.tasks.ptr, tasks.data(), tasks.size() * sizeof(PrTask), cudaMemcpyHostToDevice, s));
-  if (!long_first.empty())
-    ZOGCU_CUDA(cudaMemcpyAsync(L.long_first.ptr, long_first.data(), long_first.size() * 4, cudaMemcpyHostToDevice, s));
+}
+
+template <typename OffT>
+static int build_task_list_t(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
+  const uint32_t V = g->V;
+  const uint32_t nseg = (V + kTaskSegRows - 1) / kTaskSegRows;
+  DevBuf cnt, offs, tmp;
+  // [tasks per segment | trailing 0 | long rows per segment | trailing 0] and
+  // their exclusive scans; the word after the scans is the error flag
+  ZOGCU_TRY(cnt.alloc(2 * ((size_t)nseg + 1) * 8, s));
+  ZOGCU_TRY(offs.alloc(2 * ((size_t)nseg + 1) * 8 + 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, cnt.bytes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(offs.ptr, 0, offs.bytes, s));
+  unsigned long long* ct = cnt.as<unsigned long long>();
+  unsigned long long* cl = ct + nseg + 1;
+  unsigned long long* ot = offs.as<unsigned long long>();
+  unsigned long long* ol = ot + nseg + 1;
+  unsigned int* err = reinterpret_cast<unsigned int*>(ol + nseg + 1);
+  const OffT* off = g->pr.off.as<OffT>();
+  const unsigned grid = (unsigned)std::max<uint32_t>((nseg + 127) / 128, 1);
+  if (nseg) {
+    k_task_segments<OffT><<<grid, 128, 0, s>>>(off, V, (uint32_t)nnz, nseg, ct, cl, nullptr, nullptr, 0, err);
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  size_t tb = 0;
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, ct, ot, (int64_t)nseg + 1, s));
+  ZOGCU_TRY(tmp.alloc(tb, s));
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, ct, ot, (int64_t)nseg + 1, s));
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, cl, ol, (int64_t)nseg + 1, s));
+  unsigned long long h[3] = {0, 0, 0};
+  ZOGCU_CUDA(cudaMemcpyAsync(&h[0], ot + nseg, 8, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(&h[1], ol + nseg, 8, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(&h[2], err, 4, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (h[2]) return fail(ZOGCU_ERR_TOO_LARGE, "row in-degree too large for the chunk schedule");
+  if (h[0] >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "too many PageRank work items");
+  L.num_tasks = (uint32_t)h[0];
+  L.num_long = (uint32_t)h[1];
+  ZOGCU_TRY(L.tasks.alloc(std::max<size_t>(L.num_tasks, 1) * sizeof(PrTask)));
+  ZOGCU_TRY(L.long_first.alloc(std::max<size_t>(L.num_long, 1) * 4));
+  if (nseg) {
+    k_task_segments<OffT><<<grid, 128, 0, s>>>(off, V, (uint32_t)nnz, nseg, ot, ol, L.tasks.as<PrTask>(),
+                                               L.long_first.as<uint32_t>(), 1, err);
+    ZOGCU_CUDA(cudaGetLastError());
+  }
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   L.built = true;
   return ZOGCU_OK;
+}
+
+static int build_task_list(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
+  return g->offsets32 ? build_task_list_t<uint32_t>(g, nnz, L, s) : build_task_list_t<uint64_t>(g, nnz, L, s);
 }
 
 static int list_index(int nnz) { return nnz == 128 ? 0 : 1; }
@@ -766,9 +835,12 @@ struct PrWork {
   DevBuf x0, x1, c0, c1, part, chunk, lcnt, lpart, stb, tele, tmp;
 };
 
+// Launches `count` iterations of configuration `cfg`; `init` starts a new
+// chain (state cleared, start vector written).  A.max_iter bounds the whole
+// chain, so a chain may be launched in pieces of different configurations.
 template <typename OffT, typename CT>
 static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, int given, uint64_t max_iter,
-                           cudaStream_t s, uint64_t* launches) {
+                           uint64_t count, bool init, cudaStream_t s, uint64_t* launches) {
   const PrTaskList& L = g->pr.lists[list_index(kPrConfigs[cfg].nnz)];
   A.tasks = L.tasks.as<PrTask>();
   A.long_first = L.long_first.as<uint32_t>();
@@ -782,54 +854,76 @@ static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, in
   const uint32_t warps = kPrConfigs[cfg].threads / 32;
   const uint32_t need = (A.ntasks + warps - 1) / warps;
   if (need > 0 && (uint32_t)grid > need) grid = (int)need;
-  ZOGCU_CUDA(cudaMemsetAsync(A.st, 0, sizeof(PrState), s));
-  const unsigned init_grid = std::min(grid_1d(V), 148u * 4);
-  pr_init_kernel<OffT, CT><<<init_grid, 256, 0, s>>>(A, V, given);
-  ZOGCU_CUDA(cudaGetLastError());
+  if (init) {
+    ZOGCU_CUDA(cudaMemsetAsync(A.st, 0, sizeof(PrState), s));
+    const unsigned init_grid = std::min(grid_1d(V), 148u * 4);
+    pr_init_kernel<OffT, CT><<<init_grid, 256, 0, s>>>(A, V, given);
+    ZOGCU_CUDA(cudaGetLastError());
+    ++*launches;
+  }
   auto fn = PrLauncher<OffT, CT>::fn(cfg);
-  for (uint64_t k = 0; k < max_iter; ++k) fn<<<grid, kPrConfigs[cfg].threads, dyn, s>>>(A);
+  for (uint64_t k = 0; k < count; ++k) fn<<<grid, kPrConfigs[cfg].threads, dyn, s>>>(A);
   ZOGCU_CUDA(cudaGetLastError());
-  *launches += 1 + max_iter;
+  *launches += count;
   return ZOGCU_OK;
 }
 
-// Times each configuration on this graph (a few iterations from the uniform
-// start, tolerance 0) and keeps the fastest.  Small graphs keep the default.
-template <typename OffT, typename CT>
-static int pr_autotune(Graph* g, const PrArgs<OffT, CT>& A0, uint32_t V, cudaStream_t s) {
+// Kernel configuration of a graph: the one already chosen, the one forced by
+// ZOGCU_PR_CONFIG, the default for small graphs, or -1 (time them).
+static int pr_config_of(Graph* g) {
+  std::lock_guard<std::mutex> lk(g->mu);
   PrSchedule& P = g->pr;
-  if (P.config >= 0) return ZOGCU_OK;
+  if (P.config >= 0) return P.config;
   if (const char* e = std::getenv("ZOGCU_PR_CONFIG")) {
     const int c = std::atoi(e);
-    if (c >= 0 && c < kNumPrConfigs) {
-      ZOGCU_TRY(ensure_task_list(g, kPrConfigs[c].nnz, s));
-      P.config = c;
-      return ZOGCU_OK;
-    }
+    if (c >= 0 && c < kNumPrConfigs) return P.config = c;
   }
-  if (g->E < (1ull << 22)) {
-    ZOGCU_TRY(ensure_task_list(g, kPrConfigs[kDefaultPrConfig].nnz, s));
-    P.config = kDefaultPrConfig;
-    return ZOGCU_OK;
+  if (g->E < (1ull << 22)) return P.config = kDefaultPrConfig;
+  return -1;
+}
+
+// A chain of up to max_iter iterations.  When the graph has no configuration
+// yet, the chain's own first iterations choose it: one iteration with the
+// default configuration (caches warm), then one timed iteration of each
+// configuration; the fastest runs the rest and is kept for the graph.  Every
+// configuration computes the same iteration, so the tuning iterations are
+// ordinary iterations of the solve.  If the chain converges before every
+// configuration was timed, nothing is kept.
+template <typename OffT, typename CT>
+static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V, int given, uint64_t max_iter,
+                        cudaStream_t s, uint64_t* launches, int* used_cfg) {
+  constexpr uint64_t kTuneIters = 1 + kNumPrConfigs;
+  if (cfg >= 0 || max_iter <= kTuneIters) {
+    if (cfg < 0) cfg = kDefaultPrConfig;
+    *used_cfg = cfg;
+    return pr_launch_chain<OffT, CT>(g, cfg, A, V, given, max_iter, max_iter, true, s, launches);
   }
-  EventTimer tm;
-  float best = 1e30f;
-  int best_cfg = kDefaultPrConfig;
+  ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, kDefaultPrConfig, A, V, given, max_iter, 1, true, s, launches)));
+  EventTimer tm[kNumPrConfigs];
   for (int c = 0; c < kNumPrConfigs; ++c) {
-    ZOGCU_TRY(ensure_task_list(g, kPrConfigs[c].nnz, s));
-    uint64_t launches = 0;
-    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A0, V, 0, 1, s, &launches)));  // warm-up
-    ZOGCU_TRY(tm.start(s));
-    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A0, V, 0, 4, s, &launches)));
-    ZOGCU_TRY(tm.stop(s));
-    const float ms = tm.ms();
-    if (ms > 0.f && ms < best) {
-      best = ms;
-      best_cfg = c;
-    }
+    ZOGCU_TRY(tm[c].start(s));
+    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A, V, given, max_iter, 1, false, s, launches)));
+    ZOGCU_TRY(tm[c].stop(s));
   }
-  P.config = best_cfg;
-  return ZOGCU_OK;
+  PrState hs;
+  ZOGCU_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  int best = kDefaultPrConfig;
+  if (!hs.converged && hs.iter == kTuneIters) {
+    float best_ms = 1e30f;
+    for (int c = 0; c < kNumPrConfigs; ++c) {
+      const float ms = tm[c].ms();
+      if (ms > 0.f && ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (g->pr.config < 0) g->pr.config = best;
+    best = g->pr.config;
+  }
+  *used_cfg = best;
+  return pr_launch_chain<OffT, CT>(g, best, A, V, given, max_iter, max_iter - kTuneIters, false, s, launches);
 }
 
 // FP32-phase switch: the FP32 contributions carry relative rounding ~6e-8, so
@@ -890,12 +984,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   A.tol = tol;
   A.stall = 0.0;
 
-  {
-    PrArgs<OffT, double> At = A;
-    At.tol = 0.0;
-    ZOGCU_TRY((pr_autotune<OffT, double>(g, At, V, s)));
-  }
-  const int cfg = g->pr.config;
+  int cfg = pr_config_of(g);
 
   int given = 0;
   if (o && o->x0) {  // caller order -> ranked order
@@ -926,7 +1015,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     Af.c1 = cf1.as<float>();
     Af.tol = std::max(tol, kMixedSwitchTol);
     Af.stall = kMixedStall;
-    ZOGCU_TRY((pr_launch_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches)));
+    ZOGCU_TRY((pr_run_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches, &cfg)));
     ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     it32 = hs.iter;
@@ -934,7 +1023,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     if (it32 & 1ull) std::swap(A.x0, A.x1);
     given = 1;
   }
-  ZOGCU_TRY((pr_launch_chain<OffT, double>(g, cfg, A, V, given, max_iter - it32, s, &launches)));
+  ZOGCU_TRY((pr_run_chain<OffT, double>(g, cfg, A, V, given, max_iter - it32, s, &launches, &cfg)));
   ZOGCU_TRY(tm.stop(s));
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
