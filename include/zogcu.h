@@ -188,6 +188,12 @@ ZOGCU_API int zogcu_graph_export_csr(const zogcu_graph* g, uint64_t* in_off, uin
 
 ZOGCU_API void zogcu_free(void* p);
 
+/* Graphs, schedules and call workspaces come from the device's stream-ordered
+ * memory pool, which keeps freed memory reserved for the next graph.  This
+ * returns the reserve of the current device to the driver (memory still in
+ * use is kept).  No counterpart in the reference. */
+ZOGCU_API int zogcu_release_cached_memory(void);
+
 /* ---- PageRank ------------------------------------------------------------ */
 
 /* Replaces the NIF `pagerank(res, damping, max_iterations, tolerance)`

@@ -221,3 +221,33 @@ def test_in_solve_tuning_matches_each_configuration(native):
         assert sty["kernel_config"] == cfg
         assert rel_l1(x, y) <= 1e-12
         assert abs(sty["iterations"] - st["iterations"]) <= 1
+
+
+def test_graphs_reuse_pool_memory_and_release_it(native, oracle):
+    """Graph arrays come from the device's stream-ordered pool: destroying a
+    graph and building it again gives the same scores, and
+    zogcu_release_cached_memory hands the pool's reserve back to the driver."""
+    import torch
+
+    V, f, t = oracle.rmat(14, 8, 3141, directed=True)
+    ref, it, _ = oracle.ArrayGraph(V, f, t).pagerank(0.85, 200, 1e-10)
+    first = None
+    for _ in range(3):
+        G = native.Graph.from_edges(V, f, t)
+        try:
+            x = G.pagerank(0.85, 200, 1e-10)
+        finally:
+            G.destroy()
+        assert rel_l1(x, ref) <= TOL
+        if first is None:
+            first = x
+        assert np.array_equal(x, first)
+    free_before, _ = torch.cuda.mem_get_info()
+    native.release_cached_memory()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after >= free_before
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        assert np.array_equal(G.pagerank(0.85, 200, 1e-10), first)
+    finally:
+        G.destroy()

@@ -40,7 +40,7 @@ EXPORTS = (
     "zogcu_gnn_save", "zogcu_gnn_load",
     "zogcu_batch_create", "zogcu_batch_destroy", "zogcu_batch_info", "zogcu_batch_pagerank",
     "zogcu_ppr", "zogcu_betweenness_weighted", "zogcu_graph_export_weights",
-    "zogcu_graph_create_from_arraygraph_weighted",
+    "zogcu_graph_create_from_arraygraph_weighted", "zogcu_release_cached_memory",
 )
 
 
@@ -150,6 +150,7 @@ def load(path: str | None = None):
         L.zogcu_batch_destroy.argtypes = [vp]
         L.zogcu_batch_info.argtypes = [vp, C.POINTER(u32), C.POINTER(u64), C.POINTER(u64), vp]
         L.zogcu_batch_pagerank.argtypes = [vp, dbl, u64, dbl, C.POINTER(BatchOpts), vp, vp, C.POINTER(Stats)]
+        L.zogcu_release_cached_memory.argtypes = []
         for name in EXPORTS:  # every other entry point returns a zogcu_status
             if name not in ("zogcu_status_string", "zogcu_last_error", "zogcu_free"):
                 getattr(L, name).restype = C.c_int
@@ -419,6 +420,11 @@ class Graph:
         ovf = C.c_uint32(0)
         check(load().zogcu_bfs_sigma(self.handle, _ptr(src), src.size, _ptr(dist), _ptr(sigma), C.byref(ovf)))
         return dist, sigma, bool(ovf.value)
+
+
+def release_cached_memory():
+    """Returns the device memory the library's pool keeps in reserve to the driver."""
+    check(load().zogcu_release_cached_memory())
 
 
 def rmat_raw_device(scale, seed, i0, m, a=0.57, b=0.19, c=0.19):

@@ -55,7 +55,8 @@ struct DevBuf {
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
-// Persistent device allocation owned by a graph (plain cudaMalloc).
+// Persistent device allocation owned by a graph (from the stream-ordered pool;
+// release waits for the device like cudaFree).
 struct DevArray {
   void* ptr = nullptr;
   size_t bytes = 0;
