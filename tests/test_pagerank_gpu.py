@@ -14,6 +14,7 @@ from conftest import GOLDEN, rel_l1
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-9
+N_CONFIGS = 7  # kernel configurations of pr_iter_kernel / pr_iter_kernel_pipe
 
 
 def golden(name):
@@ -129,6 +130,33 @@ def test_heavy_rows_use_long_row_chunks(native, oracle):
         G.destroy()
 
 
+@pytest.mark.parametrize("cfg", range(N_CONFIGS))
+def test_every_kernel_configuration_matches_oracle(native, oracle, cfg):
+    """Each kernel configuration (hub sizes, item sizes, pipelined gathers),
+    forced with ZOGCU_PR_CONFIG, on a graph with row blocks, single heavy rows
+    and chunked long rows, in FP64 and in the precision form."""
+    rng = np.random.default_rng(11 + cfg)
+    V = 30000
+    f = np.concatenate([rng.integers(0, V, 40000), rng.integers(0, V, 150000), rng.integers(0, V, 9000)])
+    t = np.concatenate([np.zeros(40000, np.int64), rng.integers(0, V, 150000), rng.integers(1, 40, 9000)])
+    f = f.astype(np.uint32); t = t.astype(np.uint32)
+    ref, it, _ = oracle.ArrayGraph(V, f, t).pagerank(0.85, 200, 1e-10)
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        os.environ["ZOGCU_PR_CONFIG"] = str(cfg)  # read by the graph's first solve
+        try:
+            x, st = G.pagerank(0.85, 200, 1e-10, stats=True)
+        finally:
+            del os.environ["ZOGCU_PR_CONFIG"]
+        assert st["kernel_config"] == cfg
+        assert rel_l1(x, ref) <= TOL and st["iterations"] == it
+        assert np.array_equal(x, G.pagerank(0.85, 200, 1e-10))
+        xm = G.pagerank(0.85, 200, 1e-10, precision=native.PREC_MIXED)
+        assert rel_l1(xm, ref) <= 12e-10
+    finally:
+        G.destroy()
+
+
 def test_warm_start_and_personalised(native, oracle):
     """Extensions against the generalised oracle: a start vector x0 and a
     personalisation (teleport) vector p."""
@@ -210,7 +238,7 @@ def test_in_solve_tuning_matches_each_configuration(native):
     finally:
         G.destroy()
     src = np.repeat(np.arange(V, dtype=np.uint32), np.diff(out_off).astype(np.int64))
-    for cfg in range(5):
+    for cfg in range(N_CONFIGS):
         os.environ["ZOGCU_PR_CONFIG"] = str(cfg)
         try:
             H = native.Graph.from_edges(V, src, out_col)

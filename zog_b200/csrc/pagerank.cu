@@ -60,13 +60,16 @@ struct PrConfig {
   int threads;      // CTA size
   int nnz;          // arcs per row-block work item
   int hub_bytes;    // shared-memory hub per CTA
+  int pipelined;    // 1: row-block gathers issued one item ahead (cp.async)
 };
 constexpr PrConfig kPrConfigs[] = {
-    {1024, 128, 192 * 1024},  // 0: one CTA per SM, biggest hub
-    {1024, 256, 160 * 1024},  // 1: one CTA per SM, bigger items
-    {512, 256, 64 * 1024},    // 2: two CTAs per SM
-    {256, 256, 0},            // 3: four CTAs per SM, no hub
-    {256, 128, 0},            // 4: four CTAs per SM, no hub, small items
+    {1024, 128, 192 * 1024, 0},  // 0: one CTA per SM, biggest hub
+    {1024, 256, 160 * 1024, 0},  // 1: one CTA per SM, bigger items
+    {512, 256, 64 * 1024, 0},    // 2: two CTAs per SM
+    {256, 256, 0, 0},            // 3: four CTAs per SM, no hub
+    {256, 128, 0, 0},            // 4: four CTAs per SM, no hub, small items
+    {256, 128, 0, 1},            // 5: four CTAs per SM, pipelined gathers
+    {256, 256, 0, 1},            // 6: three CTAs per SM, pipelined gathers, bigger items
 };
 constexpr int kNumPrConfigs = sizeof(kPrConfigs) / sizeof(kPrConfigs[0]);
 constexpr int kDefaultPrConfig = 0;
@@ -107,6 +110,7 @@ struct PrArgs {
   unsigned long long max_iter;
   double ka, kb;         // katz: alpha, beta; alpha centrality: alpha
   double* x2;            // eigenvector: third rotating buffer
+  uint32_t nv;           // node slots V (bound of every source index)
 };
 
 // Epilogue modes of the iteration kernel (all share the schedule and the
@@ -145,6 +149,24 @@ __device__ __forceinline__ double ld_contrib(const float* a, uint64_t pol) {
   float v;
   asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
   return (double)v;
+}
+
+// Asynchronous gather of one contribution into shared memory (cp.async, 8 or
+// 4 bytes, the plain sm_80 form); the copy lands without passing through
+// registers, so a warp can keep a whole work item's gathers in flight while
+// it sums the previous one.
+__device__ __forceinline__ void cp_gather(double* dst, const double* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_gather(float* dst, const float* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 template <typename CT>
@@ -540,6 +562,240 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
               MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag);
 }
 
+constexpr int pr_pipe_min_blocks(int nnz) { return nnz >= 256 ? 3 : 4; }
+
+// The same iteration with the row-block gathers software-pipelined: while a
+// warp sums work item i from one staging buffer, the gathers of item i+1 are
+// already in flight into the other (cp.async), and the arc indices of item
+// i+2 are loading into registers.  A row block thus costs about one memory
+// round trip of waiting instead of two.  Each row is summed exactly as in
+// pr_iter_kernel (same staging layout, same order); rows of kinds B and C are
+// summed synchronously, as there.
+template <typename OffT, typename CT, int THREADS, int NNZ, int MODE = kModePageRank>
+__global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kernel_pipe(PrArgs<OffT, CT> A) {
+  constexpr int WARPS = THREADS / 32;
+  constexpr int NG = NNZ / 32;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  __shared__ double s_red[2 * WARPS];
+  __shared__ int s_flag;
+
+  const PrState* st = A.st;
+  const unsigned long long iter = *(volatile const unsigned long long*)&st->iter;
+  const int converged = *(volatile const int*)&st->converged;
+  if (converged || iter >= A.max_iter) return;
+  const double sink = *(volatile const double*)&st->sink;
+
+  const int par = (int)(iter & 1ull);
+  const double* __restrict__ xcur;
+  double* __restrict__ xnxt;
+  const CT* __restrict__ ccur;
+  CT* __restrict__ cnxt;
+  if constexpr (MODE == kModeEigen) {
+    const int k3 = (int)(iter % 3ull);
+    xcur = k3 == 0 ? A.x0 : (k3 == 1 ? A.x1 : A.x2);
+    xnxt = k3 == 0 ? A.x1 : (k3 == 1 ? A.x2 : A.x0);
+    ccur = reinterpret_cast<const CT*>(xcur);
+    cnxt = nullptr;
+  } else if constexpr (MODE != kModePageRank) {
+    xcur = par ? A.x1 : A.x0;
+    xnxt = par ? A.x0 : A.x1;
+    ccur = reinterpret_cast<const CT*>(xcur);
+    cnxt = nullptr;
+  } else {
+    xcur = par ? A.x1 : A.x0;
+    xnxt = par ? A.x0 : A.x1;
+    ccur = par ? A.c1 : A.c0;
+    cnxt = par ? A.c0 : A.c1;
+  }
+  const double tele_u = (1.0 - A.damping) / A.n_f;
+  const bool personalised = A.teleport != nullptr;
+  const double damping = A.damping, n_f = A.n_f;
+  const double ka = A.ka, kb = A.kb;
+  auto epilogue = [&](uint32_t v, double s, uint32_t dg, double xo, double tp, double& el1, double& eacc) {
+    if constexpr (MODE == kModePageRank)
+      pr_row_epilogue(v, s, dg, xo, tp, personalised, damping, n_f, xnxt, cnxt, tele_u, sink, el1, eacc);
+    else
+      lin_row_epilogue<MODE>(v, s, dg, xo, ka, kb, xnxt, el1, eacc);
+  };
+
+  const uint64_t pol_arc = policy_evict_first();
+  const uint64_t pol_c = policy_evict_last();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  CT* const stage = reinterpret_cast<CT*>(s_dyn) + (size_t)warp * 2 * NNZ;  // two buffers of NNZ
+  double l1 = 0.0, dsum = 0.0;
+
+  const uint32_t nwarps = gridDim.x * WARPS;
+  const uint32_t ntasks = A.ntasks;
+  const PrTask none{0, 0};
+  auto task_at = [&](uint32_t i) { return i < ntasks ? A.tasks[i] : none; };
+  auto range_of = [&](const PrTask& tk, OffT& lo, OffT& hi) {
+    const uint32_t kind = tk.b >> 30;
+    const uint32_t end = (kind == kTaskBlock) ? (tk.b & 0x3FFFFFFFu) : tk.a + 1;
+    lo = __ldg(A.off + tk.a);
+    hi = __ldg(A.off + end);
+  };
+  // Self-checks: a row block longer than NNZ arcs or a source outside [0, V)
+  // sets bit 0 of st->pad[0] (the host reports an internal error) and the
+  // access is skipped.
+  unsigned int* const err = const_cast<unsigned int*>(&A.st->pad[0]);
+  auto block_len = [&](bool blk, OffT lo, OffT hi) -> uint32_t {
+    if (!blk) return 0u;
+    const uint64_t n = (uint64_t)(hi - lo);
+    if (n > (uint64_t)NNZ) {
+      if (lane == 0) atomicOr(err, 1u);
+      return 0u;
+    }
+    return (uint32_t)n;
+  };
+  // arc indices of a row block (lane l: arcs l, l+32, ...); zeros otherwise
+  auto load_idx = [&](bool blk, OffT lo, OffT hi, uint32_t (&q)[NG]) {
+    const uint32_t na = block_len(blk, lo, hi);
+#pragma unroll
+    for (int k = 0; k < NG; ++k)
+      q[k] = ((uint32_t)lane + 32 * k < na) ? ld_arc(A.col + lo + lane + 32 * k, pol_arc) : 0u;
+  };
+  auto issue = [&](bool blk, OffT lo, OffT hi, const uint32_t (&q)[NG], CT* dst) {
+    const uint32_t na = block_len(blk, lo, hi);
+#pragma unroll
+    for (int k = 0; k < NG; ++k) {
+      if ((uint32_t)lane + 32 * k < na) {
+        if (q[k] < A.nv) cp_gather(dst + lane + 32 * k, ccur + q[k]);
+        else atomicOr(err, 1u);
+      }
+    }
+    cp_commit();
+  };
+
+  uint32_t ti = blockIdx.x * WARPS + warp;
+  PrTask t0 = task_at(ti), t1 = task_at(ti + nwarps), t2 = task_at(ti + 2 * nwarps);
+  OffT a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+  if (ti < ntasks) range_of(t0, a0, b0);
+  if (ti + nwarps < ntasks) range_of(t1, a1, b1);
+  uint32_t q1[NG];
+  {
+    uint32_t q0[NG];
+    const bool blk0 = ti < ntasks && (t0.b >> 30) == kTaskBlock;
+    load_idx(blk0, a0, b0, q0);
+    issue(blk0, a0, b0, q0, stage);
+  }
+  load_idx(ti + nwarps < ntasks && (t1.b >> 30) == kTaskBlock, a1, b1, q1);
+  int cur = 0;
+  while (ti < ntasks) {
+    const uint32_t tn = ti + nwarps;
+    const PrTask t3 = task_at(tn + 2 * nwarps);
+    OffT a2 = 0, b2 = 0;
+    if (tn + nwarps < ntasks) range_of(t2, a2, b2);
+    const uint32_t kind = t0.b >> 30;
+    // row data of the current block (used after its gathers land)
+    const uint32_t r0 = t0.a;
+    const uint32_t nrows = kind == kTaskBlock ? (t0.b & 0x3FFFFFFFu) - t0.a : 0u;
+    uint32_t rb0 = 0, rn0 = 0, rb1 = 0, rn1 = 0, d0 = kDeletedDegree, d1 = kDeletedDegree;
+    double xo0 = 0.0, xo1 = 0.0, tp0 = 0.0, tp1 = 0.0;
+    if ((uint32_t)lane < nrows) {
+      const uint32_t r = r0 + lane;
+      rb0 = (uint32_t)(__ldg(A.off + r) - a0);
+      rn0 = (uint32_t)(__ldg(A.off + r + 1) - a0);
+      d0 = __ldg(A.deg + r);
+      xo0 = __ldg(xcur + r);
+      if (personalised) tp0 = __ldg(A.teleport + r);
+    }
+    if ((uint32_t)lane + 32 < nrows) {
+      const uint32_t r = r0 + lane + 32;
+      rb1 = (uint32_t)(__ldg(A.off + r) - a0);
+      rn1 = (uint32_t)(__ldg(A.off + r + 1) - a0);
+      d1 = __ldg(A.deg + r);
+      xo1 = __ldg(xcur + r);
+      if (personalised) tp1 = __ldg(A.teleport + r);
+    }
+    // gathers of item i+1 (indices already in registers), then indices of i+2
+    issue(tn < ntasks && (t1.b >> 30) == kTaskBlock, a1, b1, q1, stage + (cur ^ 1) * NNZ);
+    uint32_t q2[NG];
+    load_idx(tn + nwarps < ntasks && (t2.b >> 30) == kTaskBlock, a2, b2, q2);
+    if (kind == kTaskBlock) {
+      cp_wait<1>();  // this item's gathers (all but the group just issued)
+      __syncwarp();
+      const CT* sv = stage + cur * NNZ;
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        const uint32_t i = lane + 32 * half;
+        const bool valid = i < nrows;
+        const uint32_t b = half ? rb1 : rb0, en = half ? rn1 : rn0;
+        const uint32_t dg = half ? d1 : d0;
+        const double xo = half ? xo1 : xo0, tp = half ? tp1 : tp0;
+        const bool is_short = valid && (en - b) <= (uint32_t)kShortLen;
+        if (is_short) {
+          double sum = 0.0;
+          for (uint32_t k = b; k < en; ++k) sum += (double)sv[k];  // ascending source order
+          epilogue(r0 + i, sum, dg, xo, tp, l1, dsum);
+        }
+        unsigned med = __ballot_sync(0xffffffffu, valid && !is_short);
+        while (med) {
+          const int k = __ffs(med) - 1;
+          med &= med - 1;
+          const uint32_t bk = __shfl_sync(0xffffffffu, b, k), ek = __shfl_sync(0xffffffffu, en, k);
+          double sum = 0.0;
+          for (uint32_t j = bk + lane; j < ek; j += 32) sum += (double)sv[j];
+          sum = warp_sum(sum);
+          if (lane == k) epilogue(r0 + i, sum, dg, xo, tp, l1, dsum);
+        }
+      }
+      __syncwarp();  // the buffer is refilled two items later
+    } else {
+      // ---- one heavy row (B) or one chunk of a long row (C) -----------------
+      const uint32_t row = t0.a;
+      uint32_t dg = 0;
+      double xo = 0.0, tp = 0.0;
+      if (lane == 0) {
+        dg = __ldg(A.deg + row);
+        xo = __ldg(xcur + row);
+        if (personalised) tp = __ldg(A.teleport + row);
+      }
+      if (kind == kTaskRow) {
+        const double sum = warp_range_sum<OffT, CT>(A.col, ccur, nullptr, 0u, a0, b0, lane, pol_arc, pol_c);
+        if (lane == 0) epilogue(row, sum, dg, xo, tp, l1, dsum);
+      } else {
+        const uint32_t c = t0.b & 0xFFFFu;
+        const uint32_t nch = (uint32_t)((b0 - a0 + kLongChunk - 1) / kLongChunk);
+        const OffT e0 = a0 + (OffT)c * kLongChunk;
+        const OffT e1 = min(e0 + (OffT)kLongChunk, b0);
+        const double sum = warp_range_sum<OffT, CT>(A.col, ccur, nullptr, 0u, e0, e1, lane, pol_arc, pol_c);
+        const uint32_t first = ti - c;
+        unsigned int last = 0;
+        if (lane == 0) {
+          A.chunk_part[ti] = sum;
+          __threadfence();
+          last = (atomicAdd(A.long_cnt + first, 1u) == nch - 1) ? 1u : 0u;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && lane == 0) {
+          __threadfence();
+          double tot = 0.0;
+          for (uint32_t k = 0; k < nch; ++k) tot += __ldcg(A.chunk_part + (first + k));
+          double rl1 = 0.0, rds = 0.0;
+          epilogue(row, tot, dg, xo, tp, rl1, rds);
+          A.long_part[2 * (size_t)first] = rl1;
+          A.long_part[2 * (size_t)first + 1] = rds;
+          A.long_cnt[first] = 0;
+        }
+      }
+    }
+    t0 = t1;
+    t1 = t2;
+    t2 = t3;
+    a0 = a1;
+    b0 = b1;
+    a1 = a2;
+    b1 = b2;
+#pragma unroll
+    for (int k = 0; k < NG; ++k) q1[k] = q2[k];
+    cur ^= 1;
+    ti = tn;
+  }
+  cp_wait<0>();
+  cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol,
+              MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag);
+}
+
 // ---------------------------------------------------------------------------
 // PageRank view: degree ranking, re-laid in-CSR, schedules
 // ---------------------------------------------------------------------------
@@ -805,10 +1061,14 @@ struct PrLauncher {
       case 1: return pr_iter_kernel<OffT, CT, 1024, 256>;
       case 2: return pr_iter_kernel<OffT, CT, 512, 256>;
       case 3: return pr_iter_kernel<OffT, CT, 256, 256>;
-      default: return pr_iter_kernel<OffT, CT, 256, 128>;
+      case 4: return pr_iter_kernel<OffT, CT, 256, 128>;
+      case 5: return pr_iter_kernel_pipe<OffT, CT, 256, 128>;
+      default: return pr_iter_kernel_pipe<OffT, CT, 256, 256>;
     }
   }
-  static size_t staging_bytes(int cfg) { return (size_t)(kPrConfigs[cfg].threads / 32) * kPrConfigs[cfg].nnz * 8; }
+  static size_t staging_bytes(int cfg) {
+    return (size_t)(kPrConfigs[cfg].threads / 32) * kPrConfigs[cfg].nnz * 8 * (kPrConfigs[cfg].pipelined ? 2 : 1);
+  }
   // hub entries and dynamic shared memory of configuration `cfg` for V nodes
   static uint32_t hub_entries(int cfg, uint32_t V) {
     const uint32_t cap = (uint32_t)(kPrConfigs[cfg].hub_bytes / sizeof(CT));
@@ -983,6 +1243,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   A.n_f = (double)g->n_live;
   A.tol = tol;
   A.stall = 0.0;
+  A.nv = V;
 
   int cfg = pr_config_of(g);
 
@@ -1018,6 +1279,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     ZOGCU_TRY((pr_run_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches, &cfg)));
     ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
+    if (hs.pad[0]) return fail(ZOGCU_ERR_INTERNAL, "PageRank work item failed a bound check");
     it32 = hs.iter;
     // ---- FP64 polish from the FP32 phase's last vector ----------------------
     if (it32 & 1ull) std::swap(A.x0, A.x1);
@@ -1027,6 +1289,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   ZOGCU_TRY(tm.stop(s));
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (hs.pad[0]) return fail(ZOGCU_ERR_INTERNAL, "PageRank work item failed a bound check");
   const double* result = (hs.iter & 1ull) ? A.x1 : A.x0;
   double* unperm = (hs.iter & 1ull) ? A.x0 : A.x1;  // the other buffer is free now
   k_permute_out<<<grid_1d(V), 256, 0, s>>>(result, P.rank.as<uint32_t>(), V, unperm);
