@@ -60,7 +60,15 @@ DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
 # kernels one zogcu_gnn_predict launches: features, chunk rows, 3 x (SpMM,
 # dense), head, and the 4 softmax kernels
 GNN_PREDICT_LAUNCHES = 13
-# DRAM bytes (read + write) of one pr_iter_kernel launch on the default
+
+
+def pr_kernel_name(cfg):
+    """Kernel behind a PageRank configuration: 5 and 6 pipeline the row-block
+    gathers (pr_iter_kernel_pipe), the others are pr_iter_kernel."""
+    return "pr_iter_kernel_pipe" if cfg >= 5 else "pr_iter_kernel"
+
+
+# DRAM bytes (read + write) of one PageRank iteration launch on the default
 # workload (scale 24), dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture of this command with only the PageRank block enabled (kernel
 # configuration 4; configurations 3 and 4 move the same bytes).
@@ -749,7 +757,8 @@ def run_zog(args):
                          "frac": achieved / hbm_peak,
                          "traffic": PROFILED_TRAFFIC.get(PR_SCALE),
                          "peak_kind": peak_kind,
-                         "kernel": "pr_iter_kernel", "kernel_config": int(st["kernel_config"]),
+                         "kernel": pr_kernel_name(int(st["kernel_config"])),
+                         "kernel_config": int(st["kernel_config"]),
                          "ms_per_launch": t_iter_ms,
                          "algorithmic_bytes_per_launch": bytes_per_iter},
             "clocks": clk,

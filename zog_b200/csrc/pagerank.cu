@@ -1144,43 +1144,76 @@ static int pr_config_of(Graph* g) {
 
 // A chain of up to max_iter iterations.  When the graph has no configuration
 // yet, the chain's own first iterations choose it: one iteration with the
-// default configuration (caches warm), then one timed iteration of each
-// configuration; the fastest runs the rest and is kept for the graph.  Every
-// configuration computes the same iteration, so the tuning iterations are
-// ordinary iterations of the solve.  If the chain converges before every
-// configuration was timed, nothing is kept.
+// default configuration (caches warm), then two timed iterations of each
+// configuration, in ascending and then descending order so that no
+// configuration always follows the same one; the one with the lowest time
+// runs the rest and is kept for the graph.  Every configuration computes the same
+// iteration, so the tuning iterations are ordinary iterations of the solve.
+// Only iterations that ran before convergence count; if some configuration
+// has none, nothing is kept.
 template <typename OffT, typename CT>
 static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V, int given, uint64_t max_iter,
                         cudaStream_t s, uint64_t* launches, int* used_cfg) {
-  constexpr uint64_t kTuneIters = 1 + kNumPrConfigs;
+  constexpr int kRounds = 2;
+  constexpr int kTimed = kRounds * kNumPrConfigs;
+  constexpr uint64_t kTuneIters = 1 + (uint64_t)kTimed;
   if (cfg >= 0 || max_iter <= kTuneIters) {
     if (cfg < 0) cfg = kDefaultPrConfig;
     *used_cfg = cfg;
     return pr_launch_chain<OffT, CT>(g, cfg, A, V, given, max_iter, max_iter, true, s, launches);
   }
+  // one-time launch setup of every configuration (attributes, occupancy,
+  // module loading) happens here, outside the timed launches
+  for (int c = 0; c < kNumPrConfigs; ++c)
+    if (PrLauncher<OffT, CT>::grid(c, 0) <= 0) return fail(ZOGCU_ERR_CUDA, "PageRank kernel configuration could not be set up");
   ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, kDefaultPrConfig, A, V, given, max_iter, 1, true, s, launches)));
-  EventTimer tm[kNumPrConfigs];
-  for (int c = 0; c < kNumPrConfigs; ++c) {
-    ZOGCU_TRY(tm[c].start(s));
-    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A, V, given, max_iter, 1, false, s, launches)));
-    ZOGCU_TRY(tm[c].stop(s));
+  EventTimer tm[kTimed];
+  int order[kTimed];
+  for (int i = 0; i < kTimed; ++i) {
+    const int j = i % kNumPrConfigs;
+    order[i] = (i / kNumPrConfigs) % 2 == 0 ? j : kNumPrConfigs - 1 - j;
+    ZOGCU_TRY(tm[i].start(s));
+    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, order[i], A, V, given, max_iter, 1, false, s, launches)));
+    ZOGCU_TRY(tm[i].stop(s));
   }
   PrState hs;
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
-  int best = kDefaultPrConfig;
-  if (!hs.converged && hs.iter == kTuneIters) {
-    float best_ms = 1e30f;
-    for (int c = 0; c < kNumPrConfigs; ++c) {
-      const float ms = tm[c].ms();
-      if (ms > 0.f && ms < best_ms) {
-        best_ms = ms;
-        best = c;
-      }
+  // timed launch i ran iteration 1 + i, which did work iff the chain reached
+  // 2 + i; a configuration's time is the lower of its two launches
+  double best_of[kNumPrConfigs];
+  int cnt[kNumPrConfigs] = {};
+  for (int i = 0; i < kTimed; ++i) {
+    if (hs.iter < (unsigned long long)(2 + i)) break;
+    const double ms = tm[i].ms();
+    const int c = order[i];
+    best_of[c] = cnt[c] ? std::min(best_of[c], ms) : ms;
+    ++cnt[c];
+  }
+  if (std::getenv("ZOGCU_PR_TUNE_LOG")) {  // diagnostic: the tuning launches in order
+    for (int i = 0; i < kTimed; ++i)
+      std::fprintf(stderr, "zogcu pagerank tuning: iteration %d config %d %.4f ms%s\n", 1 + i, order[i],
+                   tm[i].ms(), hs.iter < (unsigned long long)(2 + i) ? " (after convergence)" : "");
+  }
+  int best = -1;
+  double best_ms = 1e30;
+  for (int c = 0; c < kNumPrConfigs; ++c) {
+    if (cnt[c] == 0) {
+      best = -1;
+      break;
     }
+    const double ms = best_of[c];
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  if (best >= 0) {
     std::lock_guard<std::mutex> lk(g->mu);
     if (g->pr.config < 0) g->pr.config = best;
     best = g->pr.config;
+  } else {
+    best = kDefaultPrConfig;
   }
   *used_cfg = best;
   return pr_launch_chain<OffT, CT>(g, best, A, V, given, max_iter, max_iter - kTuneIters, false, s, launches);
