@@ -914,64 +914,73 @@ static int build_ranked_view(Graph* g, cudaStream_t s) {
 }
 
 // Work items for row blocks of at most `nnz` arcs, built on the device.  The
-// ranked rows are cut into segments of kTaskSegRows rows and one thread walks
+// ranked rows are cut into segments of kTaskSegRows rows, and one warp walks
 // each segment with the greedy rule: a row longer than nnz becomes one row
-// item (<= kLongChunk arcs) or its run of chunk items; otherwise consecutive
-// rows of <= nnz arcs join a block while the block stays within nnz arcs and
-// kWarpRows rows.  Blocks never cross a segment boundary, so the segments are
-// independent: a counting pass, a scan over the segments, and a writing pass
-// that repeats the walk.  Which rows share a block does not change any row's
-// sum: a row's summation order depends only on its own arcs.
-constexpr uint32_t kTaskSegRows = 1024;
+// item (<= kLongChunk arcs) or its run of chunk items; otherwise the block
+// starting at row r ends at the largest e <= r + kWarpRows with
+// off[e] - off[r] <= nnz (offsets never decrease, so the 64 candidates form
+// a prefix the warp finds with two ballots).  Blocks never cross a segment
+// boundary, so the segments are independent: a counting pass, a scan over
+// the segments, and a writing pass that repeats the walk.  A cut costs a work
+// item (one extra item per 4,096 rows at most); longer segments leave too few
+// warps to hide the walk's dependent loads.
+// Which rows share a block does not change any row's sum: a row's summation
+// order depends only on its own arcs.
+constexpr uint32_t kTaskSegRows = 4096;
 
 template <typename OffT>
 __global__ void k_task_segments(const OffT* __restrict__ off, uint32_t V, uint32_t nnz, uint32_t nseg,
                                 unsigned long long* __restrict__ seg_tasks, unsigned long long* __restrict__ seg_long,
                                 PrTask* __restrict__ tasks, uint32_t* __restrict__ long_first, int write,
                                 unsigned int* __restrict__ err) {
-  for (uint32_t sg = blockIdx.x * blockDim.x + threadIdx.x; sg < nseg; sg += gridDim.x * blockDim.x) {
-    uint32_t r = sg * kTaskSegRows;
-    const uint32_t rend = min(V, r + kTaskSegRows);  // V < 2^30
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t sg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < nseg; sg += nw) {
+    uint32_t r = sg * kTaskSegRows;  // V < 2^30, so no overflow
+    const uint32_t rend = min(V, r + kTaskSegRows);
     unsigned long long nt = write ? seg_tasks[sg] : 0ull, nl = write ? seg_long[sg] : 0ull;
-    OffT o_r = off[r];
-    while (r < rend) {
-      OffT o_n = off[r + 1];
-      uint64_t len = (uint64_t)(o_n - o_r);
+    while (r < rend) {  // r is the same in every lane
+      if (lane == 0) {
+        const uint32_t pf = min(r + 1024u, V);
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(off + pf));
+      }
+      const OffT o0 = __ldg(off + r);
+      const uint64_t len = (uint64_t)(__ldg(off + r + 1) - o0);
       if (len > nnz) {
         if (len <= (uint64_t)kLongChunk) {
-          if (write) tasks[nt] = PrTask{r, (kTaskRow << 30) | (r + 1)};
+          if (write && lane == 0) tasks[nt] = PrTask{r, (kTaskRow << 30) | (r + 1)};
           ++nt;
         } else {
           uint64_t nch = (len + kLongChunk - 1) / kLongChunk;
           if (nch > 0xFFFFull) {
-            atomicOr(err, 1u);
+            if (lane == 0) atomicOr(err, 1u);
             nch = 0;
           }
           if (write) {
-            long_first[nl] = (uint32_t)nt;
-            for (uint32_t c = 0; c < (uint32_t)nch; ++c) tasks[nt + c] = PrTask{r, (kTaskChunk << 30) | c};
+            if (lane == 0) long_first[nl] = (uint32_t)nt;
+            for (uint32_t c = lane; c < (uint32_t)nch; c += 32) tasks[nt + c] = PrTask{r, (kTaskChunk << 30) | c};
           }
           ++nl;
           nt += nch;
         }
         ++r;
-        o_r = o_n;
         continue;
       }
-      const uint32_t r0 = r;
-      uint64_t tot = 0;
-      while (r < rend && r - r0 < (uint32_t)kWarpRows) {
-        o_n = off[r + 1];
-        len = (uint64_t)(o_n - o_r);
-        if (len > nnz || tot + len > nnz) break;
-        tot += len;
-        ++r;
-        o_r = o_n;
+      const uint32_t lim = min(r + (uint32_t)kWarpRows, rend);
+      const uint32_t c1 = r + 1 + lane;
+      const bool ok1 = c1 <= lim && (uint64_t)(__ldg(off + c1) - o0) <= nnz;
+      const unsigned m1 = __ballot_sync(0xffffffffu, ok1);
+      uint32_t cnt = __popc(m1);
+      if (m1 == 0xffffffffu) {
+        const uint32_t c2 = r + 33 + lane;
+        const bool ok2 = c2 <= lim && (uint64_t)(__ldg(off + c2) - o0) <= nnz;
+        cnt += __popc(__ballot_sync(0xffffffffu, ok2));
       }
-      if (write) tasks[nt] = PrTask{r0, (kTaskBlock << 30) | r};
+      if (write && lane == 0) tasks[nt] = PrTask{r, (kTaskBlock << 30) | (r + cnt)};
       ++nt;
+      r += cnt;
     }
-    if (!write) {
+    if (!write && lane == 0) {
       seg_tasks[sg] = nt;
       seg_long[sg] = nl;
     }
@@ -995,7 +1004,7 @@ static int build_task_list_t(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
   unsigned long long* ol = ot + nseg + 1;
   unsigned int* err = reinterpret_cast<unsigned int*>(ol + nseg + 1);
   const OffT* off = g->pr.off.as<OffT>();
-  const unsigned grid = (unsigned)std::max<uint32_t>((nseg + 127) / 128, 1);
+  const unsigned grid = (unsigned)std::max<uint32_t>((nseg + 3) / 4, 1);  // 4 warps (segments) per CTA
   if (nseg) {
     k_task_segments<OffT><<<grid, 128, 0, s>>>(off, V, (uint32_t)nnz, nseg, ct, cl, nullptr, nullptr, 0, err);
     ZOGCU_CUDA(cudaGetLastError());
@@ -1144,20 +1153,20 @@ static int pr_config_of(Graph* g) {
 
 // A chain of up to max_iter iterations.  When the graph has no configuration
 // yet, the chain's own first iterations choose it: one iteration with the
-// default configuration (caches warm), then two timed iterations of each
-// configuration, in ascending and then descending order so that no
-// configuration always follows the same one; the one with the lowest time
-// runs the rest and is kept for the graph.  Every configuration computes the same
-// iteration, so the tuning iterations are ordinary iterations of the solve.
-// Only iterations that ran before convergence count; if some configuration
-// has none, nothing is kept.
+// default configuration (caches warm), one timed iteration of each
+// configuration in ascending order, then a second timed iteration, in
+// descending order, of each configuration within kSecondRound of the first
+// round's best.  A configuration's time is the lower of its launches; the
+// fastest runs the rest of the chain and is kept for the graph.  Every
+// configuration computes the same iteration, so the tuning iterations are
+// ordinary iterations of the solve.  Only iterations that ran before
+// convergence count; if some configuration has none, nothing is kept.
 template <typename OffT, typename CT>
 static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V, int given, uint64_t max_iter,
                         cudaStream_t s, uint64_t* launches, int* used_cfg) {
-  constexpr int kRounds = 2;
-  constexpr int kTimed = kRounds * kNumPrConfigs;
-  constexpr uint64_t kTuneIters = 1 + (uint64_t)kTimed;
-  if (cfg >= 0 || max_iter <= kTuneIters) {
+  constexpr double kSecondRound = 1.15;
+  constexpr uint64_t kMaxTuneIters = 1 + 2 * (uint64_t)kNumPrConfigs;
+  if (cfg >= 0 || max_iter <= kMaxTuneIters) {
     if (cfg < 0) cfg = kDefaultPrConfig;
     *used_cfg = cfg;
     return pr_launch_chain<OffT, CT>(g, cfg, A, V, given, max_iter, max_iter, true, s, launches);
@@ -1167,46 +1176,55 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
   for (int c = 0; c < kNumPrConfigs; ++c)
     if (PrLauncher<OffT, CT>::grid(c, 0) <= 0) return fail(ZOGCU_ERR_CUDA, "PageRank kernel configuration could not be set up");
   ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, kDefaultPrConfig, A, V, given, max_iter, 1, true, s, launches)));
-  EventTimer tm[kTimed];
-  int order[kTimed];
-  for (int i = 0; i < kTimed; ++i) {
-    const int j = i % kNumPrConfigs;
-    order[i] = (i / kNumPrConfigs) % 2 == 0 ? j : kNumPrConfigs - 1 - j;
-    ZOGCU_TRY(tm[i].start(s));
-    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, order[i], A, V, given, max_iter, 1, false, s, launches)));
-    ZOGCU_TRY(tm[i].stop(s));
-  }
+  EventTimer tm[2 * kNumPrConfigs];
+  int order[2 * kNumPrConfigs];
+  int n = 0;
+  auto timed = [&](int c) -> int {
+    order[n] = c;
+    ZOGCU_TRY(tm[n].start(s));
+    ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A, V, given, max_iter, 1, false, s, launches)));
+    ZOGCU_TRY(tm[n].stop(s));
+    ++n;
+    return ZOGCU_OK;
+  };
   PrState hs;
-  ZOGCU_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
-  ZOGCU_CUDA(cudaStreamSynchronize(s));
-  // timed launch i ran iteration 1 + i, which did work iff the chain reached
-  // 2 + i; a configuration's time is the lower of its two launches
   double best_of[kNumPrConfigs];
-  int cnt[kNumPrConfigs] = {};
-  for (int i = 0; i < kTimed; ++i) {
-    if (hs.iter < (unsigned long long)(2 + i)) break;
-    const double ms = tm[i].ms();
-    const int c = order[i];
-    best_of[c] = cnt[c] ? std::min(best_of[c], ms) : ms;
-    ++cnt[c];
+  int cnt[kNumPrConfigs];
+  // timed launch i ran iteration 1 + i, which did work iff the chain reached 2 + i
+  auto collect = [&]() -> int {
+    ZOGCU_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(PrState), cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    for (int c = 0; c < kNumPrConfigs; ++c) cnt[c] = 0;
+    for (int i = 0; i < n && hs.iter >= (unsigned long long)(2 + i); ++i) {
+      const double ms = tm[i].ms();
+      const int c = order[i];
+      best_of[c] = cnt[c] ? std::min(best_of[c], ms) : ms;
+      ++cnt[c];
+    }
+    return ZOGCU_OK;
+  };
+  auto fastest = [&]() {
+    int best = -1;
+    for (int c = 0; c < kNumPrConfigs; ++c) {
+      if (cnt[c] == 0) return -1;
+      if (best < 0 || best_of[c] < best_of[best]) best = c;
+    }
+    return best;
+  };
+  for (int c = 0; c < kNumPrConfigs; ++c) ZOGCU_TRY(timed(c));
+  ZOGCU_TRY(collect());
+  int best = fastest();
+  if (best >= 0) {
+    const double cut = kSecondRound * best_of[best];
+    for (int c = kNumPrConfigs - 1; c >= 0; --c)
+      if (best_of[c] <= cut) ZOGCU_TRY(timed(c));
+    ZOGCU_TRY(collect());
+    best = fastest();
   }
   if (std::getenv("ZOGCU_PR_TUNE_LOG")) {  // diagnostic: the tuning launches in order
-    for (int i = 0; i < kTimed; ++i)
+    for (int i = 0; i < n; ++i)
       std::fprintf(stderr, "zogcu pagerank tuning: iteration %d config %d %.4f ms%s\n", 1 + i, order[i],
                    tm[i].ms(), hs.iter < (unsigned long long)(2 + i) ? " (after convergence)" : "");
-  }
-  int best = -1;
-  double best_ms = 1e30;
-  for (int c = 0; c < kNumPrConfigs; ++c) {
-    if (cnt[c] == 0) {
-      best = -1;
-      break;
-    }
-    const double ms = best_of[c];
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = c;
-    }
   }
   if (best >= 0) {
     std::lock_guard<std::mutex> lk(g->mu);
@@ -1216,7 +1234,7 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     best = kDefaultPrConfig;
   }
   *used_cfg = best;
-  return pr_launch_chain<OffT, CT>(g, best, A, V, given, max_iter, max_iter - kTuneIters, false, s, launches);
+  return pr_launch_chain<OffT, CT>(g, best, A, V, given, max_iter, max_iter - 1 - (uint64_t)n, false, s, launches);
 }
 
 // FP32-phase switch: the FP32 contributions carry relative rounding ~6e-8, so
