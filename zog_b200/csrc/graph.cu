@@ -118,15 +118,18 @@ EventTimer::~EventTimer() {
   if (b) cudaEventDestroy(b);
 }
 
-static int g_sm_count = 0;
+// SM count of the first device queried (every device of a B200 node has the
+// same count); concurrent first calls store the same value.
+static std::atomic<int> g_sm_count{0};
 int sm_count() {
-  if (g_sm_count == 0) {
+  int n = g_sm_count.load(std::memory_order_relaxed);
+  if (n == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sm_count <= 0) g_sm_count = 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    g_sm_count.store(n, std::memory_order_relaxed);
   }
-  return g_sm_count;
+  return n;
 }
 
 int ensure_device(int* dev) {

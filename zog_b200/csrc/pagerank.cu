@@ -44,6 +44,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -1083,19 +1084,28 @@ struct PrLauncher {
     const uint32_t cap = (uint32_t)(kPrConfigs[cfg].hub_bytes / sizeof(CT));
     return std::min<uint32_t>(cap, V & ~3u);
   }
+  // Grid of configuration `cfg` on the current device (resident CTAs per SM x
+  // SMs).  The first call per device sets the kernel's dynamic shared-memory
+  // limit; concurrent first calls do the same idempotent work.
   static int grid(int cfg, size_t dyn) {
-    static int cache[kNumPrConfigs] = {};
-    if (!cache[cfg]) {
-      Fn f = fn(cfg);
-      const size_t maxdyn = (size_t)kPrConfigs[cfg].hub_bytes + staging_bytes(cfg);
-      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxdyn) != cudaSuccess) return 0;
-      int per_sm = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kPrConfigs[cfg].threads, maxdyn) != cudaSuccess)
-        return 0;
-      cache[cfg] = std::max(per_sm, 1) * sm_count();
-    }
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cache[kMaxDevices][kNumPrConfigs];
     (void)dyn;
-    return cache[cfg];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    const int known = cache[dev][cfg].load(std::memory_order_acquire);
+    if (known > 0) return known;
+    Fn f = fn(cfg);
+    const size_t maxdyn = (size_t)kPrConfigs[cfg].hub_bytes + staging_bytes(cfg);
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxdyn) != cudaSuccess) return 0;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kPrConfigs[cfg].threads, maxdyn) != cudaSuccess)
+      return 0;
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) return 0;
+    const int g = std::max(per_sm, 1) * nsm;
+    cache[dev][cfg].store(g, std::memory_order_release);
+    return g;
   }
 };
 
@@ -1518,13 +1528,13 @@ static int run_linear(Graph* g, double ka, double kb, double start, uint64_t max
   auto fn = pr_iter_kernel<OffT, double, 256, 256, MODE>;
   constexpr int cfg = 3;
   const size_t dyn = PrLauncher<OffT, double>::staging_bytes(cfg);
-  static int grid = 0;
-  if (!grid) {
+  static std::atomic<int> grid{0};  // same value for every B200 device
+  if (!grid.load(std::memory_order_acquire)) {
     int per_sm = 0;
     ZOGCU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, dyn));
-    grid = std::max(per_sm, 1) * sm_count();
+    grid.store(std::max(per_sm, 1) * sm_count(), std::memory_order_release);
   }
-  int gr = grid;
+  int gr = grid.load(std::memory_order_acquire);
   const uint32_t need = (A.ntasks + 7) / 8;
   if (need > 0 && (uint32_t)gr > need) gr = (int)need;
   const unsigned gn = std::min(grid_1d(V), 148u * 4);
