@@ -1164,18 +1164,17 @@ static int pr_config_of(Graph* g) {
 // A chain of up to max_iter iterations.  When the graph has no configuration
 // yet, the chain's own first iterations choose it: one iteration with the
 // default configuration (caches warm), one timed iteration of each
-// configuration in ascending order, then a second timed iteration, in
-// descending order, of each configuration within kSecondRound of the first
-// round's best.  A configuration's time is the lower of its launches; the
-// fastest runs the rest of the chain and is kept for the graph.  Every
+// configuration, then, for each configuration within kSecondRound of that
+// round's best, two iterations back to back of which the second is timed.
+// The fastest runs the rest of the chain and is kept for the graph.  Every
 // configuration computes the same iteration, so the tuning iterations are
 // ordinary iterations of the solve.  Only iterations that ran before
-// convergence count; if some configuration has none, nothing is kept.
+// convergence count; if a configuration has none, nothing is kept.
 template <typename OffT, typename CT>
 static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V, int given, uint64_t max_iter,
                         cudaStream_t s, uint64_t* launches, int* used_cfg) {
   constexpr double kSecondRound = 1.15;
-  constexpr uint64_t kMaxTuneIters = 1 + 2 * (uint64_t)kNumPrConfigs;
+  constexpr uint64_t kMaxTuneIters = 1 + 3 * (uint64_t)kNumPrConfigs;
   if (cfg >= 0 || max_iter <= kMaxTuneIters) {
     if (cfg < 0) cfg = kDefaultPrConfig;
     *used_cfg = cfg;
@@ -1186,8 +1185,8 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
   for (int c = 0; c < kNumPrConfigs; ++c)
     if (PrLauncher<OffT, CT>::grid(c, 0) <= 0) return fail(ZOGCU_ERR_CUDA, "PageRank kernel configuration could not be set up");
   ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, kDefaultPrConfig, A, V, given, max_iter, 1, true, s, launches)));
-  EventTimer tm[2 * kNumPrConfigs];
-  int order[2 * kNumPrConfigs];
+  EventTimer tm[3 * kNumPrConfigs];
+  int order[3 * kNumPrConfigs];
   int n = 0;
   auto timed = [&](int c) -> int {
     order[n] = c;
@@ -1206,9 +1205,10 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     for (int c = 0; c < kNumPrConfigs; ++c) cnt[c] = 0;
     for (int i = 0; i < n && hs.iter >= (unsigned long long)(2 + i); ++i) {
-      const double ms = tm[i].ms();
       const int c = order[i];
-      best_of[c] = cnt[c] ? std::min(best_of[c], ms) : ms;
+      if (c < 0) continue;  // untimed launch
+      const double ms = tm[i].ms();
+      best_of[c] = ms;  // the latest timed launch of a configuration counts
       ++cnt[c];
     }
     return ZOGCU_OK;
@@ -1221,20 +1221,45 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     }
     return best;
   };
+  auto fastest_of = [&](const bool* set) {
+    int best = -1;
+    for (int c = 0; c < kNumPrConfigs; ++c) {
+      if (!set[c]) continue;
+      if (cnt[c] == 0) return -1;
+      if (best < 0 || best_of[c] < best_of[best]) best = c;
+    }
+    return best;
+  };
   for (int c = 0; c < kNumPrConfigs; ++c) ZOGCU_TRY(timed(c));
   ZOGCU_TRY(collect());
   int best = fastest();
   if (best >= 0) {
+    // second round: each close configuration runs twice back to back and
+    // only the second launch is timed, the one that starts from the caches
+    // the configuration itself leaves (a configuration's first launch after
+    // another one ran up to 8 % slow)
     const double cut = kSecondRound * best_of[best];
-    for (int c = kNumPrConfigs - 1; c >= 0; --c)
-      if (best_of[c] <= cut) ZOGCU_TRY(timed(c));
+    bool close[kNumPrConfigs];
+    for (int c = 0; c < kNumPrConfigs; ++c) close[c] = best_of[c] <= cut;
+    const int first_round = n;
+    for (int c = kNumPrConfigs - 1; c >= 0; --c) {
+      if (!close[c]) continue;
+      ZOGCU_TRY((pr_launch_chain<OffT, CT>(g, c, A, V, given, max_iter, 1, false, s, launches)));
+      order[n] = -1;  // untimed
+      ++n;
+      ZOGCU_TRY(timed(c));
+    }
     ZOGCU_TRY(collect());
-    best = fastest();
+    // the close configurations are ranked by their second-round time alone
+    for (int i = 0; i < first_round; ++i)
+      if (close[order[i]]) --cnt[order[i]];
+    best = fastest_of(close);
   }
   if (std::getenv("ZOGCU_PR_TUNE_LOG")) {  // diagnostic: the tuning launches in order
     for (int i = 0; i < n; ++i)
-      std::fprintf(stderr, "zogcu pagerank tuning: iteration %d config %d %.4f ms%s\n", 1 + i, order[i],
-                   tm[i].ms(), hs.iter < (unsigned long long)(2 + i) ? " (after convergence)" : "");
+      if (order[i] >= 0)
+        std::fprintf(stderr, "zogcu pagerank tuning: iteration %d config %d %.4f ms%s\n", 1 + i, order[i],
+                     tm[i].ms(), hs.iter < (unsigned long long)(2 + i) ? " (after convergence)" : "");
   }
   if (best >= 0) {
     std::lock_guard<std::mutex> lk(g->mu);
