@@ -133,3 +133,36 @@ def test_sigma_overflow_wraps_like_usize(native, oracle):
         assert np.array_equal(dist[0], d_ref) and np.array_equal(sigma[0], s_ref)
     finally:
         G.destroy()
+
+
+@pytest.mark.parametrize("directed", [True, False])
+def test_hubs_split_over_several_ctas(native, oracle, directed):
+    """Hubs far above the 1,024-arc work item: one with 5,000 in- and 3,000
+    out-arcs, one with 2,500 duplicated in-arcs, on a random background.  The
+    forward (in-arcs) and backward (out-arcs) steps split each hub over
+    several CTAs and add the chunk partials in chunk order.  dist and sigma
+    stay bit-exact; betweenness within the FP64 bar."""
+    rng = np.random.default_rng(21 if directed else 22)
+    V = 9000
+    bg_f = rng.integers(0, V, 30000); bg_t = rng.integers(0, V, 30000)
+    hub_in = rng.integers(0, V, 5000); hub_out = rng.integers(0, V, 3000)
+    dup = np.repeat(rng.integers(0, V, 500), 5)
+    f = np.concatenate([bg_f, hub_in, np.zeros(3000, np.int64), dup]).astype(np.uint32)
+    t = np.concatenate([bg_t, np.zeros(5000, np.int64), hub_out, np.full(2500, 7)]).astype(np.uint32)
+    if not directed:  # store both arcs of every edge, as undirected SoA graphs do
+        f, t = np.concatenate([f, t]), np.concatenate([t, f])
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        srcs = np.concatenate([np.array([0, 7], np.uint32), (np.arange(126, dtype=np.uint32) * 71 + 3) % V])
+        bc = G.betweenness_unweighted(sources=srcs)
+        A = oracle.ArrayGraph(V, f, t)
+        ref, _ = A.betweenness_sources(srcs)
+        assert rel_l1(bc, ref) <= TOL
+        assert np.array_equal(bc == 0.0, ref == 0.0)
+        dist, sigma, _ = G.bfs_sigma(srcs[:3])
+        for i, s in enumerate(srcs[:3]):
+            d_ref, s_ref, _ = A.bfs(int(s))
+            assert np.array_equal(dist[i], d_ref) and np.array_equal(sigma[i], s_ref)
+        assert np.array_equal(bc, G.betweenness_unweighted(sources=srcs))  # deterministic
+    finally:
+        G.destroy()
