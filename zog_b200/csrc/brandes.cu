@@ -409,11 +409,17 @@ __global__ void bc_seed_kernel(const uint32_t* __restrict__ sources, int nb, uns
   }
 }
 
-static int bc_grid(uint32_t V) {
-  const uint64_t warps = V;
-  uint64_t blocks = (warps + (kBcThreads / 32) - 1) / (kBcThreads / 32);
-  const uint64_t cap = (uint64_t)sm_count() * (2048 / kBcThreads);
-  if (blocks > cap) blocks = cap;
+// Grid of a Brandes kernel: the CTAs that are resident at once (occupancy x
+// SMs), at most one per task, so the grid-stride task loop runs in a single
+// wave and no CTA waits for a slot while others idle at the end of a level.
+template <typename K>
+static int bc_grid(K kernel, uint32_t V) {
+  const uint64_t tasks = ((uint64_t)V + (kBcThreads / 32) - 1) / (kBcThreads / 32);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBcThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  uint64_t blocks = (uint64_t)sm_count() * (uint64_t)per_sm;
+  if (blocks > tasks) blocks = tasks;
   if (blocks < 1) blocks = 1;
   return (int)blocks;
 }
@@ -498,7 +504,7 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
                             cudaStream_t s, uint32_t* depth, bool* overflow, uint64_t* launches,
                             unsigned int* h_flags) {
   const uint32_t V = g->V;
-  const int grid = bc_grid(V);
+  const int grid = bc_grid(bc_forward_kernel<OffT>, V);
   const unsigned long long full = nb == 64 ? ~0ull : ((1ull << nb) - 1);
   ZOGCU_CUDA(cudaMemsetAsync(W.visited.ptr, 0, (size_t)V * 8, s));
   ZOGCU_CUDA(cudaMemsetAsync(W.level(0, V), 0, (size_t)V * 8, s));
@@ -555,7 +561,7 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
     unsigned int* p;
     ~HostFree() { cudaFreeHost(p); }
   } hf{h_flags};
-  const int grid = bc_grid(V);
+  const int grid = bc_grid(bc_backward_kernel<OffT>, V);
   bool overflow = false;
   uint32_t max_depth = 0;
   uint64_t launches = 0;
