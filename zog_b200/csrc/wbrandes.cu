@@ -258,6 +258,17 @@ unsigned wb_grid(uint64_t warps) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)sm_count() * 8));
 }
 
+// Grid of a round kernel: the CTAs of 256 threads resident at once
+// (occupancy x SMs), at most one per 8 warps of work, so the grid-stride loop
+// runs in one wave.
+template <typename K>
+unsigned wb_grid_of(K kernel, uint64_t warps) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+  const uint64_t g = (warps * 32 + 255) / 256;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)sm_count() * (uint64_t)per_sm));
+}
+
 // Runs launch(k) for k = 0, 1, ... in chains of kWbChain until round k has no
 // work (work[k] == 0).  Both sweeps have work in at most V + 1 rounds when the
 // weights are positive; `work` holds V + 3 + 2 kWbChain flags.
@@ -331,7 +342,9 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     if (bad) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "weighted betweenness needs positive finite weights");
   }
-  const unsigned grid = wb_grid(std::max<uint32_t>(ntasks, V));
+  const uint64_t nwork = std::max<uint32_t>(ntasks, V);
+  const unsigned g_relax = wb_grid_of(k_wb_relax, nwork), g_count = wb_grid_of(k_wb_dagcount, nwork);
+  const unsigned g_sigma = wb_grid_of(k_wb_sigma, nwork), g_delta = wb_grid_of(k_wb_delta, nwork);
   unsigned long long* dist = bdist.as<unsigned long long>();
   unsigned long long* sigma = bsigma.as<unsigned long long>();
   double* delta = bdelta.as<double>();
@@ -359,12 +372,12 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
     uint32_t r1 = 0;
     ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
-      k_wb_relax<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, masks[k % 3], masks[(k + 1) % 3],
+      k_wb_relax<<<g_relax, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, masks[k % 3], masks[(k + 1) % 3],
                                        masks[(k + 2) % 3], V, work, k);
     }, &r1));
     launches += r1;
     // phase 2: DAG in-counts, then sigma in topological rounds from the sources
-    k_wb_dagcount<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, cnt, flags);
+    k_wb_dagcount<<<g_count, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, cnt, flags);
     for (int i = 0; i < 3; ++i) ZOGCU_CUDA(cudaMemsetAsync(masks[i], 0, Vs * 4, s));
     k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
     ZOGCU_CUDA(cudaGetLastError());
@@ -372,7 +385,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
     uint32_t r2 = 0;
     ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
-      k_wb_sigma<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, cnt, round, masks[k % 3],
+      k_wb_sigma<<<g_sigma, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, cnt, round, masks[k % 3],
                                        masks[(k + 1) % 3], masks[(k + 2) % 3], V, work, flags, k);
     }, &r2));
     launches += r2 + 2;
@@ -386,7 +399,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     const uint32_t maxr = hf[kFlagMaxRound];
     deepest = std::max(deepest, maxr);
     for (int64_t r = maxr; r >= 0; --r)
-      k_wb_delta<<<grid, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, delta, round, src, ns,
+      k_wb_delta<<<g_delta, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, delta, round, src, ns,
                                       bc.as<double>(), (uint32_t)r);
     ZOGCU_CUDA(cudaGetLastError());
     launches += (uint64_t)maxr + 1;
