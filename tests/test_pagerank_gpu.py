@@ -96,10 +96,11 @@ def test_in_csr_order_matches_reference(native, oracle):
         G.destroy()
 
 
-@pytest.mark.parametrize("max_iter", [0, 1, 2, 7])
+@pytest.mark.parametrize("max_iter", [0, 1, 2, 7, 60])
 def test_iteration_prefix_exact(native, oracle, max_iter):
     """Stopping after k iterations returns the k-th iterate (the swap happens
-    before the tolerance test, centrality.zig:953-957)."""
+    before the tolerance test, centrality.zig:953-957).  60 iterations run as
+    a CUDA-graph while loop that must stop exactly at max_iter."""
     V, f, t = oracle.rmat(13, 8, 4242, directed=True)
     G = native.Graph.from_edges(V, f, t)
     try:

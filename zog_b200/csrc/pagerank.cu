@@ -112,6 +112,8 @@ struct PrArgs {
   double ka, kb;         // katz: alpha, beta; alpha centrality: alpha
   double* x2;            // eigenvector: third rotating buffer
   uint32_t nv;           // node slots V (bound of every source index)
+  unsigned long long cond;  // conditional handle of the CUDA-graph while loop running the chain
+  int use_cond;             // 1: launched inside that loop; clear the condition when the chain ends
 };
 
 // Epilogue modes of the iteration kernel (all share the schedule and the
@@ -268,7 +270,8 @@ __device__ __forceinline__ void cta_sum2(double& a, double& b, double* s_red) {
 // order, then publication of the iteration's result.
 __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta, const double* long_part,
                              const uint32_t* long_first, uint32_t nlong, unsigned long long next_iter, double tol,
-                             double stall, bool set_l1, double* s_red) {
+                             double stall, bool set_l1, double* s_red, unsigned long long max_iter = 0,
+                             unsigned long long cond = 0, int use_cond = 0) {
   double a = 0.0, b = 0.0;
   for (uint32_t i = threadIdx.x; i < ncta; i += blockDim.x) {
     a += __ldcg(cta_part + 2 * i);
@@ -296,6 +299,8 @@ __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta,
       st->converged = 0;
     }
     st->iter = next_iter;
+    // inside a CUDA-graph while loop: the chain is over, run no further body
+    if (use_cond && (st->converged || next_iter >= max_iter)) cudaGraphSetConditional(cond, 0u);
     __threadfence();
     st->done_ctas = 0;
   }
@@ -305,7 +310,8 @@ __device__ void final_reduce(PrState* st, const double* cta_part, uint32_t ncta,
 __device__ __forceinline__ void cta_publish(PrState* st, double* cta_part, const double* long_part,
                                             const uint32_t* long_first, uint32_t nlong, double l1, double dsum,
                                             unsigned long long next_iter, double tol, double stall, bool set_l1,
-                                            double* s_red, int* s_flag) {
+                                            double* s_red, int* s_flag, unsigned long long max_iter = 0,
+                                            unsigned long long cond = 0, int use_cond = 0) {
   cta_sum2(l1, dsum, s_red);
   if (threadIdx.x == 0) {
     cta_part[2 * blockIdx.x] = l1;
@@ -317,7 +323,8 @@ __device__ __forceinline__ void cta_publish(PrState* st, double* cta_part, const
   __syncthreads();
   if (*s_flag) {
     __threadfence();
-    final_reduce(st, cta_part, gridDim.x, long_part, long_first, nlong, next_iter, tol, stall, set_l1, s_red);
+    final_reduce(st, cta_part, gridDim.x, long_part, long_first, nlong, next_iter, tol, stall, set_l1, s_red,
+                 max_iter, cond, use_cond);
   }
 }
 
@@ -377,7 +384,11 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
   const PrState* st = A.st;
   const unsigned long long iter = *(volatile const unsigned long long*)&st->iter;
   const int converged = *(volatile const int*)&st->converged;
-  if (converged || iter >= A.max_iter) return;
+  if (converged || iter >= A.max_iter) {
+    // the chain is over; inside a CUDA-graph while loop, also stop the loop
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0u);
+    return;
+  }
   const double sink = *(volatile const double*)&st->sink;
 
   const int par = (int)(iter & 1ull);
@@ -560,7 +571,7 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
     ti = tn;
   }
   cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol,
-              MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag);
+              MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag, A.max_iter, A.cond, A.use_cond);
 }
 
 constexpr int pr_pipe_min_blocks(int nnz) { return nnz >= 256 ? 3 : 4; }
@@ -583,7 +594,11 @@ __global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kern
   const PrState* st = A.st;
   const unsigned long long iter = *(volatile const unsigned long long*)&st->iter;
   const int converged = *(volatile const int*)&st->converged;
-  if (converged || iter >= A.max_iter) return;
+  if (converged || iter >= A.max_iter) {
+    // the chain is over; inside a CUDA-graph while loop, also stop the loop
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0u);
+    return;
+  }
   const double sink = *(volatile const double*)&st->sink;
 
   const int par = (int)(iter & 1ull);
@@ -794,7 +809,7 @@ __global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kern
   }
   cp_wait<0>();
   cta_publish(A.st, A.cta_part, A.long_part, A.long_first, A.nlong, l1, dsum, iter + 1, A.tol,
-              MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag);
+              MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag, A.max_iter, A.cond, A.use_cond);
 }
 
 // ---------------------------------------------------------------------------
@@ -1114,12 +1129,68 @@ struct PrWork {
   DevBuf x0, x1, c0, c1, part, chunk, lcnt, lpart, stb, tele, tmp;
 };
 
-// Launches `count` iterations of configuration `cfg`; `init` starts a new
-// chain (state cleared, start vector written).  A.max_iter bounds the whole
-// chain, so a chain may be launched in pieces of different configurations.
+// Runs kernel `fn` as the body of a CUDA-graph while loop on stream s.  The
+// body repeats until a launch clears the loop's condition, which the kernel
+// does when the chain has converged or reached max_iter (the last CTA of the
+// final iteration, or the first CTA of a launch that finds the chain over).
+// So no launches are spent after convergence, and the host enqueues one graph
+// launch instead of max_iter kernel launches.  The loop ends by construction:
+// every body launch either completes one more iteration, at most max_iter in
+// all, or clears the condition.
+template <typename OffT, typename CT>
+static int pr_launch_loop(void (*fn)(PrArgs<OffT, CT>), PrArgs<OffT, CT> A, int grid, int threads, size_t dyn,
+                          cudaStream_t s) {
+  cudaGraph_t graph = nullptr;
+  ZOGCU_CUDA(cudaGraphCreate(&graph, 0));
+  struct GraphGuard {
+    cudaGraph_t g;
+    ~GraphGuard() { cudaGraphDestroy(g); }
+  } guard{graph};
+  cudaGraphConditionalHandle h;
+  ZOGCU_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  ZOGCU_CUDA(cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp));
+  A.cond = h;
+  A.use_cond = 1;
+  void* args[] = {&A};
+  cudaKernelNodeParams kp = {};
+  kp.func = reinterpret_cast<void*>(fn);
+  kp.gridDim = dim3((unsigned)grid);
+  kp.blockDim = dim3((unsigned)threads);
+  kp.sharedMemBytes = (unsigned)dyn;
+  kp.kernelParams = args;
+  cudaGraphNode_t knode;
+  ZOGCU_CUDA(cudaGraphAddKernelNode(&knode, cp.conditional.phGraph_out[0], nullptr, 0, &kp));
+  cudaGraphExec_t exec = nullptr;
+  ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  const cudaError_t e = cudaGraphLaunch(exec, s);
+  cudaGraphExecDestroy(exec);  // an executable graph in flight is freed when it completes
+  ZOGCU_CUDA(e);
+  return ZOGCU_OK;
+}
+
+// Chains of at least this many iterations run as a CUDA-graph while loop.
+// Building and instantiating the graph costs about 0.19 ms per call; a
+// launch that returns at once after convergence costs about 5 us, so the loop
+// pays off once some 40 launches would otherwise be spent after convergence.
+constexpr uint64_t kLoopMinIters = 48;
+
+// Launches up to `count` iterations of configuration `cfg`; `init` starts a
+// new chain (state cleared, start vector written).  A.max_iter bounds the
+// whole chain, so a chain may be launched in pieces of different
+// configurations.  A piece of kLoopMinIters or more iterations runs as a
+// CUDA-graph while loop; then *loop_from is set to `from_iter` (the chain's
+// iteration count when the piece starts), and the caller adds the iterations
+// the loop actually ran to *launches once it has read the chain's state.
 template <typename OffT, typename CT>
 static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, int given, uint64_t max_iter,
-                           uint64_t count, bool init, cudaStream_t s, uint64_t* launches) {
+                           uint64_t count, bool init, cudaStream_t s, uint64_t* launches,
+                           int64_t* loop_from = nullptr, uint64_t from_iter = 0) {
   const PrTaskList& L = g->pr.lists[list_index(kPrConfigs[cfg].nnz)];
   A.tasks = L.tasks.as<PrTask>();
   A.long_first = L.long_first.as<uint32_t>();
@@ -1127,6 +1198,8 @@ static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, in
   A.nlong = L.num_long;
   A.hub = PrLauncher<OffT, CT>::hub_entries(cfg, V);
   A.max_iter = max_iter;
+  A.cond = 0;
+  A.use_cond = 0;
   const size_t dyn = (((size_t)A.hub * sizeof(CT) + 15) & ~(size_t)15) + PrLauncher<OffT, CT>::staging_bytes(cfg);
   int grid = PrLauncher<OffT, CT>::grid(cfg, dyn);
   if (grid <= 0) return fail(ZOGCU_ERR_CUDA, "PageRank kernel configuration could not be set up");
@@ -1141,6 +1214,11 @@ static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, in
     ++*launches;
   }
   auto fn = PrLauncher<OffT, CT>::fn(cfg);
+  if (loop_from && count >= kLoopMinIters) {
+    ZOGCU_TRY((pr_launch_loop<OffT, CT>(fn, A, grid, kPrConfigs[cfg].threads, dyn, s)));
+    *loop_from = (int64_t)from_iter;
+    return ZOGCU_OK;
+  }
   for (uint64_t k = 0; k < count; ++k) fn<<<grid, kPrConfigs[cfg].threads, dyn, s>>>(A);
   ZOGCU_CUDA(cudaGetLastError());
   *launches += count;
@@ -1172,13 +1250,14 @@ static int pr_config_of(Graph* g) {
 // convergence count; if a configuration has none, nothing is kept.
 template <typename OffT, typename CT>
 static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V, int given, uint64_t max_iter,
-                        cudaStream_t s, uint64_t* launches, int* used_cfg) {
+                        cudaStream_t s, uint64_t* launches, int* used_cfg, int64_t* loop_from) {
   constexpr double kSecondRound = 1.15;
   constexpr uint64_t kMaxTuneIters = 1 + 3 * (uint64_t)kNumPrConfigs;
+  *loop_from = -1;
   if (cfg >= 0 || max_iter <= kMaxTuneIters) {
     if (cfg < 0) cfg = kDefaultPrConfig;
     *used_cfg = cfg;
-    return pr_launch_chain<OffT, CT>(g, cfg, A, V, given, max_iter, max_iter, true, s, launches);
+    return pr_launch_chain<OffT, CT>(g, cfg, A, V, given, max_iter, max_iter, true, s, launches, loop_from, 0);
   }
   // one-time launch setup of every configuration (attributes, occupancy,
   // module loading) happens here, outside the timed launches
@@ -1269,7 +1348,9 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     best = kDefaultPrConfig;
   }
   *used_cfg = best;
-  return pr_launch_chain<OffT, CT>(g, best, A, V, given, max_iter, max_iter - 1 - (uint64_t)n, false, s, launches);
+  if (hs.converged || hs.iter >= max_iter) return ZOGCU_OK;  // the chain ended during tuning
+  return pr_launch_chain<OffT, CT>(g, best, A, V, given, max_iter, max_iter - 1 - (uint64_t)n, false, s, launches,
+                                   loop_from, hs.iter);
 }
 
 // FP32-phase switch: the FP32 contributions carry relative rounding ~6e-8, so
@@ -1362,20 +1443,26 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     Af.c1 = cf1.as<float>();
     Af.tol = std::max(tol, kMixedSwitchTol);
     Af.stall = kMixedStall;
-    ZOGCU_TRY((pr_run_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches, &cfg)));
+    int64_t from32 = -1;
+    ZOGCU_TRY((pr_run_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches, &cfg, &from32)));
     ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     if (hs.pad[0]) return fail(ZOGCU_ERR_INTERNAL, "PageRank work item failed a bound check");
+    if (from32 >= 0) launches += hs.iter - (uint64_t)from32 + (hs.iter == (uint64_t)from32 ? 1 : 0);
     it32 = hs.iter;
     // ---- FP64 polish from the FP32 phase's last vector ----------------------
     if (it32 & 1ull) std::swap(A.x0, A.x1);
     given = 1;
   }
-  ZOGCU_TRY((pr_run_chain<OffT, double>(g, cfg, A, V, given, max_iter - it32, s, &launches, &cfg)));
+  int64_t from64 = -1;
+  ZOGCU_TRY((pr_run_chain<OffT, double>(g, cfg, A, V, given, max_iter - it32, s, &launches, &cfg, &from64)));
   ZOGCU_TRY(tm.stop(s));
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   if (hs.pad[0]) return fail(ZOGCU_ERR_INTERNAL, "PageRank work item failed a bound check");
+  // kernel launches of a graph loop: one per iteration it ran (a loop that
+  // found the chain already over ran one launch that only ended the loop)
+  if (from64 >= 0) launches += hs.iter - (uint64_t)from64 + (hs.iter == (uint64_t)from64 ? 1 : 0);
   const double* result = (hs.iter & 1ull) ? A.x1 : A.x0;
   double* unperm = (hs.iter & 1ull) ? A.x0 : A.x1;  // the other buffer is free now
   k_permute_out<<<grid_1d(V), 256, 0, s>>>(result, P.rank.as<uint32_t>(), V, unperm);
