@@ -280,3 +280,35 @@ def test_graphs_reuse_pool_memory_and_release_it(native, oracle):
         assert np.array_equal(G.pagerank(0.85, 200, 1e-10), first)
     finally:
         G.destroy()
+
+
+@pytest.mark.parametrize("order", ["sorted", "shuffled"])
+def test_csr_build_sorted_and_unsorted_sources(native, oracle, order):
+    """The CSR build places the out-CSR with one scatter when the sources come
+    non-decreasing, and sorts otherwise.  Both give the reference's successor
+    order (reverse insertion, array_graph.zig:94-104), in-neighbour order and
+    weights; multi-arcs and self-loops included."""
+    rng = np.random.default_rng(8 if order == "sorted" else 9)
+    V = 5000
+    f = rng.integers(0, V, 60000).astype(np.uint32)
+    t = rng.integers(0, V, 60000).astype(np.uint32)
+    t[:500] = f[:500]                                    # self-loops
+    f = np.concatenate([f, f[:3000]]); t = np.concatenate([t, t[:3000]])  # multi-arcs
+    if order == "sorted":
+        p = np.argsort(f, kind="stable"); f, t = f[p], t[p]
+    w = rng.uniform(1.0, 100.0, f.size)
+    G = native.Graph.from_edges(V, f, t, weight=w)
+    try:
+        in_off, in_col, out_off, out_col, deg = G.export_csr()
+        off_r, col_r, deg_r = oracle.in_csr_from_edges(V, f, t)
+        assert np.array_equal(in_off, off_r) and np.array_equal(in_col, col_r) and np.array_equal(deg, deg_r)
+        so, sc = oracle.ArrayGraph(V, f, t).successor_csr()
+        assert np.array_equal(out_off, so) and np.array_equal(out_col, sc)
+        # weights in successor order: each source's arcs, last inserted first
+        wexp = np.concatenate([w[np.flatnonzero(f == v)][::-1] for v in range(V)])
+        assert np.array_equal(G.export_weights(), wexp)
+        x = G.pagerank(0.85, 100, 1e-10)
+        ref, it, _ = oracle.ArrayGraph(V, f, t).pagerank(0.85, 100, 1e-10)
+        assert rel_l1(x, ref) <= TOL
+    finally:
+        G.destroy()

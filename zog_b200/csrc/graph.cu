@@ -180,11 +180,37 @@ __global__ void k_reverse_copy_u64(const unsigned long long* __restrict__ w, uns
     out[i] = w[reverse ? (E - 1 - i) : i];
 }
 
+// flags[0]: an endpoint is >= V; flags[1]: the sources are not in
+// non-decreasing order (the sorted-input fast path of the CSR build is off)
 __global__ void k_validate(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint64_t E,
-                           uint32_t V, unsigned int* bad) {
+                           uint32_t V, unsigned int* flags) {
+  bool bad = false, unsorted = false;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < E;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    if (a[i] >= V || b[i] >= V) atomicOr(bad, 1u);
+    const uint32_t ai = a[i];
+    bad |= ai >= V || b[i] >= V;
+    unsorted |= i + 1 < E && a[i + 1] < ai;
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
+  if (__any_sync(0xffffffffu, unsorted) && (threadIdx.x & 31) == 0) atomicOr(flags + 1, 1u);
+}
+
+// Sorted-input out-CSR: input arc j of source r = src[j] goes to position
+// off[r] + off[r+1] - 1 - j when each row is reversed (ArrayGraph successor
+// order is the reverse of insertion order), or stays at j otherwise.
+__global__ void k_scatter_sorted(const uint32_t* __restrict__ src, const uint32_t* __restrict__ dst,
+                                 const unsigned long long* __restrict__ w, const uint64_t* __restrict__ off,
+                                 uint64_t E, int reverse, uint32_t* __restrict__ out_col,
+                                 unsigned long long* __restrict__ out_w) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < E;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t p = j;
+    if (reverse) {
+      const uint32_t r = src[j];
+      p = off[r] + off[r + 1] - 1 - j;
+    }
+    out_col[p] = dst[j];
+    if (w) out_w[p] = w[j];
   }
 }
 
@@ -248,7 +274,7 @@ static int counts_to_offsets(unsigned long long* d_cnt, uint64_t* d_off, uint32_
 
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, const uint32_t* d_dst,
                                   uint64_t E, bool reverse_within_source, const uint8_t* h_node_deleted,
-                                  cudaStream_t s, const double* d_w) {
+                                  cudaStream_t s, const double* d_w, int src_sorted) {
   ZOGCU_TRY(ensure_device(&g->device));
   g->V = V;
   g->E = E;
@@ -270,8 +296,9 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
   ZOGCU_TRY(g->in_off64.alloc((size_t)(V + 1) * 8));
   ZOGCU_TRY(g->out_off64.alloc((size_t)(V + 1) * 8));
   ZOGCU_TRY(g->out_deg.alloc((size_t)std::max<uint32_t>(V, 1) * 4));
-  ZOGCU_CUDA(cudaMemsetAsync(g->in_col.ptr, 0, colBytes, s));
-  ZOGCU_CUDA(cudaMemsetAsync(g->out_col.ptr, 0, colBytes, s));
+  // the 4 padding entries after the arcs (16-byte loads read them) are zero
+  ZOGCU_CUDA(cudaMemsetAsync(g->in_col.as<uint32_t>() + E, 0, 4 * sizeof(uint32_t), s));
+  ZOGCU_CUDA(cudaMemsetAsync(g->out_col.as<uint32_t>() + E, 0, 4 * sizeof(uint32_t), s));
   if (g->has_deleted) {
     ZOGCU_TRY(g->live.alloc(V));
     std::vector<uint8_t> lv(V);
@@ -283,59 +310,90 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
   DevBuf cnt;
   ZOGCU_TRY(cnt.alloc((size_t)(V + 1) * 8, s));
   if (E > 0) {
-    DevBuf ks, vs, ks2;
-    ZOGCU_TRY(ks.alloc(E * 4, s));
-    ZOGCU_TRY(vs.alloc(E * 4, s));
-    ZOGCU_TRY(ks2.alloc(E * 4, s));
-    k_reverse_copy<<<grid_for(E), 256, 0, s>>>(d_src, d_dst, ks.as<uint32_t>(), vs.as<uint32_t>(), E,
-                                               reverse_within_source ? 1 : 0);
-    ZOGCU_CUDA(cudaGetLastError());
     const int bits = bits_for(V);
-    // (1) stable sort by source: rows in successor order -> out-CSR
-    size_t tmp = 0;
-    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
-                                               vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
-                                               0, bits, s));
-    DevBuf t;
-    ZOGCU_TRY(t.alloc(tmp, s));
-    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
-                                               vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
-                                               0, bits, s));
-    if (d_w) {
-      // the same stable sort of the same keys carries the weights along
-      DevBuf wr, kd;
-      ZOGCU_TRY(wr.alloc(E * 8, s));
-      ZOGCU_TRY(kd.alloc(E * 4, s));
-      ZOGCU_TRY(g->out_w.alloc(E * 8));
-      k_reverse_copy_u64<<<grid_for(E), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(d_w),
-                                                     wr.as<unsigned long long>(), E, reverse_within_source ? 1 : 0);
+    bool sorted = src_sorted > 0;
+    if (src_sorted < 0) {  // find out: one pass over the sources
+      DevBuf fl;
+      ZOGCU_TRY(fl.alloc(8, s));
+      ZOGCU_CUDA(cudaMemsetAsync(fl.ptr, 0, 8, s));
+      k_validate<<<grid_for(E), 256, 0, s>>>(d_src, d_src, E, 0xFFFFFFFFu, fl.as<unsigned int>());
       ZOGCU_CUDA(cudaGetLastError());
-      size_t tmpw = 0;
-      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpw, ks.as<uint32_t>(), kd.as<uint32_t>(),
-                                                 wr.as<unsigned long long>(), g->out_w.as<unsigned long long>(),
-                                                 (int64_t)E, 0, bits, s));
-      DevBuf tw;
-      ZOGCU_TRY(tw.alloc(tmpw, s));
-      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tw.ptr, tmpw, ks.as<uint32_t>(), kd.as<uint32_t>(),
-                                                 wr.as<unsigned long long>(), g->out_w.as<unsigned long long>(),
-                                                 (int64_t)E, 0, bits, s));
-      g->weighted = true;
+      unsigned int h[2] = {0, 0};
+      ZOGCU_CUDA(cudaMemcpyAsync(h, fl.ptr, 8, cudaMemcpyDeviceToHost, s));
+      ZOGCU_CUDA(cudaStreamSynchronize(s));
+      sorted = h[1] == 0;
     }
-    // out offsets
-    ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
-    k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks2.as<uint32_t>(), E, cnt.as<unsigned long long>());
-    ZOGCU_CUDA(cudaGetLastError());
-    ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
+    DevBuf ks, vs, ks2, t;
+    size_t tmp = 0;
+    ZOGCU_TRY(ks.alloc(E * 4, s));
+    const uint32_t* keys_out;  // the source of every out-CSR arc (rows ascending)
+    if (sorted) {
+      // Sources already non-decreasing: the out offsets come straight from
+      // them, and one scatter places each row (reversed for insertion order).
+      ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
+      k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(d_src, E, cnt.as<unsigned long long>());
+      ZOGCU_CUDA(cudaGetLastError());
+      ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
+      if (d_w) {
+        ZOGCU_TRY(g->out_w.alloc(E * 8));
+        g->weighted = true;
+      }
+      k_scatter_sorted<<<grid_for(E), 256, 0, s>>>(d_src, d_dst, reinterpret_cast<const unsigned long long*>(d_w),
+                                                   g->out_off64.as<uint64_t>(), E, reverse_within_source ? 1 : 0,
+                                                   g->out_col.as<uint32_t>(), g->out_w.as<unsigned long long>());
+      ZOGCU_CUDA(cudaGetLastError());
+      keys_out = d_src;  // rows are contiguous, so the sources stay in place
+    } else {
+      ZOGCU_TRY(vs.alloc(E * 4, s));
+      ZOGCU_TRY(ks2.alloc(E * 4, s));
+      k_reverse_copy<<<grid_for(E), 256, 0, s>>>(d_src, d_dst, ks.as<uint32_t>(), vs.as<uint32_t>(), E,
+                                                 reverse_within_source ? 1 : 0);
+      ZOGCU_CUDA(cudaGetLastError());
+      // (1) stable sort by source: rows in successor order -> out-CSR
+      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
+                                                 vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
+                                                 0, bits, s));
+      ZOGCU_TRY(t.alloc(tmp, s));
+      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, ks.as<uint32_t>(), ks2.as<uint32_t>(),
+                                                 vs.as<uint32_t>(), g->out_col.as<uint32_t>(), (int64_t)E,
+                                                 0, bits, s));
+      if (d_w) {
+        // the same stable sort of the same keys carries the weights along
+        DevBuf wr, kd;
+        ZOGCU_TRY(wr.alloc(E * 8, s));
+        ZOGCU_TRY(kd.alloc(E * 4, s));
+        ZOGCU_TRY(g->out_w.alloc(E * 8));
+        k_reverse_copy_u64<<<grid_for(E), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(d_w),
+                                                       wr.as<unsigned long long>(), E, reverse_within_source ? 1 : 0);
+        ZOGCU_CUDA(cudaGetLastError());
+        size_t tmpw = 0;
+        ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpw, ks.as<uint32_t>(), kd.as<uint32_t>(),
+                                                   wr.as<unsigned long long>(), g->out_w.as<unsigned long long>(),
+                                                   (int64_t)E, 0, bits, s));
+        DevBuf tw;
+        ZOGCU_TRY(tw.alloc(tmpw, s));
+        ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tw.ptr, tmpw, ks.as<uint32_t>(), kd.as<uint32_t>(),
+                                                   wr.as<unsigned long long>(), g->out_w.as<unsigned long long>(),
+                                                   (int64_t)E, 0, bits, s));
+        g->weighted = true;
+      }
+      // out offsets
+      ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
+      k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks2.as<uint32_t>(), E, cnt.as<unsigned long long>());
+      ZOGCU_CUDA(cudaGetLastError());
+      ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
+      keys_out = ks2.as<uint32_t>();
+    }
     // (2) stable sort of (dst, src) pairs by dst: sources stay ascending
     size_t tmp2 = 0;
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
-                                               ks2.as<uint32_t>(), g->in_col.as<uint32_t>(), (int64_t)E, 0,
-                                               bits, s));
-    if (tmp2 > tmp) ZOGCU_TRY(t.alloc(tmp2, s));
-    tmp2 = std::max(tmp, tmp2);
-    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp2, g->out_col.as<uint32_t>(),
-                                               ks.as<uint32_t>(), ks2.as<uint32_t>(),
-                                               g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
+                                               keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
+    if (tmp2 > tmp) {
+      ZOGCU_TRY(t.alloc(tmp2, s));
+      tmp = tmp2;
+    }
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
+                                               keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
     ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
     k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks.as<uint32_t>(), E, cnt.as<unsigned long long>());
     ZOGCU_CUDA(cudaGetLastError());
@@ -442,20 +500,23 @@ static void rmat_thresholds(double a, double b, double c, uint64_t* ta, uint64_t
 static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_from, const uint32_t* d_to,
                                        uint64_t num_edges, cudaStream_t s, zogcu_graph** out,
                                        const double* d_w = nullptr) {
+  int sorted = 0;
   if (num_edges) {
-    DevBuf bad;
-    ZOGCU_TRY(bad.alloc(4, s));
-    ZOGCU_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
-    k_validate<<<grid_for(num_edges), 256, 0, s>>>(d_from, d_to, num_edges, node_count, bad.as<unsigned int>());
+    DevBuf fl;
+    ZOGCU_TRY(fl.alloc(8, s));
+    ZOGCU_CUDA(cudaMemsetAsync(fl.ptr, 0, 8, s));
+    k_validate<<<grid_for(num_edges), 256, 0, s>>>(d_from, d_to, num_edges, node_count, fl.as<unsigned int>());
     ZOGCU_CUDA(cudaGetLastError());
-    unsigned int h = 0;
-    ZOGCU_CUDA(cudaMemcpyAsync(&h, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+    unsigned int h[2] = {0, 0};
+    ZOGCU_CUDA(cudaMemcpyAsync(h, fl.ptr, 8, cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
-    if (h) return fail(ZOGCU_ERR_NODE_NOT_FOUND, "edge endpoint >= node_count");
+    if (h[0]) return fail(ZOGCU_ERR_NODE_NOT_FOUND, "edge endpoint >= node_count");
+    sorted = h[1] == 0 ? 1 : 0;
   }
   std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
   if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
-  ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s, d_w));
+  ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s, d_w,
+                                          sorted));
   *out = G.release();
   return ZOGCU_OK;
 }
