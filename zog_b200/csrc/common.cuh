@@ -5,6 +5,9 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -160,6 +163,30 @@ struct StreamGuard {
   bool owned = false;
   int init(void* user);
   ~StreamGuard();
+};
+
+// Phase timing of one call, for diagnostics: with ZOGCU_TRACE set in the
+// environment, mark() synchronises the stream and prints the wall time since
+// the previous mark to stderr.  Off by default; it changes no result.
+struct PhaseTrace {
+  const char* what;
+  cudaStream_t s;
+  bool on;
+  std::chrono::steady_clock::time_point t;
+  PhaseTrace(const char* w, cudaStream_t st) : what(w), s(st), on(std::getenv("ZOGCU_TRACE") != nullptr) {
+    if (on) {
+      cudaStreamSynchronize(s);
+      t = std::chrono::steady_clock::now();
+    }
+  }
+  void mark(const char* phase) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    const auto n = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "zogcu trace: %s: %s %.3f ms\n", what, phase,
+                 std::chrono::duration<double, std::milli>(n - t).count());
+    t = n;
+  }
 };
 
 // Event timer on one stream.

@@ -585,6 +585,7 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
   ZOGCU_TRY(ensure_device(&dev));
   StreamGuard sg;
   ZOGCU_TRY(sg.init(nullptr));
+  PhaseTrace tr("graph_create_from_edges", sg.s);
   DevBuf df, dt;
   ZOGCU_TRY(df.alloc(num_edges * 4, sg.s));
   ZOGCU_TRY(dt.alloc(num_edges * 4, sg.s));
@@ -597,8 +598,11 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
       ZOGCU_CUDA(cudaMemcpyAsync(dw.ptr, weight, num_edges * 8, cudaMemcpyHostToDevice, sg.s));
     }
   }
-  return create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out,
-                                     weight ? dw.as<double>() : nullptr);
+  tr.mark("arcs to the device");
+  const int rc = create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out,
+                                             weight ? dw.as<double>() : nullptr);
+  tr.mark("validation and CSR build");
+  return rc;
 }
 
 static int create_from_arraygraph(uint32_t V, const uint32_t* first_edge, const uint8_t* node_deleted,

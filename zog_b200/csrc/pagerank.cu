@@ -944,24 +944,37 @@ static int build_ranked_view(Graph* g, cudaStream_t s) {
 // order depends only on its own arcs.
 constexpr uint32_t kTaskSegRows = 4096;
 
+constexpr uint32_t kTaskWin = 1024 + 72;  // offsets a warp stages: a window of rows plus one block's reach
+constexpr int kTaskWarps = 4;              // warps (segments in flight) per CTA
+
 template <typename OffT>
-__global__ void k_task_segments(const OffT* __restrict__ off, uint32_t V, uint32_t nnz, uint32_t nseg,
-                                unsigned long long* __restrict__ seg_tasks, unsigned long long* __restrict__ seg_long,
-                                PrTask* __restrict__ tasks, uint32_t* __restrict__ long_first, int write,
-                                unsigned int* __restrict__ err) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t sg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < nseg; sg += nw) {
+__global__ void __launch_bounds__(32 * kTaskWarps) k_task_segments(
+    const OffT* __restrict__ off, uint32_t V, uint32_t nnz, uint32_t nseg, unsigned long long* __restrict__ seg_tasks,
+    unsigned long long* __restrict__ seg_long, PrTask* __restrict__ tasks, uint32_t* __restrict__ long_first,
+    int write, unsigned int* __restrict__ err) {
+  // Each warp stages its segment's offsets in shared memory, a window at a
+  // time with coalesced loads, so the walk's dependent steps read shared
+  // memory instead of waiting on global loads.
+  __shared__ OffT s_win[kTaskWarps][kTaskWin];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  OffT* const win = s_win[wib];
+  const uint32_t nw = gridDim.x * kTaskWarps;
+  for (uint32_t sg = blockIdx.x * kTaskWarps + wib; sg < nseg; sg += nw) {
     uint32_t r = sg * kTaskSegRows;  // V < 2^30, so no overflow
     const uint32_t rend = min(V, r + kTaskSegRows);
     unsigned long long nt = write ? seg_tasks[sg] : 0ull, nl = write ? seg_long[sg] : 0ull;
+    uint32_t base = 0, have = 0;  // win[i] = off[base + i] for i < have
     while (r < rend) {  // r is the same in every lane
-      if (lane == 0) {
-        const uint32_t pf = min(r + 1024u, V);
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(off + pf));
+      // a step reads offsets r .. min(r + kWarpRows, rend) <= V
+      if (min(r + (uint32_t)kWarpRows, rend) >= base + have) {
+        base = r;
+        have = min(kTaskWin, V + 1 - r);
+        __syncwarp();
+        for (uint32_t i = lane; i < have; i += 32) win[i] = __ldg(off + base + i);
+        __syncwarp();
       }
-      const OffT o0 = __ldg(off + r);
-      const uint64_t len = (uint64_t)(__ldg(off + r + 1) - o0);
+      const OffT o0 = win[r - base];
+      const uint64_t len = (uint64_t)(win[r + 1 - base] - o0);
       if (len > nnz) {
         if (len <= (uint64_t)kLongChunk) {
           if (write && lane == 0) tasks[nt] = PrTask{r, (kTaskRow << 30) | (r + 1)};
@@ -984,12 +997,12 @@ __global__ void k_task_segments(const OffT* __restrict__ off, uint32_t V, uint32
       }
       const uint32_t lim = min(r + (uint32_t)kWarpRows, rend);
       const uint32_t c1 = r + 1 + lane;
-      const bool ok1 = c1 <= lim && (uint64_t)(__ldg(off + c1) - o0) <= nnz;
+      const bool ok1 = c1 <= lim && (uint64_t)(win[c1 - base] - o0) <= nnz;
       const unsigned m1 = __ballot_sync(0xffffffffu, ok1);
       uint32_t cnt = __popc(m1);
       if (m1 == 0xffffffffu) {
         const uint32_t c2 = r + 33 + lane;
-        const bool ok2 = c2 <= lim && (uint64_t)(__ldg(off + c2) - o0) <= nnz;
+        const bool ok2 = c2 <= lim && (uint64_t)(win[c2 - base] - o0) <= nnz;
         cnt += __popc(__ballot_sync(0xffffffffu, ok2));
       }
       if (write && lane == 0) tasks[nt] = PrTask{r, (kTaskBlock << 30) | (r + cnt)};
@@ -1007,6 +1020,7 @@ template <typename OffT>
 static int build_task_list_t(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
   const uint32_t V = g->V;
   const uint32_t nseg = (V + kTaskSegRows - 1) / kTaskSegRows;
+  PhaseTrace tr(nnz == 128 ? "work items (128 arcs)" : "work items (256 arcs)", s);
   DevBuf cnt, offs, tmp;
   // [tasks per segment | trailing 0 | long rows per segment | trailing 0] and
   // their exclusive scans; the word after the scans is the error flag
@@ -1020,11 +1034,13 @@ static int build_task_list_t(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
   unsigned long long* ol = ot + nseg + 1;
   unsigned int* err = reinterpret_cast<unsigned int*>(ol + nseg + 1);
   const OffT* off = g->pr.off.as<OffT>();
-  const unsigned grid = (unsigned)std::max<uint32_t>((nseg + 3) / 4, 1);  // 4 warps (segments) per CTA
+  const unsigned grid = (unsigned)std::max<uint32_t>((nseg + kTaskWarps - 1) / kTaskWarps, 1);
   if (nseg) {
-    k_task_segments<OffT><<<grid, 128, 0, s>>>(off, V, (uint32_t)nnz, nseg, ct, cl, nullptr, nullptr, 0, err);
+    k_task_segments<OffT><<<grid, 32 * kTaskWarps, 0, s>>>(off, V, (uint32_t)nnz, nseg, ct, cl, nullptr, nullptr, 0,
+                                                           err);
     ZOGCU_CUDA(cudaGetLastError());
   }
+  tr.mark("counting pass");
   size_t tb = 0;
   ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, ct, ot, (int64_t)nseg + 1, s));
   ZOGCU_TRY(tmp.alloc(tb, s));
@@ -1035,18 +1051,21 @@ static int build_task_list_t(Graph* g, int nnz, PrTaskList& L, cudaStream_t s) {
   ZOGCU_CUDA(cudaMemcpyAsync(&h[1], ol + nseg, 8, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaMemcpyAsync(&h[2], err, 4, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  tr.mark("scan and totals");
   if (h[2]) return fail(ZOGCU_ERR_TOO_LARGE, "row in-degree too large for the chunk schedule");
   if (h[0] >= 0xFFFFFFFFull) return fail(ZOGCU_ERR_TOO_LARGE, "too many PageRank work items");
   L.num_tasks = (uint32_t)h[0];
   L.num_long = (uint32_t)h[1];
   ZOGCU_TRY(L.tasks.alloc(std::max<size_t>(L.num_tasks, 1) * sizeof(PrTask)));
   ZOGCU_TRY(L.long_first.alloc(std::max<size_t>(L.num_long, 1) * 4));
+  tr.mark("allocation");
   if (nseg) {
-    k_task_segments<OffT><<<grid, 128, 0, s>>>(off, V, (uint32_t)nnz, nseg, ot, ol, L.tasks.as<PrTask>(),
+    k_task_segments<OffT><<<grid, 32 * kTaskWarps, 0, s>>>(off, V, (uint32_t)nnz, nseg, ot, ol, L.tasks.as<PrTask>(),
                                                L.long_first.as<uint32_t>(), 1, err);
     ZOGCU_CUDA(cudaGetLastError());
   }
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  tr.mark("writing pass");
   L.built = true;
   return ZOGCU_OK;
 }
@@ -1362,7 +1381,7 @@ constexpr double kMixedStall = 0.97;
 
 template <typename OffT>
 static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol, const zogcu_pr_opts* o, double* out,
-                        zogcu_stats* stats, cudaStream_t s) {
+                        zogcu_stats* stats, cudaStream_t s, PhaseTrace* tr) {
   const PrSchedule& P = g->pr;
   const uint32_t V = g->V;
   const bool dev_ptrs = o && o->device_pointers;
@@ -1370,6 +1389,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   // workspace sized for every configuration's schedule
   ZOGCU_TRY(ensure_task_list(g, 128, s));
   ZOGCU_TRY(ensure_task_list(g, 256, s));
+  tr->mark("work-item lists");
   const uint32_t max_tasks = std::max(P.lists[0].num_tasks, P.lists[1].num_tasks);
   PrWork W;
   DevBuf cf0, cf1;
@@ -1413,6 +1433,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   A.nv = V;
 
   int cfg = pr_config_of(g);
+  tr->mark("workspace");
 
   int given = 0;
   if (o && o->x0) {  // caller order -> ranked order
@@ -1463,6 +1484,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   // kernel launches of a graph loop: one per iteration it ran (a loop that
   // found the chain already over ran one launch that only ended the loop)
   if (from64 >= 0) launches += hs.iter - (uint64_t)from64 + (hs.iter == (uint64_t)from64 ? 1 : 0);
+  tr->mark("solve");
   const double* result = (hs.iter & 1ull) ? A.x1 : A.x0;
   double* unperm = (hs.iter & 1ull) ? A.x0 : A.x1;  // the other buffer is free now
   k_permute_out<<<grid_1d(V), 256, 0, s>>>(result, P.rank.as<uint32_t>(), V, unperm);
@@ -1470,6 +1492,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   ++launches;
   ZOGCU_CUDA(cudaMemcpyAsync(out, unperm, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  tr->mark("scores to the caller");
   if (stats) {
     stats->iterations = it32 + hs.iter;
     stats->residual = hs.l1;
@@ -1774,10 +1797,12 @@ int zogcu_pagerank_ex(zogcu_graph* G, double damping, uint64_t max_iterations, d
   }
   StreamGuard sg;
   ZOGCU_TRY(sg.init(opts ? opts->stream : nullptr));
+  PhaseTrace tr("pagerank", sg.s);
   ZOGCU_TRY(ensure_pr_schedule(g, sg.s));
+  tr.mark("degree-ranked view");
   if (g->offsets32)
-    return run_pagerank<uint32_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
-  return run_pagerank<uint64_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s);
+    return run_pagerank<uint32_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s, &tr);
+  return run_pagerank<uint64_t>(g, damping, max_iterations, tolerance, opts, out_scores, stats, sg.s, &tr);
 }
 
 int zogcu_pagerank(zogcu_graph* G, double damping, uint64_t max_iterations, double tolerance, double* out_scores,
