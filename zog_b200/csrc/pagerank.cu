@@ -912,7 +912,8 @@ static int build_ranked_view(Graph* g, cudaStream_t s) {
                                              poff64.as<unsigned long long>(), (int64_t)V + 1, s));
   }
   ZOGCU_TRY(P.col.alloc((g->E + 4) * 4));
-  ZOGCU_CUDA(cudaMemsetAsync(P.col.ptr, 0, (g->E + 4) * 4, s));
+  // k_rank_rows writes every arc; only the 4 padding entries need zeros
+  ZOGCU_CUDA(cudaMemsetAsync(P.col.as<uint32_t>() + g->E, 0, 4 * 4, s));
   k_rank_rows<<<grid_1d((uint64_t)V * 32), 256, 0, s>>>(P.perm.as<uint32_t>(), P.rank.as<uint32_t>(), V,
                                                          g->in_off64.as<uint64_t>(), g->in_col.as<uint32_t>(),
                                                          poff64.as<uint64_t>(), P.col.as<uint32_t>());
