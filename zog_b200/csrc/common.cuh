@@ -43,17 +43,25 @@ int fail(int status, const std::string& msg);
     if (_s != ZOGCU_OK) return _s;      \
   } while (0)
 
-// Stream-ordered device buffer (cudaMallocAsync on the owning stream).
+// Stream-ordered device buffer (cudaMallocAsync on the owning stream), or a
+// view of memory owned elsewhere (borrow: release() then frees nothing).
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
   cudaStream_t stream = nullptr;
+  bool owned = true;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes), stream(o.stream) { o.ptr = nullptr; }
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes), stream(o.stream), owned(o.owned) { o.ptr = nullptr; }
   ~DevBuf() { release(); }
   int alloc(size_t n, cudaStream_t s);
+  void borrow(void* p, size_t n) {
+    release();
+    ptr = p;
+    bytes = n;
+    owned = false;
+  }
   void release();
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
@@ -70,6 +78,46 @@ struct DevArray {
   int alloc(size_t n);
   void release();
   template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Scratch kept by a graph or a model between calls, so that repeated calls
+// allocate nothing.  Alternating calls with differently sized per-call
+// allocations (a warm-start inference, then a PageRank solve) made the
+// stream-ordered pool stall the host for up to 0.2 s per call.  A call that
+// takes the cache (try_lock) holds it until its work on the GPU has finished;
+// a concurrent call finds it taken and allocates its own buffers as before.
+struct WorkCache {
+  static constexpr int kSlots = 16;
+  std::mutex mu;
+  DevArray slot[kSlots];
+};
+
+// One call's hold on a WorkCache.  get() hands out slot i (grown to n bytes
+// when needed) when the cache was free, else a buffer of its own on stream s.
+// The destructor waits for stream s before letting the next call in.
+struct WorkLease {
+  WorkCache* cache = nullptr;
+  cudaStream_t s = nullptr;
+  bool held = false;
+  WorkLease(WorkCache* c, cudaStream_t st) : cache(c), s(st) { held = c && c->mu.try_lock(); }
+  WorkLease(const WorkLease&) = delete;
+  WorkLease& operator=(const WorkLease&) = delete;
+  ~WorkLease() {
+    if (held) {
+      cudaStreamSynchronize(s);
+      cache->mu.unlock();
+    }
+  }
+  int get(DevBuf& b, int i, size_t n) {
+    if (!held) return b.alloc(n, s);
+    DevArray& a = cache->slot[i];
+    if (a.bytes < n) {
+      const int rc = a.alloc(n);
+      if (rc != ZOGCU_OK) return rc;
+    }
+    b.borrow(a.ptr, n);
+    return ZOGCU_OK;
+  }
 };
 
 // PageRank work-item schedule (shared by the single-vector kernel and the
@@ -129,6 +177,7 @@ struct Graph {
   DevArray live;                  // uint8_t[V] (when has_deleted)
   std::mutex mu;                  // guards lazy schedule builds
   PrSchedule pr;                  // PageRank schedule (built on first call)
+  WorkCache pr_ws;                // PageRank solve scratch, reused by later calls
   // Brandes: vertices whose in- / out-degree exceeds the heavy threshold,
   // by degree descending (built on the first betweenness call)
   bool bc_built = false;

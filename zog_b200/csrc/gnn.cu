@@ -634,6 +634,9 @@ struct zogcu_gnn {
   int device = 0;
   DevArray p, pb, m, s, g, loss;   // masters, BF16 copy, Adam moments, gradient, loss (FP64)
   uint64_t step = 0;
+  // activations of the largest graph seen so far (about 940 bytes per node),
+  // reused by later calls until the model is destroyed
+  mutable WorkCache acts;
 };
 
 namespace zogcu {
@@ -644,15 +647,16 @@ namespace {
 struct GnnActs {
   DevBuf F, inv, y, t, ctr, rows;
   DevBuf H[kLayers], A[kLayers];
-  int alloc(uint32_t V, cudaStream_t s) {
+  // from the model's cache when the lease holds it, else per call
+  int alloc(uint32_t V, WorkLease& L) {
     const size_t Vs = std::max<uint32_t>(V, 1);
-    ZOGCU_TRY(F.alloc(Vs * kF * 4, s));
-    ZOGCU_TRY(inv.alloc(Vs * 4, s));
-    ZOGCU_TRY(y.alloc(Vs * 4, s));
-    ZOGCU_TRY(ctr.alloc(16, s));
+    ZOGCU_TRY(L.get(F, 0, Vs * kF * 4));
+    ZOGCU_TRY(L.get(inv, 1, Vs * 4));
+    ZOGCU_TRY(L.get(y, 2, Vs * 4));
+    ZOGCU_TRY(L.get(ctr, 3, 16));
     for (int l = 0; l < kLayers; ++l) {
-      ZOGCU_TRY(H[l].alloc(Vs * kH * 2, s));
-      ZOGCU_TRY(A[l].alloc(Vs * (size_t)layer_in(l) * 4, s));
+      ZOGCU_TRY(L.get(H[l], 4 + l, Vs * kH * 2));
+      ZOGCU_TRY(L.get(A[l], 4 + kLayers + l, Vs * (size_t)layer_in(l) * 4));
     }
     return ZOGCU_OK;
   }
@@ -874,8 +878,9 @@ int zogcu_gnn_loss_grad(zogcu_gnn* M, zogcu_graph* G, const double* target_pr, i
   DevBuf pr;
   ZOGCU_TRY(pr.alloc((size_t)std::max<uint32_t>(g->V, 1) * 8, sg.s));
   ZOGCU_CUDA(cudaMemcpyAsync(pr.ptr, target_pr, (size_t)g->V * 8, cudaMemcpyHostToDevice, sg.s));
+  WorkLease lease(&M->acts, sg.s);
   GnnActs act;
-  ZOGCU_TRY(act.alloc(g->V, sg.s));
+  ZOGCU_TRY(act.alloc(g->V, lease));
   ZOGCU_TRY(gnn_forward(M, g, act, sg.s));
   ZOGCU_TRY(gnn_backward(M, g, act, pr.as<double>(), loss_kind, sg.s));
   double l = 0.0;
@@ -896,8 +901,9 @@ int zogcu_gnn_train_step(zogcu_gnn* M, zogcu_graph* G, const double* d_target_pr
   ZOGCU_CUDA(cudaSetDevice(M->device));
   StreamGuard sg;
   ZOGCU_TRY(sg.init(nullptr));
+  WorkLease lease(&M->acts, sg.s);
   GnnActs act;
-  ZOGCU_TRY(act.alloc(g->V, sg.s));
+  ZOGCU_TRY(act.alloc(g->V, lease));
   ZOGCU_TRY(gnn_forward(M, g, act, sg.s));
   ZOGCU_TRY(gnn_backward(M, g, act, d_target_pr, loss_kind, sg.s));
   M->step += 1;
@@ -923,8 +929,9 @@ int zogcu_gnn_predict(const zogcu_gnn* M, zogcu_graph* G, double* x0, int device
   ZOGCU_CUDA(cudaSetDevice(M->device));
   StreamGuard sg;
   ZOGCU_TRY(sg.init(stream));
+  WorkLease lease(&M->acts, sg.s);
   GnnActs act;
-  ZOGCU_TRY(act.alloc(V, sg.s));
+  ZOGCU_TRY(act.alloc(V, lease));
   ZOGCU_TRY(gnn_forward(M, g, act, sg.s));
   DevBuf xd;
   double* xo = x0;

@@ -48,9 +48,10 @@ int DevBuf::alloc(size_t n, cudaStream_t s) {
   return ZOGCU_OK;
 }
 void DevBuf::release() {
-  if (ptr) cudaFreeAsync(ptr, stream);
+  if (ptr && owned) cudaFreeAsync(ptr, stream);
   ptr = nullptr;
   bytes = 0;
+  owned = true;
 }
 
 // Persistent arrays come from the device's stream-ordered pool as well, so

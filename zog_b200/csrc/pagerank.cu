@@ -1411,23 +1411,26 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   ZOGCU_TRY(ensure_task_list(g, 256, s));
   tr->mark("work-item lists");
   const uint32_t max_tasks = std::max(P.lists[0].num_tasks, P.lists[1].num_tasks);
+  // the graph's cached scratch when no other call holds it (declared before
+  // the buffers, so it outlives them)
+  WorkLease lease(&g->pr_ws, s);
   PrWork W;
   DevBuf cf0, cf1;
-  ZOGCU_TRY(W.x0.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(W.x1.alloc((size_t)V * 8, s));
-  ZOGCU_TRY(W.c0.alloc((size_t)V * 8 + 16, s));
-  ZOGCU_TRY(W.c1.alloc((size_t)V * 8 + 16, s));
-  ZOGCU_TRY(W.part.alloc((size_t)std::max<int>(sm_count() * 8, 148 * 4) * 16, s));
-  ZOGCU_TRY(W.chunk.alloc((size_t)std::max<uint32_t>(max_tasks, 1) * 8, s));
-  ZOGCU_TRY(W.lcnt.alloc((size_t)std::max<uint32_t>(max_tasks, 1) * 4, s));
-  ZOGCU_TRY(W.lpart.alloc((size_t)std::max<uint32_t>(max_tasks, 1) * 16, s));
-  ZOGCU_TRY(W.stb.alloc(sizeof(PrState), s));
+  ZOGCU_TRY(lease.get(W.x0, 0, (size_t)V * 8));
+  ZOGCU_TRY(lease.get(W.x1, 1, (size_t)V * 8));
+  ZOGCU_TRY(lease.get(W.c0, 2, (size_t)V * 8 + 16));
+  ZOGCU_TRY(lease.get(W.c1, 3, (size_t)V * 8 + 16));
+  ZOGCU_TRY(lease.get(W.part, 4, (size_t)std::max<int>(sm_count() * 8, 148 * 4) * 16));
+  ZOGCU_TRY(lease.get(W.chunk, 5, (size_t)std::max<uint32_t>(max_tasks, 1) * 8));
+  ZOGCU_TRY(lease.get(W.lcnt, 6, (size_t)std::max<uint32_t>(max_tasks, 1) * 4));
+  ZOGCU_TRY(lease.get(W.lpart, 7, (size_t)std::max<uint32_t>(max_tasks, 1) * 16));
+  ZOGCU_TRY(lease.get(W.stb, 8, sizeof(PrState)));
   ZOGCU_CUDA(cudaMemsetAsync(W.lcnt.ptr, 0, W.lcnt.bytes, s));
   ZOGCU_CUDA(cudaMemsetAsync(W.c0.ptr, 0, W.c0.bytes, s));
   ZOGCU_CUDA(cudaMemsetAsync(W.c1.ptr, 0, W.c1.bytes, s));
   if (mixed) {
-    ZOGCU_TRY(cf0.alloc((size_t)V * 4 + 16, s));
-    ZOGCU_TRY(cf1.alloc((size_t)V * 4 + 16, s));
+    ZOGCU_TRY(lease.get(cf0, 9, (size_t)V * 4 + 16));
+    ZOGCU_TRY(lease.get(cf1, 10, (size_t)V * 4 + 16));
     ZOGCU_CUDA(cudaMemsetAsync(cf0.ptr, 0, cf0.bytes, s));
     ZOGCU_CUDA(cudaMemsetAsync(cf1.ptr, 0, cf1.bytes, s));
   }
@@ -1457,15 +1460,15 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
 
   int given = 0;
   if (o && o->x0) {  // caller order -> ranked order
-    ZOGCU_TRY(W.tmp.alloc((size_t)V * 8, s));
+    ZOGCU_TRY(lease.get(W.tmp, 11, (size_t)V * 8));
     ZOGCU_CUDA(cudaMemcpyAsync(W.tmp.ptr, o->x0, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     k_permute_in<<<grid_1d(V), 256, 0, s>>>(W.tmp.as<double>(), P.perm.as<uint32_t>(), V, W.x0.as<double>());
     ZOGCU_CUDA(cudaGetLastError());
     given = 1;
   }
   if (o && o->teleport) {
-    ZOGCU_TRY(W.tele.alloc((size_t)V * 8, s));
-    if (!W.tmp.ptr) ZOGCU_TRY(W.tmp.alloc((size_t)V * 8, s));
+    ZOGCU_TRY(lease.get(W.tele, 12, (size_t)V * 8));
+    if (!W.tmp.ptr) ZOGCU_TRY(lease.get(W.tmp, 11, (size_t)V * 8));
     ZOGCU_CUDA(cudaMemcpyAsync(W.tmp.ptr, o->teleport, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     k_permute_in<<<grid_1d(V), 256, 0, s>>>(W.tmp.as<double>(), P.perm.as<uint32_t>(), V, W.tele.as<double>());
     ZOGCU_CUDA(cudaGetLastError());
