@@ -206,7 +206,11 @@ ZOGCU_API int zogcu_pagerank(zogcu_graph* g, double damping, uint64_t max_iterat
                    double* out_scores, zogcu_stats* stats);
 
 /* As zogcu_pagerank with options (precision form, warm start, personalised
- * teleport, device pointers, caller stream); opts may be NULL. */
+ * teleport, device pointers, caller stream); opts may be NULL.  In the
+ * precision form on graphs of at least 2^23 nodes and 2^24 arcs the FP32 phase runs
+ * propagation-blocked (streamed messages, exact integer row sums; environment
+ * ZOGCU_PR_BLOCKED=0 turns it off, =1 forces it), and stats->reserved is 1
+ * when it did. */
 ZOGCU_API int zogcu_pagerank_ex(zogcu_graph* g, double damping, uint64_t max_iterations,
                       double tolerance, const zogcu_pr_opts* opts, double* out_scores,
                       zogcu_stats* stats);

@@ -149,6 +149,37 @@ struct PrTaskList {
   DevArray long_first;        // uint32_t[num_long]: first chunk task of each long row
 };
 
+// Propagation-blocked layout of the PageRank view (pagerank.cu), built on the
+// first precision-form solve of a large graph.  Rows are cut into partitions
+// (at most kPbRows rows, about 2^20 in-arcs each) and sources into blocks (at
+// most kPbSrcs sources, about 2^20 out-arcs each); the arcs of block b into
+// partition p form one piece.  Pieces are stored block by block, each padded
+// to a multiple of 4 positions; a position holds the arc's source relative to
+// its block (sl) and its row relative to its partition (dl; padding points at
+// a spare row).
+struct PbItem {
+  uint32_t b, lo, hi, pad;  // positions [lo, hi) of block b
+};
+struct PbView {
+  int state = 0;              // 0 not built, 1 built, -1 not usable for this graph
+  uint32_t P = 0, B = 0, nitems = 0;
+  uint64_t npad = 0;
+  DevArray row_lo, row_n, part_order;   // uint32_t[P]; part_order: partitions by arcs, largest first
+  DevArray blk_lo, blk_n;               // uint32_t[B]
+  DevArray pstart, pcount;              // uint32_t[P * B], partition-major
+  DevArray sl, dl;                      // uint16_t[npad]
+  DevArray items;                       // PbItem[nitems]: emit work, largest first
+  DevArray msg;                         // float[npad]: one contribution per position
+  DevArray heavy;                       // uint16_t[P][4]: each partition's heaviest rows (local)
+  void reset() {
+    for (DevArray* a : {&row_lo, &row_n, &part_order, &blk_lo, &blk_n, &pstart, &pcount, &sl, &dl, &items, &msg, &heavy})
+      a->release();
+    state = 0;
+    P = B = nitems = 0;
+    npad = 0;
+  }
+};
+
 struct PrSchedule {
   bool built = false;
   DevArray rank;              // uint32_t[V]: rank of node v
@@ -178,6 +209,7 @@ struct Graph {
   std::mutex mu;                  // guards lazy schedule builds
   PrSchedule pr;                  // PageRank schedule (built on first call)
   WorkCache pr_ws;                // PageRank solve scratch, reused by later calls
+  PbView pb;                      // propagation-blocked layout (precision form)
   // Brandes: vertices whose in- / out-degree exceeds the heavy threshold,
   // by degree descending (built on the first betweenness call)
   bool bc_built = false;

@@ -1392,6 +1392,622 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
                                    loop_from, hs.iter);
 }
 
+// ---------------------------------------------------------------------------
+// Propagation-blocked iteration: the FP32 bulk phase of the precision form
+// ---------------------------------------------------------------------------
+// The gather kernels above spend one L1 tag lookup per arc on a random 4- or
+// 8-byte contribution, which caps them near one arc per SM clock whatever the
+// contribution's width.  The blocked iteration streams instead:
+//   emit:       a CTA stages the FP32 contributions of one source block in
+//               shared memory and writes one message per position of the
+//               block's pieces (coalesced 16-byte stores);
+//   accumulate: a CTA zeroes integer accumulators for one partition's rows in
+//               shared memory, streams the partition's pieces from every block
+//               (16-byte loads), adds each message scaled by 2^kPbShift, and
+//               runs the row epilogue of pr_iter_kernel.
+// Integer sums do not depend on the order of the additions, so the result is
+// deterministic although many warps add at once.  Shared-memory atomics are
+// native for 32-bit integers only (64-bit and floating-point additions
+// measured 9-15x slower on this part), so each 64-bit accumulator is two
+// 32-bit words: the low word's atomicAdd returns the old value, and an
+// addition that wraps it adds its carry to the high word.  A message below
+// 2^(32 - kPbShift) = 6e-8 touches the low word only.
+// Scale: messages lie in [0, 1] and a row's sum is at most the total mass
+// (1), far below 2^(64 - kPbShift); rounding a message to a multiple of
+// 2^-kPbShift (error <= 6.9e-18) is below the FP32 rounding of any message
+// above 1.2e-10.  Within a piece, the arcs of one row are spread by a
+// multiplicative permutation, so that lanes of one warp rarely add to the
+// same word (measured 1.02 -> 0.65 ms per accumulate at scale 24).
+constexpr uint32_t kPbRows = 24576;          // rows per partition (accumulators in shared memory)
+constexpr uint32_t kPbSrcs = 24576;          // sources per block (contributions in shared memory)
+constexpr uint64_t kPbCutArcs = 1ull << 20;  // arcs per partition / block before a cut
+constexpr uint32_t kPbItem = 65536;          // positions per emit work item
+constexpr uint64_t kPbMaxPieces = 1ull << 26;
+constexpr int kPbShift = 56;
+constexpr int kPbThreads = 1024;
+constexpr size_t kPbAccBytes = (size_t)2 * (kPbRows + 1) * 4;
+constexpr size_t kPbEmitBytes = (size_t)kPbSrcs * 4;
+
+// Group starts: element i starts a group when i is a multiple of rows_max or
+// the running count before it crosses a multiple of arcs_max.
+template <typename T>
+__global__ void k_pb_cut(const T* __restrict__ cum, uint32_t n, uint32_t rows_max, uint64_t arcs_max,
+                         uint32_t* __restrict__ flag) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    bool c = (i % rows_max) == 0;
+    if (!c) c = ((uint64_t)cum[i] / arcs_max) != ((uint64_t)cum[i - 1] / arcs_max);
+    flag[i] = c ? 1u : 0u;
+  }
+}
+
+// Group of every element (idx = exclusive scan of flag) and first element of
+// every group.
+__global__ void k_pb_groups(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ idx, uint32_t n,
+                            uint32_t* __restrict__ lo, uint32_t* __restrict__ of) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = idx[i] + flag[i] - 1u;
+    of[i] = g;
+    if (flag[i]) lo[g] = (uint32_t)i;
+  }
+}
+
+__global__ void k_pb_sizes(const uint32_t* __restrict__ lo, uint32_t ng, uint32_t n, uint32_t* __restrict__ sz) {
+  for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < ng; g += (uint64_t)gridDim.x * blockDim.x)
+    sz[g] = (g + 1 < ng ? lo[g + 1] : n) - lo[g];
+}
+
+__global__ void k_pb_outdeg(const uint32_t* __restrict__ deg, uint32_t V, unsigned long long* __restrict__ d) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = deg[v];
+    d[v] = x == kDeletedDegree ? 0ull : x;
+  }
+}
+
+// Arcs per piece (key = block * P + partition); one warp per row.
+template <typename OffT>
+__global__ void k_pb_count(const OffT* __restrict__ off, const uint32_t* __restrict__ col, uint32_t V,
+                           const uint32_t* __restrict__ blk_of, const uint32_t* __restrict__ part_of, uint32_t P,
+                           uint32_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; r < V; r += nw) {
+    const uint64_t pr = part_of[r];
+    const OffT e = off[r + 1];
+    for (OffT k = off[r] + lane; k < e; k += 32) atomicAdd(&cnt[(uint64_t)blk_of[col[k]] * P + pr], 1u);
+  }
+}
+
+// Padded piece sizes; the extra last element makes the exclusive scan's last
+// entry the total.
+__global__ void k_pb_pad(const uint32_t* __restrict__ cnt, uint64_t nkeys, unsigned long long* __restrict__ padded) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k <= nkeys; k += (uint64_t)gridDim.x * blockDim.x)
+    padded[k] = k < nkeys ? (unsigned long long)((cnt[k] + 3u) & ~3u) : 0ull;
+}
+
+// Multiplier of each piece's position permutation j -> (j * m) mod n: a prime
+// not dividing n, whose residue is neither 1 nor n - 1 (those keep runs
+// together); m = 1 (identity) when n <= 2.  Four primes above 7,900 cannot
+// all divide an n below 2^32.
+__global__ void k_pb_mult(const uint32_t* __restrict__ cnt, uint64_t nkeys, uint32_t* __restrict__ mult) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nkeys; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t n = cnt[k];
+    uint32_t m = 1u;
+    if (n > 2u) {
+      const uint32_t cand[4] = {7919u, 104729u, 1299709u, 15485863u};
+      for (int i = 0; i < 4; ++i) {
+        const uint32_t r = cand[i] % n;
+        if (n % cand[i] != 0u && r > 1u && r != n - 1u) {
+          m = cand[i];
+          break;
+        }
+      }
+    }
+    mult[k] = m;
+  }
+}
+
+__global__ void k_fill_u16(uint16_t* __restrict__ a, uint64_t n, uint16_t v) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+// Places every arc at its piece's next position (permuted); one warp per row.
+// The same traversal as k_pb_count, so each piece receives exactly cnt arcs.
+template <typename OffT>
+__global__ void k_pb_scatter(const OffT* __restrict__ off, const uint32_t* __restrict__ col, uint32_t V,
+                             const uint32_t* __restrict__ blk_of, const uint32_t* __restrict__ blk_lo,
+                             const uint32_t* __restrict__ part_of, const uint32_t* __restrict__ row_lo, uint32_t P,
+                             const uint32_t* __restrict__ start, const uint32_t* __restrict__ cnt,
+                             const uint32_t* __restrict__ mult, uint32_t* __restrict__ cursor,
+                             uint16_t* __restrict__ sl, uint16_t* __restrict__ dl) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; r < V; r += nw) {
+    const uint32_t pr = part_of[r];
+    const uint16_t dloc = (uint16_t)(r - row_lo[pr]);
+    const OffT e = off[r + 1];
+    for (OffT k = off[r] + lane; k < e; k += 32) {
+      const uint32_t src = col[k];
+      const uint32_t b = blk_of[src];
+      const uint64_t key = (uint64_t)b * P + pr;
+      const uint32_t j = atomicAdd(&cursor[key], 1u);
+      const uint32_t pos = start[key] + (uint32_t)(((uint64_t)j * mult[key]) % cnt[key]);
+      sl[pos] = (uint16_t)(src - blk_lo[b]);
+      dl[pos] = dloc;
+    }
+  }
+}
+
+// Partition-major piece tables, and the first position of every block (the
+// block-major position of piece (b, 0)).
+__global__ void k_pb_tables(const unsigned long long* __restrict__ start, const uint32_t* __restrict__ cnt, uint32_t B,
+                            uint32_t P, uint32_t* __restrict__ pstart, uint32_t* __restrict__ pcount,
+                            unsigned long long* __restrict__ blk_pos) {
+  const uint64_t nkeys = (uint64_t)B * P;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k <= nkeys; k += (uint64_t)gridDim.x * blockDim.x) {
+    if (k < nkeys) {
+      const uint64_t b = k / P, p = k % P;
+      pstart[p * B + b] = (uint32_t)start[k];
+      pcount[p * B + b] = (cnt[k] + 3u) & ~3u;
+    }
+    if (k % P == 0) blk_pos[k / P] = start[k];
+  }
+}
+
+// The four rows of largest in-degree (at least kPbHeavyMin) of every
+// partition, as local indices (0xFFFF = none); one warp per partition.
+constexpr uint32_t kPbHeavyMin = 64;
+template <typename OffT>
+__global__ void k_pb_heavy(const OffT* __restrict__ off, const uint32_t* __restrict__ row_lo,
+                           const uint32_t* __restrict__ row_n, uint32_t P, uint2* __restrict__ heavy) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t p = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; p < P; p += nw) {
+    const uint32_t r0 = row_lo[p], nr = row_n[p];
+    uint64_t best[4] = {0, 0, 0, 0};  // (in-degree << 16 | 0xFFFF - local row), largest first
+    for (uint32_t r = lane; r < nr; r += 32) {
+      const uint64_t d = (uint64_t)(off[r0 + r + 1] - off[r0 + r]);
+      uint64_t key = (d << 16) | (0xFFFFu - r);
+      for (int k = 0; k < 4; ++k)
+        if (key > best[k]) {
+          const uint64_t t = best[k];
+          best[k] = key;
+          key = t;
+        }
+    }
+    uint32_t pick[4];
+    for (int k = 0; k < 4; ++k) {  // k-th largest over the warp; its lane drops it
+      uint64_t m = best[0];
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = t > m ? t : m;
+      }
+      const unsigned owner = __ballot_sync(0xffffffffu, best[0] == m && m != 0);
+      if (m != 0 && lane == __ffs(owner) - 1) {
+        best[0] = best[1];
+        best[1] = best[2];
+        best[2] = best[3];
+        best[3] = 0;
+      }
+      pick[k] = (m >> 16) >= kPbHeavyMin ? 0xFFFFu - (uint32_t)(m & 0xFFFFu) : 0xFFFFu;
+    }
+    if (lane == 0) heavy[p] = make_uint2(pick[0] | (pick[1] << 16), pick[2] | (pick[3] << 16));
+  }
+}
+
+template <typename OffT>
+__global__ void k_pb_part_arcs(const OffT* __restrict__ off, const uint32_t* __restrict__ row_lo,
+                               const uint32_t* __restrict__ row_n, uint32_t P, unsigned long long* __restrict__ arcs) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < P; p += (uint64_t)gridDim.x * blockDim.x)
+    arcs[p] = (unsigned long long)(off[row_lo[p] + row_n[p]] - off[row_lo[p]]);
+}
+
+// Cuts n elements into groups (flags, exclusive scan, first elements); returns
+// the group count, the group of every element (of) and each group's first
+// element (lo) and size (sz).
+template <typename T>
+static int pb_groups(const T* cum, uint32_t n, uint32_t rows_max, uint64_t arcs_max, DevBuf& of, DevArray& lo,
+                     DevArray& sz, uint32_t* ngroups, cudaStream_t s) {
+  DevBuf flag, idx, tmp;
+  ZOGCU_TRY(flag.alloc((size_t)n * 4, s));
+  ZOGCU_TRY(idx.alloc((size_t)n * 4, s));
+  ZOGCU_TRY(of.alloc((size_t)n * 4, s));
+  k_pb_cut<T><<<grid_1d(n), 256, 0, s>>>(cum, n, rows_max, arcs_max, flag.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  size_t tb = 0;
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.as<uint32_t>(), idx.as<uint32_t>(), (int64_t)n, s));
+  ZOGCU_TRY(tmp.alloc(tb, s));
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, flag.as<uint32_t>(), idx.as<uint32_t>(), (int64_t)n, s));
+  uint32_t last[2] = {0, 0};
+  ZOGCU_CUDA(cudaMemcpyAsync(&last[0], idx.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(&last[1], flag.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  const uint32_t ng = last[0] + last[1];
+  ZOGCU_TRY(lo.alloc((size_t)ng * 4));
+  ZOGCU_TRY(sz.alloc((size_t)ng * 4));
+  k_pb_groups<<<grid_1d(n), 256, 0, s>>>(flag.as<uint32_t>(), idx.as<uint32_t>(), n, lo.as<uint32_t>(),
+                                         of.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  k_pb_sizes<<<grid_1d(ng), 256, 0, s>>>(lo.as<uint32_t>(), ng, n, sz.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  *ngroups = ng;
+  return ZOGCU_OK;
+}
+
+// Builds the blocked layout from the degree-ranked view (caller holds g->mu).
+// Leaves state -1 (the gather kernels are used instead) when the graph is too
+// large for 32-bit positions or the piece tables would exceed kPbMaxPieces.
+template <typename OffT>
+static int build_pb_view(Graph* g, cudaStream_t s) {
+  PbView& Q = g->pb;
+  const PrSchedule& S = g->pr;
+  const uint32_t V = g->V;
+  const OffT* off = S.off.as<OffT>();
+  const uint32_t* col = S.col.as<uint32_t>();
+  Q.state = -1;
+  if (V == 0 || g->E == 0) return ZOGCU_OK;
+  DevBuf part_of, blk_of;
+  ZOGCU_TRY(pb_groups<OffT>(off, V, kPbRows, kPbCutArcs, part_of, Q.row_lo, Q.row_n, &Q.P, s));
+  {
+    DevBuf d, cum, tmp;
+    ZOGCU_TRY(d.alloc((size_t)V * 8, s));
+    ZOGCU_TRY(cum.alloc((size_t)V * 8, s));
+    k_pb_outdeg<<<grid_1d(V), 256, 0, s>>>(S.deg.as<uint32_t>(), V, d.as<unsigned long long>());
+    ZOGCU_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, d.as<unsigned long long>(), cum.as<unsigned long long>(),
+                                             (int64_t)V, s));
+    ZOGCU_TRY(tmp.alloc(tb, s));
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, d.as<unsigned long long>(), cum.as<unsigned long long>(),
+                                             (int64_t)V, s));
+    ZOGCU_TRY(pb_groups<unsigned long long>(cum.as<unsigned long long>(), V, kPbSrcs, kPbCutArcs, blk_of, Q.blk_lo,
+                                            Q.blk_n, &Q.B, s));
+  }
+  const uint64_t nkeys = (uint64_t)Q.B * Q.P;
+  if (nkeys > kPbMaxPieces) return ZOGCU_OK;
+  DevBuf cnt, padded, start64, start32, mult, cursor, blk_pos;
+  ZOGCU_TRY(cnt.alloc(nkeys * 4, s));
+  ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, nkeys * 4, s));
+  k_pb_count<OffT><<<grid_1d((uint64_t)V * 32), 256, 0, s>>>(off, col, V, blk_of.as<uint32_t>(), part_of.as<uint32_t>(),
+                                                              Q.P, cnt.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_TRY(padded.alloc((nkeys + 1) * 8, s));
+  ZOGCU_TRY(start64.alloc((nkeys + 1) * 8, s));
+  k_pb_pad<<<grid_1d(nkeys + 1), 256, 0, s>>>(cnt.as<uint32_t>(), nkeys, padded.as<unsigned long long>());
+  ZOGCU_CUDA(cudaGetLastError());
+  {
+    size_t tb = 0;
+    DevBuf tmp;
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, padded.as<unsigned long long>(),
+                                             start64.as<unsigned long long>(), (int64_t)nkeys + 1, s));
+    ZOGCU_TRY(tmp.alloc(tb, s));
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, padded.as<unsigned long long>(),
+                                             start64.as<unsigned long long>(), (int64_t)nkeys + 1, s));
+  }
+  unsigned long long npad = 0;
+  ZOGCU_CUDA(cudaMemcpyAsync(&npad, start64.as<unsigned long long>() + nkeys, 8, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (npad >= (1ull << 32) - 4) return ZOGCU_OK;
+  Q.npad = npad;
+  ZOGCU_TRY(start32.alloc(nkeys * 4, s));
+  k_off_narrow<<<grid_1d(nkeys), 256, 0, s>>>(start64.as<uint64_t>(), start32.as<uint32_t>(), nkeys);
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_TRY(mult.alloc(nkeys * 4, s));
+  k_pb_mult<<<grid_1d(nkeys), 256, 0, s>>>(cnt.as<uint32_t>(), nkeys, mult.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_TRY(cursor.alloc(nkeys * 4, s));
+  ZOGCU_CUDA(cudaMemsetAsync(cursor.ptr, 0, nkeys * 4, s));
+  ZOGCU_TRY(Q.sl.alloc(npad * 2 + 16));
+  ZOGCU_TRY(Q.dl.alloc(npad * 2 + 16));
+  ZOGCU_CUDA(cudaMemsetAsync(Q.sl.ptr, 0, npad * 2 + 16, s));
+  k_fill_u16<<<grid_1d(npad + 8), 256, 0, s>>>(Q.dl.as<uint16_t>(), npad + 8, (uint16_t)kPbRows);
+  ZOGCU_CUDA(cudaGetLastError());
+  k_pb_scatter<OffT><<<grid_1d((uint64_t)V * 32), 256, 0, s>>>(
+      off, col, V, blk_of.as<uint32_t>(), Q.blk_lo.as<uint32_t>(), part_of.as<uint32_t>(), Q.row_lo.as<uint32_t>(),
+      Q.P, start32.as<uint32_t>(), cnt.as<uint32_t>(), mult.as<uint32_t>(), cursor.as<uint32_t>(), Q.sl.as<uint16_t>(),
+      Q.dl.as<uint16_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_TRY(Q.pstart.alloc(nkeys * 4));
+  ZOGCU_TRY(Q.pcount.alloc(nkeys * 4));
+  ZOGCU_TRY(blk_pos.alloc(((size_t)Q.B + 1) * 8, s));
+  k_pb_tables<<<grid_1d(nkeys + 1), 256, 0, s>>>(start64.as<unsigned long long>(), cnt.as<uint32_t>(), Q.B, Q.P,
+                                                 Q.pstart.as<uint32_t>(), Q.pcount.as<uint32_t>(),
+                                                 blk_pos.as<unsigned long long>());
+  ZOGCU_CUDA(cudaGetLastError());
+  // emit work items (chunks of each block's positions, largest first) and
+  // partitions ordered by arcs (largest first), so the longest CTAs start first
+  std::vector<unsigned long long> bpos((size_t)Q.B + 1), parcs(Q.P);
+  {
+    DevBuf pa;
+    ZOGCU_TRY(pa.alloc((size_t)Q.P * 8, s));
+    k_pb_part_arcs<OffT><<<grid_1d(Q.P), 256, 0, s>>>(off, Q.row_lo.as<uint32_t>(), Q.row_n.as<uint32_t>(), Q.P,
+                                                      pa.as<unsigned long long>());
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_CUDA(cudaMemcpyAsync(parcs.data(), pa.ptr, (size_t)Q.P * 8, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(bpos.data(), blk_pos.ptr, ((size_t)Q.B + 1) * 8, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+  }
+  std::vector<PbItem> items;
+  for (uint32_t b = 0; b < Q.B; ++b)
+    for (uint64_t a = bpos[b]; a < bpos[b + 1]; a += kPbItem)
+      items.push_back(PbItem{b, (uint32_t)a, (uint32_t)std::min<uint64_t>(a + kPbItem, bpos[b + 1]), 0u});
+  std::stable_sort(items.begin(), items.end(),
+                   [](const PbItem& x, const PbItem& y) { return x.hi - x.lo > y.hi - y.lo; });
+  std::vector<uint32_t> order(Q.P);
+  for (uint32_t p = 0; p < Q.P; ++p) order[p] = p;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return parcs[x] > parcs[y]; });
+  Q.nitems = (uint32_t)items.size();
+  ZOGCU_TRY(Q.items.alloc(std::max<size_t>(items.size(), 1) * sizeof(PbItem)));
+  ZOGCU_TRY(Q.part_order.alloc((size_t)Q.P * 4));
+  ZOGCU_TRY(Q.msg.alloc(npad * 4 + 16));
+  ZOGCU_TRY(Q.heavy.alloc((size_t)Q.P * 8));
+  k_pb_heavy<OffT><<<grid_1d((uint64_t)Q.P * 32), 256, 0, s>>>(off, Q.row_lo.as<uint32_t>(), Q.row_n.as<uint32_t>(),
+                                                               Q.P, Q.heavy.as<uint2>());
+  ZOGCU_CUDA(cudaGetLastError());
+  ZOGCU_CUDA(cudaMemcpyAsync(Q.items.ptr, items.data(), items.size() * sizeof(PbItem), cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(Q.part_order.ptr, order.data(), (size_t)Q.P * 4, cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaMemsetAsync(Q.msg.ptr, 0, npad * 4 + 16, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  Q.state = 1;
+  return ZOGCU_OK;
+}
+
+// The blocked layout, built on first use; false when the graph cannot use it.
+static int ensure_pb_view(Graph* g, cudaStream_t s, bool* usable) {
+  std::lock_guard<std::mutex> lk(g->mu);
+  if (g->pb.state == 0) {
+    if (g->offsets32) {
+      const int rc = build_pb_view<uint32_t>(g, s);
+      if (rc != ZOGCU_OK) {
+        g->pb.reset();
+        return rc;
+      }
+    } else {
+      g->pb.state = -1;
+    }
+  }
+  *usable = g->pb.state == 1;
+  return ZOGCU_OK;
+}
+
+template <typename OffT>
+struct PbArgs {
+  PrArgs<OffT, float> A;  // state, vectors, options (FP32 contributions)
+  const PbItem* items;
+  uint32_t nitems, P, B;
+  const uint32_t* blk_lo;
+  const uint32_t* blk_n;
+  const uint16_t* sl;
+  const uint16_t* dl;
+  float* msg;
+  const uint32_t* pstart;
+  const uint32_t* pcount;
+  const uint32_t* row_lo;
+  const uint32_t* row_n;
+  const uint32_t* part_order;
+  const uint2* heavy;  // per partition: 4 local rows (16 bits each, 0xFFFF = none)
+};
+
+template <typename OffT>
+__global__ void __launch_bounds__(kPbThreads) pb_emit_kernel(PbArgs<OffT> Q) {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  float* const sc = reinterpret_cast<float*>(s_dyn);
+  const PrState* st = Q.A.st;
+  const unsigned long long iter = *(volatile const unsigned long long*)&st->iter;
+  if (*(volatile const int*)&st->converged || iter >= Q.A.max_iter) return;
+  const float* __restrict__ c = (iter & 1ull) ? Q.A.c1 : Q.A.c0;
+  for (uint32_t it = blockIdx.x; it < Q.nitems; it += gridDim.x) {
+    const PbItem I = Q.items[it];
+    const uint32_t lo = Q.blk_lo[I.b], n = Q.blk_n[I.b];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sc[i] = c[lo + i];
+    __syncthreads();
+    for (uint32_t p = I.lo + 4 * threadIdx.x; p < I.hi; p += 4 * blockDim.x) {
+      const uint2 s4 = __ldcs(reinterpret_cast<const uint2*>(Q.sl + p));
+      const float4 v = make_float4(sc[s4.x & 0xFFFFu], sc[s4.x >> 16], sc[s4.y & 0xFFFFu], sc[s4.y >> 16]);
+      __stcs(reinterpret_cast<float4*>(Q.msg + p), v);
+    }
+    __syncthreads();
+  }
+}
+
+// Adds the fixed-point value f to row d's accumulator (low word lo_w[d],
+// high word hi_w[d]); exact, whatever the order of the additions.
+__device__ __forceinline__ void pb_add_fixed(uint32_t* lo_w, uint32_t* hi_w, uint32_t d, unsigned long long f) {
+  const uint32_t lo = (uint32_t)f;
+  uint32_t hi = (uint32_t)(f >> 32);
+  if (lo) {
+    const uint32_t old = atomicAdd(lo_w + d, lo);
+    if (old + lo < old) ++hi;
+  }
+  if (hi) atomicAdd(hi_w + d, hi);
+}
+
+// Adds message m (scaled by 2^kPbShift) to row d.  The partition's four
+// heaviest rows (h) are summed in the lane's registers (reg), because their
+// messages make up much of some pieces, and lanes of one warp adding to one
+// shared-memory word serialise.
+__device__ __forceinline__ void pb_add(uint32_t* lo_w, uint32_t* hi_w, uint32_t d, float m, const uint32_t (&h)[4],
+                                       unsigned long long (&reg)[4]) {
+  const unsigned long long f = __float2ull_rn(m * 0x1p56f);
+  if (d == h[0]) reg[0] += f;
+  else if (d == h[1]) reg[1] += f;
+  else if (d == h[2]) reg[2] += f;
+  else if (d == h[3]) reg[3] += f;
+  else pb_add_fixed(lo_w, hi_w, d, f);
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kPbThreads, 1) pb_accum_kernel(PbArgs<OffT> Q) {
+  static_assert(kPbShift == 56, "pb_add scales by 2^56");
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  uint32_t* const lo_w = reinterpret_cast<uint32_t*>(s_dyn);  // [kPbRows + 1], row kPbRows takes the padding
+  uint32_t* const hi_w = lo_w + (kPbRows + 1);
+  __shared__ double s_red[2 * (kPbThreads / 32)];
+  __shared__ int s_flag;
+  const PrArgs<OffT, float>& A = Q.A;
+  PrState* st = A.st;
+  const unsigned long long iter = *(volatile const unsigned long long*)&st->iter;
+  if (*(volatile const int*)&st->converged || iter >= A.max_iter) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0u);
+    return;
+  }
+  const double sink = *(volatile const double*)&st->sink;
+  const int par = (int)(iter & 1ull);
+  const double* __restrict__ xcur = par ? A.x1 : A.x0;
+  double* __restrict__ xnxt = par ? A.x0 : A.x1;
+  float* __restrict__ cnxt = par ? A.c0 : A.c1;
+  const double tele_u = (1.0 - A.damping) / A.n_f;
+  const bool personalised = A.teleport != nullptr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t p = Q.part_order[blockIdx.x];
+  const uint32_t r0 = Q.row_lo[p], nr = Q.row_n[p];
+  for (uint32_t i = threadIdx.x; i < 2 * (kPbRows + 1); i += blockDim.x) lo_w[i] = 0u;
+  __syncthreads();
+  const uint32_t* __restrict__ ps = Q.pstart + (size_t)p * Q.B;
+  const uint32_t* __restrict__ pc = Q.pcount + (size_t)p * Q.B;
+  // Each warp streams whole pieces, 128 positions per step; the loads of the
+  // next step are issued before the current step's additions.  Lanes past a
+  // piece's end add 0 to the spare row.
+  constexpr uint32_t kPad2 = kPbRows | (kPbRows << 16);
+  const uint2 hv = __ldg(Q.heavy + p);
+  const uint32_t h[4] = {hv.x & 0xFFFFu, hv.x >> 16, hv.y & 0xFFFFu, hv.y >> 16};
+  unsigned long long reg[4] = {0ull, 0ull, 0ull, 0ull};
+  for (uint32_t b = warp; b < Q.B; b += kPbThreads / 32) {
+    const uint32_t s0 = __ldg(ps + b), n = __ldg(pc + b);
+    uint2 d4 = make_uint2(kPad2, kPad2);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (4 * lane < n) {
+      d4 = __ldcs(reinterpret_cast<const uint2*>(Q.dl + s0 + 4 * lane));
+      v = __ldcs(reinterpret_cast<const float4*>(Q.msg + s0 + 4 * lane));
+    }
+    for (uint32_t j0 = 0; j0 < n; j0 += 128) {
+      uint2 dn = make_uint2(kPad2, kPad2);
+      float4 vn = make_float4(0.f, 0.f, 0.f, 0.f);
+      const uint32_t jn = j0 + 128 + 4 * lane;
+      if (jn < n) {
+        dn = __ldcs(reinterpret_cast<const uint2*>(Q.dl + s0 + jn));
+        vn = __ldcs(reinterpret_cast<const float4*>(Q.msg + s0 + jn));
+      }
+      pb_add(lo_w, hi_w, d4.x & 0xFFFFu, v.x, h, reg);
+      pb_add(lo_w, hi_w, d4.x >> 16, v.y, h, reg);
+      pb_add(lo_w, hi_w, d4.y & 0xFFFFu, v.z, h, reg);
+      pb_add(lo_w, hi_w, d4.y >> 16, v.w, h, reg);
+      d4 = dn;
+      v = vn;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    unsigned long long t = reg[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0 && h[k] < kPbRows) pb_add_fixed(lo_w, hi_w, h[k], t);
+  }
+  __syncthreads();
+  double l1 = 0.0, dsum = 0.0;
+  for (uint32_t r = threadIdx.x; r < nr; r += blockDim.x) {
+    const uint32_t v = r0 + r;
+    const double sum = (double)(((unsigned long long)hi_w[r] << 32) | lo_w[r]) * 0x1p-56;
+    pr_row_epilogue<float>(v, sum, __ldg(A.deg + v), xcur[v], personalised ? __ldg(A.teleport + v) : 0.0,
+                           personalised, A.damping, A.n_f, xnxt, cnxt, tele_u, sink, l1, dsum);
+  }
+  cta_publish(st, A.cta_part, nullptr, nullptr, 0u, l1, dsum, iter + 1, A.tol, A.stall, true, s_red, &s_flag,
+              A.max_iter, A.cond, A.use_cond);
+}
+
+// Runs the emit / accumulate pair as the body of a CUDA-graph while loop (the
+// accumulate's last CTA clears the condition; see pr_launch_loop).
+template <typename OffT>
+static int pb_launch_loop(PbArgs<OffT> Q, int egrid, int agrid, cudaStream_t s) {
+  cudaGraph_t graph = nullptr;
+  ZOGCU_CUDA(cudaGraphCreate(&graph, 0));
+  struct GraphGuard {
+    cudaGraph_t g;
+    ~GraphGuard() { cudaGraphDestroy(g); }
+  } guard{graph};
+  cudaGraphConditionalHandle h;
+  ZOGCU_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  ZOGCU_CUDA(cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp));
+  Q.A.cond = h;
+  Q.A.use_cond = 1;
+  void* args[] = {&Q};
+  cudaKernelNodeParams ke = {};
+  ke.func = reinterpret_cast<void*>(pb_emit_kernel<OffT>);
+  ke.gridDim = dim3((unsigned)egrid);
+  ke.blockDim = dim3((unsigned)kPbThreads);
+  ke.sharedMemBytes = (unsigned)kPbEmitBytes;
+  ke.kernelParams = args;
+  cudaKernelNodeParams ka = ke;
+  ka.func = reinterpret_cast<void*>(pb_accum_kernel<OffT>);
+  ka.gridDim = dim3((unsigned)agrid);
+  ka.sharedMemBytes = (unsigned)kPbAccBytes;
+  cudaGraphNode_t en, an;
+  ZOGCU_CUDA(cudaGraphAddKernelNode(&en, cp.conditional.phGraph_out[0], nullptr, 0, &ke));
+  ZOGCU_CUDA(cudaGraphAddKernelNode(&an, cp.conditional.phGraph_out[0], &en, 1, &ka));
+  cudaGraphExec_t exec = nullptr;
+  ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  const cudaError_t e = cudaGraphLaunch(exec, s);
+  cudaGraphExecDestroy(exec);
+  ZOGCU_CUDA(e);
+  return ZOGCU_OK;
+}
+
+// A blocked chain of up to max_iter iterations (start vector as in
+// pr_init_kernel).  Adds the launches it enqueued to *launches; the caller
+// adds two per iteration the chain ran (*looped = true) once it has read the
+// chain's state.
+template <typename OffT>
+static int pb_run_chain(const PbArgs<OffT>& Q, uint32_t V, int given, uint64_t max_iter, cudaStream_t s,
+                        uint64_t* launches, bool* looped) {
+  PbArgs<OffT> R = Q;
+  R.A.max_iter = max_iter;
+  R.A.cond = 0;
+  R.A.use_cond = 0;
+  ZOGCU_CUDA(cudaFuncSetAttribute(pb_emit_kernel<OffT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPbEmitBytes));
+  ZOGCU_CUDA(cudaFuncSetAttribute(pb_accum_kernel<OffT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPbAccBytes));
+  int per_sm = 0;
+  ZOGCU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb_emit_kernel<OffT>, kPbThreads, kPbEmitBytes));
+  const int egrid = (int)std::min<uint64_t>(std::max<uint64_t>(R.nitems, 1), (uint64_t)std::max(per_sm, 1) * sm_count());
+  const int agrid = (int)R.P;
+  ZOGCU_CUDA(cudaMemsetAsync(R.A.st, 0, sizeof(PrState), s));
+  const unsigned init_grid = std::min(grid_1d(V), 148u * 4);
+  pr_init_kernel<OffT, float><<<init_grid, 256, 0, s>>>(R.A, V, given);
+  ZOGCU_CUDA(cudaGetLastError());
+  ++*launches;
+  *looped = false;
+  if (max_iter >= kLoopMinIters) {
+    ZOGCU_TRY(pb_launch_loop<OffT>(R, egrid, agrid, s));
+    *looped = true;
+    return ZOGCU_OK;
+  }
+  for (uint64_t k = 0; k < max_iter; ++k) {
+    pb_emit_kernel<OffT><<<egrid, kPbThreads, kPbEmitBytes, s>>>(R);
+    pb_accum_kernel<OffT><<<agrid, kPbThreads, kPbAccBytes, s>>>(R);
+  }
+  ZOGCU_CUDA(cudaGetLastError());
+  *launches += 2 * max_iter;
+  return ZOGCU_OK;
+}
+
+// Whether the precision form's FP32 phase runs blocked: ZOGCU_PR_BLOCKED=0
+// never, =1 whenever the layout can be built, otherwise on graphs of at least
+// 2^23 nodes and 2^24 arcs.  Below that the FP32 contributions (4 bytes per
+// node) sit in L2 and the gather kernels win: on Barabasi-Albert n = 2^22
+// (33.5M arcs) a blocked iteration took 0.67 ms against 0.23 ms.
+static bool pb_wanted(const Graph* g) {
+  if (const char* e = std::getenv("ZOGCU_PR_BLOCKED")) {
+    if (e[0] == '0') return false;
+    if (e[0] == '1') return true;
+  }
+  return g->V >= (1u << 23) && g->E >= (1ull << 24);
+}
+
 // FP32-phase switch: the FP32 contributions carry relative rounding ~6e-8, so
 // the L1 step of the FP32 iterates floors near 1e-7; the FP32 phase stops at
 // kMixedSwitchTol or when the step stops shrinking (kMixedStall), and the FP64
@@ -1415,7 +2031,8 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   // the buffers, so it outlives them)
   WorkLease lease(&g->pr_ws, s);
   PrWork W;
-  DevBuf cf0, cf1;
+  DevBuf cf0, cf1, pbpart;
+  bool blocked32 = false;
   ZOGCU_TRY(lease.get(W.x0, 0, (size_t)V * 8));
   ZOGCU_TRY(lease.get(W.x1, 1, (size_t)V * 8));
   ZOGCU_TRY(lease.get(W.c0, 2, (size_t)V * 8 + 16));
@@ -1488,11 +2105,40 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     Af.tol = std::max(tol, kMixedSwitchTol);
     Af.stall = kMixedStall;
     int64_t from32 = -1;
-    ZOGCU_TRY((pr_run_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches, &cfg, &from32)));
+    bool blocked = false, looped = false;
+    if (pb_wanted(g)) ZOGCU_TRY(ensure_pb_view(g, s, &blocked));
+    if (blocked) {
+      // the propagation-blocked iteration (same update, streamed messages)
+      const PbView& B = g->pb;
+      PbArgs<OffT> Q{};
+      Q.A = Af;
+      ZOGCU_TRY(lease.get(pbpart, 13, (size_t)std::max<uint32_t>(B.P, 148u * 4u) * 16));
+      Q.A.cta_part = pbpart.as<double>();
+      Q.items = B.items.as<PbItem>();
+      Q.nitems = B.nitems;
+      Q.P = B.P;
+      Q.B = B.B;
+      Q.blk_lo = B.blk_lo.as<uint32_t>();
+      Q.blk_n = B.blk_n.as<uint32_t>();
+      Q.sl = B.sl.as<uint16_t>();
+      Q.dl = B.dl.as<uint16_t>();
+      Q.msg = B.msg.as<float>();
+      Q.pstart = B.pstart.as<uint32_t>();
+      Q.pcount = B.pcount.as<uint32_t>();
+      Q.row_lo = B.row_lo.as<uint32_t>();
+      Q.row_n = B.row_n.as<uint32_t>();
+      Q.part_order = B.part_order.as<uint32_t>();
+      Q.heavy = B.heavy.as<uint2>();
+      ZOGCU_TRY(pb_run_chain<OffT>(Q, V, given, max_iter, s, &launches, &looped));
+    } else {
+      ZOGCU_TRY((pr_run_chain<OffT, float>(g, cfg, Af, V, given, max_iter, s, &launches, &cfg, &from32)));
+    }
     ZOGCU_CUDA(cudaMemcpyAsync(&hs, W.stb.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     if (hs.pad[0]) return fail(ZOGCU_ERR_INTERNAL, "PageRank work item failed a bound check");
     if (from32 >= 0) launches += hs.iter - (uint64_t)from32 + (hs.iter == (uint64_t)from32 ? 1 : 0);
+    if (looped) launches += 2 * hs.iter;
+    blocked32 = blocked;
     it32 = hs.iter;
     // ---- FP64 polish from the FP32 phase's last vector ----------------------
     if (it32 & 1ull) std::swap(A.x0, A.x1);
@@ -1526,6 +2172,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     stats->launches = launches;
     stats->polish_iterations = mixed ? hs.iter : 0;
     stats->kernel_config = (uint32_t)cfg;
+    stats->reserved = blocked32 ? 1u : 0u;
   }
   return ZOGCU_OK;
 }
