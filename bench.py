@@ -86,59 +86,104 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during a timed region."""
+    """SM clocks and throttle reasons sampled during a timed region.
+
+    Polls NVML every 5 ms from a thread (no process start-up, so even a
+    timed region of ~0.2 s gets samples); falls back to `nvidia-smi -lms`.
+    start() returns once the first sample is in.  Only reads settings."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index: int, interval_ms: int = 25):
+    def __init__(self, gpu_index: int, interval_ms: int = 5):
         self.gpu = gpu_index
         self.interval = interval_ms
         self.proc = None
-        self.lines = []
         self.t = None
+        self.samples = []  # (sm_mhz, sm_max_mhz, set of reason names)
+        self.first = 0
+        self.running = False
+        self.nvml = None
 
-    def start(self):
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", str(self.interval)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (OSError, FileNotFoundError):
-            self.proc = None
-            return
-        self.t = threading.Thread(target=self._read, daemon=True)
-        self.t.start()
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+        bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+        return pynvml, h, bits
 
-    def _read(self):
+    def _poll_nvml(self):
+        pynvml, h, bits = self.nvml
+        smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        while self.running:
+            try:
+                sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, smax, {nm for nm, b in zip(self.NAMES, bits) if r & b}))
+            except Exception:
+                pass
+            time.sleep(self.interval / 1000.0)
+
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        if self.t:
-            self.t.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
+            parts = [q.strip() for q in line.strip().split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1])); smax.append(float(parts[2]))
+                sm, smax = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+            self.samples.append((sm, smax, {nm for nm, v in zip(self.NAMES, parts[5:9])
+                                            if v.lower().startswith("active")}))
+
+    def start(self):
+        self.running = True
+        try:
+            self.nvml = self._nvml_handle()
+            self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+        except Exception:
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                     "-lms", "25"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            except (OSError, FileNotFoundError):
+                self.proc = None
+                return
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
+        self.t.start()
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 3.0:
+            time.sleep(0.002)
+        self.first = len(self.samples)  # samples taken before the timed region are dropped
+
+    def stop(self):
+        self.running = False
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        if self.t is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
+        got = self.samples[self.first:] or self.samples[-1:]
+        sm = [g[0] for g in got]
+        reasons = set().union(*[g[2] for g in got]) if got else set()
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(g[1] for g in got) if got else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def peaks():

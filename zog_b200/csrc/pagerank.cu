@@ -1200,6 +1200,14 @@ static int pr_launch_loop(void (*fn)(PrArgs<OffT, CT>), PrArgs<OffT, CT> A, int 
 // pays off once some 40 launches would otherwise be spent after convergence.
 constexpr uint64_t kLoopMinIters = 48;
 
+// ZOGCU_PR_GRAPH_LOOP=0 launches every chain as plain kernel launches (same
+// iterations, same results), e.g. for a profiler that cannot see kernels
+// inside a conditional graph node.
+static bool graph_loop_allowed() {
+  const char* e = std::getenv("ZOGCU_PR_GRAPH_LOOP");
+  return !(e && e[0] == '0');
+}
+
 // Launches up to `count` iterations of configuration `cfg`; `init` starts a
 // new chain (state cleared, start vector written).  A.max_iter bounds the
 // whole chain, so a chain may be launched in pieces of different
@@ -1234,7 +1242,7 @@ static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, in
     ++*launches;
   }
   auto fn = PrLauncher<OffT, CT>::fn(cfg);
-  if (loop_from && count >= kLoopMinIters) {
+  if (loop_from && count >= kLoopMinIters && graph_loop_allowed()) {
     ZOGCU_TRY((pr_launch_loop<OffT, CT>(fn, A, grid, kPrConfigs[cfg].threads, dyn, s)));
     *loop_from = (int64_t)from_iter;
     return ZOGCU_OK;
@@ -1421,7 +1429,7 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
 constexpr uint32_t kPbRows = 24576;          // rows per partition (accumulators in shared memory)
 constexpr uint32_t kPbSrcs = 24576;          // sources per block (contributions in shared memory)
 constexpr uint64_t kPbCutArcs = 1ull << 20;  // arcs per partition / block before a cut
-constexpr uint32_t kPbItem = 65536;          // positions per emit work item
+constexpr uint32_t kPbItem = 1u << 18;        // positions per emit work item (about one per block)
 constexpr uint64_t kPbMaxPieces = 1ull << 26;
 constexpr int kPbShift = 56;
 constexpr int kPbThreads = 1024;
@@ -1981,7 +1989,7 @@ static int pb_run_chain(const PbArgs<OffT>& Q, uint32_t V, int given, uint64_t m
   ZOGCU_CUDA(cudaGetLastError());
   ++*launches;
   *looped = false;
-  if (max_iter >= kLoopMinIters) {
+  if (max_iter >= kLoopMinIters && graph_loop_allowed()) {
     ZOGCU_TRY(pb_launch_loop<OffT>(R, egrid, agrid, s));
     *looped = true;
     return ZOGCU_OK;
