@@ -1253,8 +1253,30 @@ static int pr_launch_chain(Graph* g, int cfg, PrArgs<OffT, CT> A, uint32_t V, in
   return ZOGCU_OK;
 }
 
+// Configurations the tuner chose, per device and graph signature (node and
+// arc counts rounded up to powers of two), so that a later graph of the same
+// shape (a resource rebuilt from the same kind of data) starts with it instead
+// of spending its first iterations on tuning.  Every configuration computes
+// the same iteration; ZOGCU_PR_TUNE_CACHE=0 turns the sharing off.
+static std::mutex g_tune_mu;
+static std::vector<std::pair<uint64_t, int>> g_tune_cache;
+
+static bool tune_cache_on() {
+  const char* e = std::getenv("ZOGCU_PR_TUNE_CACHE");
+  return !(e && e[0] == '0');
+}
+static uint64_t tune_key(const Graph* g) {
+  auto lg = [](uint64_t x) {
+    int b = 0;
+    while (b < 63 && (1ull << b) < x) ++b;
+    return (uint64_t)b;
+  };
+  return ((uint64_t)g->device << 16) | (lg(g->V) << 8) | lg(g->E);
+}
+
 // Kernel configuration of a graph: the one already chosen, the one forced by
-// ZOGCU_PR_CONFIG, the default for small graphs, or -1 (time them).
+// ZOGCU_PR_CONFIG, the default for small graphs, the one chosen for an
+// earlier graph of the same signature, or -1 (time them).
 static int pr_config_of(Graph* g) {
   std::lock_guard<std::mutex> lk(g->mu);
   PrSchedule& P = g->pr;
@@ -1264,7 +1286,23 @@ static int pr_config_of(Graph* g) {
     if (c >= 0 && c < kNumPrConfigs) return P.config = c;
   }
   if (g->E < (1ull << 22)) return P.config = kDefaultPrConfig;
+  if (tune_cache_on()) {
+    std::lock_guard<std::mutex> tl(g_tune_mu);
+    for (const auto& kv : g_tune_cache)
+      if (kv.first == tune_key(g)) return P.config = kv.second;
+  }
   return -1;
+}
+
+static void remember_config(const Graph* g, int cfg) {
+  std::lock_guard<std::mutex> tl(g_tune_mu);
+  const uint64_t k = tune_key(g);
+  for (auto& kv : g_tune_cache)
+    if (kv.first == k) {
+      kv.second = cfg;
+      return;
+    }
+  g_tune_cache.emplace_back(k, cfg);
 }
 
 // A chain of up to max_iter iterations.  When the graph has no configuration
@@ -1391,6 +1429,7 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     std::lock_guard<std::mutex> lk(g->mu);
     if (g->pr.config < 0) g->pr.config = best;
     best = g->pr.config;
+    remember_config(g, best);
   } else {
     best = kDefaultPrConfig;
   }
