@@ -63,7 +63,7 @@ GNN_PREDICT_LAUNCHES = 13
 
 
 def pr_kernel_name(cfg):
-    """Kernel behind a PageRank configuration: 5 and 6 pipeline the row-block
+    """Kernel behind a PageRank configuration: 5-8 pipeline the row-block
     gathers (pr_iter_kernel_pipe), the others are pr_iter_kernel."""
     return "pr_iter_kernel_pipe" if cfg >= 5 else "pr_iter_kernel"
 
@@ -71,8 +71,9 @@ def pr_kernel_name(cfg):
 # DRAM bytes (read + write) of one PageRank iteration launch on the default
 # workload (scale 24), dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture of this command with only the PageRank block enabled (kernel
-# configuration 4; configurations 3 and 4 move the same bytes).
-PROFILED_TRAFFIC = {24: 1.53e9 + 0.1763e9}
+# configuration 7, the pipelined kernel with a 16 KB hub; configurations 3, 4
+# and 6 moved 1.70-1.71 GB as well).
+PROFILED_TRAFFIC = {24: 1.5198e9 + 0.1725e9}
 
 
 # --------------------------------------------------------------------------

@@ -71,6 +71,8 @@ constexpr PrConfig kPrConfigs[] = {
     {256, 128, 0, 0},            // 4: four CTAs per SM, no hub, small items
     {256, 128, 0, 1},            // 5: four CTAs per SM, pipelined gathers
     {256, 256, 0, 1},            // 6: three CTAs per SM, pipelined gathers, bigger items
+    {256, 256, 16 * 1024, 1},    // 7: as 6 with a 16 KB hub (a 40 KB hub measured 1.9x slower)
+    {256, 256, 20 * 1024, 1},    // 8: as 6 with a 20 KB hub (the largest whose three CTAs fit a 164 KB carveout)
 };
 constexpr int kNumPrConfigs = sizeof(kPrConfigs) / sizeof(kPrConfigs[0]);
 constexpr int kDefaultPrConfig = 0;
@@ -583,7 +585,7 @@ constexpr int pr_pipe_min_blocks(int nnz) { return nnz >= 256 ? 3 : 4; }
 // round trip of waiting instead of two.  Each row is summed exactly as in
 // pr_iter_kernel (same staging layout, same order); rows of kinds B and C are
 // summed synchronously, as there.
-template <typename OffT, typename CT, int THREADS, int NNZ, int MODE = kModePageRank>
+template <typename OffT, typename CT, int THREADS, int NNZ, int MODE = kModePageRank, bool HUB = false>
 __global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kernel_pipe(PrArgs<OffT, CT> A) {
   constexpr int WARPS = THREADS / 32;
   constexpr int NG = NNZ / 32;
@@ -634,10 +636,23 @@ __global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kern
       lin_row_epilogue<MODE>(v, s, dg, xo, ka, kb, xnxt, el1, eacc);
   };
 
+  // ---- dynamic shared memory: [hub | per-warp staging] ----------------------
+  const uint32_t nhub = HUB ? A.hub : 0u;
+  const size_t hub_bytes = ((size_t)nhub * sizeof(CT) + 15) & ~(size_t)15;
+  CT* const hub = reinterpret_cast<CT*>(s_dyn);
+  if constexpr (HUB) {
+    if (nhub) {
+      const uint4* src = reinterpret_cast<const uint4*>(ccur);
+      uint4* dst = reinterpret_cast<uint4*>(hub);
+      const uint32_t n16 = (uint32_t)(((size_t)nhub * sizeof(CT)) >> 4);
+      for (uint32_t i = threadIdx.x; i < n16; i += THREADS) dst[i] = __ldcg(src + i);
+      __syncthreads();
+    }
+  }
   const uint64_t pol_arc = policy_evict_first();
   const uint64_t pol_c = policy_evict_last();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  CT* const stage = reinterpret_cast<CT*>(s_dyn) + (size_t)warp * 2 * NNZ;  // two buffers of NNZ
+  CT* const stage = reinterpret_cast<CT*>(s_dyn + hub_bytes) + (size_t)warp * 2 * NNZ;  // two buffers of NNZ
   double l1 = 0.0, dsum = 0.0;
 
   const uint32_t nwarps = gridDim.x * WARPS;
@@ -675,7 +690,8 @@ __global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kern
 #pragma unroll
     for (int k = 0; k < NG; ++k) {
       if ((uint32_t)lane + 32 * k < na) {
-        if (q[k] < A.nv) cp_gather(dst + lane + 32 * k, ccur + q[k]);
+        if (HUB && q[k] < nhub) dst[lane + 32 * k] = hub[q[k]];  // the hub's contributions, from shared memory
+        else if (q[k] < A.nv) cp_gather(dst + lane + 32 * k, ccur + q[k]);
         else atomicOr(err, 1u);
       }
     }
@@ -767,14 +783,14 @@ __global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kern
         if (personalised) tp = __ldg(A.teleport + row);
       }
       if (kind == kTaskRow) {
-        const double sum = warp_range_sum<OffT, CT>(A.col, ccur, nullptr, 0u, a0, b0, lane, pol_arc, pol_c);
+        const double sum = warp_range_sum<OffT, CT>(A.col, ccur, hub, nhub, a0, b0, lane, pol_arc, pol_c);
         if (lane == 0) epilogue(row, sum, dg, xo, tp, l1, dsum);
       } else {
         const uint32_t c = t0.b & 0xFFFFu;
         const uint32_t nch = (uint32_t)((b0 - a0 + kLongChunk - 1) / kLongChunk);
         const OffT e0 = a0 + (OffT)c * kLongChunk;
         const OffT e1 = min(e0 + (OffT)kLongChunk, b0);
-        const double sum = warp_range_sum<OffT, CT>(A.col, ccur, nullptr, 0u, e0, e1, lane, pol_arc, pol_c);
+        const double sum = warp_range_sum<OffT, CT>(A.col, ccur, hub, nhub, e0, e1, lane, pol_arc, pol_c);
         const uint32_t first = ti - c;
         unsigned int last = 0;
         if (lane == 0) {
@@ -1108,7 +1124,9 @@ struct PrLauncher {
       case 3: return pr_iter_kernel<OffT, CT, 256, 256>;
       case 4: return pr_iter_kernel<OffT, CT, 256, 128>;
       case 5: return pr_iter_kernel_pipe<OffT, CT, 256, 128>;
-      default: return pr_iter_kernel_pipe<OffT, CT, 256, 256>;
+      case 6: return pr_iter_kernel_pipe<OffT, CT, 256, 256>;
+      case 7:
+      default: return pr_iter_kernel_pipe<OffT, CT, 256, 256, kModePageRank, true>;
     }
   }
   static size_t staging_bytes(int cfg) {
@@ -1132,7 +1150,12 @@ struct PrLauncher {
     if (known > 0) return known;
     Fn f = fn(cfg);
     const size_t maxdyn = (size_t)kPrConfigs[cfg].hub_bytes + staging_bytes(cfg);
-    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxdyn) != cudaSuccess) return 0;
+    // configurations can share a kernel (hub sizes differ): its limit must
+    // admit the largest of them, whichever was set up last
+    size_t limit = maxdyn;
+    for (int c2 = 0; c2 < kNumPrConfigs; ++c2)
+      if (fn(c2) == f) limit = std::max(limit, (size_t)kPrConfigs[c2].hub_bytes + staging_bytes(c2));
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit) != cudaSuccess) return 0;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kPrConfigs[cfg].threads, maxdyn) != cudaSuccess)
       return 0;
