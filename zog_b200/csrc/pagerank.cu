@@ -1931,6 +1931,8 @@ __global__ void __launch_bounds__(kPbThreads, 1) pb_accum_kernel(PbArgs<OffT> Q)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t p = Q.part_order[blockIdx.x];
   const uint32_t r0 = Q.row_lo[p], nr = Q.row_n[p];
+  __shared__ unsigned int s_next;  // next piece to hand out
+  if (threadIdx.x == 0) s_next = kPbThreads / 32;
   for (uint32_t i = threadIdx.x; i < 2 * (kPbRows + 1); i += blockDim.x) lo_w[i] = 0u;
   __syncthreads();
   const uint32_t* __restrict__ ps = Q.pstart + (size_t)p * Q.B;
@@ -1942,7 +1944,10 @@ __global__ void __launch_bounds__(kPbThreads, 1) pb_accum_kernel(PbArgs<OffT> Q)
   const uint2 hv = __ldg(Q.heavy + p);
   const uint32_t h[4] = {hv.x & 0xFFFFu, hv.x >> 16, hv.y & 0xFFFFu, hv.y >> 16};
   unsigned long long reg[4] = {0ull, 0ull, 0ull, 0ull};
-  for (uint32_t b = warp; b < Q.B; b += kPbThreads / 32) {
+  // Warp w starts with piece w and then takes the next piece not yet handed
+  // out; the heavy blocks' large pieces come first, so the warps reach the
+  // barrier below within about one piece of each other.
+  for (uint32_t b = warp; b < Q.B;) {
     const uint32_t s0 = __ldg(ps + b), n = __ldg(pc + b);
     uint2 d4 = make_uint2(kPad2, kPad2);
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1965,6 +1970,9 @@ __global__ void __launch_bounds__(kPbThreads, 1) pb_accum_kernel(PbArgs<OffT> Q)
       d4 = dn;
       v = vn;
     }
+    unsigned int nb = 0u;
+    if (lane == 0) nb = atomicAdd(&s_next, 1u);
+    b = __shfl_sync(0xffffffffu, nb, 0);
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
