@@ -2100,11 +2100,18 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   const uint32_t V = g->V;
   const bool dev_ptrs = o && o->device_pointers;
   const bool mixed = o && o->precision == ZOGCU_PREC_MIXED;
-  // workspace sized for every configuration's schedule
-  ZOGCU_TRY(ensure_task_list(g, 128, s));
-  ZOGCU_TRY(ensure_task_list(g, 256, s));
+  // the work-item list of the graph's configuration, or both lists when the
+  // solve will tune; the workspace is sized for the lists built so far
+  int cfg = pr_config_of(g);
+  if (cfg >= 0) {
+    ZOGCU_TRY(ensure_task_list(g, kPrConfigs[cfg].nnz, s));
+  } else {
+    ZOGCU_TRY(ensure_task_list(g, 128, s));
+    ZOGCU_TRY(ensure_task_list(g, 256, s));
+  }
   tr->mark("work-item lists");
-  const uint32_t max_tasks = std::max(P.lists[0].num_tasks, P.lists[1].num_tasks);
+  const uint32_t max_tasks = cfg >= 0 ? P.lists[list_index(kPrConfigs[cfg].nnz)].num_tasks
+                                      : std::max(P.lists[0].num_tasks, P.lists[1].num_tasks);
   // the graph's cached scratch when no other call holds it (declared before
   // the buffers, so it outlives them)
   WorkLease lease(&g->pr_ws, s);
@@ -2150,7 +2157,6 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   A.stall = 0.0;
   A.nv = V;
 
-  int cfg = pr_config_of(g);
   tr->mark("workspace");
 
   int given = 0;
