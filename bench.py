@@ -284,9 +284,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT)",
-        "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 tol1e-9; "
-                               f"brandes rmat{BC_SCALE} ef{BC_EF} undirected all sources",
-                   "l2": "inputs larger than L2"},
+        "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 uniform start, d={DAMPING}, "
+                               f"tol={TOL}, max_iter={MAX_ITER}", "vertices": int(V), "arcs": int(len(in_col)),
+                   "iterations": iters_full, "l2": "inputs larger than L2", "parallelism": "single"},
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
                          "sample": f"{args.ref_iters_per_step} iterations of the reference PageRank loop "
                                    f"(oracle restatement, 1 thread) over the full scale-{PR_SCALE} graph per step, "
