@@ -14,7 +14,7 @@ from conftest import GOLDEN, rel_l1
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-9
-N_CONFIGS = 9  # kernel configurations of pr_iter_kernel / pr_iter_kernel_pipe
+N_CONFIGS = 11  # kernel configurations of pr_iter_kernel / pr_iter_kernel_pipe
 
 
 def golden(name):

@@ -73,6 +73,8 @@ constexpr PrConfig kPrConfigs[] = {
     {256, 256, 0, 1},            // 6: three CTAs per SM, pipelined gathers, bigger items
     {256, 256, 16 * 1024, 1},    // 7: as 6 with a 16 KB hub (a 40 KB hub measured 1.9x slower)
     {256, 256, 20 * 1024, 1},    // 8: as 6 with a 20 KB hub (the largest whose three CTAs fit a 164 KB carveout)
+    {768, 256, 56 * 1024, 1},    // 9: one CTA of 24 warps per SM sharing a 56 KB hub
+    {768, 256, 64 * 1024, 1},    // 10: as 9 with a 64 KB hub
 };
 constexpr int kNumPrConfigs = sizeof(kPrConfigs) / sizeof(kPrConfigs[0]);
 constexpr int kDefaultPrConfig = 0;
@@ -576,7 +578,7 @@ __global__ void __launch_bounds__(THREADS, pr_min_blocks(THREADS)) pr_iter_kerne
               MODE == kModeEigen ? -1.0 : A.stall, true, s_red, &s_flag, A.max_iter, A.cond, A.use_cond);
 }
 
-constexpr int pr_pipe_min_blocks(int nnz) { return nnz >= 256 ? 3 : 4; }
+constexpr int pr_pipe_min_blocks(int threads, int nnz) { return threads > 256 ? 1 : (nnz >= 256 ? 3 : 4); }
 
 // The same iteration with the row-block gathers software-pipelined: while a
 // warp sums work item i from one staging buffer, the gathers of item i+1 are
@@ -586,7 +588,7 @@ constexpr int pr_pipe_min_blocks(int nnz) { return nnz >= 256 ? 3 : 4; }
 // pr_iter_kernel (same staging layout, same order); rows of kinds B and C are
 // summed synchronously, as there.
 template <typename OffT, typename CT, int THREADS, int NNZ, int MODE = kModePageRank, bool HUB = false>
-__global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(NNZ)) pr_iter_kernel_pipe(PrArgs<OffT, CT> A) {
+__global__ void __launch_bounds__(THREADS, pr_pipe_min_blocks(THREADS, NNZ)) pr_iter_kernel_pipe(PrArgs<OffT, CT> A) {
   constexpr int WARPS = THREADS / 32;
   constexpr int NG = NNZ / 32;
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -1125,6 +1127,8 @@ struct PrLauncher {
       case 4: return pr_iter_kernel<OffT, CT, 256, 128>;
       case 5: return pr_iter_kernel_pipe<OffT, CT, 256, 128>;
       case 6: return pr_iter_kernel_pipe<OffT, CT, 256, 256>;
+      case 9:
+      case 10: return pr_iter_kernel_pipe<OffT, CT, 768, 256, kModePageRank, true>;
       case 7:
       default: return pr_iter_kernel_pipe<OffT, CT, 256, 256, kModePageRank, true>;
     }
@@ -1336,7 +1340,10 @@ static void remember_config(const Graph* g, int cfg) {
 // The fastest runs the rest of the chain and is kept for the graph.  Every
 // configuration computes the same iteration, so the tuning iterations are
 // ordinary iterations of the solve.  Only iterations that ran before
-// convergence count; if a configuration has none, nothing is kept.
+// convergence count: a chain that converges during the second round keeps
+// the first round's best among the configurations it timed, so one solve
+// settles the choice and later solves repeat bit for bit; nothing is kept
+// only when no timed iteration ran before convergence.
 template <typename OffT, typename CT>
 static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V, int given, uint64_t max_iter,
                         cudaStream_t s, uint64_t* launches, int* used_cfg, int64_t* loop_from) {
@@ -1398,20 +1405,12 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     for (int c = 0; c < kNumPrConfigs; ++c)
       cand[c] = big_hub_pays || !(kPrConfigs[c].threads >= 1024 && kPrConfigs[c].hub_bytes > 0);
   }
-  auto fastest = [&]() {
-    int best = -1;
-    for (int c = 0; c < kNumPrConfigs; ++c) {
-      if (!cand[c]) continue;
-      if (cnt[c] == 0) return -1;
-      if (best < 0 || best_of[c] < best_of[best]) best = c;
-    }
-    return best;
-  };
+  // fastest configuration of `set` among those with a timing that counts
+  // (-1 when none has one)
   auto fastest_of = [&](const bool* set) {
     int best = -1;
     for (int c = 0; c < kNumPrConfigs; ++c) {
-      if (!set[c]) continue;
-      if (cnt[c] == 0) return -1;
+      if (!set[c] || cnt[c] == 0) continue;
       if (best < 0 || best_of[c] < best_of[best]) best = c;
     }
     return best;
@@ -1419,7 +1418,7 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
   for (int c = 0; c < kNumPrConfigs; ++c)
     if (cand[c]) ZOGCU_TRY(timed(c));
   ZOGCU_TRY(collect());
-  int best = fastest();
+  int best = fastest_of(cand);
   if (best >= 0) {
     // second round: each close configuration runs twice back to back and
     // only the second launch is timed, the one that starts from the caches
@@ -1427,7 +1426,7 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
     // another one ran up to 8 % slow)
     const double cut = kSecondRound * best_of[best];
     bool close[kNumPrConfigs];
-    for (int c = 0; c < kNumPrConfigs; ++c) close[c] = cand[c] && best_of[c] <= cut;
+    for (int c = 0; c < kNumPrConfigs; ++c) close[c] = cand[c] && cnt[c] > 0 && best_of[c] <= cut;
     const int first_round = n;
     for (int c = kNumPrConfigs - 1; c >= 0; --c) {
       if (!close[c]) continue;
@@ -1437,10 +1436,13 @@ static int pr_run_chain(Graph* g, int cfg, const PrArgs<OffT, CT>& A, uint32_t V
       ZOGCU_TRY(timed(c));
     }
     ZOGCU_TRY(collect());
-    // the close configurations are ranked by their second-round time alone
+    // the close configurations are ranked by their second-round time alone;
+    // if the chain converged before any of those counted, the first round's
+    // best is kept
     for (int i = 0; i < first_round; ++i)
-      if (close[order[i]]) --cnt[order[i]];
-    best = fastest_of(close);
+      if (order[i] >= 0 && close[order[i]] && cnt[order[i]] > 0) --cnt[order[i]];
+    const int second = fastest_of(close);
+    if (second >= 0) best = second;
   }
   if (std::getenv("ZOGCU_PR_TUNE_LOG")) {  // diagnostic: the tuning launches in order
     for (int i = 0; i < n; ++i)
