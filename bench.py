@@ -71,9 +71,9 @@ def pr_kernel_name(cfg):
 # DRAM bytes (read + write) of one PageRank iteration launch on the default
 # workload (scale 24), dram__bytes_read.sum + dram__bytes_write.sum from one
 # ncu capture of this command with only the PageRank block enabled (kernel
-# configuration 7, the pipelined kernel with a 16 KB hub; configurations 3, 4
-# and 6 moved 1.70-1.71 GB as well).
-PROFILED_TRAFFIC = {24: 1.5198e9 + 0.1725e9}
+# configuration 10, the 768-thread pipelined kernel with a 64 KB hub;
+# configurations 3, 4, 6 and 7 moved 1.69-1.71 GB as well).
+PROFILED_TRAFFIC = {24: 1.5448e9 + 0.1721e9}
 
 
 # --------------------------------------------------------------------------
