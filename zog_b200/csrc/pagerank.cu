@@ -31,7 +31,13 @@
 //     trips, and warps never wait on each other inside the pass;
 //   * the kernel is a template over (CTA size, arcs per item, hub size); the
 //     first PageRank solve on a graph times each configuration on its own
-//     early iterations and keeps the fastest (ZOGCU_PR_CONFIG forces one);
+//     early iterations and keeps the fastest (ZOGCU_PR_CONFIG forces one),
+//     also for later graphs of the same size on the device.  The fastest at
+//     scale 24 is the pipelined kernel (pr_iter_kernel_pipe: the next row
+//     block's gathers in flight with cp.async while the current one is
+//     summed) with one 768-thread CTA per SM sharing a 64 KB hub: the hub's
+//     gathers skip the L1 tag stage, and hub plus staging still fit the
+//     164 KB shared-memory carveout that leaves L1 for the other gathers;
 //   * the work-item lists are built on the device (segmented greedy pass);
 //   * arc indices stream with an L2 evict-first policy, bypassing L1; gathered
 //     contributions use an L2 evict-last policy;
@@ -40,7 +46,12 @@
 //     partials, then a deterministic last-CTA reduction over fixed slots;
 //   * convergence is decided on the device: the last CTA publishes l1 and a
 //     converged flag, later launches of the chain exit at once, and the host
-//     enqueues max_iterations launches with no round trip.
+//     enqueues the chain with no round trip (a CUDA-graph while loop ended by
+//     the kernel for chains of kLoopMinIters or more iterations);
+//   * the precision form's FP32 phase runs propagation-blocked on large
+//     graphs (pb_emit_kernel / pb_accum_kernel, below): messages streamed
+//     into per-partition pieces and summed as exact integers in shared
+//     memory instead of gathered.
 #include <cub/cub.cuh>
 
 #include <algorithm>
