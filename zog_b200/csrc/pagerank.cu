@@ -1884,10 +1884,25 @@ __global__ void __launch_bounds__(kPbThreads) pb_emit_kernel(PbArgs<OffT> Q) {
     const uint32_t lo = Q.blk_lo[I.b], n = Q.blk_n[I.b];
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sc[i] = c[lo + i];
     __syncthreads();
-    for (uint32_t p = I.lo + 4 * threadIdx.x; p < I.hi; p += 4 * blockDim.x) {
-      const uint2 s4 = __ldcs(reinterpret_cast<const uint2*>(Q.sl + p));
-      const float4 v = make_float4(sc[s4.x & 0xFFFFu], sc[s4.x >> 16], sc[s4.y & 0xFFFFu], sc[s4.y >> 16]);
-      __stcs(reinterpret_cast<float4*>(Q.msg + p), v);
+    // four steps per pass, their source loads issued first (more bytes in
+    // flight per thread)
+    const uint32_t step = 4 * blockDim.x;
+    for (uint32_t p0 = I.lo + 4 * threadIdx.x; p0 < I.hi; p0 += 4 * step) {
+      uint2 s4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t p = p0 + u * step;
+        s4[u] = p < I.hi ? __ldcs(reinterpret_cast<const uint2*>(Q.sl + p)) : make_uint2(0u, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t p = p0 + u * step;
+        if (p < I.hi) {
+          const float4 v = make_float4(sc[s4[u].x & 0xFFFFu], sc[s4[u].x >> 16], sc[s4[u].y & 0xFFFFu],
+                                       sc[s4[u].y >> 16]);
+          __stcs(reinterpret_cast<float4*>(Q.msg + p), v);
+        }
+      }
     }
     __syncthreads();
   }
