@@ -72,8 +72,10 @@ def test_rebuilt_graph_of_same_shape_reuses_tuned_configuration(native):
 
 def test_warm_start_and_solve_alternating(native):
     """Inference and solve take turns on one graph (the pattern whose
-    per-call allocations once stalled the pool): each round's start vector and
-    result are the same."""
+    per-call allocations once stalled the pool).  Inference adds the rows that
+    cross a chunk boundary with FP32 atomics, so its start vector varies in
+    the last bits between runs; the rounds' start vectors agree to 1e-4 (rel
+    L1) and their results to the solve's bound 2*d/(1-d)*tol."""
     import torch
 
     from zog_b200 import warm_start as W
@@ -94,8 +96,9 @@ def test_warm_start_and_solve_alternating(native):
             if firsts is None:
                 firsts = cur
             else:
-                assert np.array_equal(cur[0], firsts[0]) and np.array_equal(cur[1], firsts[1])
-                assert cur[2] == firsts[2]
+                assert np.abs(cur[0] - firsts[0]).sum() <= 1e-4 * np.abs(firsts[0]).sum()
+                assert np.abs(cur[1] - firsts[1]).sum() <= 12 * 1e-10
+                assert abs(cur[2] - firsts[2]) <= 1
         assert abs(firsts[1].sum() - 1.0) < 1e-9
     finally:
         net.destroy()

@@ -546,17 +546,66 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
   }
 }
 
+__global__ void k_bc_add(double* __restrict__ a, const double* __restrict__ b, uint32_t V) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+    a[v] += b[v];
+}
+
+// Batches rotate over kBcLanes streams ("lanes"), each with its own workspace
+// and score vector: while the host waits for one batch's forward levels (to
+// learn its depth), the other lanes' sweeps keep the GPU busy, and one lane's
+// next kernel fills the SMs that another's finishing kernel frees.  Batch b's
+// scores add up in lane b % kBcLanes's vector, and the vectors are added to
+// d_bc at the end in lane order: a fixed order, so the result is
+// deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count (1 = one stream).
+constexpr int kBcMaxLanes = 4;
+constexpr int kBcLanes = 2;
 template <typename OffT>
 static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {
   const uint32_t V = g->V;
   const uint64_t ns = sources.size();
   ZOGCU_TRY(ensure_heavy_lists(g, s));
-  BcWork W;
-  ZOGCU_TRY(W.alloc(g, ns, s, true));
-  if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W.src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, s));
+  const uint64_t nbatches = (ns + kBcBatch - 1) / kBcBatch;
+  int nlanes = kBcLanes;
+  if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) nlanes = std::max(1, std::min(kBcMaxLanes, std::atoi(env)));
+  nlanes = (int)std::min<uint64_t>((uint64_t)nlanes, std::max<uint64_t>(nbatches, 1));
+  // the extra score vectors are declared first and the extra streams next:
+  // on every exit the workspaces are freed, then the extra streams are
+  // drained and destroyed, and only then the vectors (freed on the caller's
+  // stream) go
+  DevBuf bcx[kBcMaxLanes];
+  StreamGuard sx[kBcMaxLanes];
+  cudaStream_t ss[kBcMaxLanes];
+  double* bcs[kBcMaxLanes];
+  cudaEvent_t ev = nullptr;
+  struct EventFree {
+    cudaEvent_t* e;
+    ~EventFree() {
+      if (*e) cudaEventDestroy(*e);
+    }
+  } evf{&ev};
+  ss[0] = s;
+  bcs[0] = d_bc;
+  if (nlanes > 1) {
+    ZOGCU_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (int w = 1; w < nlanes; ++w) {
+      ZOGCU_TRY(sx[w].init(nullptr));
+      ss[w] = sx[w].s;
+      ZOGCU_TRY(bcx[w].alloc((size_t)std::max<uint32_t>(V, 1) * 8, s));
+      ZOGCU_CUDA(cudaMemsetAsync(bcx[w].ptr, 0, (size_t)std::max<uint32_t>(V, 1) * 8, s));
+      bcs[w] = bcx[w].as<double>();
+    }
+    ZOGCU_CUDA(cudaEventRecord(ev, s));
+    for (int w = 1; w < nlanes; ++w) ZOGCU_CUDA(cudaStreamWaitEvent(ss[w], ev, 0));
+  }
+  BcWork W[kBcMaxLanes];
+  for (int w = 0; w < nlanes; ++w) {
+    ZOGCU_TRY(W[w].alloc(g, ns, ss[w], true));
+    if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W[w].src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, ss[w]));
+  }
   unsigned int* h_flags = nullptr;
-  ZOGCU_CUDA(cudaMallocHost(&h_flags, kFlagWords * 4));
+  ZOGCU_CUDA(cudaMallocHost(&h_flags, (size_t)kBcMaxLanes * kFlagWords * 4));
   struct HostFree {
     unsigned int* p;
     ~HostFree() { cudaFreeHost(p); }
@@ -565,32 +614,47 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   bool overflow = false;
   uint32_t max_depth = 0;
   uint64_t launches = 0;
-  for (uint64_t first = 0; first < ns; first += kBcBatch) {
+  for (uint64_t bi = 0; bi < nbatches; ++bi) {
+    const int lane_w = (int)(bi % (uint64_t)nlanes);
+    BcWork& Wb = W[lane_w];
+    const cudaStream_t sb = ss[lane_w];
+    double* const bcb = bcs[lane_w];
+    const uint64_t first = bi * kBcBatch;
     const int nb = (int)std::min<uint64_t>(kBcBatch, ns - first);
     uint32_t depth = 0;
-    ZOGCU_TRY(bc_forward_batch<OffT>(g, in_off, W, first, nb, s, &depth, &overflow, &launches, h_flags));
+    ZOGCU_TRY(bc_forward_batch<OffT>(g, in_off, Wb, first, nb, sb, &depth, &overflow, &launches,
+                                     h_flags + lane_w * kFlagWords));
     max_depth = std::max(max_depth, depth);
     // backward: levels depth .. 1 (the sources sit at level 0 and are excluded)
     const bool stored = depth < (uint32_t)kMaxStoredLevels;
-    unsigned long long* mnxt = W.mbuf_a.as<unsigned long long>();
-    unsigned long long* mcur = W.mbuf_b.as<unsigned long long>();
-    if (!stored) ZOGCU_CUDA(cudaMemsetAsync(mnxt, 0, (size_t)V * 8, s));
+    unsigned long long* mnxt = Wb.mbuf_a.as<unsigned long long>();
+    unsigned long long* mcur = Wb.mbuf_b.as<unsigned long long>();
+    if (!stored) ZOGCU_CUDA(cudaMemsetAsync(mnxt, 0, (size_t)V * 8, sb));
     for (uint32_t l = depth; l >= 1; --l) {
       if (stored) {
-        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(
-            V, out_off, g->out_col.as<uint32_t>(), W.level(l, V), W.level(l + 1, V), nullptr,
-            W.dist.as<uint32_t>(), W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0,
-            g->heavy_out.as<BcHeavy>(), g->n_heavy_out, W.hpart.as<double>(), W.harrive.as<unsigned int>());
+        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, sb>>>(
+            V, out_off, g->out_col.as<uint32_t>(), Wb.level(l, V), Wb.level(l + 1, V), nullptr,
+            Wb.dist.as<uint32_t>(), Wb.sigma.as<unsigned long long>(), Wb.q.as<double>(), bcb, l,
+            l == depth ? 1 : 0, g->heavy_out.as<BcHeavy>(), g->n_heavy_out, Wb.hpart.as<double>(),
+            Wb.harrive.as<unsigned int>());
       } else {
-        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, s>>>(
-            V, out_off, g->out_col.as<uint32_t>(), nullptr, mnxt, mcur, W.dist.as<uint32_t>(),
-            W.sigma.as<unsigned long long>(), W.q.as<double>(), d_bc, l, l == depth ? 1 : 0,
-            g->heavy_out.as<BcHeavy>(), g->n_heavy_out, W.hpart.as<double>(), W.harrive.as<unsigned int>());
+        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, sb>>>(
+            V, out_off, g->out_col.as<uint32_t>(), nullptr, mnxt, mcur, Wb.dist.as<uint32_t>(),
+            Wb.sigma.as<unsigned long long>(), Wb.q.as<double>(), bcb, l, l == depth ? 1 : 0,
+            g->heavy_out.as<BcHeavy>(), g->n_heavy_out, Wb.hpart.as<double>(), Wb.harrive.as<unsigned int>());
         std::swap(mnxt, mcur);
       }
       ZOGCU_CUDA(cudaGetLastError());
       ++launches;
     }
+  }
+  for (int w = 1; w < nlanes; ++w) {  // the other lanes' scores into d_bc, in lane order
+    ZOGCU_CUDA(cudaEventRecord(ev, ss[w]));
+    ZOGCU_CUDA(cudaStreamWaitEvent(s, ev, 0));
+    k_bc_add<<<std::max<unsigned>(1u, std::min<unsigned>((V + 255) / 256, 148u * 8)), 256, 0, s>>>(
+        d_bc, bcs[w], V);
+    ZOGCU_CUDA(cudaGetLastError());
+    ++launches;
   }
   if (stats) {
     stats->sources = ns;
