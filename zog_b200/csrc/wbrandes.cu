@@ -253,6 +253,11 @@ __global__ void __launch_bounds__(256) k_wb_delta(const uint32_t* __restrict__ o
   }
 }
 
+__global__ void k_wb_add(double* __restrict__ a, const double* __restrict__ b, uint32_t V) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+    a[v] += b[v];
+}
+
 unsigned wb_grid(uint64_t warps) {
   const uint64_t g = (warps * 32 + 255) / 256;
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)sm_count() * 8));
@@ -299,16 +304,8 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   const double* w = g->weighted ? g->out_w.as<double>() : nullptr;
   const size_t n = (size_t)std::max<uint32_t>(V, 1) * kWb;
   const size_t Vs = std::max<uint32_t>(V, 1);
-  DevBuf bdist, bsigma, bdelta, bround, bcnt, bm0, bm1, bm2, bwork, bflags, bsrc, bc, btn, btb;
-  ZOGCU_TRY(bdist.alloc(n * 8, s));
-  ZOGCU_TRY(bsigma.alloc(n * 8, s));
-  ZOGCU_TRY(bdelta.alloc(n * 8, s));
-  ZOGCU_TRY(bround.alloc(n * 4, s));
-  ZOGCU_TRY(bcnt.alloc(n * 4, s));
-  ZOGCU_TRY(bm0.alloc(Vs * 4, s));
-  ZOGCU_TRY(bm1.alloc(Vs * 4, s));
-  ZOGCU_TRY(bm2.alloc(Vs * 4, s));
   // work items: (node, first arc) per kWbChunk arcs of every node's out-row
+  DevBuf btn, btb;
   std::vector<uint32_t> h_off((size_t)V + 1), tn, tb;
   if (V) ZOGCU_CUDA(cudaMemcpyAsync(h_off.data(), off, ((size_t)V + 1) * 4, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
@@ -327,71 +324,123 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   const uint32_t* tnode = btn.as<uint32_t>();
   const uint32_t* tbeg = btb.as<uint32_t>();
   const size_t work_n = (size_t)V + 3 + 2 * kWbChain;
-  ZOGCU_TRY(bwork.alloc(work_n * 4, s));
-  ZOGCU_TRY(bflags.alloc(kFlags * 4, s));
-  ZOGCU_TRY(bsrc.alloc(kWb * 4, s));
-  ZOGCU_TRY(bc.alloc(Vs * 8, s));
-  ZOGCU_CUDA(cudaMemsetAsync(bc.ptr, 0, Vs * 8, s));
-  ZOGCU_CUDA(cudaMemsetAsync(bflags.ptr, 0, kFlags * 4, s));
-  uint32_t* flags = bflags.as<uint32_t>();
   if (w && E) {
-    k_wb_check_weights<<<wb_grid(E / 32 + 1), 256, 0, s>>>(w, E, flags);
+    DevBuf chk;
+    ZOGCU_TRY(chk.alloc(kFlags * 4, s));
+    ZOGCU_CUDA(cudaMemsetAsync(chk.ptr, 0, kFlags * 4, s));
+    k_wb_check_weights<<<wb_grid(E / 32 + 1), 256, 0, s>>>(w, E, chk.as<uint32_t>());
     ZOGCU_CUDA(cudaGetLastError());
     uint32_t bad = 0;
-    ZOGCU_CUDA(cudaMemcpyAsync(&bad, flags + kFlagBadWeight, 4, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(&bad, chk.as<uint32_t>() + kFlagBadWeight, 4, cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     if (bad) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "weighted betweenness needs positive finite weights");
   }
   const uint64_t nwork = std::max<uint32_t>(ntasks, V);
   const unsigned g_relax = wb_grid_of(k_wb_relax, nwork), g_count = wb_grid_of(k_wb_dagcount, nwork);
   const unsigned g_sigma = wb_grid_of(k_wb_sigma, nwork), g_delta = wb_grid_of(k_wb_delta, nwork);
-  unsigned long long* dist = bdist.as<unsigned long long>();
-  unsigned long long* sigma = bsigma.as<unsigned long long>();
-  double* delta = bdelta.as<double>();
-  uint32_t* round = bround.as<uint32_t>();
-  uint32_t* cnt = bcnt.as<uint32_t>();
-  uint32_t* masks[3] = {bm0.as<uint32_t>(), bm1.as<uint32_t>(), bm2.as<uint32_t>()};
-  uint32_t* work = bwork.as<uint32_t>();
-  const uint32_t* src = bsrc.as<uint32_t>();
+
+  // Batches alternate between two streams ("lanes"), each with its own state
+  // and score vector: while the host waits on one lane's rounds, the other
+  // lane's dependency rounds keep the GPU busy.  The second lane's scores are
+  // added to the first's at the end.  The score vectors are declared first
+  // and the second stream next, so on every exit the lanes' state is freed,
+  // then the stream is drained, and only then the vectors (on stream s) go.
+  const size_t nbatches = (sources.size() + kWb - 1) / kWb;
+  const char* env = std::getenv("ZOGCU_BC_STREAMS");
+  const int nlanes = (nbatches >= 2 && !(env && env[0] == '1')) ? 2 : 1;
+  DevBuf bcv[2];
+  StreamGuard s1g;
+  cudaStream_t ls[2] = {s, s};
+  cudaEvent_t ev = nullptr;
+  struct EventFree {
+    cudaEvent_t* e;
+    ~EventFree() {
+      if (*e) cudaEventDestroy(*e);
+    }
+  } evf{&ev};
+  for (int l = 0; l < nlanes; ++l) {
+    ZOGCU_TRY(bcv[l].alloc(Vs * 8, s));
+    ZOGCU_CUDA(cudaMemsetAsync(bcv[l].ptr, 0, Vs * 8, s));
+  }
+  if (nlanes == 2) {
+    ZOGCU_TRY(s1g.init(nullptr));
+    ls[1] = s1g.s;
+    ZOGCU_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    ZOGCU_CUDA(cudaEventRecord(ev, s));
+    ZOGCU_CUDA(cudaStreamWaitEvent(ls[1], ev, 0));
+  }
+  struct Lane {
+    DevBuf bdist, bsigma, bdelta, bround, bcnt, bm0, bm1, bm2, bwork, bflags, bsrc;
+  } L[2];
+  for (int l = 0; l < nlanes; ++l) {
+    Lane& A = L[l];
+    const cudaStream_t st = ls[l];
+    ZOGCU_TRY(A.bdist.alloc(n * 8, st));
+    ZOGCU_TRY(A.bsigma.alloc(n * 8, st));
+    ZOGCU_TRY(A.bdelta.alloc(n * 8, st));
+    ZOGCU_TRY(A.bround.alloc(n * 4, st));
+    ZOGCU_TRY(A.bcnt.alloc(n * 4, st));
+    ZOGCU_TRY(A.bm0.alloc(Vs * 4, st));
+    ZOGCU_TRY(A.bm1.alloc(Vs * 4, st));
+    ZOGCU_TRY(A.bm2.alloc(Vs * 4, st));
+    ZOGCU_TRY(A.bwork.alloc(work_n * 4, st));
+    ZOGCU_TRY(A.bflags.alloc(kFlags * 4, st));
+    ZOGCU_TRY(A.bsrc.alloc(kWb * 4, st));
+    ZOGCU_CUDA(cudaMemsetAsync(A.bflags.ptr, 0, kFlags * 4, st));
+  }
   EventTimer tm;
   ZOGCU_TRY(tm.start(s));
   uint64_t launches = 0;
   uint32_t deepest = 0;
   const uint32_t one = 1;
-  for (size_t b0 = 0; b0 < sources.size(); b0 += kWb) {
+  for (size_t bi = 0; bi < nbatches; ++bi) {
+    const int l = (int)(bi % (size_t)nlanes);
+    Lane& A = L[l];
+    const cudaStream_t st = ls[l];
+    unsigned long long* dist = A.bdist.as<unsigned long long>();
+    unsigned long long* sigma = A.bsigma.as<unsigned long long>();
+    double* delta = A.bdelta.as<double>();
+    uint32_t* round = A.bround.as<uint32_t>();
+    uint32_t* cnt = A.bcnt.as<uint32_t>();
+    uint32_t* masks[3] = {A.bm0.as<uint32_t>(), A.bm1.as<uint32_t>(), A.bm2.as<uint32_t>()};
+    uint32_t* work = A.bwork.as<uint32_t>();
+    uint32_t* flags = A.bflags.as<uint32_t>();
+    const uint32_t* src = A.bsrc.as<uint32_t>();
+    double* bcl = bcv[l].as<double>();
+    const size_t b0 = bi * kWb;
     const uint32_t ns = (uint32_t)std::min<size_t>(kWb, sources.size() - b0);
-    ZOGCU_CUDA(cudaMemcpyAsync(bsrc.ptr, sources.data() + b0, ns * 4, cudaMemcpyHostToDevice, s));
-    k_wb_init<<<wb_grid(V), 256, 0, s>>>(V, dist, sigma, delta, round, cnt, masks[0], masks[1]);
-    ZOGCU_CUDA(cudaMemsetAsync(masks[2], 0, Vs * 4, s));
-    k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
+    ZOGCU_CUDA(cudaMemcpyAsync(A.bsrc.ptr, sources.data() + b0, ns * 4, cudaMemcpyHostToDevice, st));
+    k_wb_init<<<wb_grid(V), 256, 0, st>>>(V, dist, sigma, delta, round, cnt, masks[0], masks[1]);
+    ZOGCU_CUDA(cudaMemsetAsync(masks[2], 0, Vs * 4, st));
+    k_wb_seed<<<1, kWb, 0, st>>>(src, ns, dist, sigma, round, masks[0]);
     ZOGCU_CUDA(cudaGetLastError());
-    ZOGCU_CUDA(cudaMemsetAsync(flags + kFlagMaxRound, 0, 4, s));
+    ZOGCU_CUDA(cudaMemsetAsync(flags + kFlagMaxRound, 0, 4, st));
     launches += 2;
     // phase 1: distances
-    ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, s));
-    ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, st));
+    ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, st));
     uint32_t r1 = 0;
-    ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
-      k_wb_relax<<<g_relax, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, masks[k % 3], masks[(k + 1) % 3],
-                                       masks[(k + 2) % 3], V, work, k);
+    ZOGCU_TRY(run_rounds(work, V, st, [&](uint32_t k) {
+      k_wb_relax<<<g_relax, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, masks[k % 3], masks[(k + 1) % 3],
+                                        masks[(k + 2) % 3], V, work, k);
     }, &r1));
     launches += r1;
     // phase 2: DAG in-counts, then sigma in topological rounds from the sources
-    k_wb_dagcount<<<g_count, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, cnt, flags);
-    for (int i = 0; i < 3; ++i) ZOGCU_CUDA(cudaMemsetAsync(masks[i], 0, Vs * 4, s));
-    k_wb_seed<<<1, kWb, 0, s>>>(src, ns, dist, sigma, round, masks[0]);
+    k_wb_dagcount<<<g_count, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, cnt, flags);
+    for (int i = 0; i < 3; ++i) ZOGCU_CUDA(cudaMemsetAsync(masks[i], 0, Vs * 4, st));
+    k_wb_seed<<<1, kWb, 0, st>>>(src, ns, dist, sigma, round, masks[0]);
     ZOGCU_CUDA(cudaGetLastError());
-    ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, s));
-    ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, s));
+    ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, st));
+    ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, st));
     uint32_t r2 = 0;
-    ZOGCU_TRY(run_rounds(work, V, s, [&](uint32_t k) {
-      k_wb_sigma<<<g_sigma, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, cnt, round, masks[k % 3],
-                                       masks[(k + 1) % 3], masks[(k + 2) % 3], V, work, flags, k);
+    ZOGCU_TRY(run_rounds(work, V, st, [&](uint32_t k) {
+      k_wb_sigma<<<g_sigma, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, cnt, round, masks[k % 3],
+                                        masks[(k + 1) % 3], masks[(k + 2) % 3], V, work, flags, k);
     }, &r2));
     launches += r2 + 2;
     uint32_t hf[kFlags];
-    ZOGCU_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s));
-    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    ZOGCU_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    ZOGCU_CUDA(cudaStreamSynchronize(st));
     if (hf[kFlagZeroArc])
       return fail(ZOGCU_ERR_INVALID_ARGUMENT,
                   "weighted betweenness: a shortest path holds an arc of effective length zero (fl(d + w) == d)");
@@ -399,23 +448,31 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     const uint32_t maxr = hf[kFlagMaxRound];
     deepest = std::max(deepest, maxr);
     for (int64_t r = maxr; r >= 0; --r)
-      k_wb_delta<<<g_delta, 256, 0, s>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, delta, round, src, ns,
-                                      bc.as<double>(), (uint32_t)r);
+      k_wb_delta<<<g_delta, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, delta, round, src, ns, bcl,
+                                       (uint32_t)r);
     ZOGCU_CUDA(cudaGetLastError());
     launches += (uint64_t)maxr + 1;
   }
+  if (nlanes == 2) {  // the second lane's scores into the first's, on stream s
+    ZOGCU_CUDA(cudaEventRecord(ev, ls[1]));
+    ZOGCU_CUDA(cudaStreamWaitEvent(s, ev, 0));
+    k_wb_add<<<wb_grid(Vs / 32 + 1), 256, 0, s>>>(bcv[0].as<double>(), bcv[1].as<double>(), V);
+    ZOGCU_CUDA(cudaGetLastError());
+    ++launches;
+  }
   ZOGCU_TRY(tm.stop(s));
-  uint32_t ovf = 0;
-  ZOGCU_CUDA(cudaMemcpyAsync(&ovf, flags + kFlagOverflow, 4, cudaMemcpyDeviceToHost, s));
+  uint32_t ovf[2] = {0, 0};
+  for (int l = 0; l < nlanes; ++l)
+    ZOGCU_CUDA(cudaMemcpyAsync(&ovf[l], L[l].bflags.as<uint32_t>() + kFlagOverflow, 4, cudaMemcpyDeviceToHost, s));
   if (V)
-    ZOGCU_CUDA(cudaMemcpyAsync(out, bc.ptr, (size_t)V * 8, dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                               s));
+    ZOGCU_CUDA(cudaMemcpyAsync(out, bcv[0].ptr, (size_t)V * 8,
+                               dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   if (stats) {
     stats->sources = sources.size();
     stats->elapsed_ms = tm.ms();
     stats->max_depth = deepest;
-    stats->sigma_overflow = ovf;
+    stats->sigma_overflow = (ovf[0] | ovf[1]) ? 1u : 0u;
     stats->launches = launches;
   }
   return ZOGCU_OK;
