@@ -9,7 +9,7 @@
 // from the uniform start 1/n -- the generalised form the CPU oracle's
 // og_pagerank_ext computes for one seed.
 //
-// B200 design: S seeds (64, 128 or 256 per pass) are the columns of node-major matrices
+// B200 design: S seeds (64 per pass; the kernel also builds for 128 and 256) are the columns of node-major matrices
 // X, C = X/deg (V x S, FP64), so every arc of the in-CSR gathers one
 // contiguous row of S values (2 KB at S = 256: whole lines, streamed) instead
 // of S scattered scalars.  The degree-ranked view and warp work items of the
@@ -449,14 +449,15 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   ZOGCU_TRY(ensure_task_list(g, 256, sg.s));
   const bool dev_out = opts && opts->device_pointers;
   const size_t V = g->V;
+  // Passes of 64 seeds: the 64-column kernel (62 registers) runs twice the
+  // warps per SM of the 256-column one (128 registers), which outweighs
+  // streaming the arc indices once per pass (256 seeds at scale 22: 4 x 64
+  // in 461 ms, 2 x 128 in 486 ms, 1 x 256 in 587 ms).
   for (uint32_t s0 = 0; s0 < num_seeds;) {
-    const uint32_t left = num_seeds - s0;
-    const uint32_t ns = std::min<uint32_t>(left, 256);
+    const uint32_t ns = std::min<uint32_t>(num_seeds - s0, 64);
     double* o = out_scores + (size_t)s0 * V;
     uint64_t* it = iterations ? iterations + s0 : nullptr;
-    if (ns > 128) ZOGCU_TRY(ppr_pass<256>(g, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
-    else if (ns > 64) ZOGCU_TRY(ppr_pass<128>(g, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
-    else ZOGCU_TRY(ppr_pass<64>(g, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
+    ZOGCU_TRY(ppr_pass<64>(g, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
     s0 += ns;
   }
   return ZOGCU_OK;
