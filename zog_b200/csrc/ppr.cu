@@ -297,10 +297,31 @@ unsigned grid_for(uint64_t n) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)sm_count() * 16));
 }
 
+// What every pass of a call needs from the host: the rank of every node, and
+// the sink of the uniform start -- x/n summed over the dangling nodes in
+// ascending order, as the reference's first sink (centrality.zig:926-931).
+struct PprHost {
+  std::vector<uint32_t> rank;
+  double sink0 = 0.0;
+  int load(const Graph* g, cudaStream_t s) {
+    const uint32_t V = g->V;
+    rank.resize(V);
+    std::vector<uint32_t> deg(V);
+    ZOGCU_CUDA(cudaMemcpyAsync(rank.data(), g->pr.rank.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(deg.data(), g->out_deg.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    const double n_f = (double)V;
+    const double x0 = 1.0 / n_f;
+    for (uint32_t v = 0; v < V; ++v)
+      if (deg[v] == 0) sink0 += x0 / n_f;
+    return ZOGCU_OK;
+  }
+};
+
 // One pass over up to S seeds.
 template <int S>
-int ppr_pass(Graph* g, const uint32_t* seeds, uint32_t ns, double damping, uint64_t max_iter, double tol, double* out,
-             bool dev_out, uint64_t* iters_out, zogcu_stats* stats, cudaStream_t s) {
+int ppr_pass(Graph* g, const PprHost& H, const uint32_t* seeds, uint32_t ns, double damping, uint64_t max_iter,
+             double tol, double* out, bool dev_out, uint64_t* iters_out, zogcu_stats* stats, cudaStream_t s) {
   const PrSchedule& P = g->pr;
   const PrTaskList& L = g->pr.lists[1];  // row blocks of up to 256 arcs
   const uint32_t V = g->V;
@@ -315,25 +336,15 @@ int ppr_pass(Graph* g, const uint32_t* seeds, uint32_t ns, double damping, uint6
   ZOGCU_CUDA(cudaMemsetAsync(Y.ptr, 0, mat, s));
   ZOGCU_CUDA(cudaMemsetAsync(arrive.ptr, 0, (size_t)V * 4, s));
   // per-column state: seeds as ranks (padding columns never start)
-  std::vector<uint32_t> h_rank(V);
-  ZOGCU_CUDA(cudaMemcpyAsync(h_rank.data(), P.rank.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
-  std::vector<uint32_t> h_deg(V);
-  ZOGCU_CUDA(cudaMemcpyAsync(h_deg.data(), g->out_deg.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, s));
-  ZOGCU_CUDA(cudaStreamSynchronize(s));
   std::vector<uint32_t> h_seed(S, kNoSeed);
   std::vector<int> h_active(S, 0);
   for (uint32_t i = 0; i < ns; ++i) {
-    h_seed[i] = h_rank[seeds[i]];
+    h_seed[i] = H.rank[seeds[i]];
     h_active[i] = 1;
   }
-  // sink of the uniform start: x/n summed over the dangling nodes in ascending
-  // order, as the reference's first sink (centrality.zig:926-931)
   const double n_f = (double)V;
   const double x0 = 1.0 / n_f;
-  double sink0 = 0.0;
-  for (uint32_t v = 0; v < V; ++v)
-    if (h_deg[v] == 0) sink0 += x0 / n_f;
-  std::vector<double> h_sink(S, sink0);
+  std::vector<double> h_sink(S, H.sink0);
   ZOGCU_TRY(seed_rank.alloc(S * 4, s));
   ZOGCU_TRY(active.alloc(S * 4, s));
   ZOGCU_TRY(iters.alloc(S * 8, s));
@@ -453,11 +464,13 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   // warps per SM of the 256-column one (128 registers), which outweighs
   // streaming the arc indices once per pass (256 seeds at scale 22: 4 x 64
   // in 461 ms, 2 x 128 in 486 ms, 1 x 256 in 587 ms).
+  PprHost H;
+  ZOGCU_TRY(H.load(g, sg.s));
   for (uint32_t s0 = 0; s0 < num_seeds;) {
     const uint32_t ns = std::min<uint32_t>(num_seeds - s0, 64);
     double* o = out_scores + (size_t)s0 * V;
     uint64_t* it = iterations ? iterations + s0 : nullptr;
-    ZOGCU_TRY(ppr_pass<64>(g, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
+    ZOGCU_TRY(ppr_pass<64>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
     s0 += ns;
   }
   return ZOGCU_OK;
