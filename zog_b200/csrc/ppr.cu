@@ -460,17 +460,29 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   ZOGCU_TRY(ensure_task_list(g, 256, sg.s));
   const bool dev_out = opts && opts->device_pointers;
   const size_t V = g->V;
-  // Passes of 64 seeds: the 64-column kernel (62 registers) runs twice the
-  // warps per SM of the 256-column one (128 registers), which outweighs
-  // streaming the arc indices once per pass (256 seeds at scale 22: 4 x 64
-  // in 461 ms, 2 x 128 in 486 ms, 1 x 256 in 587 ms).
+  // Pass width: on graphs of 2^19 nodes and more, passes of 64 seeds -- the
+  // 64-column kernel (62 registers) runs twice the warps per SM of the
+  // 256-column one (128 registers), which outweighs streaming the arc indices
+  // once per pass (256 seeds: 422 against 570 ms at scale 22, 98 against
+  // 114 ms at scale 20); on smaller graphs one pass of 256 (47 against 58 ms
+  // at scale 18).
   PprHost H;
   ZOGCU_TRY(H.load(g, sg.s));
+  uint32_t width = V < (1u << 19) ? 256u : 64u;  // ZOGCU_PPR_PASS=64/128/256 overrides
+  if (const char* e = std::getenv("ZOGCU_PPR_PASS")) {
+    const int w = std::atoi(e);
+    if (w == 64 || w == 128 || w == 256) width = (uint32_t)w;
+  }
   for (uint32_t s0 = 0; s0 < num_seeds;) {
-    const uint32_t ns = std::min<uint32_t>(num_seeds - s0, 64);
+    const uint32_t ns = std::min<uint32_t>(num_seeds - s0, width);
     double* o = out_scores + (size_t)s0 * V;
     uint64_t* it = iterations ? iterations + s0 : nullptr;
-    ZOGCU_TRY(ppr_pass<64>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
+    if (ns > 128)
+      ZOGCU_TRY(ppr_pass<256>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
+    else if (ns > 64)
+      ZOGCU_TRY(ppr_pass<128>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
+    else
+      ZOGCU_TRY(ppr_pass<64>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
     s0 += ns;
   }
   return ZOGCU_OK;
