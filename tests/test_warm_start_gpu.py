@@ -119,7 +119,7 @@ def test_weight_file_round_trip(native, tmp_path):
 
 def test_training_on_gpu_gains_over_uniform_start(native):
     """Train on small seeded graphs with the CUDA kernels, then solve held-out
-    graphs from both starts: the same answer (the plain method judges), and on
+    graphs from both starts: the same answer (the power iteration decides it), and on
     the skewed R-MAT graph a start much closer to it and fewer iterations; the
     learned start never costs more than one extra iteration."""
     import torch

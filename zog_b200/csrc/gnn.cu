@@ -1,6 +1,6 @@
 // gnn.cu -- the learned PageRank warm start: a small message-passing network
 // whose prediction is only the start vector of the power iteration, which
-// then runs to the same residual (so the plain method stays the judge).
+// then runs to the same residual (so the plain method alone decides the result).
 //
 // Model (hidden width 64; FP32 master weights, BF16 weights and BF16 operands
 // in the dense layers, FP32 accumulation everywhere):

@@ -5,7 +5,7 @@ The reference always starts PageRank from the uniform vector
 (hidden 64, BF16 weights, FP32 accumulation; kernels in csrc/gnn.cu) predicts
 log(n * pagerank) from degree features, its softmax becomes the start vector,
 and power iteration still runs to the caller's tolerance -- the plain method
-decides the result and judges the network.
+decides the result; the network only sets where it starts.
 
 Training data are seeded synthetic graphs (R-MAT scales 12-18, Barabasi-Albert
 m = 2-16, Watts-Strogatz k = 10, p = 0.1; n = 4k-262k); targets are FP64
