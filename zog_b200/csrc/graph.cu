@@ -310,6 +310,7 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
 
   DevBuf cnt;
   ZOGCU_TRY(cnt.alloc((size_t)(V + 1) * 8, s));
+  PhaseTrace tr("csr_build", s);
   if (E > 0) {
     const int bits = bits_for(V);
     bool sorted = src_sorted > 0;
@@ -385,6 +386,7 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
       ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
       keys_out = ks2.as<uint32_t>();
     }
+    tr.mark(sorted ? "out-CSR (sorted sources)" : "out-CSR (radix sort)");
     // (2) stable sort of (dst, src) pairs by dst: sources stay ascending
     size_t tmp2 = 0;
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
@@ -395,6 +397,7 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
     }
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
                                                keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
+    tr.mark("in-CSR radix sort");
     ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
     k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks.as<uint32_t>(), E, cnt.as<unsigned long long>());
     ZOGCU_CUDA(cudaGetLastError());
@@ -416,6 +419,7 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
     ZOGCU_CUDA(cudaGetLastError());
   }
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  tr.mark("in offsets, degrees, 32-bit offsets");
   return ZOGCU_OK;
 }
 
