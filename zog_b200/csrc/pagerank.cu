@@ -866,15 +866,79 @@ __global__ void k_rank_invert(const uint32_t* __restrict__ perm, uint32_t V, uin
 
 // Row p of the ranked in-CSR = row perm[p] of the in-CSR with every source
 // replaced by its rank; the order inside the row is kept.
+// Rows of at most kLongRow arcs: a warp takes 32 consecutive ranked rows,
+// each lane loads one row's source start, length and output start (so the
+// perm -> in_off lookups of 32 rows overlap), and a warp scan numbers the
+// group's arcs.  The warp then copies them 32 at a time across row
+// boundaries: the lane for arc t finds its row as the last lane whose scan
+// offset is <= t (five shuffles), and four such rounds issue their loads
+// together.  Longer rows count as empty here; k_rank_rows_long copies them
+// with one CTA per row, because ranking by out-degree gathers the rows of
+// largest in-degree into the first groups, where one warp would copy them
+// all in turn.
+constexpr uint32_t kLongRow = 1024;
+
 __global__ void k_rank_rows(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ rank, uint32_t V,
                             const uint64_t* __restrict__ in_off, const uint32_t* __restrict__ in_col,
-                            const uint64_t* __restrict__ poff, uint32_t* __restrict__ pcol) {
+                            const uint64_t* __restrict__ poff, uint32_t* __restrict__ pcol,
+                            uint32_t* __restrict__ long_rows, unsigned int* __restrict__ n_long) {
   const int lane = threadIdx.x & 31;
   const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t p = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; p < V; p += nw) {
+  for (uint64_t p0 = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * 32; p0 < V; p0 += nw * 32) {
+    const uint64_t p = p0 + lane;
+    unsigned long long src = 0ull, dst = 0ull;
+    uint32_t len = 0;
+    if (p < V) {
+      const uint32_t v = perm[p];
+      src = in_off[v];
+      const uint64_t n = in_off[v + 1] - src;
+      dst = poff[p];
+      if (n > kLongRow) long_rows[atomicAdd(n_long, 1u)] = (uint32_t)p;
+      else len = (uint32_t)n;
+    }
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t pre = incl - len;  // empty, long and past-V rows add nothing
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);  // <= 32 * kLongRow
+    for (uint32_t base = 0; base < total; base += 4 * 32) {
+      unsigned long long k[4], q[4];
+      uint32_t c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t t = base + u * 32 + lane;
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+          if (__shfl_sync(0xffffffffu, pre, j + step) <= t) j += step;
+        const uint32_t off = t - __shfl_sync(0xffffffffu, pre, j);
+        k[u] = __shfl_sync(0xffffffffu, src, j) + off;
+        q[u] = __shfl_sync(0xffffffffu, dst, j) + off;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c[u] = (base + u * 32 + lane < total) ? in_col[k[u]] : 0u;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (base + u * 32 + lane < total) pcol[q[u]] = rank[c[u]];
+    }
+  }
+}
+
+// The rows longer than kLongRow listed by k_rank_rows, one CTA per row.
+__global__ void k_rank_rows_long(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ rank,
+                                 const uint64_t* __restrict__ in_off, const uint32_t* __restrict__ in_col,
+                                 const uint64_t* __restrict__ poff, const uint32_t* __restrict__ long_rows,
+                                 const unsigned int* __restrict__ n_long, uint32_t* __restrict__ pcol) {
+  const unsigned int n = *n_long;
+  for (unsigned int i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t p = long_rows[i];
     const uint32_t v = perm[p];
-    const uint64_t s = in_off[v], e = in_off[v + 1], d = poff[p];
-    for (uint64_t k = s + lane; k < e; k += 32) pcol[d + (k - s)] = rank[in_col[k]];
+    const uint64_t s = in_off[v], len = in_off[v + 1] - s, d = poff[p];
+#pragma unroll 4
+    for (uint64_t k = threadIdx.x; k < len; k += blockDim.x) pcol[d + k] = rank[in_col[s + k]];
   }
 }
 
@@ -906,6 +970,7 @@ static unsigned grid_1d(uint64_t n) {
 static int build_ranked_view(Graph* g, cudaStream_t s) {
   PrSchedule& P = g->pr;
   const uint32_t V = g->V;
+  PhaseTrace tr("ranked_view", s);
   ZOGCU_TRY(P.rank.alloc((size_t)V * 4));
   ZOGCU_TRY(P.perm.alloc((size_t)V * 4));
   ZOGCU_TRY(P.deg.alloc((size_t)V * 4));
@@ -923,6 +988,7 @@ static int build_ranked_view(Graph* g, cudaStream_t s) {
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, key.as<uint32_t>(), key2.as<uint32_t>(),
                                                ids.as<uint32_t>(), P.perm.as<uint32_t>(), (int64_t)V, 0, 32, s));
   }
+  tr.mark("ranking sort");
   DevBuf cnt, poff64;
   ZOGCU_TRY(cnt.alloc(((size_t)V + 1) * 8, s));
   ZOGCU_TRY(poff64.alloc(((size_t)V + 1) * 8, s));
@@ -941,12 +1007,27 @@ static int build_ranked_view(Graph* g, cudaStream_t s) {
                                              poff64.as<unsigned long long>(), (int64_t)V + 1, s));
   }
   ZOGCU_TRY(P.col.alloc((g->E + 4) * 4));
+  tr.mark("ranks, row offsets, column allocation");
   // k_rank_rows writes every arc; only the 4 padding entries need zeros
   ZOGCU_CUDA(cudaMemsetAsync(P.col.as<uint32_t>() + g->E, 0, 4 * 4, s));
-  k_rank_rows<<<grid_1d((uint64_t)V * 32), 256, 0, s>>>(P.perm.as<uint32_t>(), P.rank.as<uint32_t>(), V,
-                                                         g->in_off64.as<uint64_t>(), g->in_col.as<uint32_t>(),
-                                                         poff64.as<uint64_t>(), P.col.as<uint32_t>());
-  ZOGCU_CUDA(cudaGetLastError());
+  {
+    // at most E / kLongRow rows are long
+    DevBuf lrows, nl;
+    ZOGCU_TRY(lrows.alloc((g->E / kLongRow + 1) * 4, s));
+    ZOGCU_TRY(nl.alloc(4, s));
+    ZOGCU_CUDA(cudaMemsetAsync(nl.ptr, 0, 4, s));
+    k_rank_rows<<<grid_1d(V), 256, 0, s>>>(P.perm.as<uint32_t>(), P.rank.as<uint32_t>(), V,
+                                            g->in_off64.as<uint64_t>(), g->in_col.as<uint32_t>(),
+                                            poff64.as<uint64_t>(), P.col.as<uint32_t>(), lrows.as<uint32_t>(),
+                                            nl.as<unsigned int>());
+    ZOGCU_CUDA(cudaGetLastError());
+    k_rank_rows_long<<<sm_count() * 4, 512, 0, s>>>(P.perm.as<uint32_t>(), P.rank.as<uint32_t>(),
+                                                    g->in_off64.as<uint64_t>(), g->in_col.as<uint32_t>(),
+                                                    poff64.as<uint64_t>(), lrows.as<uint32_t>(),
+                                                    nl.as<unsigned int>(), P.col.as<uint32_t>());
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  tr.mark("ranked rows");
   if (g->offsets32) {
     ZOGCU_TRY(P.off.alloc(((size_t)V + 1) * 4));
     k_off_narrow<<<grid_1d(V + 1), 256, 0, s>>>(poff64.as<uint64_t>(), P.off.as<uint32_t>(), (uint64_t)V + 1);
