@@ -834,8 +834,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="zog", choices=["zog", "reference"])
-    ap.add_argument("--steps-e2e", type=int, default=3)
-    ap.add_argument("--warmup-e2e", type=int, default=1)
+    ap.add_argument("--steps-e2e", type=int, default=5)
+    ap.add_argument("--warmup-e2e", type=int, default=3)
     ap.add_argument("--bc-steps", type=int, default=0, help="Brandes steps of 4,096 sources (0 = all sources)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-brandes", action="store_true")
