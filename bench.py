@@ -57,6 +57,8 @@ PPR_SCALE, PPR_EF, PPR_SEED, PPR_SEEDS = 22, 16, 1022, 256
 BCB_SCALE, BCB_EF, BCB_SEED, BCB_SOURCES = 18, 16, 1018, 4096
 WBC_SOURCES, WBC_WSEED = 1024, 77                # weighted Brandes: sources timed, weight seed
 DAMPING, TOL, MAX_ITER = 0.85, 1e-9, 200
+# the tightly converged FP64 vector every result's error is reported against
+TIGHT_TOL = 1e-14
 # kernels one zogcu_gnn_predict launches: features, chunk rows, 3 x (SpMM,
 # dense), head, and the 4 softmax kernels
 GNN_PREDICT_LAUNCHES = 13
@@ -218,32 +220,55 @@ def barrier(ws):
 # CPU baseline: the oracle (a loop-for-loop restatement of the reference's
 # single-threaded Zig code) on a bounded sample of the same workload.
 # --------------------------------------------------------------------------
-def cpu_pagerank_sample(V, in_off, in_col, outdeg, iters_full, budget_s=12.0):
+def host_threads() -> int:
+    """Host threads this process may run on (the CPU baseline uses all of them)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def pr_config(V, E):
+    """The PageRank workload both arms report (identical dicts)."""
+    return {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 uniform start, d={DAMPING}, "
+                        f"tol={TOL}, max_iter={MAX_ITER}", "vertices": int(V), "arcs": int(E),
+            "l2": "inputs larger than L2", "parallelism": "single"}
+
+
+def cpu_pagerank_full(V, in_off, in_col, outdeg, threads):
+    """One full solve of the reference loop (oracle restatement) with its row
+    sums spread over `threads` host threads; iterates are bit for bit the
+    single-threaded loop's.  Returns (ms, iterations, residual)."""
     from oracle import oracle as O
 
     O.build()
-    k = 1
-    _, _, _, secs = O.pagerank_csr(V, in_off, in_col, outdeg, DAMPING, 1, 0.0)
-    per_iter = secs
-    k_more = max(1, min(int(budget_s / max(per_iter, 1e-3)), 10))
-    _, _, _, secs = O.pagerank_csr(V, in_off, in_col, outdeg, DAMPING, k_more, 0.0)
-    per_iter = secs / k_more
-    k = k_more
-    return per_iter * iters_full * 1e3, k, per_iter
+    _, it, l1, secs = O.pagerank_csr_mt(V, in_off, in_col, outdeg, DAMPING, MAX_ITER, TOL, threads=threads)
+    return secs * 1e3, it, l1
 
 
-def cpu_brandes_sample(V, out_off, out_col, arcs, budget_s=12.0):
+def cpu_pagerank_single_thread_iteration(V, in_off, in_col, outdeg, iterations=2):
+    """ms per iteration of the single-threaded reference loop (the reference's
+    own threading), from `iterations` iterations over the full graph."""
     from oracle import oracle as O
 
     O.build()
-    n = 16
-    _, _, secs = O.betweenness_csr_sources(V, out_off, out_col, np.arange(n, dtype=np.uint32))
-    per_src = secs / n
-    n2 = int(min(max(budget_s / max(per_src, 1e-6), 16), V))
-    _, _, secs = O.betweenness_csr_sources(V, out_off, out_col, np.arange(n2, dtype=np.uint32))
-    per_src = secs / n2
-    gteps = arcs / per_src / 1e9
-    return gteps, n2, per_src
+    _, _, _, secs = O.pagerank_csr(V, in_off, in_col, outdeg, DAMPING, iterations, 0.0)
+    return secs * 1e3 / iterations
+
+
+def cpu_brandes_sample(V, out_off, out_col, arcs, threads, sources=4096):
+    """GTEPS of the reference Brandes loop (oracle restatement) over the first
+    `sources` sources, the sources split over `threads` host threads."""
+    import time as _t
+
+    from oracle import oracle as O
+
+    O.build()
+    n = int(min(sources, V))
+    t0 = _t.perf_counter()
+    O.betweenness_csr_sources_mt(V, out_off, out_col, np.arange(n, dtype=np.uint32), threads=threads)
+    secs = _t.perf_counter() - t0
+    return n * arcs / secs / 1e9, n, secs
 
 
 def host_graph(scale, ef, seed, directed):
@@ -259,41 +284,54 @@ def host_graph(scale, ef, seed, directed):
 # reference arm
 # --------------------------------------------------------------------------
 def run_reference(args):
+    """The reference's CPU PageRank (the oracle restatement of
+    centrality.zig:858-965) on this host's cores, on the same workload as the
+    library arm.  Each timed step is one full solve from the uniform start to
+    L1 < tol; the row sums run on every host thread, and the iterates are bit
+    for bit the single-threaded loop's.  Warm-up steps run two iterations each
+    (they page the arrays in and start the threads).  If the solves are slow
+    enough that `steps` of them would exceed --ref-budget seconds, fewer are
+    timed and the line says how many."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     from oracle import oracle as O
 
     O.build()
+    threads = host_threads()
     V, f, t = host_graph(PR_SCALE, PR_EF, PR_SEED, True)
     in_off, in_col, deg = O.in_csr_from_edges(V, f, t)
     del f, t
-    iters_full = int(args.ref_pr_iterations)
-    step_ms = []
-    for i in range(args.warmup + args.steps):
-        # each step: a bounded sample of the solve -- k iterations of the
-        # reference loop over the full graph, extrapolated to the full solve
-        _, _, _, secs = O.pagerank_csr(V, in_off, in_col, deg, DAMPING, args.ref_iters_per_step, 0.0)
-        if i >= args.warmup:
-            step_ms.append(secs / args.ref_iters_per_step * iters_full * 1e3)
+    for _ in range(args.warmup):
+        O.pagerank_csr_mt(V, in_off, in_col, deg, DAMPING, 2, 0.0, threads=threads)
+    step_ms, its, res = [], [], []
+    t_start = time.perf_counter()
+    for i in range(args.steps):
+        ms_i, it, l1 = cpu_pagerank_full(V, in_off, in_col, deg, threads)
+        step_ms.append(ms_i)
+        its.append(it)
+        res.append(l1)
+        if time.perf_counter() - t_start + ms_i / 1e3 > args.ref_budget:
+            break
     ms = float(np.mean(step_ms))
     Vb, fb, tb = host_graph(BC_SCALE, BC_EF, BC_SEED, False)
     ag_off, ag_col = _successor_csr_undirected(Vb, fb, tb)
-    gteps, nsrc, per_src = cpu_brandes_sample(Vb, ag_off, ag_col, len(fb), budget_s=args.cpu_budget)
+    gteps, nsrc, bsecs = cpu_brandes_sample(Vb, ag_off, ag_col, len(fb), threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT)",
-        "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 uniform start, d={DAMPING}, "
-                               f"tol={TOL}, max_iter={MAX_ITER}", "vertices": int(V), "arcs": int(len(in_col)),
-                   "iterations": iters_full, "l2": "inputs larger than L2", "parallelism": "single"},
-        "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
-                         "sample": f"{args.ref_iters_per_step} iterations of the reference PageRank loop "
-                                   f"(oracle restatement, 1 thread) over the full scale-{PR_SCALE} graph per step, "
-                                   f"extrapolated to {iters_full} iterations; preprocessing excluded"},
+        "steps": len(step_ms), "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded R-MAT)", "config": pr_config(V, len(in_col)),
+        "result": {"iterations": int(its[-1]), "residual": float(res[-1])},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"{len(step_ms)} full solves ({its[-1]} iterations each, measured) of the "
+                                   f"reference PageRank loop (oracle restatement) over the scale-{PR_SCALE} graph, "
+                                   f"row sums on {threads} host threads, iterates bit-identical to the "
+                                   f"single-threaded loop; preprocessing excluded"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "brandes": {"gteps": gteps, "sources_timed": nsrc, "arcs": int(len(fb)),
-                    "sample": f"{nsrc} sources of the all-sources run, 1 thread"},
+        "brandes": {"gteps": gteps, "sources_timed": nsrc, "arcs": int(len(fb)), "seconds": bsecs,
+                    "sample": f"the first {nsrc} sources of undirected rmat{BC_SCALE}, "
+                              f"sources split over {threads} host threads"},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -326,7 +364,7 @@ def _timed(stream, steps, fn):
     return e0.elapsed_time(e1) / max(steps, 1), res
 
 
-def learned_start_block(N, G, like, ms_uniform, it_uniform, args, stream, ws):
+def learned_start_block(N, G, like, ms_uniform, it_uniform, args, stream, ws, x_tight=None):
     """Solve from the shipped network's start and compare with the FP64
     uniform-start solve of the same graph (timed before: ms_uniform)."""
     import torch
@@ -360,6 +398,8 @@ def learned_start_block(N, G, like, ms_uniform, it_uniform, args, stream, ws):
            "start_l1_error_learned": float((x0 - x_uniform).abs().sum()),
            "start_l1_error_uniform": float((x_uniform - 1.0 / max(n_live, 1)).abs().sum()),
            "weights": "zog_b200/data/warm_start.zogn"}
+    if x_tight is not None:
+        res["rel_l1_vs_tight_fp64"] = float((xl - x_tight).abs().sum()) / float(x_tight.abs().sum())
     nl = args.steps * (GNN_PREDICT_LAUNCHES + int(sts[-1]["launches"])) + args.steps * GNN_PREDICT_LAUNCHES
     net.destroy()
     del x0, xl, x_uniform
@@ -405,20 +445,29 @@ def ba_block(N, args, stream, ws):
         out[name] = (max_over_ranks(t, ws), sts[-1])
         launches += sum(int(st["launches"]) for st in sts) + (args.steps * GNN_PREDICT_LAUNCHES if name == "learned" else 0)
     den = float(x64.abs().sum())
+    xt = torch.empty_like(x64)
+    stt = B.pagerank_device(xt.data_ptr(), DAMPING, MAX_ITER, TIGHT_TOL, stream=sp)
+    torch.cuda.synchronize()
+    dent = float(xt.abs().sum())
     res = {"workload": f"directed barabasi-albert n={BA_N} m={BA_M} seed={BA_SEED}", "vertices": V, "arcs": E,
+           "tight_fp64": {"tol": TIGHT_TOL, "iterations": int(stt["iterations"]), "residual": float(stt["residual"])},
            "generate_s": gen_s,
-           "fp64": {"ms": out["fp64"][0], "iterations": int(out["fp64"][1]["iterations"])},
+           "fp64": {"ms": out["fp64"][0], "iterations": int(out["fp64"][1]["iterations"]),
+                    "rel_l1_vs_tight_fp64": float((x64 - xt).abs().sum()) / dent},
            "mixed": {"ms": out["mixed"][0], "iterations": int(out["mixed"][1]["iterations"]),
                      "fp64_polish_iterations": int(out["mixed"][1]["polish_iterations"]),
                      "speedup_vs_fp64": out["fp64"][0] / out["mixed"][0],
-                     "rel_l1_vs_fp64": float((xm - x64).abs().sum()) / den},
+                     "rel_l1_vs_fp64": float((xm - x64).abs().sum()) / den,
+                     "rel_l1_vs_tight_fp64": float((xm - xt).abs().sum()) / dent},
            "learned": {"ms": out["learned"][0], "iterations": int(out["learned"][1]["iterations"]),
                        "speedup_vs_fp64_uniform": out["fp64"][0] / out["learned"][0],
                        "rel_l1_vs_fp64": float((xl - x64).abs().sum()) / den,
+                       "rel_l1_vs_tight_fp64": float((xl - xt).abs().sum()) / dent,
                        "start_l1_error_learned": float((x0 - x64).abs().sum()),
                        "start_l1_error_uniform": float((x64 - 1.0 / V).abs().sum())}}
     net.destroy()
     B.destroy()
+    del xt
     return res, launches
 
 
@@ -647,6 +696,16 @@ def run_zog(args):
     hbm_peak, peak_kind = peaks()
     achieved = bytes_per_iter / (t_iter_ms * 1e-3) / 1e9
 
+    # the tightly converged FP64 vector (same kernels, tol 1e-14) that every
+    # result's error is reported against
+    x_tight = torch.empty_like(out)
+    st_t = G.pagerank_device(x_tight.data_ptr(), DAMPING, MAX_ITER, TIGHT_TOL, stream=sp)
+    G.pagerank_device(out.data_ptr(), DAMPING, MAX_ITER, TOL, stream=sp)
+    torch.cuda.synchronize()
+    den_t = float(x_tight.abs().sum())
+    tight = {"tol": TIGHT_TOL, "iterations": int(st_t["iterations"]), "residual": float(st_t["residual"]),
+             "fp64_rel_l1": float((out - x_tight).abs().sum()) / den_t}
+
     # ---------------- precision form: FP32 SpMV + FP64 polish ----------------
     mixed = None
     if not args.no_mixed:
@@ -665,16 +724,18 @@ def run_zog(args):
         torch.cuda.synchronize()
         mms = max_over_ranks(m0.elapsed_time(m1) / args.steps, ws)
         err = float((outm - x64).abs().sum() / x64.abs().sum())
+        err_t = float((outm - x_tight).abs().sum()) / den_t
         mixed = {"ms": mms, "speedup_vs_fp64": ms / mms, "iterations": int(stm["iterations"]),
                  "fp64_polish_iterations": int(stm["polish_iterations"]), "residual": float(stm["residual"]),
-                 "rel_l1_vs_fp64": err, "bound": "rel L1 <= 2*d/(1-d)*tol = %.2e" % (2 * DAMPING / (1 - DAMPING) * TOL)}
+                 "rel_l1_vs_fp64": err, "rel_l1_vs_tight_fp64": err_t, "bound": "rel L1 <= 2*d/(1-d)*tol = %.2e" % (2 * DAMPING / (1 - DAMPING) * TOL)}
         del x64, outm
 
     # ---------------- learned warm start on the same graph ----------------
     learned = None
     if not args.no_learned:
-        learned, nl = learned_start_block(N, G, out, ms, iterations, args, stream, ws)
+        learned, nl = learned_start_block(N, G, out, ms, iterations, args, stream, ws, x_tight=x_tight)
         launches += nl
+    del x_tight
 
     # ---------------- e2e through the C ABI with host buffers ----------------
     e2e = None
@@ -712,11 +773,14 @@ def run_zog(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         ih, ic, _, _, deg = G.export_csr()
-        cpu_ms, k, per_iter = cpu_pagerank_sample(V, ih, ic, deg, iterations, budget_s=args.cpu_budget)
-        cpu = {"value": cpu_ms, "unit": "ms", "cores": 1, "kind": "port",
-               "sample": f"{k} iterations of the reference PageRank loop (oracle restatement, 1 thread) over "
-                         f"the full scale-{PR_SCALE} graph, extrapolated to {iterations} iterations; "
-                         f"preprocessing excluded ({per_iter * 1e3:.0f} ms/iteration)"}
+        threads = host_threads()
+        cpu_ms, cpu_it, _ = cpu_pagerank_full(V, ih, ic, deg, threads)
+        st_iter = cpu_pagerank_single_thread_iteration(V, ih, ic, deg)
+        cpu = {"value": cpu_ms, "unit": "ms", "cores": threads, "kind": "port",
+               "sample": f"one full solve ({cpu_it} iterations, measured) of the reference PageRank loop "
+                         f"(oracle restatement) over the full scale-{PR_SCALE} graph, row sums on {threads} host "
+                         f"threads with iterates bit-identical to the single-threaded loop; preprocessing excluded",
+               "single_thread_ms_per_iteration": st_iter}
         del ih, ic
     G.destroy()
     torch.cuda.empty_cache()
@@ -780,9 +844,11 @@ def run_zog(args):
                                f"{BC_STEP_SOURCES} sources per step"}
         if rank == 0 and ws == 1 and not args.no_cpu_baseline:
             _, _, oo, oc, _ = B.export_csr()
-            cg, nsrc, per_src = cpu_brandes_sample(Vb, oo, oc, Eb, budget_s=args.cpu_budget)
-            bc_line["cpu_baseline"] = {"gteps": cg, "cores": 1, "kind": "port",
-                                       "sample": f"{nsrc} sources of the same graph, oracle restatement, 1 thread"}
+            threads = host_threads()
+            cg, nsrc, _ = cpu_brandes_sample(Vb, oo, oc, Eb, threads)
+            bc_line["cpu_baseline"] = {"gteps": cg, "cores": threads, "kind": "port",
+                                       "sample": f"the first {nsrc} sources of the same graph, oracle "
+                                                 f"restatement, sources split over {threads} host threads"}
         B.destroy()
 
     wbc_line = None
@@ -795,10 +861,8 @@ def run_zog(args):
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT)",
-            "config": {"workload": f"pagerank rmat{PR_SCALE} ef{PR_EF} directed fp64 uniform start, d={DAMPING}, "
-                                   f"tol={TOL}, max_iter={MAX_ITER}", "vertices": V, "arcs": E,
-                       "iterations": iterations, "residual": residual, "l2": "inputs larger than L2",
-                       "parallelism": "replicas" if ws > 1 else "single"},
+            "config": {**pr_config(V, E), "parallelism": "replicas" if ws > 1 else "single"},
+            "result": {"iterations": iterations, "residual": residual, "tight_fp64": tight},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak,
                          "traffic": PROFILED_TRAFFIC.get(PR_SCALE),
@@ -845,8 +909,8 @@ def main():
     ap.add_argument("--no-ba", action="store_true", help="skip the Barabasi-Albert graph")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched forms")
     ap.add_argument("--no-weighted", action="store_true", help="skip weighted Brandes")
-    ap.add_argument("--cpu-budget", type=float, default=12.0)
-    ap.add_argument("--ref-iters-per-step", type=int, default=2)
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="seconds of timed full solves the reference arm may spend (at least one is timed)")
     ap.add_argument("--pr-scale", type=int, default=PR_SCALE, help="R-MAT scale of the PageRank graph")
     ap.add_argument("--bc-scale", type=int, default=BC_SCALE, help="R-MAT scale of the Brandes graph")
     ap.add_argument("--batch-graphs", type=int, default=BATCH_GRAPHS, help="graphs of the batched form")
@@ -855,9 +919,6 @@ def main():
     ap.add_argument("--bcb-scale", type=int, default=BCB_SCALE, help="R-MAT scale of the batched Brandes form")
     ap.add_argument("--ba-n", type=int, default=BA_N, help="nodes of the Barabasi-Albert graph")
     ap.add_argument("--wbc-sources", type=int, default=WBC_SOURCES, help="sources of the weighted Brandes line")
-    ap.add_argument("--ref-pr-iterations", type=int, default=28,
-                    help="iterations the full solve takes on the benchmark graph: 28 for the seeded scale-24 "
-                         "R-MAT (the GPU arm measures the same count, since both follow the reference iteration)")
     args = ap.parse_args()
     if args.pr_scale != PR_SCALE:
         PR_SCALE, PR_SEED = args.pr_scale, 1000 + args.pr_scale

@@ -245,13 +245,18 @@ ZOGCU_API int zogcu_eigenvector(zogcu_graph* g, uint64_t max_iterations, double 
  * addition of this library.  The caller passes device arrays it owns -- the
  * in-CSR (in_off[V+1], in_col[E], sources ascending per row), out-degrees
  * (out_degree[V]) and the output (out_scores[V]) -- and every node counts as
- * live.  Scratch comes from one fixed device array reserved when the library
- * loads (about 8 MiB, kept until exit), so V is limited to 262,144 nodes;
- * larger graphs return ZOGCU_ERR_TOO_LARGE.  The first call on a device looks
- * up that array's address (do it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race, so serialise them.  Runs on
- * `stream` (NULL = the default stream) and returns when the scores are
- * written.  Same options and result as zogcu_pagerank. */
+ * live.  Scratch comes from one fixed device array of about 8 MiB, so V is
+ * limited to 262,144 nodes; larger graphs return ZOGCU_ERR_TOO_LARGE.  The
+ * first call on a device does the set-up: it looks up that array's address
+ * and loads the entry point's kernels, and since CUDA loads modules lazily
+ * that is when the array (kept until exit) and the kernels' code take their
+ * device memory -- make that first call before another runtime takes the
+ * device's memory, and before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race, so serialise them.  Runs on
+ * `stream` (NULL = the default stream), reading the chain's state back after
+ * every 32 iteration launches so that it stops once converged whatever
+ * max_iterations is, and returns when the scores are written.  Same options
+ * and result as zogcu_pagerank. */
 ZOGCU_API int zogcu_pagerank_noalloc(const uint32_t* d_in_off, const uint32_t* d_in_col,
                                      const uint32_t* d_out_degree, uint32_t num_nodes,
                                      uint64_t num_arcs, double damping, uint64_t max_iterations,

@@ -74,6 +74,13 @@ def lib():
     L.og_pagerank_ext.argtypes = [C.c_uint32, _u64p, _u32p, _u32p, C.c_void_p, C.c_void_p,
                                   C.c_double, C.c_uint64, C.c_double, _f64p,
                                   C.POINTER(C.c_double)]
+    L.og_pagerank_csr_mt.argtypes = [C.c_uint32, _u64p, _u32p, _u32p, C.c_void_p, C.c_void_p, C.c_double,
+                                     C.c_uint64, C.c_double, _f64p, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), C.c_int]
+    L.og_pagerank_csr_mt.restype = C.c_uint64
+    L.og_bfs_csr_many.argtypes = [C.c_uint32, _u64p, _u32p, _u32p, C.c_uint64, _u32p, _u64p, _u8p, C.c_int]
+    L.og_betweenness_csr_sources_mt.argtypes = [C.c_uint32, _u64p, _u32p, _u32p, C.c_uint64, _f64p,
+                                                C.POINTER(C.c_uint32), C.c_int]
     L.og_betweenness_csr_sources.argtypes = [C.c_uint32, _u64p, _u32p, _u32p, C.c_uint64, _f64p,
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_double)]
     L.og_rmat.restype = vp
@@ -342,3 +349,48 @@ def betweenness_csr_sources(V, off, col, sources):
                                      np.ascontiguousarray(col, np.uint32), src, len(src), out,
                                      C.byref(ovf), C.byref(secs))
     return out[:V], bool(ovf.value), float(secs.value)
+
+
+def pagerank_csr_mt(V, in_off, in_col, outdeg, damping=0.85, max_iterations=100, tolerance=1e-4,
+                    x0=None, p=None, threads=0):
+    """The reference PageRank loop with its row sums spread over host threads;
+    iterates are bit for bit those of pagerank_csr (see og_pagerank_csr_mt).
+    Returns (scores, iterations, last L1 step, loop seconds)."""
+    out = np.zeros(max(V, 1), np.float64)
+    l1 = C.c_double(0); secs = C.c_double(0)
+    x0a = None if x0 is None else np.ascontiguousarray(x0, np.float64)
+    pa = None if p is None else np.ascontiguousarray(p, np.float64)
+    it = lib().og_pagerank_csr_mt(V, np.ascontiguousarray(in_off, np.uint64),
+                                  np.ascontiguousarray(in_col, np.uint32),
+                                  np.ascontiguousarray(outdeg, np.uint32),
+                                  x0a.ctypes.data if x0a is not None else None,
+                                  pa.ctypes.data if pa is not None else None,
+                                  damping, max_iterations, tolerance, out, C.byref(l1), C.byref(secs),
+                                  int(threads))
+    return out[:V], int(it), float(l1.value), float(secs.value)
+
+
+def bfs_csr_many(V, off, col, sources, threads=0):
+    """Per-source BFS distances (0xFFFFFFFF = unreached) and wrapping u64 path
+    counts over a successor CSR, sources spread over host threads.  Returns
+    (dist [S, V] u32, sigma [S, V] u64, overflow [S] bool)."""
+    src = np.ascontiguousarray(sources, np.uint32)
+    S = len(src)
+    dist = np.empty((S, max(V, 1)), np.uint32)
+    sigma = np.empty((S, max(V, 1)), np.uint64)
+    ovf = np.zeros(max(S, 1), np.uint8)
+    lib().og_bfs_csr_many(V, np.ascontiguousarray(off, np.uint64), np.ascontiguousarray(col, np.uint32),
+                          src, S, dist, sigma, ovf, int(threads))
+    return dist[:, :V], sigma[:, :V], ovf[:S].astype(bool)
+
+
+def betweenness_csr_sources_mt(V, off, col, sources, threads=0):
+    """betweenness_csr_sources with the sources split over host threads; agrees
+    with it to rounding (the sum over sources is taken in another order)."""
+    out = np.zeros(max(V, 1), np.float64)
+    ovf = C.c_uint32(0)
+    src = np.ascontiguousarray(sources, np.uint32)
+    lib().og_betweenness_csr_sources_mt(V, np.ascontiguousarray(off, np.uint64),
+                                        np.ascontiguousarray(col, np.uint32), src, len(src), out,
+                                        C.byref(ovf), int(threads))
+    return out[:V], bool(ovf.value)

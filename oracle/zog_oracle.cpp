@@ -50,6 +50,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include <omp.h>
 #include <parallel/algorithm>
 
 namespace {
@@ -706,6 +707,143 @@ uint64_t og_pagerank_csr(uint32_t V, const uint64_t* in_off, const uint32_t* in_
   for (uint32_t node : nodes) out[node] = ranks[node];
   *l1_out = l1_norm;
   return iteration;
+}
+
+// The same iteration with the row loop spread over `threads` host threads
+// (extension, no reference counterpart; <= 0 = all OpenMP threads).  Each row
+// is still summed by one thread in ascending in_col order, and the two global
+// sums -- the dangling mass and the L1 step -- are still taken in ascending
+// node order by one thread.  The L1 pass of iteration k also accumulates the
+// dangling mass of iteration k+1, which reads the same new ranks in the same
+// order as the separate loop of centrality.zig:926-931, so every iterate is
+// bit for bit the single-threaded og_pagerank_csr's.  x0 (null = uniform 1/n)
+// and p (null = the reference's uniform teleport) generalise it like
+// og_pagerank_ext; with both null and every node live it is the reference loop.
+uint64_t og_pagerank_csr_mt(uint32_t V, const uint64_t* in_off, const uint32_t* in_col,
+                            const uint32_t* outdeg, const double* x0, const double* p, double damping,
+                            uint64_t max_iter, double tol, double* out, double* l1_out, double* secs,
+                            int threads) {
+  for (uint32_t i = 0; i < V; ++i) out[i] = 0.0;
+  *l1_out = 0.0;
+  if (secs) *secs = 0.0;
+  if (V == 0) return 0;
+  if (V == 1 && !x0 && !p) { out[0] = 1.0; return 0; }
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+  const double n_f = (double)V;
+  std::vector<double> ranks(V), new_ranks(V, 0.0);
+  for (uint32_t i = 0; i < V; ++i) ranks[i] = x0 ? x0[i] : 1.0 / n_f;
+  auto t0 = std::chrono::steady_clock::now();
+  double sink_sum = 0.0;
+  for (uint32_t node = 0; node < V; ++node)
+    if (outdeg[node] == 0) sink_sum += ranks[node] / n_f;
+  uint64_t iteration = 0;
+  double l1_norm = 0.0;
+  while (iteration < max_iter) {
+    const double sink = sink_sum;
+    const double* rk = ranks.data();
+    double* nr = new_ranks.data();
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nt)
+    for (int64_t node = 0; node < (int64_t)V; ++node) {
+      double rank_sum = 0.0;
+      for (uint64_t j = in_off[node]; j < in_off[node + 1]; ++j) {
+        const uint32_t nb = in_col[j];
+        const uint64_t deg = outdeg[nb];
+        if (deg > 0) rank_sum += rk[nb] / (double)deg;
+      }
+      const double tele = p ? (1.0 - damping) * p[node] : (1.0 - damping) / n_f;
+      nr[node] = tele + damping * (sink + rank_sum);
+    }
+    l1_norm = 0.0;
+    sink_sum = 0.0;
+    for (uint32_t node = 0; node < V; ++node) {
+      l1_norm += std::fabs(nr[node] - rk[node]);
+      if (outdeg[node] == 0) sink_sum += nr[node] / n_f;
+    }
+    std::swap(ranks, new_ranks);
+    iteration += 1;
+    if (l1_norm < tol) break;
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  if (secs) *secs = std::chrono::duration<double>(t1 - t0).count();
+  for (uint32_t i = 0; i < V; ++i) out[i] = ranks[i];
+  *l1_out = l1_norm;
+  return iteration;
+}
+
+// Per-source BFS distances and path counts (centrality.zig:740-767 restated,
+// the dist / sigma half of the Brandes body) for many sources at once, the
+// sources spread over host threads (extension for checking the CUDA library).
+// Row k of dist_out / sigma_out (V entries each) belongs to sources[k]; sigma
+// wraps like the reference's usize and overflow_out[k] records a wrap.
+void og_bfs_csr_many(uint32_t V, const uint64_t* off, const uint32_t* col, const uint32_t* sources,
+                     uint64_t ns, uint32_t* dist_out, uint64_t* sigma_out, uint8_t* overflow_out,
+                     int threads) {
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<uint32_t> queue;
+    queue.reserve(V);
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t k = 0; k < (int64_t)ns; ++k) {
+      uint32_t* dist = dist_out + (size_t)k * V;
+      uint64_t* sigma = sigma_out + (size_t)k * V;
+      for (uint32_t v = 0; v < V; ++v) { dist[v] = kNull; sigma[v] = 0; }
+      uint8_t ovf = 0;
+      const uint32_t s = sources[k];
+      dist[s] = 0;
+      sigma[s] = 1;
+      queue.clear();
+      queue.push_back(s);
+      size_t head = 0;
+      while (head < queue.size()) {
+        const uint32_t v = queue[head++];
+        const uint32_t d_v = dist[v];
+        for (uint64_t j = off[v]; j < off[v + 1]; ++j) {
+          const uint32_t w = col[j];
+          if (dist[w] == kNull) { dist[w] = d_v + 1; queue.push_back(w); }
+          if (dist[w] == d_v + 1) {
+            const uint64_t before = sigma[w];
+            sigma[w] += sigma[v];
+            if (sigma[w] < before) ovf = 1;
+          }
+        }
+      }
+      overflow_out[k] = ovf;
+    }
+  }
+}
+
+// The betweenness loop of og_betweenness_csr_sources with the sources split
+// over host threads in contiguous runs (extension for checking the CUDA
+// library at full size).  Each thread keeps its own score vector, added in
+// thread order at the end; the per-source dependencies are the reference's,
+// only the order in which sources' dependencies are summed into a score
+// differs, so scores agree with the single-threaded loop to rounding.
+void og_betweenness_csr_sources(uint32_t V, const uint64_t* off, const uint32_t* col,
+                                const uint32_t* sources, uint64_t ns, double* out,
+                                uint32_t* overflow_out, double* secs);
+void og_betweenness_csr_sources_mt(uint32_t V, const uint64_t* off, const uint32_t* col,
+                                   const uint32_t* sources, uint64_t ns, double* out,
+                                   uint32_t* overflow_out, int threads) {
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+  std::vector<std::vector<double>> part(nt);
+  std::vector<uint32_t> ovf_t(nt, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num();
+    const uint64_t lo = ns * t / nt, hi = ns * (t + 1) / nt;
+    double secs = 0.0;
+    part[t].assign(V, 0.0);
+    if (hi > lo)
+      og_betweenness_csr_sources(V, off, col, sources + lo, hi - lo, part[t].data(), &ovf_t[t], &secs);
+  }
+  for (uint32_t v = 0; v < V; ++v) out[v] = 0.0;
+  uint32_t ovf = 0;
+  for (int t = 0; t < nt; ++t) {
+    for (uint32_t v = 0; v < V; ++v) out[v] += part[t][v];
+    ovf |= ovf_t[t];
+  }
+  if (overflow_out) *overflow_out = ovf;
 }
 
 // Generalised iteration (extension, no reference counterpart): start vector x0

@@ -260,3 +260,43 @@ def test_rmat_config_sizes(oracle):
     removing self-loops and duplicates."""
     V, f, t = oracle.rmat(14, 8, 1014, directed=True)
     assert V == 16384 and 100_000 < len(f) <= 131072
+
+
+def test_multithreaded_pagerank_is_bit_identical(oracle):
+    """og_pagerank_csr_mt (rows over threads, global sums in node order) gives
+    the single-threaded restatement's iterates bit for bit, with and without a
+    start vector and a teleport vector, and on a graph with dangling nodes."""
+    V, f, t = oracle.rmat(14, 8, 1014, directed=True)
+    off, col, deg = oracle.in_csr_from_edges(V, f, t)
+    assert (deg == 0).any()
+    a = oracle.pagerank_csr(V, off, col, deg, 0.85, 200, 1e-9)
+    for threads in (1, 3, 8):
+        b = oracle.pagerank_csr_mt(V, off, col, deg, 0.85, 200, 1e-9, threads=threads)
+        assert b[1] == a[1] and b[2] == a[2] and np.array_equal(a[0], b[0])
+    rng = np.random.default_rng(5)
+    x0 = rng.random(V); x0 /= x0.sum()
+    p = np.zeros(V); p[123] = 1.0
+    c = oracle.pagerank_ext(V, off, col, deg, x0, p, 0.85, 200, 1e-9)
+    d = oracle.pagerank_csr_mt(V, off, col, deg, 0.85, 200, 1e-9, x0=x0, p=p, threads=4)
+    assert d[1] == c[1] and np.array_equal(c[0], d[0])
+    for cap in (0, 1, 3):
+        a = oracle.pagerank_csr(V, off, col, deg, 0.85, cap, 1e-9)
+        b = oracle.pagerank_csr_mt(V, off, col, deg, 0.85, cap, 1e-9, threads=4)
+        assert b[1] == a[1] and np.array_equal(a[0], b[0])
+
+
+def test_multithreaded_bfs_and_betweenness(oracle):
+    V, f, t = oracle.rmat(11, 8, 1011, directed=False)
+    g = oracle.ArrayGraph(V, f, t)
+    so, sc = g.successor_csr()
+    srcs = np.array([0, 1, 5, 77, V - 1], np.uint32)
+    dist, sigma, ovf = oracle.bfs_csr_many(V, so, sc, srcs, threads=3)
+    for k, s in enumerate(srcs):
+        d1, s1, o1 = g.bfs(int(s))
+        assert np.array_equal(dist[k], d1) and np.array_equal(sigma[k], s1) and ovf[k] == o1
+    bc1 = g.betweenness_sources(np.arange(V))
+    bc2, _ = oracle.betweenness_csr_sources_mt(V, so, sc, np.arange(V, dtype=np.uint32), threads=5)
+    bc1 = bc1[0] if isinstance(bc1, tuple) else bc1
+    assert np.abs(bc1 - bc2).sum() <= 1e-12 * np.abs(bc1).sum()
+    assert np.array_equal(bc1 == 0, bc2 == 0)
+    g.close()

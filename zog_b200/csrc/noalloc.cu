@@ -7,18 +7,25 @@
 // must not allocate between two pre-planned phases.  zogcu_pagerank_noalloc
 // serves them: the caller owns every input and output buffer, and the
 // iteration's scratch (two rank vectors, two contribution vectors, CTA
-// partials and the convergence state) lives in one file-scope device array
-// that the library reserves when it is loaded and keeps until the process
-// exits.
+// partials and the convergence state) lives in one file-scope device array of
+// about 8 MiB that stays reserved until the process exits.
 //
 // Contract:
 //   * at most kNoAllocMaxNodes nodes; larger graphs get ZOGCU_ERR_TOO_LARGE;
 //   * no cudaMalloc / cudaMallocAsync / cudaFree, no stream or event creation,
 //     no allocating library call -- only kernel launches, memsets and copies
 //     on the caller's stream (NULL = the legacy default stream);
-//   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress while that device is current (cached per device);
-//     make that first call before any stream capture;
+//   * the first call on a device does the set-up, with that device current:
+//     it looks up the array's device address with cudaGetSymbolAddress (cached
+//     per device) and loads this file's kernels.  CUDA loads modules lazily
+//     by default, so that first call is when the array and the kernels' code
+//     take their device memory: make it before another runtime takes the
+//     device's memory, and before any stream capture;
+//   * the iterations are enqueued in chunks of kNaChunk launches; after each
+//     chunk the call reads the chain's state back (a small copy and a stream
+//     synchronisation) and stops once the chain has converged or reached
+//     max_iterations, so any cap, UINT64_MAX included, costs only the
+//     iterations actually run plus at most one partial chunk;
 //   * all calls share the one array, and it keeps the last call's contents:
 //     the state each call needs zeroed is cleared at its start, and two calls
 //     whose work overlaps on the GPU (different streams, or host threads
@@ -42,6 +49,7 @@ constexpr size_t kNaStateBytes = 256;
 constexpr size_t kNaPartBytes = (size_t)kNaMaxCtas * 16;
 constexpr size_t kNaVecBytes = (size_t)kNoAllocMaxNodes * 8;
 constexpr size_t kNaScratchBytes = kNaStateBytes + kNaPartBytes + 4 * kNaVecBytes;  // ~8 MiB
+constexpr uint64_t kNaChunk = 32;                // iteration launches between state reads
 
 // The scratch array.  In host code its name is only a stand-in: kernels get
 // the device address that cudaGetSymbolAddress returns.
@@ -197,8 +205,15 @@ extern "C" int zogcu_pagerank_noalloc(const uint32_t* d_in_off, const uint32_t* 
   {
     std::lock_guard<std::mutex> lk(g_na_mu);
     if (!g_na_ptr[dev]) {
-      // once per device, with that device current
-      ZOGCU_CUDA(cudaGetSymbolAddress(&g_na_ptr[dev], g_noalloc_scratch));
+      // once per device, with that device current: the array's device address,
+      // and the kernels loaded now rather than at their first launch
+      cudaFuncAttributes fa;
+      ZOGCU_CUDA(cudaFuncGetAttributes(&fa, na_init_kernel));
+      ZOGCU_CUDA(cudaFuncGetAttributes(&fa, na_iter_kernel));
+      ZOGCU_CUDA(cudaFuncGetAttributes(&fa, na_copy_out));
+      void* addr = nullptr;
+      ZOGCU_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+      g_na_ptr[dev] = addr;
     }
     base = g_na_ptr[dev];
   }
@@ -230,17 +245,30 @@ extern "C" int zogcu_pagerank_noalloc(const uint32_t* d_in_off, const uint32_t* 
   ZOGCU_CUDA(cudaMemsetAsync(A.st, 0, kNaStateBytes, s));  // iteration state starts at zero
   na_init_kernel<<<grid, kNaThreads, 0, s>>>(A);
   ZOGCU_CUDA(cudaGetLastError());
-  for (uint64_t k = 0; k < max_iterations; ++k) na_iter_kernel<<<grid, kNaThreads, 0, s>>>(A);
-  ZOGCU_CUDA(cudaGetLastError());
+  uint64_t launches = 1;
+  NaState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  // Chunks of iteration launches; a launch after the chain is over returns at
+  // once, and the chain's state read after each chunk ends the loop.
+  for (uint64_t queued = 0; queued < max_iterations;) {
+    const uint64_t k = std::min<uint64_t>(kNaChunk, max_iterations - queued);
+    for (uint64_t i = 0; i < k; ++i) na_iter_kernel<<<grid, kNaThreads, 0, s>>>(A);
+    ZOGCU_CUDA(cudaGetLastError());
+    queued += k;
+    launches += k;
+    ZOGCU_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(NaState), cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    if (hs.converged || hs.iter >= max_iterations) break;
+  }
   na_copy_out<<<grid, kNaThreads, 0, s>>>(A, d_out_scores);
   ZOGCU_CUDA(cudaGetLastError());
-  NaState hs;
+  ++launches;
   ZOGCU_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(NaState), cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   if (stats) {
     stats->iterations = hs.iter;
     stats->residual = hs.l1;
-    stats->launches = 2 + max_iterations;
+    stats->launches = launches;
   }
   return ZOGCU_OK;
 }
