@@ -550,7 +550,11 @@ def batched_block(N, args, stream, ws):
                   "loop_sample": f"{k} single-seed solves timed, scaled to {PPR_SEEDS}",
                   "speedup_vs_loop": sms * PPR_SEEDS / k / pms, "iterations_max": int(pit.max()),
                   "iterations_mean": float(pit.mean()),
-                  "achieved_gbs": psts[-1]["bytes_moved"] / (pms * 1e-3) / 1e9,
+                  "gathered_row_bytes_per_s": psts[-1]["bytes_moved"] / (pms * 1e-3),
+                  "gathered_row_bytes_note": "every gathered C row counted as moved, L2 hits included: "
+                                             "a work rate, not DRAM traffic",
+                  "launches_per_step": int(psts[-1]["reserved"]),
+                  "kernels_per_step": int(psts[-1]["launches"]),
                   "rel_l1_vs_single_seed_solve": err}
     G.destroy()
     del pout, x1, tp
@@ -574,7 +578,8 @@ def batched_block(N, args, stream, ws):
                       "vertices": Vb, "arcs": Eb, "ms": cms, "gteps": BCB_SOURCES * Eb / (cms * 1e-3) / 1e9,
                       "loop_of_single_launches_ms": one_ms * BCB_SOURCES / k1,
                       "loop_sample": f"{k1} one-source launches timed, scaled to {BCB_SOURCES}",
-                      "speedup_vs_loop": one_ms * BCB_SOURCES / k1 / cms, "max_depth": int(csts[0]["max_depth"])}
+                      "speedup_vs_loop": one_ms * BCB_SOURCES / k1 / cms, "max_depth": int(csts[0]["max_depth"]),
+                      "launches_per_step": int(csts[0]["reserved"]), "kernels_per_step": int(csts[0]["launches"])}
     Bg.destroy()
     return res, launches
 

@@ -301,11 +301,14 @@ ZOGCU_API int zogcu_bfs_sigma(zogcu_graph* g, const uint32_t* sources, uint64_t 
  * An extension: the reference's teleport is always uniform (centrality.zig:
  * 943).  For each seed s: uniform start 1/n, teleport (1-d) e_s, dangling mass
  * spread uniformly, stop once the seed's L1 step is below tol (each seed
- * stops on its own).  All seeds (256 per pass) advance together as the
- * columns of one SpMM over the in-CSR.  out_scores[num_seeds * V] is
- * seed-major (seed i's vector at i * V); iterations[num_seeds] may be NULL.
- * opts (may be NULL) gives the stream and device_pointers; precision must be
- * FP64 and x0 / teleport NULL.  Graphs with deleted nodes are rejected. */
+ * stops on its own).  The seeds advance together as the columns of an SpMM
+ * over the in-CSR, in passes of 64 to 256 seeds; the whole call is one CUDA
+ * graph (per pass a device-ended while loop of iterations), launched once:
+ * stats->reserved is 1 (the host-side launches) and stats->launches counts
+ * the kernels the graph ran.  out_scores[num_seeds * V] is seed-major (seed
+ * i's vector at i * V); iterations[num_seeds] may be NULL.  opts (may be
+ * NULL) gives the stream and device_pointers; precision must be FP64 and x0 /
+ * teleport NULL.  Graphs with deleted nodes are rejected. */
 ZOGCU_API int zogcu_ppr(zogcu_graph* g, const uint32_t* seeds, uint32_t num_seeds, double damping,
                         uint64_t max_iterations, double tolerance, const zogcu_pr_opts* opts,
                         double* out_scores, uint64_t* iterations, zogcu_stats* stats);

@@ -8,18 +8,27 @@ library's own extension, written directly from the model's definition with a
 hand-derived backward pass (float64 throughout).  The CPU tests pin it against
 torch autograd; the GPU tests compare the CUDA kernels with it.
 
-Model (hidden 64; parameters in one flat FP32 vector, BF16-rounded for the
-forward pass; b() = round to BF16, nearest-even):
+Model (hidden 64, messages 8 wide; parameters in one flat FP32 vector,
+BF16-rounded for the forward pass; b() = round to BF16, nearest-even):
     features  F(v) = [log(1+indeg), log(1+outdeg), outdeg == 0, 1/n]  (FP32)
-    agg(X)(v) = sum_{u in in(v)} X(u) / outdeg(u)
-    layer l   A_l = agg(H_{l-1}),  H_0 = F
-              H_l = b(relu(b(H_{l-1}) Ws_l + b(A_l) Wn_l + b_l)),  l = 1..3
-    head      y = H_3 w_o + b_o      (a prediction of log(n * pr))
+    inv(u)    = 1/outdeg(u) (0 for dangling and deleted nodes)
+    layer 0   M_0(u) = F(u) inv(u)                         (FP32, 4 wide)
+              A_0(v) = sum_{u in in(v)} M_0(u)
+              H_0 = b(relu(b(F) Ws_0 + b(A_0) Wn_0 + b_0))
+    layer l   M_l(u) = b(inv(u) (H_{l-1}(u) U_l))         (8 wide, l = 1, 2)
+              A_l(v) = sum_{u in in(v)} M_l(u)
+              H_l = b(relu(H_{l-1} Ws_l + b(A_l) Wn_l + b_l))
+    head      y = H_2 w_o + b_o      (a prediction of log(n * pr))
     loss      "mse": mean over live nodes of (y - log(n pr))^2
               "kl":  KL(pr || softmax(y)) = sum_v pr(v) log(pr(v) / x0(v))
     start     x0 = softmax(y) over live nodes
-Flat layout: per layer [Ws (din x 64) | Wn (din x 64) | b (64)], then
-[w_o (64) | b_o].  The roundings b() pass gradients straight through.
+Each layer's aggregate is the PageRank propagation of a message; the message
+of layers 1 and 2 is a learned 8-wide projection U_l of the hidden state, so
+the aggregate H -> agg(H) Wn of a full-width layer is replaced by the
+rank-8 form agg(H U) Wn, and every arc carries 16 bytes instead of 128.
+Flat layout: layer 0 [Ws (4 x 64) | Wn (4 x 64) | b (64)]; layers 1, 2
+[U (64 x 8) | Ws (64 x 64) | Wn (8 x 64) | b (64)]; then [w_o (64) | b_o].
+The roundings b() pass gradients straight through.
 """
 from __future__ import annotations
 
@@ -27,6 +36,7 @@ import numpy as np
 
 HID = 64
 NFEAT = 4
+MSG = 8
 LAYERS = 3
 DELETED = 0xFFFFFFFF
 
@@ -35,11 +45,21 @@ def layer_in(l):
     return NFEAT if l == 0 else HID
 
 
+def layer_msg(l):
+    """Width of layer l's message (and aggregate)."""
+    return NFEAT if l == 0 else MSG
+
+
+def layer_size(l):
+    d, r = layer_in(l), layer_msg(l)
+    return (0 if l == 0 else d * r) + d * HID + r * HID + HID
+
+
 def layer_offsets():
     offs, o = [], 0
     for l in range(LAYERS):
         offs.append(o)
-        o += 2 * layer_in(l) * HID + HID
+        o += layer_size(l)
     return offs, o
 
 
@@ -56,15 +76,20 @@ def bf16_round(p):
 
 
 def unpack(p):
+    """Per layer (U or None, Ws, Wn, b), then w_o and b_o."""
     p = np.asarray(p, np.float64)
     offs, head = layer_offsets()
     layers = []
     for l in range(LAYERS):
-        d, o = layer_in(l), offs[l]
+        d, r, o = layer_in(l), layer_msg(l), offs[l]
+        U = None
+        if l > 0:
+            U = p[o:o + d * r].reshape(d, r)
+            o += d * r
         Ws = p[o:o + d * HID].reshape(d, HID)
-        Wn = p[o + d * HID:o + 2 * d * HID].reshape(d, HID)
-        b = p[o + 2 * d * HID:o + 2 * d * HID + HID]
-        layers.append((Ws, Wn, b))
+        Wn = p[o + d * HID:o + d * HID + r * HID].reshape(r, HID)
+        b = p[o + d * HID + r * HID:o + d * HID + r * HID + HID]
+        layers.append((U, Ws, Wn, b))
     return layers, p[head:head + HID], p[head + HID]
 
 
@@ -80,6 +105,7 @@ class Csr:
         self.n = int(self.live.sum())
         od = self.out_deg.astype(np.float64)
         self.inv = np.where(self.live & (self.out_deg > 0), 1.0 / np.where(od > 0, od, 1.0), 0.0)
+        self.inv32 = self.inv.astype(np.float32).astype(np.float64)  # the kernels' FP32 1/outdeg
         self.rows = np.repeat(np.arange(self.V), np.diff(self.in_off))
 
     @classmethod
@@ -94,16 +120,17 @@ class Csr:
         out_deg = np.bincount(frm, minlength=V).astype(np.uint32)
         return cls(in_off, in_col, out_deg)
 
-    def agg(self, X):
-        A = np.zeros_like(X)
-        np.add.at(A, self.rows, X[self.in_col] * self.inv[self.in_col, None])
+    def agg(self, M):
+        """A(v) = sum over in-arcs u->v of M(u)."""
+        A = np.zeros_like(M)
+        np.add.at(A, self.rows, M[self.in_col])
         return A
 
     def agg_t(self, G):
-        """Transpose of agg: out(u) = inv(u) * sum over arcs u->v of G(v)."""
+        """Transpose of agg: out(u) = sum over arcs u->v of G(v)."""
         out = np.zeros_like(G)
         np.add.at(out, self.in_col, G[self.rows])
-        return out * self.inv[:, None]
+        return out
 
     def features(self):
         """FP32 features (as float64 values)."""
@@ -121,15 +148,19 @@ def b16(x):
 
 def forward(p, g: Csr):
     """Network output y (float64) and the activations the backward pass needs
-    (per layer: the rounded dense operands Xb, Ab and the output H)."""
+    (per layer: the dense operands X, b(A) and the output H)."""
     layers, wo, bo = unpack(bf16_round(p))
-    X = g.features()
+    F = g.features()
+    X = b16(F)
     cache = []
-    for Ws, Wn, b in layers:
-        A = g.agg(X)
-        Xb, Ab = b16(X), b16(A)
-        H = b16(np.maximum(Xb @ Ws + Ab @ Wn + b, 0.0))
-        cache.append((Xb, Ab, H))
+    for l, (U, Ws, Wn, b) in enumerate(layers):
+        if l == 0:
+            M = (F.astype(np.float32) * g.inv32.astype(np.float32)[:, None]).astype(np.float64)
+        else:
+            M = b16(g.inv32[:, None] * (X @ U))
+        Ab = b16(g.agg(M))
+        H = b16(np.maximum(X @ Ws + Ab @ Wn + b, 0.0))
+        cache.append((X, Ab, H))
         X = H
     y = X @ wo + bo
     return y, cache
@@ -160,20 +191,24 @@ def loss_grad(p, g: Csr, pr, kind: str = "kl"):
         raise ValueError(kind)
     offs, head = layer_offsets()
     grad = np.zeros(num_params())
-    H3 = cache[-1][2]
-    grad[head:head + HID] = H3.T @ dy
+    H_last = cache[-1][2]
+    grad[head:head + HID] = H_last.T @ dy
     grad[head + HID] = dy.sum()
     dH = np.outer(dy, wo)
     for l in range(LAYERS - 1, -1, -1):
-        X, A, H = cache[l]
-        Ws, Wn, _ = layers[l]
-        d, o = layer_in(l), offs[l]
+        X, Ab, H = cache[l]
+        U, Ws, Wn, _ = layers[l]
+        d, r, o = layer_in(l), layer_msg(l), offs[l]
+        if l > 0:
+            o_u, o = o, o + d * r
         dP = dH * (H > 0)
         grad[o:o + d * HID] = (X.T @ dP).ravel()
-        grad[o + d * HID:o + 2 * d * HID] = (A.T @ dP).ravel()
-        grad[o + 2 * d * HID:o + 2 * d * HID + HID] = dP.sum(axis=0)
+        grad[o + d * HID:o + d * HID + r * HID] = (Ab.T @ dP).ravel()
+        grad[o + d * HID + r * HID:o + d * HID + r * HID + HID] = dP.sum(axis=0)
         if l > 0:
-            dH = dP @ Ws.T + g.agg_t(dP @ Wn.T)
+            dQ = g.inv32[:, None] * g.agg_t(dP @ Wn.T)  # through M = b(inv * (X U))
+            grad[o_u:o_u + d * r] = (X.T @ dQ).ravel()
+            dH = dP @ Ws.T + dQ @ U.T
     return loss, grad
 
 
@@ -188,7 +223,8 @@ def start_vector(y, g: Csr):
 
 def glorot_init(seed):
     """Initial weights of zogcu_gnn_create(seed): Glorot-uniform from a
-    SplitMix64 stream (24-bit uniforms), biases zero."""
+    SplitMix64 stream (24-bit uniforms) in flat-layout order, each matrix with
+    its own fan (din + dout), biases zero."""
     mask = (1 << 64) - 1
     state = [seed & mask]
 
@@ -199,16 +235,20 @@ def glorot_init(seed):
         z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
         return z ^ (z >> 31)
 
+    def fill(p, o, rows, cols):
+        a = np.float32(np.sqrt(np.float32(6.0) / np.float32(rows + cols)))
+        for i in range(rows * cols):
+            u = np.float32((nxt() >> 40) * (1.0 / 16777216.0)) * np.float32(2.0) - np.float32(1.0)
+            p[o + i] = a * u
+        return o + rows * cols
+
     p = np.zeros(num_params(), np.float32)
     offs, head = layer_offsets()
     for l in range(LAYERS):
-        d = layer_in(l)
-        a = np.float32(np.sqrt(np.float32(6.0) / np.float32(d + HID)))
-        for i in range(2 * d * HID):
-            u = np.float32((nxt() >> 40) * (1.0 / 16777216.0)) * np.float32(2.0) - np.float32(1.0)
-            p[offs[l] + i] = a * u
-    a = np.float32(np.sqrt(np.float32(6.0) / np.float32(HID + 1)))
-    for i in range(HID):
-        u = np.float32((nxt() >> 40) * (1.0 / 16777216.0)) * np.float32(2.0) - np.float32(1.0)
-        p[head + i] = a * u
+        d, r, o = layer_in(l), layer_msg(l), offs[l]
+        if l > 0:
+            o = fill(p, o, d, r)
+        o = fill(p, o, d, HID)
+        fill(p, o, r, HID)
+    fill(p, head, HID, 1)
     return p

@@ -14,21 +14,28 @@ def torch_loss(p, g: G.Csr, pr, kind="kl"):
     offs, head = G.layer_offsets()
     rows = torch.from_numpy(g.rows)
     cols = torch.from_numpy(g.in_col)
-    inv = torch.from_numpy(g.inv)
+    inv = torch.from_numpy(g.inv32)
 
-    def agg(X):
-        return torch.zeros_like(X).index_add(0, rows, X[cols] * inv[cols, None])
+    def agg(M):
+        return torch.zeros_like(M).index_add(0, rows, M[cols])
 
     def b16(x):  # BF16 rounding in the forward pass, identity in the backward pass
         return x + (x.float().to(torch.bfloat16).double() - x).detach()
 
-    X = torch.from_numpy(g.features())
+    F = torch.from_numpy(g.features())
+    X = b16(F)
     for l in range(G.LAYERS):
-        d, o = G.layer_in(l), offs[l]
+        d, r, o = G.layer_in(l), G.layer_msg(l), offs[l]
+        if l == 0:
+            M = (F.float() * inv.float()[:, None]).double()
+        else:
+            U = p[o:o + d * r].reshape(d, r)
+            o += d * r
+            M = b16(inv[:, None] * (X @ U))
         Ws = p[o:o + d * G.HID].reshape(d, G.HID)
-        Wn = p[o + d * G.HID:o + 2 * d * G.HID].reshape(d, G.HID)
-        b = p[o + 2 * d * G.HID:o + 2 * d * G.HID + G.HID]
-        X = b16(torch.relu(b16(X) @ Ws + b16(agg(X)) @ Wn + b))
+        Wn = p[o + d * G.HID:o + d * G.HID + r * G.HID].reshape(r, G.HID)
+        b = p[o + d * G.HID + r * G.HID:o + d * G.HID + r * G.HID + G.HID]
+        X = b16(torch.relu(X @ Ws + b16(agg(M)) @ Wn + b))
     y = X @ p[head:head + G.HID] + p[head + G.HID]
     live = torch.from_numpy(g.live)
     if kind == "mse":

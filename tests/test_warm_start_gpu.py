@@ -34,6 +34,20 @@ def sample_graphs(native, oracle):
                                            np.array([1, 2, 0, 2, 0], np.uint32))
 
 
+def param_blocks():
+    """Boundaries of every weight matrix, bias and the head in the flat vector."""
+    offs, head = GO.layer_offsets()
+    b = []
+    for l in range(GO.LAYERS):
+        d, r, o = GO.layer_in(l), GO.layer_msg(l), offs[l]
+        b.append(o)
+        if l > 0:
+            o += d * r
+            b.append(o)
+        b += [o + d * GO.HID, o + d * GO.HID + r * GO.HID]
+    return sorted(set(b + [head, head + GO.HID, GO.num_params()]))
+
+
 def perturbed_params(seed):
     p = GO.glorot_init(seed)
     rng = np.random.default_rng(seed)
@@ -85,8 +99,7 @@ def test_loss_and_gradient_match_oracle(native, oracle):
                     loss, grad = net.loss_grad(G, pr, code)
                     loss_ref, grad_ref = GO.loss_grad(p, g, pr, kind)
                     assert abs(loss - loss_ref) <= 1e-2 * abs(loss_ref) + 1e-6, (name, kind, loss, loss_ref)
-                    offs, head = GO.layer_offsets()
-                    bounds = sorted(set(offs + [head, GO.num_params()]))
+                    bounds = param_blocks()
                     scale = np.linalg.norm(grad_ref)
                     for a, b in zip(bounds[:-1], bounds[1:]):
                         err = np.linalg.norm(grad[a:b] - grad_ref[a:b])

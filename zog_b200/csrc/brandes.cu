@@ -53,6 +53,17 @@ struct BcHeavy {
   uint32_t nch;
 };
 
+// Level state of one batch when its levels run as CUDA-graph while loops: the
+// forward level, the depth found (the first level that discovered nothing),
+// the backward level still to sweep, and the deepest depth of the lane's
+// batches so far (kept across batches).
+struct BcLoop {
+  uint32_t level;
+  uint32_t depth;
+  uint32_t blevel;
+  uint32_t max_depth;
+};
+
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
   return __shfl_sync(0xffffffffu, v, src);
 }
@@ -158,9 +169,16 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
     unsigned long long* __restrict__ visited, unsigned long long* __restrict__ sigma, uint32_t* __restrict__ dist,
     unsigned long long full, uint32_t level, unsigned int* __restrict__ flags, const BcHeavy* __restrict__ heavy,
     uint32_t nheavy, unsigned long long* __restrict__ hpart, unsigned long long* __restrict__ hgot,
-    unsigned int* __restrict__ harrive) {
+    unsigned int* __restrict__ harrive, const BcLoop* __restrict__ loop, unsigned long long* __restrict__ masks) {
   // flags[l % kMaxStoredLevels] = 1 when level l discovered a vertex;
-  // flags[kOverflowFlag] = some path count wrapped
+  // flags[kOverflowFlag] = some path count wrapped.  With `loop` (the level
+  // loop runs on the device) the level and its frontier masks come from the
+  // batch's loop state and the mask ring `masks`.
+  if (loop) {
+    level = *(volatile const uint32_t*)&loop->level;
+    front_cur = masks + (size_t)(level % (kMaxStoredLevels + 1)) * V;
+    front_nxt = masks + (size_t)((level + 1) % (kMaxStoredLevels + 1)) * V;
+  }
   if (level > 0 && *(volatile unsigned int*)(flags + (level - 1) % kMaxStoredLevels) == 0u) return;
   constexpr int W = kBcThreads / 32;
   __shared__ unsigned long long s_acc[W][kBcBatch];
@@ -326,7 +344,28 @@ __global__ void __launch_bounds__(kBcThreads) bc_backward_kernel(
     unsigned long long* __restrict__ mask_out, const uint32_t* __restrict__ dist,
     const unsigned long long* __restrict__ sigma, double* __restrict__ q, double* __restrict__ bc, uint32_t level,
     int last_level, const BcHeavy* __restrict__ heavy, uint32_t nheavy, double* __restrict__ hpart,
-    unsigned int* __restrict__ harrive) {
+    unsigned int* __restrict__ harrive, const BcLoop* __restrict__ loop, unsigned long long* __restrict__ masks,
+    unsigned long long* __restrict__ mbuf_a, unsigned long long* __restrict__ mbuf_b) {
+  if (loop) {
+    // the level, and where its masks come from, from the batch's loop state:
+    // stored frontiers when the BFS was shallower than the ring, else masks
+    // derived from dist that alternate between two buffers (level depth - k
+    // reads buffer k % 2 and writes the other)
+    level = *(volatile const uint32_t*)&loop->blevel;
+    if (level == 0) return;
+    const uint32_t depth = *(volatile const uint32_t*)&loop->depth;
+    last_level = level == depth ? 1 : 0;
+    if (depth < (uint32_t)kMaxStoredLevels) {
+      mask_l = masks + (size_t)(level % (kMaxStoredLevels + 1)) * V;
+      mask_next = masks + (size_t)((level + 1) % (kMaxStoredLevels + 1)) * V;
+      mask_out = nullptr;
+    } else {
+      const bool odd = ((depth - level) & 1u) != 0;
+      mask_l = nullptr;
+      mask_next = odd ? mbuf_b : mbuf_a;
+      mask_out = odd ? mbuf_a : mbuf_b;
+    }
+  }
   constexpr int W = kBcThreads / 32;
   __shared__ double s_acc[W][kBcBatch];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -529,7 +568,8 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
                                                           full, l, W.flags.as<unsigned int>(),
                                                           g->heavy_in.as<BcHeavy>(), g->n_heavy_in,
                                                           W.hpart.as<unsigned long long>(),
-                                                          W.hgot.as<unsigned long long>(), W.harrive.as<unsigned int>());
+                                                          W.hgot.as<unsigned long long>(), W.harrive.as<unsigned int>(),
+                                                          nullptr, nullptr);
       ZOGCU_CUDA(cudaGetLastError());
       *launches += 1;
     }
@@ -551,15 +591,104 @@ __global__ void k_bc_add(double* __restrict__ a, const double* __restrict__ b, u
     a[v] += b[v];
 }
 
-// Batches rotate over kBcLanes streams ("lanes"), each with its own workspace
-// and score vector: while the host waits for one batch's forward levels (to
-// learn its depth), the other lanes' sweeps keep the GPU busy, and one lane's
-// next kernel fills the SMs that another's finishing kernel frees.  Batch b's
-// scores add up in lane b % kBcLanes's vector, and the vectors are added to
-// d_bc at the end in lane order: a fixed order, so the result is
-// deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count (1 = one stream).
+// Resets one batch's state: visited and level-0 masks zero, dist all
+// unreached, the level flags zero (the overflow word is kept), loop state zero.
+__global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visited,
+                               unsigned long long* __restrict__ mask0, uint32_t* __restrict__ dist,
+                               unsigned int* __restrict__ flags, BcLoop* __restrict__ loop) {
+  const uint64_t n = (uint64_t)V * kBcBatch;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    dist[i] = kUnreached;
+    if (i < V) {
+      visited[i] = 0ull;
+      mask0[i] = 0ull;
+    }
+  }
+  if (blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < kMaxStoredLevels; i += blockDim.x) flags[i] = 0u;
+    if (threadIdx.x == 0) {
+      loop->level = 0u;
+      loop->depth = 0u;
+      loop->blevel = 0u;
+    }
+  }
+}
+
+// After forward level l: if it discovered nothing the BFS depth is l -- the
+// backward sweep starts there and the forward loop ends; otherwise the next
+// level follows (and the flag words of the previous 63 levels are cleared when
+// the ring of flag words wraps, as the host loop did).  One thread.
+__global__ void bc_fwd_advance(BcLoop* __restrict__ loop, unsigned int* __restrict__ flags,
+                               uint32_t* __restrict__ depth_slot, unsigned long long cond) {
+  if (threadIdx.x != 0) return;
+  const uint32_t l = loop->level;
+  if (flags[l % kMaxStoredLevels] == 0u) {
+    loop->depth = l;
+    loop->blevel = l;
+    if (l > loop->max_depth) loop->max_depth = l;
+    *depth_slot = l;
+    cudaGraphSetConditional(cond, 0u);
+    return;
+  }
+  const uint32_t nl = l + 1;
+  if (nl % kMaxStoredLevels == 0)
+    for (int i = 0; i < kMaxStoredLevels - 1; ++i) flags[i] = 0u;
+  loop->level = nl;
+}
+
+// After backward level l: the next shallower level, or the end of the loop
+// once level 1 is done (a batch of depth 0 has no level to sweep).  One thread.
+__global__ void bc_bwd_advance(BcLoop* __restrict__ loop, unsigned long long cond) {
+  if (threadIdx.x != 0) return;
+  const uint32_t b = loop->blevel;
+  if (b <= 1u) {
+    loop->blevel = 0u;
+    cudaGraphSetConditional(cond, 0u);
+  } else {
+    loop->blevel = b - 1u;
+  }
+}
+
+static int bc_kernel_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
+                          const void* fn, unsigned grid, unsigned threads, void** args) {
+  cudaKernelNodeParams kp = {};
+  kp.func = const_cast<void*>(fn);
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(threads);
+  kp.kernelParams = args;
+  ZOGCU_CUDA(cudaGraphAddKernelNode(node, graph, deps, ndeps, &kp));
+  return ZOGCU_OK;
+}
+
+// A conditional while node after `deps`; its body graph is returned in *body.
+static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
+                         cudaGraphConditionalHandle* h, cudaGraph_t* body) {
+  ZOGCU_CUDA(cudaGraphConditionalHandleCreate(h, graph, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = *h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  ZOGCU_CUDA(cudaGraphAddNode(node, graph, deps, ndeps, &cp));
+  *body = cp.conditional.phGraph_out[0];
+  return ZOGCU_OK;
+}
+
+// Batches of kBcBatch sources are dealt to kBcLanes "lanes" (batch b to lane
+// b % lanes), each with its own workspace and score vector.  A call's batches
+// run as CUDA graphs of up to kBcGraphBatches batches: in a graph, every lane
+// is a chain of its batches -- reset, seed, a while loop of forward levels
+// (each level kernel followed by a one-thread kernel that ends the loop when
+// the level discovered nothing), a while loop of backward levels from that
+// depth up to level 1 -- and the lanes' chains are independent branches, so
+// one lane's levels fill the SMs another's finishing level frees.  No host
+// synchronisation happens between batches or levels: the host launches each
+// graph once and reads the depths and flags at the end.  The lanes' score
+// vectors are added to d_bc at the end in lane order: a fixed order, so the
+// result is deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count.
 constexpr int kBcMaxLanes = 4;
 constexpr int kBcLanes = 2;
+constexpr uint64_t kBcGraphBatches = 64;
 template <typename OffT>
 static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {
@@ -570,97 +699,171 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   int nlanes = kBcLanes;
   if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) nlanes = std::max(1, std::min(kBcMaxLanes, std::atoi(env)));
   nlanes = (int)std::min<uint64_t>((uint64_t)nlanes, std::max<uint64_t>(nbatches, 1));
-  // the extra score vectors are declared first and the extra streams next:
-  // on every exit the workspaces are freed, then the extra streams are
-  // drained and destroyed, and only then the vectors (freed on the caller's
-  // stream) go
-  DevBuf bcx[kBcMaxLanes];
-  StreamGuard sx[kBcMaxLanes];
-  cudaStream_t ss[kBcMaxLanes];
+  DevBuf bcx[kBcMaxLanes], loops, depths;
   double* bcs[kBcMaxLanes];
-  cudaEvent_t ev = nullptr;
-  struct EventFree {
-    cudaEvent_t* e;
-    ~EventFree() {
-      if (*e) cudaEventDestroy(*e);
-    }
-  } evf{&ev};
-  ss[0] = s;
   bcs[0] = d_bc;
-  if (nlanes > 1) {
-    ZOGCU_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    for (int w = 1; w < nlanes; ++w) {
-      ZOGCU_TRY(sx[w].init(nullptr));
-      ss[w] = sx[w].s;
-      ZOGCU_TRY(bcx[w].alloc((size_t)std::max<uint32_t>(V, 1) * 8, s));
-      ZOGCU_CUDA(cudaMemsetAsync(bcx[w].ptr, 0, (size_t)std::max<uint32_t>(V, 1) * 8, s));
-      bcs[w] = bcx[w].as<double>();
-    }
-    ZOGCU_CUDA(cudaEventRecord(ev, s));
-    for (int w = 1; w < nlanes; ++w) ZOGCU_CUDA(cudaStreamWaitEvent(ss[w], ev, 0));
+  for (int w = 1; w < nlanes; ++w) {
+    ZOGCU_TRY(bcx[w].alloc((size_t)std::max<uint32_t>(V, 1) * 8, s));
+    ZOGCU_CUDA(cudaMemsetAsync(bcx[w].ptr, 0, (size_t)std::max<uint32_t>(V, 1) * 8, s));
+    bcs[w] = bcx[w].as<double>();
   }
   BcWork W[kBcMaxLanes];
   for (int w = 0; w < nlanes; ++w) {
-    ZOGCU_TRY(W[w].alloc(g, ns, ss[w], true));
-    if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W[w].src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, ss[w]));
+    ZOGCU_TRY(W[w].alloc(g, ns, s, true));
+    ZOGCU_CUDA(cudaMemsetAsync(W[w].flags.ptr, 0, kFlagWords * 4, s));
+    if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W[w].src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, s));
   }
-  unsigned int* h_flags = nullptr;
-  ZOGCU_CUDA(cudaMallocHost(&h_flags, (size_t)kBcMaxLanes * kFlagWords * 4));
-  struct HostFree {
-    unsigned int* p;
-    ~HostFree() { cudaFreeHost(p); }
-  } hf{h_flags};
-  const int grid = bc_grid(bc_backward_kernel<OffT>, V);
-  bool overflow = false;
-  uint32_t max_depth = 0;
-  uint64_t launches = 0;
-  for (uint64_t bi = 0; bi < nbatches; ++bi) {
-    const int lane_w = (int)(bi % (uint64_t)nlanes);
-    BcWork& Wb = W[lane_w];
-    const cudaStream_t sb = ss[lane_w];
-    double* const bcb = bcs[lane_w];
-    const uint64_t first = bi * kBcBatch;
-    const int nb = (int)std::min<uint64_t>(kBcBatch, ns - first);
-    uint32_t depth = 0;
-    ZOGCU_TRY(bc_forward_batch<OffT>(g, in_off, Wb, first, nb, sb, &depth, &overflow, &launches,
-                                     h_flags + lane_w * kFlagWords));
-    max_depth = std::max(max_depth, depth);
-    // backward: levels depth .. 1 (the sources sit at level 0 and are excluded)
-    const bool stored = depth < (uint32_t)kMaxStoredLevels;
-    unsigned long long* mnxt = Wb.mbuf_a.as<unsigned long long>();
-    unsigned long long* mcur = Wb.mbuf_b.as<unsigned long long>();
-    if (!stored) ZOGCU_CUDA(cudaMemsetAsync(mnxt, 0, (size_t)V * 8, sb));
-    for (uint32_t l = depth; l >= 1; --l) {
-      if (stored) {
-        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, sb>>>(
-            V, out_off, g->out_col.as<uint32_t>(), Wb.level(l, V), Wb.level(l + 1, V), nullptr,
-            Wb.dist.as<uint32_t>(), Wb.sigma.as<unsigned long long>(), Wb.q.as<double>(), bcb, l,
-            l == depth ? 1 : 0, g->heavy_out.as<BcHeavy>(), g->n_heavy_out, Wb.hpart.as<double>(),
-            Wb.harrive.as<unsigned int>());
-      } else {
-        bc_backward_kernel<OffT><<<grid, kBcThreads, 0, sb>>>(
-            V, out_off, g->out_col.as<uint32_t>(), nullptr, mnxt, mcur, Wb.dist.as<uint32_t>(),
-            Wb.sigma.as<unsigned long long>(), Wb.q.as<double>(), bcb, l, l == depth ? 1 : 0,
-            g->heavy_out.as<BcHeavy>(), g->n_heavy_out, Wb.hpart.as<double>(), Wb.harrive.as<unsigned int>());
-        std::swap(mnxt, mcur);
+  ZOGCU_TRY(loops.alloc(sizeof(BcLoop) * kBcMaxLanes, s));
+  ZOGCU_CUDA(cudaMemsetAsync(loops.ptr, 0, sizeof(BcLoop) * kBcMaxLanes, s));
+  ZOGCU_TRY(depths.alloc(std::max<uint64_t>(nbatches, 1) * 4, s));
+  ZOGCU_CUDA(cudaMemsetAsync(depths.ptr, 0, std::max<uint64_t>(nbatches, 1) * 4, s));
+  // the sources copy above reads a host vector the caller keeps alive
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  const unsigned fgrid = (unsigned)bc_grid(bc_forward_kernel<OffT>, V);
+  const unsigned bgrid = (unsigned)bc_grid(bc_backward_kernel<OffT>, V);
+  const unsigned rgrid = std::max<unsigned>(1u, std::min<unsigned>((unsigned)(((uint64_t)V * kBcBatch + 255) / 256),
+                                                                   (unsigned)sm_count() * 8));
+  uint64_t host_launches = 0;
+  for (uint64_t b0 = 0; b0 < nbatches; b0 += kBcGraphBatches) {
+    const uint64_t b1 = std::min<uint64_t>(nbatches, b0 + kBcGraphBatches);
+    const bool final_chunk = b1 == nbatches;
+    cudaGraph_t graph = nullptr;
+    ZOGCU_CUDA(cudaGraphCreate(&graph, 0));
+    struct GraphGuard {
+      cudaGraph_t gr;
+      ~GraphGuard() { cudaGraphDestroy(gr); }
+    } guard{graph};
+    cudaGraphNode_t tail[kBcMaxLanes] = {};
+    for (uint64_t bi = b0; bi < b1; ++bi) {
+      const int w = (int)(bi % (uint64_t)nlanes);
+      BcWork& Wb = W[w];
+      const uint64_t first = bi * kBcBatch;
+      int nb = (int)std::min<uint64_t>(kBcBatch, ns - first);
+      unsigned long long full = nb == 64 ? ~0ull : ((1ull << nb) - 1);
+      BcLoop* loop = loops.as<BcLoop>() + w;
+      uint32_t* depth_slot = depths.as<uint32_t>() + bi;
+      unsigned long long* visited = Wb.visited.as<unsigned long long>();
+      unsigned long long* masks = Wb.masks.as<unsigned long long>();
+      unsigned long long* mask0 = Wb.level(0, V);
+      unsigned long long* sigma = Wb.sigma.as<unsigned long long>();
+      uint32_t* dist = Wb.dist.as<uint32_t>();
+      unsigned int* flags = Wb.flags.as<unsigned int>();
+      const uint32_t* src = Wb.src.as<uint32_t>() + first;
+      uint32_t Vv = V;
+      const cudaGraphNode_t* dep = tail[w] ? &tail[w] : nullptr;
+      const size_t ndep = tail[w] ? 1 : 0;
+      // reset and seed
+      cudaGraphNode_t n_reset, n_seed;
+      void* reset_args[] = {&Vv, &visited, &mask0, &dist, &flags, &loop};
+      ZOGCU_TRY(bc_kernel_node(graph, &n_reset, dep, ndep, (const void*)bc_batch_reset, rgrid, 256, reset_args));
+      void* seed_args[] = {(void*)&src, &nb, &visited, &mask0, &sigma, &dist};
+      ZOGCU_TRY(bc_kernel_node(graph, &n_seed, &n_reset, 1, (const void*)bc_seed_kernel, 1, 64, seed_args));
+      // forward levels
+      cudaGraphNode_t n_fwd;
+      cudaGraphConditionalHandle hf;
+      cudaGraph_t fbody;
+      ZOGCU_TRY(bc_while_node(graph, &n_fwd, &n_seed, 1, &hf, &fbody));
+      {
+        const uint32_t* col = g->in_col.as<uint32_t>();
+        const unsigned long long* fcur = nullptr;
+        unsigned long long* fnxt = nullptr;
+        uint32_t level0 = 0;
+        const BcHeavy* heavy = g->heavy_in.as<BcHeavy>();
+        uint32_t nheavy = g->n_heavy_in;
+        unsigned long long* hpart = Wb.hpart.as<unsigned long long>();
+        unsigned long long* hgot = Wb.hgot.as<unsigned long long>();
+        unsigned int* harrive = Wb.harrive.as<unsigned int>();
+        const BcLoop* cloop = loop;
+        void* fargs[] = {&Vv, (void*)&in_off, (void*)&col, (void*)&fcur, &fnxt, &visited, &sigma, &dist, &full,
+                         &level0, &flags, (void*)&heavy, &nheavy, &hpart, &hgot, &harrive, (void*)&cloop, &masks};
+        cudaGraphNode_t k1, k2;
+        ZOGCU_TRY(bc_kernel_node(fbody, &k1, nullptr, 0, (const void*)bc_forward_kernel<OffT>, fgrid, kBcThreads, fargs));
+        unsigned long long cond = hf;
+        void* aargs[] = {&loop, &flags, &depth_slot, &cond};
+        ZOGCU_TRY(bc_kernel_node(fbody, &k2, &k1, 1, (const void*)bc_fwd_advance, 1, 32, aargs));
       }
-      ZOGCU_CUDA(cudaGetLastError());
-      ++launches;
+      // backward levels
+      cudaGraphNode_t n_bwd;
+      cudaGraphConditionalHandle hb;
+      cudaGraph_t bbody;
+      ZOGCU_TRY(bc_while_node(graph, &n_bwd, &n_fwd, 1, &hb, &bbody));
+      {
+        const uint32_t* col = g->out_col.as<uint32_t>();
+        const unsigned long long* ml = nullptr;
+        const unsigned long long* mn = nullptr;
+        unsigned long long* mo = nullptr;
+        double* q = Wb.q.as<double>();
+        double* bcb = bcs[w];
+        uint32_t level0 = 0;
+        int last0 = 0;
+        const BcHeavy* heavy = g->heavy_out.as<BcHeavy>();
+        uint32_t nheavy = g->n_heavy_out;
+        double* hpart = Wb.hpart.as<double>();
+        unsigned int* harrive = Wb.harrive.as<unsigned int>();
+        const BcLoop* cloop = loop;
+        unsigned long long* ma = Wb.mbuf_a.as<unsigned long long>();
+        unsigned long long* mb = Wb.mbuf_b.as<unsigned long long>();
+        const uint32_t* cdist = dist;
+        const unsigned long long* csigma = sigma;
+        void* bargs[] = {&Vv, (void*)&out_off, (void*)&col, (void*)&ml, (void*)&mn, &mo, (void*)&cdist,
+                         (void*)&csigma, &q, &bcb, &level0, &last0, (void*)&heavy, &nheavy, &hpart, &harrive,
+                         (void*)&cloop, &masks, &ma, &mb};
+        cudaGraphNode_t k1, k2;
+        ZOGCU_TRY(bc_kernel_node(bbody, &k1, nullptr, 0, (const void*)bc_backward_kernel<OffT>, bgrid, kBcThreads, bargs));
+        unsigned long long cond = hb;
+        void* aargs[] = {&loop, &cond};
+        ZOGCU_TRY(bc_kernel_node(bbody, &k2, &k1, 1, (const void*)bc_bwd_advance, 1, 32, aargs));
+      }
+      tail[w] = n_bwd;
     }
+    if (final_chunk) {
+      // the other lanes' scores into d_bc, in lane order
+      cudaGraphNode_t prev = tail[0];
+      for (int w = 1; w < nlanes; ++w) {
+        cudaGraphNode_t deps[2];
+        size_t nd = 0;
+        if (prev) deps[nd++] = prev;
+        if (tail[w]) deps[nd++] = tail[w];
+        double* a = d_bc;
+        double* b = bcs[w];
+        uint32_t Vv = V;
+        void* args[] = {&a, &b, &Vv};
+        cudaGraphNode_t n_add;
+        ZOGCU_TRY(bc_kernel_node(graph, &n_add, deps, nd, (const void*)k_bc_add,
+                                 std::max<unsigned>(1u, std::min<unsigned>((V + 255) / 256, 148u * 8)), 256, args));
+        prev = n_add;
+      }
+    }
+    cudaGraphExec_t exec = nullptr;
+    ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    const cudaError_t le = cudaGraphLaunch(exec, s);
+    cudaGraphExecDestroy(exec);  // an executable graph in flight is freed when it completes
+    ZOGCU_CUDA(le);
+    ++host_launches;
   }
-  for (int w = 1; w < nlanes; ++w) {  // the other lanes' scores into d_bc, in lane order
-    ZOGCU_CUDA(cudaEventRecord(ev, ss[w]));
-    ZOGCU_CUDA(cudaStreamWaitEvent(s, ev, 0));
-    k_bc_add<<<std::max<unsigned>(1u, std::min<unsigned>((V + 255) / 256, 148u * 8)), 256, 0, s>>>(
-        d_bc, bcs[w], V);
-    ZOGCU_CUDA(cudaGetLastError());
-    ++launches;
+  // depths, overflow flags and the kernels the graphs ran
+  std::vector<uint32_t> h_depth(std::max<uint64_t>(nbatches, 1));
+  ZOGCU_CUDA(cudaMemcpyAsync(h_depth.data(), depths.ptr, h_depth.size() * 4, cudaMemcpyDeviceToHost, s));
+  std::vector<unsigned int> h_ovf(nlanes);
+  for (int w = 0; w < nlanes; ++w)
+    ZOGCU_CUDA(cudaMemcpyAsync(&h_ovf[w], W[w].flags.as<unsigned int>() + kOverflowFlag, 4, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  bool overflow = false;
+  for (int w = 0; w < nlanes; ++w) overflow |= h_ovf[w] != 0u;
+  uint32_t max_depth = 0;
+  uint64_t launches = nlanes > 1 ? (uint64_t)(nlanes - 1) : 0;
+  for (uint64_t bi = 0; bi < nbatches; ++bi) {
+    const uint32_t d = h_depth[bi];
+    max_depth = std::max(max_depth, d);
+    // reset, seed, (level + advance) x (depth + 1) forward, x max(depth, 1) backward
+    launches += 2 + 2 * ((uint64_t)d + 1) + 2 * std::max<uint64_t>(d, 1);
   }
   if (stats) {
     stats->sources = ns;
     stats->max_depth = max_depth;
     stats->sigma_overflow = overflow ? 1u : 0u;
     stats->launches = launches;
+    stats->reserved = (uint32_t)host_launches;  // graph launches of the call
   }
   return ZOGCU_OK;
 }

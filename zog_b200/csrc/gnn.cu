@@ -2,25 +2,43 @@
 // whose prediction is only the start vector of the power iteration, which
 // then runs to the same residual (so the plain method alone decides the result).
 //
-// Model (hidden width 64; FP32 master weights, BF16 weights and BF16 operands
-// in the dense layers, FP32 accumulation everywhere):
+// Model (hidden width 64, messages 8 wide; FP32 master weights, BF16 weights
+// and BF16 operands in the dense layers, FP32 accumulation everywhere):
 //   features  F(v) = [log(1+indeg), log(1+outdeg), outdeg == 0, 1/n]   (FP32)
-//   layer l   A_l = agg(H_{l-1})                                        (FP32 sums)
-//             H_l = bf16(relu(bf16(H_{l-1}) Ws_l + bf16(A_l) Wn_l + b_l)),  H_0 = F
-//   head      y(v) = H_3(v) . w_o + b_o   (a prediction of log(n * pr(v)))
+//   inv(u)    = 1/outdeg(u), 0 for dangling and deleted nodes           (FP32)
+//   layer 0   M_0(u) = F(u) inv(u);  A_0(v) = sum_{u in in(v)} M_0(u)
+//             H_0 = bf16(relu(bf16(F) Ws_0 + bf16(A_0) Wn_0 + b_0))
+//   layer l   M_l(u) = bf16(inv(u) (H_{l-1}(u) U_l));  A_l = sum over in(v)
+//             H_l = bf16(relu(H_{l-1} Ws_l + bf16(A_l) Wn_l + b_l)),  l = 1, 2
+//   head      y(v) = H_2(v) . w_o + b_o   (a prediction of log(n * pr(v)))
 //   start     x0(v) = exp(y(v)) / sum_u exp(y(u))  (positive, sums to 1)
-// where agg(H)(v) = sum over in-neighbours u of H(u) / max(outdeg(u), 1) --
-// the PageRank propagation operator, so each layer can learn one weighted
-// power step.  Training minimises KL(pr || x0) (or the mean squared error of
-// y against log(n pr)) on PageRank vectors that the plain method computes;
-// the BF16 roundings pass gradients straight through.  Every kernel below is
-// hand-written: the SpMM aggregate and its transpose, the dense layer on the
-// tensor cores (mma.m16n8k16 BF16) with its data and weight gradients, the
-// head, the softmax and Adam; the gradients are checked against a CPU oracle
-// that torch autograd pins.
+// Each layer's aggregate is the PageRank propagation operator applied to a
+// message; the message of layers 1 and 2 is a learned 8-wide projection U_l
+// of the hidden state (agg(H) Wn of a full-width layer in the rank-8 form
+// agg(H U) Wn), so every arc gathers 16 bytes instead of a 128-byte row, and
+// the aggregates that go through HBM are 32 bytes per node.
+//
+// Kernels (all hand-written):
+//   * k_gnn_spmm: the arc-chunked, load-balanced SpMM of the aggregates and of
+//     their transpose (training);
+//   * k_gnn_dense0 / k_gnn_dense_mid: the dense layers on the tensor cores
+//     (mma.m16n8k16, BF16 in, FP32 accumulate) fused with their epilogues --
+//     bias, ReLU, the BF16 hidden state, the next layer's message (a second
+//     product with U) or the head.  A warp owns 16-node tiles; the hidden
+//     tile arrives by a TMA tensor load (128-byte swizzle) and the aggregate
+//     tile by a bulk copy, both double-buffered on mbarriers, and the new
+//     hidden tile leaves by a TMA tensor store from a swizzled staging tile;
+//   * training: the data- and weight-gradient kernels of the dense layers and
+//     of the message projection, the head, the softmax (FP64), the KL and
+//     log-MSE losses, and Adam.  The gradients are checked against a CPU
+//     oracle that torch autograd pins.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -32,35 +50,47 @@ namespace {
 
 constexpr int kH = 64;     // hidden width
 constexpr int kF = 4;      // input features
+constexpr int kR = 8;      // message width of layers 1 and 2
 constexpr int kLayers = 3;
 constexpr uint32_t kGnnMagic = 0x5A4F474E;  // "ZOGN"
-constexpr uint32_t kGnnVersion = 1;
+constexpr uint32_t kGnnVersion = 2;
 
-// Flat parameter layout: per layer [Ws (din x 64) | Wn (din x 64) | b (64)], then [w_o (64) | b_o].
+// Flat parameter layout: layer 0 [Ws (4 x 64) | Wn (4 x 64) | b (64)];
+// layers 1, 2 [U (64 x 8) | Ws (64 x 64) | Wn (8 x 64) | b (64)]; then
+// [w_o (64) | b_o].  Row-major (input index first) throughout.
 constexpr int layer_in(int l) { return l == 0 ? kF : kH; }
-constexpr int layer_size(int l) { return 2 * layer_in(l) * kH + kH; }
+constexpr int layer_msg(int l) { return l == 0 ? kF : kR; }
+constexpr int layer_u(int l) { return l == 0 ? 0 : layer_in(l) * layer_msg(l); }
+constexpr int layer_size(int l) { return layer_u(l) + layer_in(l) * kH + layer_msg(l) * kH + kH; }
 constexpr int layer_offset(int l) { return l == 0 ? 0 : layer_offset(l - 1) + layer_size(l - 1); }
+constexpr int ws_offset(int l) { return layer_offset(l) + layer_u(l); }
+constexpr int wn_offset(int l) { return ws_offset(l) + layer_in(l) * kH; }
+constexpr int bias_offset(int l) { return wn_offset(l) + layer_msg(l) * kH; }
 constexpr int kHeadOffset = layer_offset(kLayers);
 constexpr int kNumParams = kHeadOffset + kH + 1;
+static_assert(kNumParams == 11009, "parameter layout");
 
-__device__ __forceinline__ float warp_sumf(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
+constexpr int kTile = 16;                       // nodes per warp tile
+constexpr int kDenseWarps = 4;                  // warps per dense CTA
+constexpr int kWarpSmem = 8192;                 // per-warp staging area
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // bounded mbarrier waits: 1 s
 
-// ---- features and inverse out-degrees -----------------------------------------
+// ---- features, inverse out-degrees and the layer-0 message ---------------------
 __global__ void k_gnn_features(const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ out_deg, uint32_t V,
-                               float inv_n, float* __restrict__ F, float* __restrict__ inv_deg) {
+                               float inv_n, float* __restrict__ F, float* __restrict__ inv_deg,
+                               float* __restrict__ M0) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     const uint32_t od = out_deg[v];
     const bool deleted = od == kDeletedDegree;
     const float id = (float)(in_off[v + 1] - in_off[v]);
-    F[(size_t)v * kF + 0] = deleted ? 0.f : log1pf(id);
-    F[(size_t)v * kF + 1] = deleted ? 0.f : log1pf((float)od);
-    F[(size_t)v * kF + 2] = (!deleted && od == 0) ? 1.f : 0.f;
-    F[(size_t)v * kF + 3] = deleted ? 0.f : inv_n;
-    inv_deg[v] = (deleted || od == 0) ? 0.f : 1.f / (float)od;
+    const float f0 = deleted ? 0.f : log1pf(id);
+    const float f1 = deleted ? 0.f : log1pf((float)od);
+    const float f2 = (!deleted && od == 0) ? 1.f : 0.f;
+    const float f3 = deleted ? 0.f : inv_n;
+    const float iv = (deleted || od == 0) ? 0.f : 1.f / (float)od;
+    *reinterpret_cast<float4*>(F + (size_t)v * kF) = make_float4(f0, f1, f2, f3);
+    *reinterpret_cast<float4*>(M0 + (size_t)v * kF) = make_float4(f0 * iv, f1 * iv, f2 * iv, f3 * iv);
+    inv_deg[v] = iv;
   }
 }
 
@@ -75,25 +105,26 @@ __device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(_
 __device__ __forceinline__ float to_f32(float x) { return x; }
 __device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162float(x); }
 
-// ---- SpMM aggregate: Z(v) = sum over row v of H(u) * w(u)  [* inv(v) when transposed]
-// Forward: in-CSR, w(u) = 1/outdeg(u).  Backward (transpose of the forward
-// operator): out-CSR, w = 1, and the row sum scaled by 1/outdeg(v).
+// ---- SpMM: Z(v) = sum over row v of X(u)  [* inv(v) when transposed] -----------
+// Forward: in-CSR, the messages already carry 1/outdeg of their source.
+// Transpose (training): out-CSR, the row sum scaled by inv(v) -- the gradient
+// of a message through its 1/outdeg factor.
 //
 // Work split: the arcs are cut into chunks of kChunk arcs that warps take from
 // a shared counter (so a hub row is shared by many warps and no warp holds a
 // fixed share of slow chunks); the first row of every chunk is precomputed
 // (k_chunk_rows).  A row that crosses a chunk boundary is added with atomics,
-// a row inside one chunk is stored directly.  Each arc's feature row (D
-// values of T) is read 16 bytes per lane by LPA = D*sizeof(T)/16 lanes, and a
-// chunk runs in one of two modes:
+// a row inside one chunk is stored directly.  Each arc's row (D values of T)
+// is read 16 bytes per lane by LPA = D*sizeof(T)/16 lanes, and a chunk runs in
+// one of two modes:
 //   * rows mode (the chunk holds several rows, none long): each group of LPA
 //     lanes owns one row and walks its arcs, 32/LPA rows in flight per warp,
 //     four independent gathers in flight per group;
 //   * arcs mode (one or two rows, or a long segment): the whole warp walks
-//     each row's arcs 32/LPA at a time (indices and weights loaded once,
-//     coalesced, and broadcast by shuffles), then folds the groups.
-// Sums are FP32.  With accumulate == 0 the caller zeroes Z first (rows that
-// hold no arc of any chunk are never visited).
+//     each row's arcs 32/LPA at a time (indices loaded once, coalesced, and
+//     broadcast by shuffles), then folds the groups.
+// Sums are FP32.  The caller zeroes Z first (rows that hold no arc of any
+// chunk are never visited).
 constexpr uint32_t kChunk = 128;
 
 __global__ void k_chunk_rows(const uint32_t* __restrict__ off, uint32_t V, uint32_t E, uint32_t* __restrict__ first_row) {
@@ -111,39 +142,31 @@ __global__ void k_chunk_rows(const uint32_t* __restrict__ off, uint32_t V, uint3
 }
 
 template <class T, int PER>
-__device__ __forceinline__ void add_row(float (&acc)[PER], const uint4 x, float w) {
+__device__ __forceinline__ void add_row(float (&acc)[PER], const uint4 x) {
   if (sizeof(T) == 4) {
-    acc[0] += __uint_as_float(x.x) * w;
-    acc[1] += __uint_as_float(x.y) * w;
-    acc[2] += __uint_as_float(x.z) * w;
-    acc[3] += __uint_as_float(x.w) * w;
+    acc[0] += __uint_as_float(x.x);
+    acc[1] += __uint_as_float(x.y);
+    acc[2] += __uint_as_float(x.z);
+    acc[3] += __uint_as_float(x.w);
   } else {
-    acc[0] += bf16_lo(x.x) * w;
-    acc[1] += bf16_hi(x.x) * w;
-    acc[2 % PER] += bf16_lo(x.y) * w;
-    acc[3 % PER] += bf16_hi(x.y) * w;
-    acc[4 % PER] += bf16_lo(x.z) * w;
-    acc[5 % PER] += bf16_hi(x.z) * w;
-    acc[6 % PER] += bf16_lo(x.w) * w;
-    acc[7 % PER] += bf16_hi(x.w) * w;
+    acc[0] += bf16_lo(x.x);
+    acc[1] += bf16_hi(x.x);
+    acc[2 % PER] += bf16_lo(x.y);
+    acc[3 % PER] += bf16_hi(x.y);
+    acc[4 % PER] += bf16_lo(x.z);
+    acc[5 % PER] += bf16_hi(x.z);
+    acc[6 % PER] += bf16_lo(x.w);
+    acc[7 % PER] += bf16_hi(x.w);
   }
 }
 
-// writes or adds one row's PER values held by one lane
+// adds one row's PER values held by one lane (whole rows are stored: Z starts at zero)
 template <int D, int PER>
-__device__ __forceinline__ void put_row(float* __restrict__ Z, uint32_t r, int sub, float (&acc)[PER], bool whole,
-                                        int accumulate) {
+__device__ __forceinline__ void put_row(float* __restrict__ Z, uint32_t r, int sub, float (&acc)[PER], bool whole) {
   float* z = Z + (size_t)r * D + sub * PER;
   if (whole) {
 #pragma unroll
-    for (int i = 0; i < PER; i += 4) {
-      float4 o = accumulate ? *reinterpret_cast<float4*>(z + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-      o.x += acc[i];
-      o.y += acc[i + 1];
-      o.z += acc[i + 2];
-      o.w += acc[i + 3];
-      *reinterpret_cast<float4*>(z + i) = o;
-    }
+    for (int i = 0; i < PER; i += 4) *reinterpret_cast<float4*>(z + i) = make_float4(acc[i], acc[i + 1], acc[i + 2], acc[i + 3]);
   } else {
 #pragma unroll
     for (int i = 0; i < PER; ++i) atomicAdd(z + i, acc[i]);
@@ -152,16 +175,16 @@ __device__ __forceinline__ void put_row(float* __restrict__ Z, uint32_t r, int s
 
 template <class T, int D>
 __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                  const float* __restrict__ inv_deg, const T* __restrict__ H,
+                                                  const float* __restrict__ inv_deg, const T* __restrict__ X,
                                                   uint32_t V, uint32_t E, int transpose, float* __restrict__ Z,
-                                                  int accumulate, uint32_t* __restrict__ next_chunk,
+                                                  uint32_t* __restrict__ next_chunk,
                                                   const uint32_t* __restrict__ first_row) {
   constexpr int PER = 16 / (int)sizeof(T);  // values per lane
   constexpr int LPA = D / PER;              // lanes per arc
   constexpr int APW = 32 / LPA;             // arcs per warp step = rows per warp in rows mode
   static_assert(LPA >= 1 && LPA <= 32 && 32 % LPA == 0, "row width");
   const int lane = threadIdx.x & 31, sub = lane % LPA, grp = lane / LPA;
-  const uint4* __restrict__ H16 = reinterpret_cast<const uint4*>(H);
+  const uint4* __restrict__ X16 = reinterpret_cast<const uint4*>(X);
   const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
   for (;;) {
     uint32_t c = 0;
@@ -193,29 +216,22 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
           uint32_t j = b;
           for (; j + 4 <= e; j += 4) {
             uint32_t u[4];
-            float w[4];
             uint4 x[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) u[k] = __ldg(col + j + k);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              w[k] = transpose ? 1.f : __ldg(inv_deg + u[k]);
-              x[k] = __ldg(H16 + (size_t)u[k] * LPA + sub);
-            }
+            for (int k = 0; k < 4; ++k) x[k] = __ldg(X16 + (size_t)u[k] * LPA + sub);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) add_row<T, PER>(acc, x[k], w[k]);
+            for (int k = 0; k < 4; ++k) add_row<T, PER>(acc, x[k]);
           }
-          for (; j < e; ++j) {
-            const uint32_t u = __ldg(col + j);
-            add_row<T, PER>(acc, __ldg(H16 + (size_t)u * LPA + sub), transpose ? 1.f : __ldg(inv_deg + u));
-          }
+          for (; j < e; ++j) add_row<T, PER>(acc, __ldg(X16 + (size_t)__ldg(col + j) * LPA + sub));
           const uint32_t r = r0 + q;
           if (transpose) {
             const float sc = __ldg(inv_deg + r);
 #pragma unroll
             for (int i = 0; i < PER; ++i) acc[i] *= sc;
           }
-          put_row<D, PER>(Z, r, sub, acc, qb >= cs && qe <= ce, accumulate);
+          put_row<D, PER>(Z, r, sub, acc, qb >= cs && qe <= ce);
         }
         // rows are sync-free in this mode; reconverge before the next ballot
         __syncwarp();
@@ -229,18 +245,12 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
           for (int i = 0; i < PER; ++i) acc[i] = 0.f;
           for (uint32_t j0 = b; j0 < e; j0 += 32) {
             const uint32_t n = min(32u, e - j0);
-            uint32_t u_l = 0;
-            float w_l = 0.f;
-            if ((uint32_t)lane < n) {
-              u_l = __ldg(col + j0 + lane);
-              w_l = transpose ? 1.f : __ldg(inv_deg + u_l);
-            }
+            const uint32_t u_l = (uint32_t)lane < n ? __ldg(col + j0 + lane) : 0u;
 #pragma unroll 4
             for (uint32_t k = 0; k < n; k += APW) {
               const uint32_t idx = k + grp;
               const uint32_t u = __shfl_sync(0xffffffffu, u_l, idx & 31);
-              const float w = __shfl_sync(0xffffffffu, w_l, idx & 31);
-              if (idx < n) add_row<T, PER>(acc, __ldg(H16 + (size_t)u * LPA + sub), w);
+              if (idx < n) add_row<T, PER>(acc, __ldg(X16 + (size_t)u * LPA + sub));
             }
           }
 #pragma unroll
@@ -254,7 +264,7 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
 #pragma unroll
               for (int i = 0; i < PER; ++i) acc[i] *= sc;
             }
-            put_row<D, PER>(Z, r, sub, acc, qb >= cs && qe <= ce, accumulate);
+            put_row<D, PER>(Z, r, sub, acc, qb >= cs && qe <= ce);
           }
         }
       }
@@ -264,14 +274,7 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
   }
 }
 
-// ---- dense layer forward on the tensor cores ---------------------------------
-// Out = bf16(relu([X | A] W + b)) with W = [Ws ; Wn] (2*DIN x 64, BF16) and the
-// operands [X | A] rounded to BF16; products accumulate in FP32
-// (mma.m16n8k16, BF16 in, FP32 out).  Each warp computes 16-node tiles: A
-// fragments come straight from global memory (row g / g+8, columns
-// 2t, 2t+1, 2t+8, 2t+9 of each 16-wide k-step), the weight fragments sit in
-// shared memory in fragment order (one conflict-free 8-byte load per mma),
-// and the epilogue adds the bias, applies ReLU and stores BF16 pairs.
+// ---- tensor-core, TMA and mbarrier primitives --------------------------------
 __device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                                  uint32_t b0, uint32_t b1) {
   asm volatile(
@@ -280,87 +283,347 @@ __device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], uint32_t a0, uin
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
-
-// elements (k, k+1) of row `row` of [X | A] as a BF16 pair (k even; 0 past 2*DIN)
-template <int DIN, class XT>
-__device__ __forceinline__ uint32_t dense_pair(const XT* __restrict__ X, const float* __restrict__ A, uint32_t row,
-                                               bool valid, int k) {
-  if (!valid || k >= 2 * DIN) return 0u;
-  if (k < DIN) {
-    if (sizeof(XT) == 2) return __ldg(reinterpret_cast<const uint32_t*>(X + (size_t)row * DIN + k));
-    const float2 v = __ldg(reinterpret_cast<const float2*>(X + (size_t)row * DIN + k));
-    return pack_bf16x2(v.x, v.y);
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// non-blocking test of the barrier's phase
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// bounded wait: false when the phase did not complete within kWaitLimitNs
+// (polls, then polls with a short sleep)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int i = 0; i < 64; ++i)
+    if (mbar_test_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_test_wait(bar, parity)) {
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+    __nanosleep(64);
   }
-  const float2 v = __ldg(reinterpret_cast<const float2*>(A + (size_t)row * DIN + (k - DIN)));
-  return pack_bf16x2(v.x, v.y);
+  return true;
+}
+__device__ __forceinline__ void tma_load_rows(void* dst, const CUtensorMap* map, int row, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(0), "r"(row), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tma_store_rows(const CUtensorMap* map, const void* src, int row) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(map), "r"(0),
+               "r"(row), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// A 16-node tile of 64 BF16 values per node as TMA lands it with the 128-byte
+// swizzle: node r's 16-byte chunk c sits at r*128 + ((c ^ (r & 7)) * 16)
+// (the buffer is 1024-byte aligned).
+__device__ __forceinline__ uint32_t swz(uint32_t base, int r, int c) {
+  return base + (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4));
 }
 
-template <int DIN, class XT>
-__global__ void __launch_bounds__(256) k_gnn_dense_fwd(const XT* __restrict__ X, const float* __restrict__ A,
-                                                       const __nv_bfloat16* __restrict__ w, uint32_t V,
-                                                       __nv_bfloat16* __restrict__ Out) {
-  constexpr int K = 2 * DIN;
-  constexpr int KS = (K + 15) / 16;  // k-steps
-  __shared__ uint2 s_b[KS][8][32];  // weight fragments: [k-step][n-tile][lane]
-  __shared__ float s_bias[kH];
-  for (int i = threadIdx.x; i < KS * 8 * 32; i += blockDim.x) {
+// Weight fragments of the dense product in mma B-fragment order:
+// frag[ks][nt][lane] = (W[k0][n], W[k0+1][n]), (W[k0+8][n], W[k0+9][n]) with
+// n = nt*8 + lane/4, k0 = ks*16 + 2*(lane%4); rows k of the stacked [Ws; Wn]
+// past its end are zero.  One 8-byte shared load per mma, conflict-free.
+__device__ void load_dense_frags(uint2* frag, int ksteps, const __nv_bfloat16* __restrict__ ws, int din,
+                                 const __nv_bfloat16* __restrict__ wn, int dmsg) {
+  const int K = din + dmsg;
+  for (int i = threadIdx.x; i < ksteps * 8 * 32; i += blockDim.x) {
     const int ks = i / 256, nt = (i / 32) % 8, l = i % 32;
     const int n = nt * 8 + (l >> 2), k0 = ks * 16 + (l & 3) * 2;
-    auto wk = [&](int k) { return k < K ? __bfloat162float(w[(size_t)k * kH + n]) : 0.f; };
-    s_b[ks][nt][l] = make_uint2(pack_bf16x2(wk(k0), wk(k0 + 1)), pack_bf16x2(wk(k0 + 8), wk(k0 + 9)));
+    auto wk = [&](int k) {
+      if (k < din) return __bfloat162float(ws[(size_t)k * kH + n]);
+      if (k < K) return __bfloat162float(wn[(size_t)(k - din) * kH + n]);
+      return 0.f;
+    };
+    frag[i] = make_uint2(pack_bf16x2(wk(k0), wk(k0 + 1)), pack_bf16x2(wk(k0 + 8), wk(k0 + 9)));
   }
-  for (int i = threadIdx.x; i < kH; i += blockDim.x) s_bias[i] = __bfloat162float(w[(size_t)K * kH + i]);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const uint32_t tiles = (V + 15) / 16;
-  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += nw) {
-    const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
-    const bool v0 = r0 < V, v1 = r1 < V;
-    float acc[8][4];
+}
+// U (64 x 8) as B fragments of the message product: frag[ks][lane], 4 k-steps
+__device__ void load_msg_frags(uint2* frag, const __nv_bfloat16* __restrict__ u) {
+  for (int i = threadIdx.x; i < 4 * 32; i += blockDim.x) {
+    const int ks = i / 32, l = i % 32;
+    const int n = l >> 2, k0 = ks * 16 + (l & 3) * 2;
+    auto uk = [&](int k) { return __bfloat162float(u[(size_t)k * kR + n]); };
+    frag[i] = make_uint2(pack_bf16x2(uk(k0), uk(k0 + 1)), pack_bf16x2(uk(k0 + 8), uk(k0 + 9)));
+  }
+}
+
+// Shared epilogue of a 16-node tile (rows r0 .. r0+15; lane = 4g + t holds
+// rows g and g+8, columns nt*8 + 2t, +1 of every n-tile):
+//   h = bf16(relu(acc + b)); optionally H out by a TMA store of a swizzled
+//   staging tile; then either the next message M = bf16(inv * (h U)) or the
+//   head y = h . w_o + b_o.
+struct DenseOut {
+  const CUtensorMap* map_h;     // hidden-state output (null: not stored)
+  const uint2* ufrag;           // message projection (null: last layer)
+  const float* bias;            // 64 (shared)
+  const float* wo;              // 65 (shared; last layer)
+  const float* inv;             // 1/outdeg
+  __nv_bfloat16* M;             // next message, V x 8
+  float* y;                     // head output, V
+  uint32_t V;
+};
+
+__device__ __forceinline__ void dense_epilogue(const DenseOut& o, float (&acc)[8][4], uint32_t r0,
+                                               unsigned char* stage, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  uint32_t hp[8][2];
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+  for (int nt = 0; nt < 8; ++nt) {
+    const int c = nt * 8 + t * 2;
+    const float b0 = o.bias[c], b1 = o.bias[c + 1];
+    hp[nt][0] = pack_bf16x2(fmaxf(acc[nt][0] + b0, 0.f), fmaxf(acc[nt][1] + b1, 0.f));
+    hp[nt][1] = pack_bf16x2(fmaxf(acc[nt][2] + b0, 0.f), fmaxf(acc[nt][3] + b1, 0.f));
+  }
+  if (o.map_h) {
+    // the previous tile's store must have read the staging tile
+    if (lane == 0) bulk_wait_read_all();
+    __syncwarp();
+    const uint32_t sb = smem_u32(stage);
 #pragma unroll
-    for (int ks = 0; ks < KS; ++ks) {
-      const int k = ks * 16 + t * 2;
-      const uint32_t a0 = dense_pair<DIN>(X, A, r0, v0, k);
-      const uint32_t a1 = dense_pair<DIN>(X, A, r1, v1, k);
-      const uint32_t a2 = dense_pair<DIN>(X, A, r0, v0, k + 8);
-      const uint32_t a3 = dense_pair<DIN>(X, A, r1, v1, k + 8);
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        const uint2 bb = s_b[ks][nt][lane];
-        mma_bf16_16x8x16(acc[nt], a0, a1, a2, a3, bb.x, bb.y);
-      }
+    for (int nt = 0; nt < 8; ++nt) {
+      asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(swz(sb, g, nt) + 4 * t), "r"(hp[nt][0]) : "memory");
+      asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(swz(sb, g + 8, nt) + 4 * t), "r"(hp[nt][1]) : "memory");
     }
+    fence_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      tma_store_rows(o.map_h, stage, (int)r0);
+      bulk_commit();
+    }
+  }
+  const uint32_t ra = r0 + g, rb = r0 + g + 8;
+  if (o.ufrag) {
+    float m[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const uint2 bb = o.ufrag[kk * 32 + lane];
+      mma_bf16_16x8x16(m, hp[2 * kk][0], hp[2 * kk][1], hp[2 * kk + 1][0], hp[2 * kk + 1][1], bb.x, bb.y);
+    }
+    if (ra < o.V) {
+      const float s = __ldg(o.inv + ra);
+      *reinterpret_cast<uint32_t*>(o.M + (size_t)ra * kR + 2 * t) = pack_bf16x2(m[0] * s, m[1] * s);
+    }
+    if (rb < o.V) {
+      const float s = __ldg(o.inv + rb);
+      *reinterpret_cast<uint32_t*>(o.M + (size_t)rb * kR + 2 * t) = pack_bf16x2(m[2] * s, m[3] * s);
+    }
+  } else {
+    float s0 = 0.f, s1 = 0.f;
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
       const int c = nt * 8 + t * 2;
-      const float b0 = s_bias[c], b1 = s_bias[c + 1];
-      if (v0)
-        *reinterpret_cast<uint32_t*>(Out + (size_t)r0 * kH + c) =
-            pack_bf16x2(fmaxf(acc[nt][0] + b0, 0.f), fmaxf(acc[nt][1] + b1, 0.f));
-      if (v1)
-        *reinterpret_cast<uint32_t*>(Out + (size_t)r1 * kH + c) =
-            pack_bf16x2(fmaxf(acc[nt][2] + b0, 0.f), fmaxf(acc[nt][3] + b1, 0.f));
+      s0 += bf16_lo(hp[nt][0]) * o.wo[c] + bf16_hi(hp[nt][0]) * o.wo[c + 1];
+      s1 += bf16_lo(hp[nt][1]) * o.wo[c] + bf16_hi(hp[nt][1]) * o.wo[c + 1];
+    }
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+    s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+    if (t == 0) {
+      if (ra < o.V) o.y[ra] = s0 + o.wo[kH];
+      if (rb < o.V) o.y[rb] = s1 + o.wo[kH];
     }
   }
 }
 
-// ---- dense layer backward (data): dP = dOut * (Out > 0); dX = dP Ws^T, dA = dP Wn^T
-// (the BF16 rounding of the forward operands passes the gradient straight
-// through).  dP is written back in place of dOut for the weight-gradient kernel.
-template <int DIN>
+// Shared-memory layout of the dense kernels: kDenseWarps per-warp areas of
+// kWarpSmem bytes (1024-aligned) -- [x tile 0 | x tile 1 | H staging | aggregate
+// tile 0 | aggregate tile 1 | 2 mbarriers] -- then the weight fragments, U
+// fragments, bias and head.
+constexpr int kXBytes = kTile * kH * 2;   // 2048
+constexpr int kABytes = kTile * kR * 4;   // 512
+constexpr int kDenseFragBytes = 5 * 8 * 32 * 8;
+constexpr int kMsgFragBytes = 4 * 32 * 8;
+constexpr size_t kDenseSmem = 1024 + kDenseWarps * kWarpSmem + kDenseFragBytes + kMsgFragBytes + (kH + kH + 1) * 4;
+
+struct DenseSmem {
+  unsigned char* warp_area;
+  uint2* frag;
+  uint2* ufrag;
+  float* bias;
+  float* wo;
+};
+__device__ __forceinline__ DenseSmem dense_smem(unsigned char* raw) {
+  DenseSmem d;
+  const uint32_t a = smem_u32(raw);
+  d.warp_area = raw + (((a + 1023u) & ~1023u) - a);
+  d.frag = reinterpret_cast<uint2*>(d.warp_area + kDenseWarps * kWarpSmem);
+  d.ufrag = d.frag + kDenseFragBytes / 8;
+  d.bias = reinterpret_cast<float*>(d.ufrag + kMsgFragBytes / 8);
+  d.wo = d.bias + kH;
+  return d;
+}
+
+// Layer 0: [F | A_0] (4 + 4 FP32 values per node, read directly; one k-step)
+// times [Ws_0; Wn_0], then the epilogue (H_0 by TMA store, M_1).
+__global__ void __launch_bounds__(kDenseWarps * 32) k_gnn_dense0(const __grid_constant__ CUtensorMap map_h,
+                                                                  const float* __restrict__ F,
+                                                                  const float* __restrict__ A0,
+                                                                  const __nv_bfloat16* __restrict__ w,
+                                                                  const float* __restrict__ inv, uint32_t V,
+                                                                  uint32_t ntiles, __nv_bfloat16* __restrict__ M1) {
+  extern __shared__ unsigned char smem_raw[];
+  const DenseSmem S = dense_smem(smem_raw);
+  load_dense_frags(S.frag, 1, w + ws_offset(0), kF, w + wn_offset(0), kF);
+  load_msg_frags(S.ufrag, w + layer_offset(1));
+  for (int i = threadIdx.x; i < kH; i += blockDim.x) S.bias[i] = __bfloat162float(w[bias_offset(0) + i]);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  unsigned char* stage = S.warp_area + warp * kWarpSmem + 2 * kXBytes;
+  DenseOut o{&map_h, S.ufrag, S.bias, nullptr, inv, M1, nullptr, V};
+  for (uint32_t tile = blockIdx.x * kDenseWarps + warp; tile < ntiles; tile += gridDim.x * kDenseWarps) {
+    const uint32_t r0 = tile * kTile, ra = r0 + g, rb = ra + 8;
+    // k = 2t, 2t+1: features for t < 2, aggregate for t = 2, 3; k >= 8 zero
+    const float* srca = t < 2 ? F + (size_t)ra * kF + 2 * t : A0 + (size_t)ra * kF + 2 * (t - 2);
+    const float* srcb = t < 2 ? F + (size_t)rb * kF + 2 * t : A0 + (size_t)rb * kF + 2 * (t - 2);
+    const float2 va = ra < V ? __ldg(reinterpret_cast<const float2*>(srca)) : make_float2(0.f, 0.f);
+    const float2 vb = rb < V ? __ldg(reinterpret_cast<const float2*>(srcb)) : make_float2(0.f, 0.f);
+    const uint32_t a0 = pack_bf16x2(va.x, va.y), a1 = pack_bf16x2(vb.x, vb.y);
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+      const uint2 bb = S.frag[nt * 32 + lane];
+      mma_bf16_16x8x16(acc[nt], a0, a1, 0u, 0u, bb.x, bb.y);
+    }
+    dense_epilogue(o, acc, r0, stage, lane);
+    __syncwarp();
+  }
+  if (lane == 0) bulk_wait_all();
+}
+
+// Layers 1 and 2: [H_{l-1} | A_l] (64 BF16 + 8 FP32 values per node; five
+// k-steps) times [Ws_l; Wn_l].  Per warp, the next tile's hidden rows (TMA
+// tensor load, 128-byte swizzle, fragments by ldmatrix) and aggregates (bulk
+// copy) land while the current tile computes.  LAST: the head instead of a
+// next message, and H_2 is stored only when store_h (training).
+template <int LAST>
+__global__ void __launch_bounds__(kDenseWarps * 32) k_gnn_dense_mid(
+    const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_h,
+    const float* __restrict__ A, const __nv_bfloat16* __restrict__ w, int layer, const float* __restrict__ inv,
+    uint32_t V, uint32_t ntiles, int store_h, __nv_bfloat16* __restrict__ M_next, float* __restrict__ y,
+    unsigned int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const DenseSmem S = dense_smem(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  // per-warp area: x tiles at wa + b*kXBytes, the H staging tile, aggregate
+  // tiles at abase + b*kABytes, two mbarriers
+  unsigned char* wa = S.warp_area + warp * kWarpSmem;
+  unsigned char* stage = wa + 2 * kXBytes;
+  unsigned char* abase = wa + 3 * kXBytes;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wa + 3 * kXBytes + 2 * kABytes);
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  load_dense_frags(S.frag, 5, w + ws_offset(layer), kH, w + wn_offset(layer), kR);
+  if (!LAST) load_msg_frags(S.ufrag, w + layer_offset(layer + 1));
+  for (int i = threadIdx.x; i < kH; i += blockDim.x) S.bias[i] = __bfloat162float(w[bias_offset(layer) + i]);
+  if (LAST)
+    for (int i = threadIdx.x; i <= kH; i += blockDim.x) S.wo[i] = __bfloat162float(w[kHeadOffset + i]);
+  __syncthreads();
+  DenseOut o{store_h ? &map_h : nullptr, LAST ? nullptr : S.ufrag, S.bias, S.wo, inv, M_next, y, V};
+  const uint32_t nw = gridDim.x * kDenseWarps;
+  const uint32_t first = blockIdx.x * kDenseWarps + warp;
+  auto issue = [&](uint32_t tile, int b) {
+    mbar_expect_tx(&bar[b], kXBytes + kABytes);
+    tma_load_rows(wa + b * kXBytes, &map_x, (int)(tile * kTile), &bar[b]);
+    bulk_load(abase + b * kABytes, A + (size_t)tile * kTile * kR, kABytes, &bar[b]);
+  };
+  if (first < ntiles && lane == 0) issue(first, 0);
+  uint32_t i = 0;
+  for (uint32_t tile = first; tile < ntiles; tile += nw, ++i) {
+    const int b = i & 1;
+    const bool more = tile + nw < ntiles;  // the next tile's load is issued now, waited for next iteration
+    if (more && lane == 0) issue(tile + nw, b ^ 1);
+    if (!mbar_wait(&bar[b], (i >> 1) & 1)) {
+      // record the failure, let the load already issued for the next tile land
+      // (bounded), and leave the loop
+      if (lane == 0) atomicExch(err, 1u);
+      if (more) mbar_wait(&bar[b ^ 1], ((i + 1) >> 1) & 1);
+      break;
+    }
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+    const uint32_t xb = smem_u32(wa + b * kXBytes);
+    const float* at = reinterpret_cast<const float*>(abase + b * kABytes);
+    const int q = lane >> 3, rr = (lane & 7) + (q & 1) * 8;
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      uint32_t a0, a1, a2, a3;
+      ldmatrix_x4(swz(xb, rr, 2 * ks + (q >> 1)), a0, a1, a2, a3);
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const uint2 bb = S.frag[(ks * 8 + nt) * 32 + lane];
+        mma_bf16_16x8x16(acc[nt], a0, a1, a2, a3, bb.x, bb.y);
+      }
+    }
+    {  // aggregate columns: k = 64 + 2t, 2t+1 (rows g, g+8); k >= 72 zero
+      const float2 va = *reinterpret_cast<const float2*>(at + g * kR + 2 * t);
+      const float2 vb = *reinterpret_cast<const float2*>(at + (g + 8) * kR + 2 * t);
+      const uint32_t a0 = pack_bf16x2(va.x, va.y), a1 = pack_bf16x2(vb.x, vb.y);
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const uint2 bb = S.frag[(4 * 8 + nt) * 32 + lane];
+        mma_bf16_16x8x16(acc[nt], a0, a1, 0u, 0u, bb.x, bb.y);
+      }
+    }
+    dense_epilogue(o, acc, tile * kTile, stage, lane);
+    __syncwarp();
+  }
+  if (lane == 0) bulk_wait_all();
+}
+
+// ---- dense layer backward (data): dP = dOut * (Out > 0); dX = dP Ws^T (DIN),
+// dA = dP Wn^T (DM) (the BF16 roundings of the forward operands pass the
+// gradient straight through).  dP is written back in place of dOut for the
+// weight-gradient kernel.
+template <int DIN, int DM>
 __global__ void __launch_bounds__(256) k_gnn_dense_bwd_data(float* __restrict__ dOut,
                                                             const __nv_bfloat16* __restrict__ Out,
-                                                            const __nv_bfloat16* __restrict__ w, uint32_t V,
+                                                            const __nv_bfloat16* __restrict__ ws,
+                                                            const __nv_bfloat16* __restrict__ wn, uint32_t V,
                                                             float* __restrict__ dX, float* __restrict__ dA) {
   __shared__ float s_ws[DIN][kH];
-  __shared__ float s_wn[DIN][kH];
-  for (int i = threadIdx.x; i < DIN * kH; i += blockDim.x) {
-    s_ws[i / kH][i % kH] = __bfloat162float(w[i]);
-    s_wn[i / kH][i % kH] = __bfloat162float(w[DIN * kH + i]);
-  }
+  __shared__ float s_wn[DM][kH];
+  for (int i = threadIdx.x; i < DIN * kH; i += blockDim.x) s_ws[i / kH][i % kH] = __bfloat162float(ws[i]);
+  for (int i = threadIdx.x; i < DM * kH; i += blockDim.x) s_wn[i / kH][i % kH] = __bfloat162float(wn[i]);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
@@ -372,54 +635,50 @@ __global__ void __launch_bounds__(256) k_gnn_dense_bwd_data(float* __restrict__ 
     d[lane] = p0;
     d[lane + 32] = p1;
     // output k of dX / dA: sum_j dP[j] W[k][j]; lane handles k = lane, lane+32
-    float x0 = 0.f, x1 = 0.f, a0 = 0.f, a1 = 0.f;
+    float x0 = 0.f, x1 = 0.f, a0 = 0.f;
 #pragma unroll 8
     for (int j = 0; j < kH; ++j) {
       const float pj = __shfl_sync(0xffffffffu, j < 32 ? p0 : p1, j & 31);
-      if (lane < DIN) {
-        x0 += pj * s_ws[lane][j];
-        a0 += pj * s_wn[lane][j];
-      }
-      if (lane + 32 < DIN) {
-        x1 += pj * s_ws[lane + 32][j];
-        a1 += pj * s_wn[lane + 32][j];
-      }
+      if (lane < DIN) x0 += pj * s_ws[lane][j];
+      if (lane + 32 < DIN) x1 += pj * s_ws[lane + 32][j];
+      if (lane < DM) a0 += pj * s_wn[lane][j];
     }
-    if (lane < DIN) {
-      dX[(size_t)v * DIN + lane] = x0;
-      dA[(size_t)v * DIN + lane] = a0;
-    }
-    if (lane + 32 < DIN) {
-      dX[(size_t)v * DIN + lane + 32] = x1;
-      dA[(size_t)v * DIN + lane + 32] = a1;
-    }
+    if (lane < DIN) dX[(size_t)v * DIN + lane] = x0;
+    if (lane + 32 < DIN) dX[(size_t)v * DIN + lane + 32] = x1;
+    if (lane < DM) dA[(size_t)v * DM + lane] = a0;
   }
 }
 
-// ---- dense layer backward (weights): dWs += bf16(X)^T dP, dWn += bf16(A)^T dP,
-// db += sum dP -- the operands the forward pass multiplied.  Each block folds
-// a tile of nodes in shared memory, then adds its partial into the global FP32
-// gradient with one atomic per weight.
-template <int DIN, class XT>
+// ---- dense layer backward (weights): dWs += X^T dP, dWn += bf16(A)^T dP,
+// db += sum dP -- the operands the forward pass multiplied (X = bf16(F) for
+// layer 0, the BF16 hidden state otherwise).  Each block folds a tile of nodes
+// in shared memory, then adds its partial into the global FP32 gradient
+// ([Ws | Wn | b] of the layer) with one atomic per weight.
+template <int DIN, int DM, class XT>
 __global__ void __launch_bounds__(256) k_gnn_dense_bwd_weight(const XT* __restrict__ X, const float* __restrict__ A,
                                                               const float* __restrict__ dP, uint32_t V,
                                                               float* __restrict__ grad) {
   constexpr int TILE = 32;
   __shared__ float s_x[TILE][DIN];
-  __shared__ float s_a[TILE][DIN];
+  __shared__ float s_a[TILE][DM];
   __shared__ float s_p[TILE][kH];
-  // thread t owns outputs (k, j) = (t / kH + r * 256 / kH, t % kH) for r < DIN*kH/256
-  constexpr int PER = (DIN * kH + 255) / 256;
-  float gs[PER], gn[PER], gb = 0.f;
+  constexpr int PS = (DIN * kH + 255) / 256;
+  constexpr int PN = (DM * kH + 255) / 256;
+  float gs[PS], gn[PN], gb = 0.f;
 #pragma unroll
-  for (int r = 0; r < PER; ++r) gs[r] = gn[r] = 0.f;
+  for (int r = 0; r < PS; ++r) gs[r] = 0.f;
+#pragma unroll
+  for (int r = 0; r < PN; ++r) gn[r] = 0.f;
   for (uint32_t base = blockIdx.x * TILE; base < V; base += gridDim.x * TILE) {
     const uint32_t cnt = min((uint32_t)TILE, V - base);
     __syncthreads();
     for (int i = threadIdx.x; i < TILE * DIN; i += blockDim.x) {
       const uint32_t n = i / DIN;
       s_x[n][i % DIN] = n < cnt ? bf16_round(to_f32(X[(size_t)(base + n) * DIN + i % DIN])) : 0.f;
-      s_a[n][i % DIN] = n < cnt ? bf16_round(A[(size_t)(base + n) * DIN + i % DIN]) : 0.f;
+    }
+    for (int i = threadIdx.x; i < TILE * DM; i += blockDim.x) {
+      const uint32_t n = i / DM;
+      s_a[n][i % DM] = n < cnt ? bf16_round(A[(size_t)(base + n) * DM + i % DM]) : 0.f;
     }
     for (int i = threadIdx.x; i < TILE * kH; i += blockDim.x) {
       const uint32_t n = i / kH;
@@ -427,16 +686,22 @@ __global__ void __launch_bounds__(256) k_gnn_dense_bwd_weight(const XT* __restri
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < PER; ++r) {
+    for (int r = 0; r < PS; ++r) {
       const int idx = threadIdx.x + r * 256;
       if (idx < DIN * kH) {
         const int k = idx / kH, j = idx % kH;
-        float s1 = 0.f, s2 = 0.f;
-        for (int n = 0; n < TILE; ++n) {
-          s1 += s_x[n][k] * s_p[n][j];
-          s2 += s_a[n][k] * s_p[n][j];
-        }
+        float s1 = 0.f;
+        for (int n = 0; n < TILE; ++n) s1 += s_x[n][k] * s_p[n][j];
         gs[r] += s1;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < PN; ++r) {
+      const int idx = threadIdx.x + r * 256;
+      if (idx < DM * kH) {
+        const int k = idx / kH, j = idx % kH;
+        float s2 = 0.f;
+        for (int n = 0; n < TILE; ++n) s2 += s_a[n][k] * s_p[n][j];
         gn[r] += s2;
       }
     }
@@ -444,29 +709,62 @@ __global__ void __launch_bounds__(256) k_gnn_dense_bwd_weight(const XT* __restri
       for (int n = 0; n < TILE; ++n) gb += s_p[n][threadIdx.x];
   }
 #pragma unroll
-  for (int r = 0; r < PER; ++r) {
+  for (int r = 0; r < PS; ++r) {
     const int idx = threadIdx.x + r * 256;
-    if (idx < DIN * kH) {
-      atomicAdd(grad + idx, gs[r]);
-      atomicAdd(grad + DIN * kH + idx, gn[r]);
-    }
+    if (idx < DIN * kH) atomicAdd(grad + idx, gs[r]);
   }
-  if (threadIdx.x < kH) atomicAdd(grad + 2 * DIN * kH + threadIdx.x, gb);
+#pragma unroll
+  for (int r = 0; r < PN; ++r) {
+    const int idx = threadIdx.x + r * 256;
+    if (idx < DM * kH) atomicAdd(grad + DIN * kH + idx, gn[r]);
+  }
+  if (threadIdx.x < kH) atomicAdd(grad + DIN * kH + DM * kH + threadIdx.x, gb);
 }
 
-// ---- head forward: y = H3 . w_o + b_o ----------------------------------------
-__global__ void __launch_bounds__(256) k_gnn_head(const __nv_bfloat16* __restrict__ H,
-                                                  const __nv_bfloat16* __restrict__ wo, uint32_t V,
-                                                  float* __restrict__ y) {
-  const int lane = threadIdx.x & 31;
-  const float w0 = __bfloat162float(wo[2 * lane]), w1 = __bfloat162float(wo[2 * lane + 1]);
-  const float bo = __bfloat162float(wo[kH]);
+// ---- message backward: with dQ = inv * agg^T(dA) (the gradient of Q = H U),
+// dH_prev = dX + dQ U^T (in place of dX) and dU += H_prev^T dQ.  One warp per
+// node, lane j owns columns j and j+32; the block folds its warps' dU in
+// shared memory and adds it with one atomic per weight.
+__global__ void __launch_bounds__(256) k_gnn_msg_bwd(const float* __restrict__ dQ,
+                                                     const __nv_bfloat16* __restrict__ Hp,
+                                                     const __nv_bfloat16* __restrict__ u, uint32_t V,
+                                                     float* __restrict__ dX, float* __restrict__ gradU) {
+  __shared__ float s_u[kH][kR];
+  __shared__ float s_g[8][kH * kR];
+  for (int i = threadIdx.x; i < kH * kR; i += blockDim.x) s_u[i / kR][i % kR] = __bfloat162float(u[i]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float g0[kR], g1[kR];
+#pragma unroll
+  for (int k = 0; k < kR; ++k) g0[k] = g1[k] = 0.f;
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
   for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nw) {
-    const uint32_t h = __ldg(reinterpret_cast<const uint32_t*>(H + (size_t)v * kH) + lane);
-    float s = bf16_lo(h) * w0 + bf16_hi(h) * w1;
-    s = warp_sumf(s);
-    if (lane == 0) y[v] = s + bo;
+    const float4 qa = __ldg(reinterpret_cast<const float4*>(dQ + (size_t)v * kR));
+    const float4 qb = __ldg(reinterpret_cast<const float4*>(dQ + (size_t)v * kR + 4));
+    const float q[kR] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+    const float h0 = __bfloat162float(Hp[(size_t)v * kH + lane]);
+    const float h1 = __bfloat162float(Hp[(size_t)v * kH + lane + 32]);
+    float d0 = dX[(size_t)v * kH + lane], d1 = dX[(size_t)v * kH + lane + 32];
+#pragma unroll
+    for (int k = 0; k < kR; ++k) {
+      d0 += q[k] * s_u[lane][k];
+      d1 += q[k] * s_u[lane + 32][k];
+      g0[k] += h0 * q[k];
+      g1[k] += h1 * q[k];
+    }
+    dX[(size_t)v * kH + lane] = d0;
+    dX[(size_t)v * kH + lane + 32] = d1;
+  }
+#pragma unroll
+  for (int k = 0; k < kR; ++k) {
+    s_g[warp][lane * kR + k] = g0[k];
+    s_g[warp][(lane + 32) * kR + k] = g1[k];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kH * kR; i += blockDim.x) {
+    float s = 0.f;
+    for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) s += s_g[w8][i];
+    atomicAdd(gradU + i, s);
   }
 }
 
@@ -476,7 +774,7 @@ __global__ void __launch_bounds__(256) k_gnn_head(const __nv_bfloat16* __restric
 // mode 1: loss = KL(pr || x0) with x0 = softmax(y) over live nodes
 //              = sum_v pr(v) (log pr(v) - (y(v) - ymax) + log S),  S = sum exp(y - ymax)
 //         dy = x0 - pr   (pr sums to 1)
-// then dH3 = dy w_o, dw_o = sum dy H3, db_o = sum dy.  The loss is summed in FP64.
+// then dH = dy w_o, dw_o = sum dy H, db_o = sum dy.  The loss is summed in FP64.
 __global__ void __launch_bounds__(256) k_gnn_head_bwd(const float* __restrict__ y, const float* __restrict__ t,
                                                       const double* __restrict__ pr, const double* __restrict__ x0,
                                                       const float* __restrict__ ymax, const double* __restrict__ stot,
@@ -625,6 +923,61 @@ unsigned gtile(uint64_t n) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)sm_count() * 2));
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda); resolved once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor map of a [rows][64] BF16 hidden-state array: 16-row x 64-column
+// boxes (2 KB), 128-byte swizzle.  rows is a multiple of 16, so no box reaches
+// past the array.
+int hidden_map(CUtensorMap* m, void* base, uint64_t rows) {
+  if (reinterpret_cast<uintptr_t>(base) & 127u) return fail(ZOGCU_ERR_INTERNAL, "hidden-state array is not 128-byte aligned");
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(ZOGCU_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[2] = {(cuuint64_t)kH, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)kH * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kH, (cuuint32_t)kTile};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ZOGCU_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return ZOGCU_OK;
+}
+
+// Dense-kernel grid: the CTAs resident at once (kDenseSmem each), at most one
+// tile per warp.  The occupancy of each kernel is looked up once.
+unsigned dense_grid(const void* kernel, uint32_t ntiles) {
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> known;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto& k : known)
+      if (k.first == kernel) per_sm = k.second;
+    if (!per_sm) {
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem);
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kDenseWarps * 32, kDenseSmem);
+      per_sm = std::max(n, 1);
+      known.emplace_back(kernel, per_sm);
+    }
+  }
+  const uint64_t want = ((uint64_t)ntiles + kDenseWarps - 1) / kDenseWarps;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count() * per_sm));
+}
+
 }  // namespace
 }  // namespace zogcu
 
@@ -632,9 +985,9 @@ using namespace zogcu;
 
 struct zogcu_gnn {
   int device = 0;
-  DevArray p, pb, m, s, g, loss;   // masters, BF16 copy, Adam moments, gradient, loss (FP64)
+  DevArray p, pb, m, s, g, loss, err;  // masters, BF16 copy, Adam moments, gradient, loss (FP64), kernel error flag
   uint64_t step = 0;
-  // activations of the largest graph seen so far (about 940 bytes per node),
+  // activations of the largest graph seen so far (about 430 bytes per node),
   // reused by later calls until the model is destroyed
   mutable WorkCache acts;
 };
@@ -643,21 +996,39 @@ namespace zogcu {
 namespace {
 
 // Activations of one forward pass over a graph (kept for the backward pass):
-// features F and aggregates A in FP32, hidden states H in BF16.
+// features F, 1/outdeg, messages M_l and aggregates A_l, hidden states H_l in
+// BF16 (rows padded to a multiple of 16 for the tile loads), output y.
 struct GnnActs {
-  DevBuf F, inv, y, t, ctr, rows;
-  DevBuf H[kLayers], A[kLayers];
-  // from the model's cache when the lease holds it, else per call
-  int alloc(uint32_t V, WorkLease& L) {
+  uint32_t Vp = 0;  // rows of the padded arrays
+  DevBuf F, inv, y, t, ctr, rows, M0;
+  DevBuf M[kLayers];   // M[1], M[2]: V x 8 BF16
+  DevBuf A[kLayers];   // A[0]: V x 4, A[1], A[2]: Vp x 8 (FP32)
+  DevBuf H[kLayers];   // Vp x 64 BF16
+  CUtensorMap mapH[kLayers];
+  // from the model's cache when the lease holds it, else per call; H[2] only
+  // when the backward pass needs it
+  int alloc(uint32_t V, WorkLease& L, bool train) {
     const size_t Vs = std::max<uint32_t>(V, 1);
+    Vp = (uint32_t)(((uint64_t)V + kTile - 1) / kTile * kTile);
+    if (Vp == 0) Vp = kTile;
     ZOGCU_TRY(L.get(F, 0, Vs * kF * 4));
     ZOGCU_TRY(L.get(inv, 1, Vs * 4));
     ZOGCU_TRY(L.get(y, 2, Vs * 4));
     ZOGCU_TRY(L.get(ctr, 3, 16));
-    for (int l = 0; l < kLayers; ++l) {
-      ZOGCU_TRY(L.get(H[l], 4 + l, Vs * kH * 2));
-      ZOGCU_TRY(L.get(A[l], 4 + kLayers + l, Vs * (size_t)layer_in(l) * 4));
+    ZOGCU_TRY(L.get(M0, 4, Vs * kF * 4));
+    ZOGCU_TRY(L.get(A[0], 5, Vs * kF * 4));
+    for (int l = 1; l < kLayers; ++l) {
+      ZOGCU_TRY(L.get(M[l], 5 + l, Vs * kR * 2));
+      ZOGCU_TRY(L.get(A[l], 7 + l, (size_t)Vp * kR * 4));
+      // the dense kernels copy 512-byte aggregate tiles with bulk copies
+      if (reinterpret_cast<uintptr_t>(A[l].ptr) & 15u) return fail(ZOGCU_ERR_INTERNAL, "aggregate array is not 16-byte aligned");
     }
+    for (int l = 0; l < kLayers; ++l) {
+      if (l == kLayers - 1 && !train) break;
+      ZOGCU_TRY(L.get(H[l], 10 + l, (size_t)Vp * kH * 2));
+      ZOGCU_TRY(hidden_map(&mapH[l], H[l].ptr, Vp));
+    }
+    if (!train) mapH[kLayers - 1] = mapH[0];  // never stored; a valid map for the kernel argument
     return ZOGCU_OK;
   }
 };
@@ -675,47 +1046,70 @@ int chunk_rows(const Graph* g, bool transpose, DevBuf& rows, cudaStream_t s) {
   return ZOGCU_OK;
 }
 
-// Z = agg(X) (forward, in-CSR) or Z (+)= agg^T(X) (transpose, out-CSR);
+// Z = agg(X) (forward, in-CSR) or Z = inv * agg^T(X) (transpose, out-CSR);
 // `ctr` is a device word for the chunk counter, `rows` the chunks' first rows.
+// Z (zrows x D, zrows >= V) is zeroed first.
 template <class T, int D>
-int spmm(const Graph* g, bool transpose, const float* inv, const T* X, float* Z, bool accumulate, uint32_t* ctr,
+int spmm(const Graph* g, bool transpose, const float* inv, const T* X, float* Z, size_t zrows, uint32_t* ctr,
          const DevBuf& rows, cudaStream_t s) {
   const uint32_t V = g->V;
   const uint32_t E = (uint32_t)g->E;
-  if (!accumulate) ZOGCU_CUDA(cudaMemsetAsync(Z, 0, (size_t)V * D * 4, s));
+  ZOGCU_CUDA(cudaMemsetAsync(Z, 0, zrows * D * 4, s));
   if (E == 0) return ZOGCU_OK;
   const uint32_t* off = (transpose ? g->out_off32 : g->in_off32).as<uint32_t>();
   const uint32_t* col = (transpose ? g->out_col : g->in_col).as<uint32_t>();
   const uint64_t chunks = ((uint64_t)E + kChunk - 1) / kChunk;
   ZOGCU_CUDA(cudaMemsetAsync(ctr, 0, 4, s));
-  k_gnn_spmm<T, D><<<gwarp(chunks), 256, 0, s>>>(off, col, inv, X, V, E, transpose ? 1 : 0, Z, accumulate ? 1 : 0,
-                                                 ctr, rows.as<uint32_t>());
+  k_gnn_spmm<T, D><<<gwarp(chunks), 256, 0, s>>>(off, col, inv, X, V, E, transpose ? 1 : 0, Z, ctr,
+                                                 rows.as<uint32_t>());
   return ZOGCU_OK;
 }
 
-unsigned gtile16(uint32_t V) { return gwarp(((uint64_t)V + 15) / 16); }
-
-int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, cudaStream_t s) {
+// Forward pass; with train the last hidden state is stored for the backward
+// pass.  err: device word the dense kernels raise when a tile load timed out.
+int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, bool train, cudaStream_t s) {
   const uint32_t V = g->V;
   if (!g->offsets32) return fail(ZOGCU_ERR_TOO_LARGE, "the warm-start network needs fewer than 2^32 arcs");
   const uint32_t* ioff = g->in_off32.as<uint32_t>();
   const __nv_bfloat16* w = M->pb.as<__nv_bfloat16>();
   uint32_t* ctr = act.ctr.as<uint32_t>();
-  k_gnn_features<<<g1d(V), 256, 0, s>>>(ioff, g->out_deg.as<uint32_t>(), V, 1.f / (float)std::max<uint64_t>(g->n_live, 1),
-                                        act.F.as<float>(), act.inv.as<float>());
+  unsigned int* err = M->err.as<unsigned int>();
+  const uint32_t ntiles = act.Vp / kTile;
+  k_gnn_features<<<g1d(V), 256, 0, s>>>(ioff, g->out_deg.as<uint32_t>(), V,
+                                        1.f / (float)std::max<uint64_t>(g->n_live, 1), act.F.as<float>(),
+                                        act.inv.as<float>(), act.M0.as<float>());
   const float* inv = act.inv.as<float>();
   ZOGCU_TRY(chunk_rows(g, false, act.rows, s));
-  ZOGCU_TRY((spmm<float, kF>(g, false, inv, act.F.as<float>(), act.A[0].as<float>(), false, ctr, act.rows, s)));
-  k_gnn_dense_fwd<kF, float><<<gtile16(V), 256, 0, s>>>(act.F.as<float>(), act.A[0].as<float>(), w + layer_offset(0), V,
-                                                        act.H[0].as<__nv_bfloat16>());
-  for (int l = 1; l < kLayers; ++l) {
-    const __nv_bfloat16* X = act.H[l - 1].as<__nv_bfloat16>();
-    ZOGCU_TRY((spmm<__nv_bfloat16, kH>(g, false, inv, X, act.A[l].as<float>(), false, ctr, act.rows, s)));
-    k_gnn_dense_fwd<kH, __nv_bfloat16><<<gtile16(V), 256, 0, s>>>(X, act.A[l].as<float>(), w + layer_offset(l), V,
-                                                                  act.H[l].as<__nv_bfloat16>());
-  }
-  k_gnn_head<<<gwarp(V), 256, 0, s>>>(act.H[kLayers - 1].as<__nv_bfloat16>(), w + kHeadOffset, V, act.y.as<float>());
+  ZOGCU_TRY((spmm<float, kF>(g, false, inv, act.M0.as<float>(), act.A[0].as<float>(), V, ctr, act.rows, s)));
+  k_gnn_dense0<<<dense_grid((const void*)k_gnn_dense0, ntiles), kDenseWarps * 32, kDenseSmem, s>>>(
+      act.mapH[0], act.F.as<float>(), act.A[0].as<float>(), w, inv, V, ntiles, act.M[1].as<__nv_bfloat16>());
   ZOGCU_CUDA(cudaGetLastError());
+  for (int l = 1; l < kLayers; ++l) {
+    ZOGCU_TRY((spmm<__nv_bfloat16, kR>(g, false, inv, act.M[l].as<__nv_bfloat16>(), act.A[l].as<float>(), act.Vp,
+                                       ctr, act.rows, s)));
+    if (l < kLayers - 1) {
+      k_gnn_dense_mid<0><<<dense_grid((const void*)k_gnn_dense_mid<0>, ntiles), kDenseWarps * 32, kDenseSmem, s>>>(
+          act.mapH[l - 1], act.mapH[l], act.A[l].as<float>(), w, l, inv, V, ntiles, 1,
+          act.M[l + 1].as<__nv_bfloat16>(), nullptr, err);
+    } else {
+      k_gnn_dense_mid<1><<<dense_grid((const void*)k_gnn_dense_mid<1>, ntiles), kDenseWarps * 32, kDenseSmem, s>>>(
+          act.mapH[l - 1], act.mapH[l], act.A[l].as<float>(), w, l, inv, V, ntiles, train ? 1 : 0, nullptr,
+          act.y.as<float>(), err);
+    }
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  return ZOGCU_OK;
+}
+
+// Reads and clears the dense kernels' error word (after the stream finished).
+int check_dense_error(const zogcu_gnn* M, cudaStream_t s) {
+  unsigned int e = 0;
+  ZOGCU_CUDA(cudaMemcpyAsync(&e, M->err.ptr, 4, cudaMemcpyDeviceToHost, s));
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (e) {
+    ZOGCU_CUDA(cudaMemsetAsync(M->err.ptr, 0, 4, s));
+    return fail(ZOGCU_ERR_INTERNAL, "warm-start dense layer: a tile load did not complete");
+  }
   return ZOGCU_OK;
 }
 
@@ -758,10 +1152,11 @@ int gnn_backward(zogcu_gnn* M, const Graph* g, GnnActs& act, const double* d_pr,
     ZOGCU_TRY(xq.alloc(Vs * 8, s));
     ZOGCU_TRY(sm.run(g, act.y.as<float>(), xq.as<double>(), s));
   }
-  DevBuf dH, dX, dA;
+  DevBuf dH, dX, dA, dQ;
   ZOGCU_TRY(dH.alloc(Vs * kH * 4, s));
   ZOGCU_TRY(dX.alloc(Vs * kH * 4, s));
-  ZOGCU_TRY(dA.alloc(Vs * kH * 4, s));
+  ZOGCU_TRY(dA.alloc(Vs * kR * 4, s));
+  ZOGCU_TRY(dQ.alloc(Vs * kR * 4, s));
   const float inv_n = 1.f / (float)std::max<uint64_t>(g->n_live, 1);
   float* pdH = dH.as<float>();
   float* pdX = dX.as<float>();
@@ -774,21 +1169,27 @@ int gnn_backward(zogcu_gnn* M, const Graph* g, GnnActs& act, const double* d_pr,
                                           g->out_deg.as<uint32_t>(), V, inv_n, mode, pdH, grad + kHeadOffset,
                                           M->loss.as<double>());
   for (int l = kLayers - 1; l >= 1; --l) {
-    const __nv_bfloat16* wl = w + layer_offset(l);
-    k_gnn_dense_bwd_data<kH><<<gwarp(V), 256, 0, s>>>(pdH, act.H[l].as<__nv_bfloat16>(), wl, V, pdX, dA.as<float>());
-    k_gnn_dense_bwd_weight<kH, __nv_bfloat16><<<gtile(V), 256, 0, s>>>(
-        act.H[l - 1].as<__nv_bfloat16>(), act.A[l].as<float>(), pdH, V, grad + layer_offset(l));
-    // gradient of H_{l-1}: dX + agg^T(dA); dX becomes the next layer's dH
-    ZOGCU_TRY((spmm<float, kH>(g, true, act.inv.as<float>(), dA.as<float>(), pdX, true, ctr, out_rows, s)));
+    k_gnn_dense_bwd_data<kH, kR><<<gwarp(V), 256, 0, s>>>(pdH, act.H[l].as<__nv_bfloat16>(), w + ws_offset(l),
+                                                          w + wn_offset(l), V, pdX, dA.as<float>());
+    k_gnn_dense_bwd_weight<kH, kR, __nv_bfloat16><<<gtile(V), 256, 0, s>>>(
+        act.H[l - 1].as<__nv_bfloat16>(), act.A[l].as<float>(), pdH, V, grad + ws_offset(l));
+    // dQ = inv * agg^T(dA): the gradient of H_{l-1} U_l
+    ZOGCU_TRY((spmm<float, kR>(g, true, act.inv.as<float>(), dA.as<float>(), dQ.as<float>(), V, ctr, out_rows, s)));
+    // dH_{l-1} = dX + dQ U^T (into dX), dU += H_{l-1}^T dQ
+    k_gnn_msg_bwd<<<g1d((uint64_t)V * 32), 256, 0, s>>>(dQ.as<float>(), act.H[l - 1].as<__nv_bfloat16>(),
+                                                        w + layer_offset(l), V, pdX, grad + layer_offset(l));
     std::swap(pdH, pdX);
   }
-  k_gnn_dense_bwd_data<kF><<<gwarp(V), 256, 0, s>>>(pdH, act.H[0].as<__nv_bfloat16>(), w, V, pdX, dA.as<float>());
-  k_gnn_dense_bwd_weight<kF, float><<<gtile(V), 256, 0, s>>>(act.F.as<float>(), act.A[0].as<float>(), pdH, V, grad);
+  k_gnn_dense_bwd_data<kF, kF><<<gwarp(V), 256, 0, s>>>(pdH, act.H[0].as<__nv_bfloat16>(), w + ws_offset(0),
+                                                        w + wn_offset(0), V, pdX, dA.as<float>());
+  k_gnn_dense_bwd_weight<kF, kF, float><<<gtile(V), 256, 0, s>>>(act.F.as<float>(), act.A[0].as<float>(), pdH, V,
+                                                                  grad + ws_offset(0));
   ZOGCU_CUDA(cudaGetLastError());
   return ZOGCU_OK;
 }
 
-// Glorot-uniform initial weights from a seeded SplitMix64 stream.
+// Glorot-uniform initial weights from a seeded SplitMix64 stream, each matrix
+// with its own fan (rows + columns) in flat-layout order; biases zero.
 void gnn_init_host(uint64_t seed, std::vector<float>& p) {
   p.assign(kNumParams, 0.f);
   uint64_t st = seed;
@@ -798,15 +1199,16 @@ void gnn_init_host(uint64_t seed, std::vector<float>& p) {
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
   };
-  auto uni = [&]() { return (float)((next() >> 40) * (1.0 / 16777216.0)) * 2.f - 1.f; };
+  auto fill = [&](int off, int rows, int cols) {
+    const float a = std::sqrt(6.f / (float)(rows + cols));
+    for (int i = 0; i < rows * cols; ++i) p[off + i] = a * ((float)((next() >> 40) * (1.0 / 16777216.0)) * 2.f - 1.f);
+  };
   for (int l = 0; l < kLayers; ++l) {
-    const int din = layer_in(l);
-    const float a = std::sqrt(6.f / (float)(din + kH));
-    float* base = p.data() + layer_offset(l);
-    for (int i = 0; i < 2 * din * kH; ++i) base[i] = a * uni();
+    if (l > 0) fill(layer_offset(l), layer_in(l), layer_msg(l));
+    fill(ws_offset(l), layer_in(l), kH);
+    fill(wn_offset(l), layer_msg(l), kH);
   }
-  const float a = std::sqrt(6.f / (float)(kH + 1));
-  for (int i = 0; i < kH; ++i) p[kHeadOffset + i] = a * uni();
+  fill(kHeadOffset, kH, 1);
 }
 
 }  // namespace
@@ -830,11 +1232,13 @@ int zogcu_gnn_create(uint64_t seed, zogcu_gnn** out) {
   ZOGCU_TRY(M->s.alloc(kNumParams * 4));
   ZOGCU_TRY(M->g.alloc(kNumParams * 4));
   ZOGCU_TRY(M->loss.alloc(16));
+  ZOGCU_TRY(M->err.alloc(16));
   std::vector<float> h;
   gnn_init_host(seed, h);
   ZOGCU_CUDA(cudaMemcpy(M->p.ptr, h.data(), kNumParams * 4, cudaMemcpyHostToDevice));
   ZOGCU_CUDA(cudaMemset(M->m.ptr, 0, kNumParams * 4));
   ZOGCU_CUDA(cudaMemset(M->s.ptr, 0, kNumParams * 4));
+  ZOGCU_CUDA(cudaMemset(M->err.ptr, 0, 16));
   k_gnn_to_bf16<<<g1d(kNumParams), 256>>>(M->p.as<float>(), M->pb.as<__nv_bfloat16>(), kNumParams);
   ZOGCU_CUDA(cudaGetLastError());
   ZOGCU_CUDA(cudaDeviceSynchronize());
@@ -880,13 +1284,13 @@ int zogcu_gnn_loss_grad(zogcu_gnn* M, zogcu_graph* G, const double* target_pr, i
   ZOGCU_CUDA(cudaMemcpyAsync(pr.ptr, target_pr, (size_t)g->V * 8, cudaMemcpyHostToDevice, sg.s));
   WorkLease lease(&M->acts, sg.s);
   GnnActs act;
-  ZOGCU_TRY(act.alloc(g->V, lease));
-  ZOGCU_TRY(gnn_forward(M, g, act, sg.s));
+  ZOGCU_TRY(act.alloc(g->V, lease, true));
+  ZOGCU_TRY(gnn_forward(M, g, act, true, sg.s));
   ZOGCU_TRY(gnn_backward(M, g, act, pr.as<double>(), loss_kind, sg.s));
   double l = 0.0;
   ZOGCU_CUDA(cudaMemcpyAsync(&l, M->loss.ptr, 8, cudaMemcpyDeviceToHost, sg.s));
   if (grad_out) ZOGCU_CUDA(cudaMemcpyAsync(grad_out, M->g.ptr, kNumParams * 4, cudaMemcpyDeviceToHost, sg.s));
-  ZOGCU_CUDA(cudaStreamSynchronize(sg.s));
+  ZOGCU_TRY(check_dense_error(M, sg.s));
   if (loss) *loss = (float)l;
   return ZOGCU_OK;
 }
@@ -903,8 +1307,8 @@ int zogcu_gnn_train_step(zogcu_gnn* M, zogcu_graph* G, const double* d_target_pr
   ZOGCU_TRY(sg.init(nullptr));
   WorkLease lease(&M->acts, sg.s);
   GnnActs act;
-  ZOGCU_TRY(act.alloc(g->V, lease));
-  ZOGCU_TRY(gnn_forward(M, g, act, sg.s));
+  ZOGCU_TRY(act.alloc(g->V, lease, true));
+  ZOGCU_TRY(gnn_forward(M, g, act, true, sg.s));
   ZOGCU_TRY(gnn_backward(M, g, act, d_target_pr, loss_kind, sg.s));
   M->step += 1;
   const float b1 = 0.9f, b2 = 0.999f;
@@ -914,7 +1318,7 @@ int zogcu_gnn_train_step(zogcu_gnn* M, zogcu_graph* G, const double* d_target_pr
   ZOGCU_CUDA(cudaGetLastError());
   double l = 0.0;
   ZOGCU_CUDA(cudaMemcpyAsync(&l, M->loss.ptr, 8, cudaMemcpyDeviceToHost, sg.s));
-  ZOGCU_CUDA(cudaStreamSynchronize(sg.s));
+  ZOGCU_TRY(check_dense_error(M, sg.s));
   if (loss) *loss = (float)l;
   return ZOGCU_OK;
 }
@@ -931,8 +1335,8 @@ int zogcu_gnn_predict(const zogcu_gnn* M, zogcu_graph* G, double* x0, int device
   ZOGCU_TRY(sg.init(stream));
   WorkLease lease(&M->acts, sg.s);
   GnnActs act;
-  ZOGCU_TRY(act.alloc(V, lease));
-  ZOGCU_TRY(gnn_forward(M, g, act, sg.s));
+  ZOGCU_TRY(act.alloc(V, lease, false));
+  ZOGCU_TRY(gnn_forward(M, g, act, false, sg.s));
   DevBuf xd;
   double* xo = x0;
   if (!device_out) {
@@ -943,7 +1347,7 @@ int zogcu_gnn_predict(const zogcu_gnn* M, zogcu_graph* G, double* x0, int device
   ZOGCU_TRY(sm.run(g, act.y.as<float>(), xo, sg.s));
   if (!device_out) ZOGCU_CUDA(cudaMemcpyAsync(x0, xo, (size_t)V * 8, cudaMemcpyDeviceToHost, sg.s));
   if (raw_out) ZOGCU_CUDA(cudaMemcpyAsync(raw_out, act.y.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, sg.s));
-  ZOGCU_CUDA(cudaStreamSynchronize(sg.s));
+  ZOGCU_TRY(check_dense_error(M, sg.s));
   return ZOGCU_OK;
 }
 
@@ -970,7 +1374,7 @@ int zogcu_gnn_load(const char* path, zogcu_gnn** out) {
   const bool ok = std::fread(hdr, 4, 3, f) == 3 && hdr[0] == kGnnMagic && hdr[1] == kGnnVersion &&
                   hdr[2] == (uint32_t)kNumParams && std::fread(h.data(), 2, h.size(), f) == h.size();
   std::fclose(f);
-  if (!ok) return fail(ZOGCU_ERR_IO, std::string("not a version-1 warm-start weight file: ") + path);
+  if (!ok) return fail(ZOGCU_ERR_IO, std::string("not a version-2 warm-start weight file: ") + path);
   std::vector<float> p(kNumParams);
   for (int i = 0; i < kNumParams; ++i) {
     const uint32_t bits = (uint32_t)h[i] << 16;

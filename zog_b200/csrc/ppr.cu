@@ -22,8 +22,12 @@
 // so every seed returns exactly the vector of its own stopping iteration.
 // Per-column L1 steps and dangling masses go lane -> warp -> CTA partials ->
 // a last-CTA reduction in a fixed order, which also updates the per-seed
-// state; the host enqueues max_iterations launches and launches after the
-// last active seed has stopped return at once.
+// state.  A whole call is one CUDA graph: per pass, the start-vector kernel,
+// a conditional while node whose body is the iteration kernel (the kernel
+// clears the loop's condition once every seed of the pass has stopped or
+// max_iterations is reached), and the kernel that writes the pass's columns
+// out; the passes follow one another and share the matrices.  The host
+// launches the graph once and no iteration launch is spent after convergence.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -68,6 +72,8 @@ struct PprArgs {
   double damping;
   double tol;
   unsigned long long max_iter;
+  unsigned long long cond;  // conditional handle of the pass's while loop
+  int use_cond;             // 1: clear the condition when the pass is over
 };
 
 // PL consecutive doubles of one contribution row, read with 32-byte loads
@@ -163,8 +169,11 @@ __global__ void __launch_bounds__(kPprThreads) k_ppr_iter(PprArgs<S> A) {
   constexpr int NW = kPprThreads / 32;
   __shared__ double s_part[NW][S][2];
   __shared__ int s_last;
-  if (*(volatile int*)&A.st->done) return;
   const unsigned long long it = *(volatile unsigned long long*)&A.st->iter;
+  if (*(volatile int*)&A.st->done || it >= A.max_iter) {
+    if (A.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(A.cond, 0u);
+    return;
+  }
   const int par = (int)(it & 1ull);
   const double* __restrict__ X = A.X[par];
   const double* __restrict__ Cc = A.C[par];
@@ -262,10 +271,12 @@ __global__ void __launch_bounds__(kPprThreads) k_ppr_iter(PprArgs<S> A) {
   }
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
+    const int done = (!any || it + 1 >= A.max_iter) ? 1 : 0;
     A.st->iter = it + 1;
-    A.st->done = (!any || it + 1 >= A.max_iter) ? 1 : 0;
+    A.st->done = done;
     *A.task_next = 0;
     *A.cta_arrive = 0;
+    if (done && A.use_cond) cudaGraphSetConditional(A.cond, 0u);
   }
 }
 
@@ -281,10 +292,13 @@ __global__ void k_ppr_init(const uint32_t* __restrict__ deg, uint32_t V, double 
   }
 }
 
-// out[s * V + node] = X[rank(node) * S + s] for the first `ns` columns
+// out[s * V + node] = X[rank(node) * S + s] for the first `ns` columns, X
+// the pass's last iterate (X0 or X1 by the parity of its iteration count)
 template <int S>
-__global__ void k_ppr_out(const double* __restrict__ X, const uint32_t* __restrict__ rank, uint32_t V, uint32_t ns,
+__global__ void k_ppr_out(const double* __restrict__ X0, const double* __restrict__ X1,
+                          const PprState* __restrict__ st, const uint32_t* __restrict__ rank, uint32_t V, uint32_t ns,
                           double* __restrict__ out) {
+  const double* __restrict__ X = (st->iter & 1ull) ? X1 : X0;
   const uint64_t total = (uint64_t)V * ns;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t s = (uint32_t)(i / V), v = (uint32_t)(i % V);
@@ -318,118 +332,152 @@ struct PprHost {
   }
 };
 
-// One pass over up to S seeds.
+// The matrices every pass of a call shares (V x width columns, node-major):
+// passes run one after another inside the call's graph.  Y and the arrival
+// counters are zero between uses (the kernel restores them).
+struct PprShared {
+  DevBuf X0, X1, C0, C1, Y, arrive;
+  int alloc(uint32_t V, uint32_t width, cudaStream_t s) {
+    const size_t mat = (size_t)V * width * 8;
+    ZOGCU_TRY(X0.alloc(mat, s));
+    ZOGCU_TRY(X1.alloc(mat, s));
+    ZOGCU_TRY(C0.alloc(mat, s));
+    ZOGCU_TRY(C1.alloc(mat, s));
+    ZOGCU_TRY(Y.alloc(mat, s));
+    ZOGCU_TRY(arrive.alloc((size_t)V * 4, s));
+    ZOGCU_CUDA(cudaMemsetAsync(Y.ptr, 0, mat, s));
+    ZOGCU_CUDA(cudaMemsetAsync(arrive.ptr, 0, (size_t)V * 4, s));
+    return ZOGCU_OK;
+  }
+};
+
+// One pass's own state (per-column seeds, flags, counts, partials), set up
+// before the graph is launched.
+struct PprPass {
+  uint32_t first = 0, ns = 0;
+  int S = 64;
+  unsigned grid = 1;
+  DevBuf seed_rank, active, iters, l1, sink, part, st, ctr;
+  double* dst = nullptr;
+};
+
 template <int S>
-int ppr_pass(Graph* g, const PprHost& H, const uint32_t* seeds, uint32_t ns, double damping, uint64_t max_iter,
-             double tol, double* out, bool dev_out, uint64_t* iters_out, zogcu_stats* stats, cudaStream_t s) {
-  const PrSchedule& P = g->pr;
-  const PrTaskList& L = g->pr.lists[1];  // row blocks of up to 256 arcs
-  const uint32_t V = g->V;
-  const size_t mat = (size_t)V * S * 8;
-  DevBuf X0, X1, C0, C1, Y, arrive, seed_rank, active, iters, l1, sink, part, st, ctr, host_seeds, res;
-  ZOGCU_TRY(X0.alloc(mat, s));
-  ZOGCU_TRY(X1.alloc(mat, s));
-  ZOGCU_TRY(C0.alloc(mat, s));
-  ZOGCU_TRY(C1.alloc(mat, s));
-  ZOGCU_TRY(Y.alloc(mat, s));
-  ZOGCU_TRY(arrive.alloc((size_t)V * 4, s));
-  ZOGCU_CUDA(cudaMemsetAsync(Y.ptr, 0, mat, s));
-  ZOGCU_CUDA(cudaMemsetAsync(arrive.ptr, 0, (size_t)V * 4, s));
+int ppr_pass_setup(const PprHost& H, const uint32_t* seeds, PprPass& P, cudaStream_t s) {
   // per-column state: seeds as ranks (padding columns never start)
   std::vector<uint32_t> h_seed(S, kNoSeed);
   std::vector<int> h_active(S, 0);
-  for (uint32_t i = 0; i < ns; ++i) {
-    h_seed[i] = H.rank[seeds[i]];
+  for (uint32_t i = 0; i < P.ns; ++i) {
+    h_seed[i] = H.rank[seeds[P.first + i]];
     h_active[i] = 1;
   }
-  const double n_f = (double)V;
-  const double x0 = 1.0 / n_f;
   std::vector<double> h_sink(S, H.sink0);
-  ZOGCU_TRY(seed_rank.alloc(S * 4, s));
-  ZOGCU_TRY(active.alloc(S * 4, s));
-  ZOGCU_TRY(iters.alloc(S * 8, s));
-  ZOGCU_TRY(l1.alloc(S * 8, s));
-  ZOGCU_TRY(sink.alloc(S * 8, s));
-  ZOGCU_CUDA(cudaMemcpyAsync(seed_rank.ptr, h_seed.data(), S * 4, cudaMemcpyHostToDevice, s));
-  ZOGCU_CUDA(cudaMemcpyAsync(active.ptr, h_active.data(), S * 4, cudaMemcpyHostToDevice, s));
-  ZOGCU_CUDA(cudaMemcpyAsync(sink.ptr, h_sink.data(), S * 8, cudaMemcpyHostToDevice, s));
-  ZOGCU_CUDA(cudaMemsetAsync(iters.ptr, 0, S * 8, s));
-  ZOGCU_CUDA(cudaMemsetAsync(l1.ptr, 0, S * 8, s));
+  ZOGCU_TRY(P.seed_rank.alloc(S * 4, s));
+  ZOGCU_TRY(P.active.alloc(S * 4, s));
+  ZOGCU_TRY(P.iters.alloc(S * 8, s));
+  ZOGCU_TRY(P.l1.alloc(S * 8, s));
+  ZOGCU_TRY(P.sink.alloc(S * 8, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(P.seed_rank.ptr, h_seed.data(), S * 4, cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(P.active.ptr, h_active.data(), S * 4, cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaMemcpyAsync(P.sink.ptr, h_sink.data(), S * 8, cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaMemsetAsync(P.iters.ptr, 0, S * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(P.l1.ptr, 0, S * 8, s));
   int per_sm = 0;
   ZOGCU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ppr_iter<S>, kPprThreads, 0));
-  const unsigned grid = (unsigned)std::max(1, per_sm) * (unsigned)sm_count();
-  ZOGCU_TRY(part.alloc((size_t)grid * S * 16, s));
-  ZOGCU_TRY(st.alloc(sizeof(PprState), s));
-  ZOGCU_TRY(ctr.alloc(16, s));
-  ZOGCU_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(PprState), s));
-  ZOGCU_CUDA(cudaMemsetAsync(ctr.ptr, 0, 16, s));
-  k_ppr_init<S><<<grid_for((uint64_t)V * S), 256, 0, s>>>(P.deg.as<uint32_t>(), V, x0, X0.as<double>(), C0.as<double>());
-  ZOGCU_CUDA(cudaGetLastError());
+  P.grid = (unsigned)std::max(1, per_sm) * (unsigned)sm_count();
+  ZOGCU_TRY(P.part.alloc((size_t)P.grid * S * 16, s));
+  ZOGCU_TRY(P.st.alloc(sizeof(PprState), s));
+  ZOGCU_TRY(P.ctr.alloc(16, s));
+  ZOGCU_CUDA(cudaMemsetAsync(P.st.ptr, 0, sizeof(PprState), s));
+  ZOGCU_CUDA(cudaMemsetAsync(P.ctr.ptr, 0, 16, s));
+  // the sync copies above come from pageable vectors that go out of scope
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  return ZOGCU_OK;
+}
+
+int add_kernel_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGraphNode_t* dep, void* fn, unsigned grid,
+                    unsigned threads, void** args) {
+  cudaKernelNodeParams kp = {};
+  kp.func = fn;
+  kp.gridDim = dim3(grid);
+  kp.blockDim = dim3(threads);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = args;
+  ZOGCU_CUDA(cudaGraphAddKernelNode(node, graph, dep, dep ? 1 : 0, &kp));
+  return ZOGCU_OK;
+}
+
+// Adds one pass to the call's graph after *tail: start vector, the while loop
+// of iterations, the columns out; *tail becomes the pass's last node.
+template <int S>
+int ppr_pass_nodes(cudaGraph_t graph, cudaGraphNode_t* tail, Graph* g, PprShared& M, PprPass& P, double damping,
+                   uint64_t max_iter, double tol) {
+  const PrSchedule& Ps = g->pr;
+  const PrTaskList& L = g->pr.lists[1];  // row blocks of up to 256 arcs
+  const uint32_t V = g->V;
+  const double n_f = (double)V;
+  double x0 = 1.0 / n_f;
+  const uint32_t* deg = Ps.deg.as<uint32_t>();
+  double* X0 = M.X0.as<double>();
+  double* C0 = M.C0.as<double>();
+  uint32_t Vv = V;
+  void* init_args[] = {(void*)&deg, &Vv, &x0, &X0, &C0};
+  cudaGraphNode_t n_init;
+  ZOGCU_TRY(add_kernel_node(graph, &n_init, *tail ? tail : nullptr, reinterpret_cast<void*>(k_ppr_init<S>),
+                            grid_for((uint64_t)V * S), 256, init_args));
   PprArgs<S> A{};
-  A.off = P.off.as<uint32_t>();
-  A.col = P.col.as<uint32_t>();
-  A.deg = P.deg.as<uint32_t>();
+  A.off = Ps.off.as<uint32_t>();
+  A.col = Ps.col.as<uint32_t>();
+  A.deg = deg;
   A.tasks = L.tasks.as<PrTask>();
   A.num_tasks = L.num_tasks;
-  A.X[0] = X0.as<double>();
-  A.X[1] = X1.as<double>();
-  A.C[0] = C0.as<double>();
-  A.C[1] = C1.as<double>();
-  A.Y = Y.as<double>();
-  A.arrive = arrive.as<uint32_t>();
-  A.seed_rank = seed_rank.as<uint32_t>();
-  A.active = active.as<int>();
-  A.iters = iters.as<unsigned long long>();
-  A.l1 = l1.as<double>();
-  A.sink = sink.as<double>();
-  A.part = part.as<double>();
-  A.st = st.as<PprState>();
-  A.task_next = ctr.as<uint32_t>();
-  A.cta_arrive = ctr.as<uint32_t>() + 1;
+  A.X[0] = X0;
+  A.X[1] = M.X1.as<double>();
+  A.C[0] = C0;
+  A.C[1] = M.C1.as<double>();
+  A.Y = M.Y.as<double>();
+  A.arrive = M.arrive.as<uint32_t>();
+  A.seed_rank = P.seed_rank.as<uint32_t>();
+  A.active = P.active.as<int>();
+  A.iters = P.iters.as<unsigned long long>();
+  A.l1 = P.l1.as<double>();
+  A.sink = P.sink.as<double>();
+  A.part = P.part.as<double>();
+  A.st = P.st.as<PprState>();
+  A.task_next = P.ctr.as<uint32_t>();
+  A.cta_arrive = P.ctr.as<uint32_t>() + 1;
   A.V = V;
   A.n_f = n_f;
   A.damping = damping;
   A.tol = tol;
   A.max_iter = max_iter;
-  if (max_iter == 0) {
-    int one = 1;
-    ZOGCU_CUDA(cudaMemcpyAsync(&st.as<PprState>()->done, &one, 4, cudaMemcpyHostToDevice, s));
-  }
-  EventTimer tm;
-  ZOGCU_TRY(tm.start(s));
-  for (uint64_t k = 0; k < max_iter; ++k) k_ppr_iter<S><<<grid, kPprThreads, 0, s>>>(A);
-  ZOGCU_CUDA(cudaGetLastError());
-  ZOGCU_TRY(tm.stop(s));
-  PprState hs{};
-  ZOGCU_CUDA(cudaMemcpyAsync(&hs, st.ptr, sizeof(hs), cudaMemcpyDeviceToHost, s));
-  std::vector<unsigned long long> h_it(S);
-  ZOGCU_CUDA(cudaMemcpyAsync(h_it.data(), iters.ptr, S * 8, cudaMemcpyDeviceToHost, s));
-  ZOGCU_CUDA(cudaStreamSynchronize(s));
-  const double* Xr = (hs.iter & 1ull) ? X1.as<double>() : X0.as<double>();
-  double* dst = out;
-  if (!dev_out) {
-    ZOGCU_TRY(res.alloc((size_t)V * ns * 8, s));
-    dst = res.as<double>();
-  }
-  k_ppr_out<S><<<grid_for((uint64_t)V * ns), 256, 0, s>>>(Xr, P.rank.as<uint32_t>(), V, ns, dst);
-  ZOGCU_CUDA(cudaGetLastError());
-  if (!dev_out) ZOGCU_CUDA(cudaMemcpyAsync(out, dst, (size_t)V * ns * 8, cudaMemcpyDeviceToHost, s));
-  ZOGCU_CUDA(cudaStreamSynchronize(s));
-  uint64_t max_it = 0;
-  for (uint32_t i = 0; i < ns; ++i) {
-    if (iters_out) iters_out[i] = h_it[i];
-    max_it = std::max<uint64_t>(max_it, h_it[i]);
-  }
-  if (stats) {
-    stats->iterations = std::max<uint64_t>(stats->iterations, max_it);
-    stats->elapsed_ms += tm.ms();
-    // per launch: arc indices and offsets once, every column of C gathered
-    // once per arc, X read and X', C' written
-    const double per_iter = 4.0 * (double)g->E + 4.0 * ((double)V + 1) + 8.0 * S * (double)g->E +
-                            24.0 * S * (double)V;
-    stats->bytes_moved += per_iter * (double)hs.iter;
-    stats->launches += hs.iter + 2;
-  }
+  // the loop's condition starts at 1 on every launch; a pass with no
+  // iterations to run is over before its first body launch, which clears it
+  cudaGraphConditionalHandle h;
+  ZOGCU_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault));
+  A.cond = h;
+  A.use_cond = 1;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t n_loop;
+  ZOGCU_CUDA(cudaGraphAddNode(&n_loop, graph, &n_init, 1, &cp));
+  void* iter_args[] = {&A};
+  cudaGraphNode_t n_body;
+  ZOGCU_TRY(add_kernel_node(cp.conditional.phGraph_out[0], &n_body, nullptr, reinterpret_cast<void*>(k_ppr_iter<S>),
+                            P.grid, kPprThreads, iter_args));
+  const double* X1c = A.X[1];
+  const double* X0c = X0;
+  const PprState* stc = A.st;
+  const uint32_t* rank = Ps.rank.as<uint32_t>();
+  uint32_t ns = P.ns;
+  double* dst = P.dst;
+  void* out_args[] = {(void*)&X0c, (void*)&X1c, (void*)&stc, (void*)&rank, &Vv, &ns, &dst};
+  cudaGraphNode_t n_out;
+  ZOGCU_TRY(add_kernel_node(graph, &n_out, &n_loop, reinterpret_cast<void*>(k_ppr_out<S>),
+                            grid_for((uint64_t)V * P.ns), 256, out_args));
+  *tail = n_out;
   return ZOGCU_OK;
 }
 
@@ -456,10 +504,11 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   ZOGCU_CUDA(cudaSetDevice(g->device));
   StreamGuard sg;
   ZOGCU_TRY(sg.init(opts ? opts->stream : nullptr));
-  ZOGCU_TRY(ensure_pr_schedule(g, sg.s));
-  ZOGCU_TRY(ensure_task_list(g, 256, sg.s));
+  const cudaStream_t s = sg.s;
+  ZOGCU_TRY(ensure_pr_schedule(g, s));
+  ZOGCU_TRY(ensure_task_list(g, 256, s));
   const bool dev_out = opts && opts->device_pointers;
-  const size_t V = g->V;
+  const uint32_t V = g->V;
   // Pass width: on graphs of 2^19 nodes and more, passes of 64 seeds -- the
   // 64-column kernel (62 registers) runs twice the warps per SM of the
   // 256-column one (128 registers), which outweighs streaming the arc indices
@@ -467,23 +516,84 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   // 114 ms at scale 20); on smaller graphs one pass of 256 (47 against 58 ms
   // at scale 18).
   PprHost H;
-  ZOGCU_TRY(H.load(g, sg.s));
+  ZOGCU_TRY(H.load(g, s));
   uint32_t width = V < (1u << 19) ? 256u : 64u;  // ZOGCU_PPR_PASS=64/128/256 overrides
   if (const char* e = std::getenv("ZOGCU_PPR_PASS")) {
     const int w = std::atoi(e);
     if (w == 64 || w == 128 || w == 256) width = (uint32_t)w;
   }
-  for (uint32_t s0 = 0; s0 < num_seeds;) {
-    const uint32_t ns = std::min<uint32_t>(num_seeds - s0, width);
-    double* o = out_scores + (size_t)s0 * V;
-    uint64_t* it = iterations ? iterations + s0 : nullptr;
-    if (ns > 128)
-      ZOGCU_TRY(ppr_pass<256>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
-    else if (ns > 64)
-      ZOGCU_TRY(ppr_pass<128>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
-    else
-      ZOGCU_TRY(ppr_pass<64>(g, H, seeds + s0, ns, damping, max_iterations, tolerance, o, dev_out, it, stats, sg.s));
-    s0 += ns;
+  const uint32_t npass = (num_seeds + width - 1) / width;
+  std::vector<PprPass> passes(npass);
+  int max_S = 64;
+  for (uint32_t p = 0; p < npass; ++p) {
+    PprPass& P = passes[p];
+    P.first = p * width;
+    P.ns = std::min<uint32_t>(num_seeds - P.first, width);
+    P.S = P.ns > 128 ? 256 : P.ns > 64 ? 128 : 64;
+    max_S = std::max(max_S, P.S);
+  }
+  PprShared M;
+  ZOGCU_TRY(M.alloc(V, (uint32_t)max_S, s));
+  DevBuf res;
+  if (!dev_out) ZOGCU_TRY(res.alloc((size_t)V * num_seeds * 8, s));
+  for (PprPass& P : passes) {
+    P.dst = (dev_out ? out_scores : res.as<double>()) + (size_t)P.first * V;
+    if (P.S == 256) ZOGCU_TRY(ppr_pass_setup<256>(H, seeds, P, s));
+    else if (P.S == 128) ZOGCU_TRY(ppr_pass_setup<128>(H, seeds, P, s));
+    else ZOGCU_TRY(ppr_pass_setup<64>(H, seeds, P, s));
+  }
+  // the call's graph: every pass after the previous one
+  cudaGraph_t graph = nullptr;
+  ZOGCU_CUDA(cudaGraphCreate(&graph, 0));
+  struct GraphGuard {
+    cudaGraph_t gr;
+    ~GraphGuard() { cudaGraphDestroy(gr); }
+  } guard{graph};
+  cudaGraphNode_t tail = nullptr;  // the previous pass's last node (none before the first)
+  for (PprPass& P : passes) {
+    if (P.S == 256) ZOGCU_TRY(ppr_pass_nodes<256>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
+    else if (P.S == 128) ZOGCU_TRY(ppr_pass_nodes<128>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
+    else ZOGCU_TRY(ppr_pass_nodes<64>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
+  }
+  cudaGraphExec_t exec = nullptr;
+  ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  EventTimer tm;
+  ZOGCU_TRY(tm.start(s));
+  const cudaError_t le = cudaGraphLaunch(exec, s);
+  cudaGraphExecDestroy(exec);  // an executable graph in flight is freed when it completes
+  ZOGCU_CUDA(le);
+  ZOGCU_TRY(tm.stop(s));
+  if (!dev_out) ZOGCU_CUDA(cudaMemcpyAsync(out_scores, res.ptr, (size_t)V * num_seeds * 8, cudaMemcpyDeviceToHost, s));
+  // per-pass iteration counts and per-seed iterations
+  uint64_t kernel_runs = 0, max_it = 0;
+  for (PprPass& P : passes) {
+    PprState hs{};
+    std::vector<unsigned long long> h_it(P.ns);
+    ZOGCU_CUDA(cudaMemcpyAsync(&hs, P.st.ptr, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(h_it.data(), P.iters.ptr, (size_t)P.ns * 8, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t i = 0; i < P.ns; ++i) {
+      if (iterations) iterations[P.first + i] = h_it[i];
+      max_it = std::max<uint64_t>(max_it, h_it[i]);
+    }
+    // the loop's body ran once per iteration (the last one clears the loop's
+    // condition; with max_iterations 0, one run finds the pass over), plus
+    // the start and out kernels
+    kernel_runs += std::max<uint64_t>(hs.iter, 1) + 2;
+    if (stats) {
+      // per iteration: arc indices and offsets once, every column of C
+      // gathered once per arc, X read and X', C' written
+      const double per_iter = 4.0 * (double)g->E + 4.0 * ((double)V + 1) + 8.0 * P.S * (double)g->E +
+                              24.0 * P.S * (double)V;
+      stats->bytes_moved += per_iter * (double)hs.iter;
+    }
+  }
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  if (stats) {
+    stats->iterations = max_it;
+    stats->elapsed_ms = tm.ms();
+    stats->launches = kernel_runs;
+    stats->reserved = 1;  // host-side launches: the call's one graph
   }
   return ZOGCU_OK;
 }

@@ -8,11 +8,13 @@ and power iteration still runs to the caller's tolerance -- the plain method
 decides the result; the network only sets where it starts.
 
 Training data are seeded synthetic graphs (R-MAT scales 12-18, Barabasi-Albert
-m = 2-16, Watts-Strogatz k = 10, p = 0.1; n = 4k-262k); targets are FP64
-PageRank vectors the plain GPU method computes to L1 1e-9.  Every step of
-training (forward, backward, Adam) runs in the library's own CUDA kernels.
+m = 2-16, Watts-Strogatz k = 10, p = 0.1; n = 4k-262k), plus a smaller set of
+larger R-MAT (scales 19-22) and Barabasi-Albert (n = 2^19-2^22) graphs so that
+the network has seen the sizes it is used on; targets are FP64 PageRank
+vectors the plain GPU method computes to L1 1e-9.  Every step of training
+(forward, backward, Adam) runs in the library's own CUDA kernels.
 
-    python -m zog_b200.warm_start --graphs 2000 --epochs 8 --out zog_b200/data/warm_start.zogn
+    python -m zog_b200.warm_start --graphs 2000 --large 96 --epochs 8 --out zog_b200/data/warm_start.zogn
 """
 from __future__ import annotations
 
@@ -52,6 +54,22 @@ def training_specs(count: int, seed: int = 2024, min_log2n: float = 12.0, max_lo
                 specs.append(("ba", dict(n=n, m=int(rng.integers(2, 17)), seed=gseed)))
             else:
                 specs.append(("ws", dict(n=n, k=10, beta=0.1, seed=gseed)))
+    return specs
+
+
+def large_specs(count: int, seed: int = 4048):
+    """`count` larger graph descriptions, alternating R-MAT scales 19-22 and
+    Barabasi-Albert n = 2^19-2^22 (log-uniform), for size generalisation."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        gseed = int(rng.integers(1, 2 ** 62))
+        if i % 2 == 0:
+            specs.append(("rmat", dict(scale=int(rng.integers(19, 23)), edge_factor=int(rng.integers(4, 17)),
+                                       seed=gseed)))
+        else:
+            specs.append(("ba", dict(n=int(round(2 ** rng.uniform(19, 22))), m=int(rng.integers(2, 17)),
+                                     seed=gseed)))
     return specs
 
 
@@ -161,6 +179,7 @@ def compare_starts(net: _native.WarmStart, g: _native.Graph, damping=0.85, tol=1
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--graphs", type=int, default=2000)
+    ap.add_argument("--large", type=int, default=96, help="extra graphs of 2^19-2^22 nodes")
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--seed", type=int, default=2024)
@@ -171,7 +190,8 @@ def main(argv=None):
     args = ap.parse_args(argv)
     net = _native.WarmStart.create(args.init_seed)
     kind = _native.LOSS_KL if args.loss == "kl" else _native.LOSS_LOG_MSE
-    train(net, training_specs(args.graphs, args.seed), args.epochs, args.lr, loss_kind=kind)
+    specs = training_specs(args.graphs, args.seed) + large_specs(args.large, args.seed + 1)
+    train(net, specs, args.epochs, args.lr, loss_kind=kind)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     net.save(args.out)
     print(f"saved {args.out}")
