@@ -700,6 +700,8 @@ def run_zog(args):
     bytes_per_iter = 4.0 * E + 4.0 * (V + 1) + 36.0 * V  # u32 offsets at this size
     hbm_peak, peak_kind = peaks()
     achieved = bytes_per_iter / (t_iter_ms * 1e-3) / 1e9
+    sm_clock_hz = float(clk.get("sm_mhz") or 1965.0) * 1e6
+    tag_floor_ms = E / (torch.cuda.get_device_properties(local).multi_processor_count * sm_clock_hz) * 1e3
 
     # the tightly converged FP64 vector (same kernels, tol 1e-14) that every
     # result's error is reported against
@@ -769,8 +771,30 @@ def run_zog(args):
         e2e_ms = max_over_ranks(e2e_ms, ws)
         # from the SoA arrays in reverse insertion order the CSR would be equal;
         # the graph here is built from (src,dst)-sorted arcs, the generator's order
+        # the same step from pageable host arrays, as a NIF hands them over
+        # (the library copies them through its pinned chunks)
+        src_pg = np.array(src_np, copy=True)
+        dst_pg = np.array(dst_np, copy=True)
+        out_pg = np.empty(V, np.float64)
+        for _ in range(args.warmup_e2e):
+            g2 = N.Graph.from_edges(V, src_pg, dst_pg)
+            g2.pagerank(DAMPING, MAX_ITER, TOL, out=out_pg)
+            g2.destroy()
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.steps_e2e):
+            g2 = N.Graph.from_edges(V, src_pg, dst_pg)
+            g2.pagerank(DAMPING, MAX_ITER, TOL, out=out_pg)
+            g2.destroy()
+        torch.cuda.synchronize()
+        e2e_pg_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps_e2e, ws)
+        del src_pg, dst_pg, out_pg
         e2e = {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(8 * E), "d2h_bytes_per_step": int(8 * V),
-               "what": "zogcu_graph_create_from_edges (host arc arrays) + zogcu_pagerank (host scores) + destroy"}
+               "what": "zogcu_graph_create_from_edges (pinned host arc arrays) + zogcu_pagerank (pinned host "
+                       "scores) + destroy",
+               "pageable": {"value": e2e_pg_ms, "unit": "ms",
+                            "what": "the same step from pageable numpy arrays (a NIF's slices)"}}
         cpu_ctx = (V, oo, oc)
         del src_t, dst_t
 
@@ -875,7 +899,11 @@ def run_zog(args):
                          "kernel": pr_kernel_name(int(st["kernel_config"])),
                          "kernel_config": int(st["kernel_config"]),
                          "ms_per_launch": t_iter_ms,
-                         "algorithmic_bytes_per_launch": bytes_per_iter},
+                         "algorithmic_bytes_per_launch": bytes_per_iter,
+                         # every arc gathers one random contribution; one SM's L1 looks up about one
+                         # 128-byte line per clock, so E / (SMs x clock) bounds an iteration
+                         "l1_tag_floor_ms": tag_floor_ms,
+                         "frac_of_l1_tag_floor": tag_floor_ms / t_iter_ms if t_iter_ms > 0 else None},
             "clocks": clk,
             "gpu_launches": int(launches + (bc_line["launches"] if bc_line else 0)),
             "e2e": e2e,

@@ -1,6 +1,6 @@
 """Generates the golden fixtures under tests/golden/ with the CPU oracle.
 
-    python tests/golden/make_golden.py [--reference-root DIR]
+    python tests/golden/make_golden.py --reference-root DIR   (or ZOG_REFERENCE_ROOT=DIR)
 
 Each fixture is an .npz holding a graph in NIF insertion order (node count,
 from, to, directed flag) and the oracle's outputs on it:
@@ -111,8 +111,11 @@ def save(name, V, frm, to, directed, extra=None, labels=None, ag=None):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--reference-root", default=os.environ.get("ZOG_REFERENCE_ROOT"),
+                    help="root of the reference checkout (or set ZOG_REFERENCE_ROOT)")
     args = ap.parse_args()
+    if not args.reference_root:
+        ap.error("give --reference-root or set ZOG_REFERENCE_ROOT")
     O.build()
     manifest = {}
     for name, (kind, edges) in GRAPHS.items():

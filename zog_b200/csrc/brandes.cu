@@ -62,6 +62,9 @@ struct BcLoop {
   uint32_t depth;
   uint32_t blevel;
   uint32_t max_depth;
+  uint32_t push;                  // direction of the current forward level: 1 push, 0 pull
+  uint32_t pad;
+  unsigned long long next_arcs;   // out-arcs of the next frontier, summed during the level
 };
 
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
@@ -169,17 +172,22 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
     unsigned long long* __restrict__ visited, unsigned long long* __restrict__ sigma, uint32_t* __restrict__ dist,
     unsigned long long full, uint32_t level, unsigned int* __restrict__ flags, const BcHeavy* __restrict__ heavy,
     uint32_t nheavy, unsigned long long* __restrict__ hpart, unsigned long long* __restrict__ hgot,
-    unsigned int* __restrict__ harrive, const BcLoop* __restrict__ loop, unsigned long long* __restrict__ masks) {
+    unsigned int* __restrict__ harrive, const BcLoop* __restrict__ loop, unsigned long long* __restrict__ masks,
+    const OffT* __restrict__ out_off) {
   // flags[l % kMaxStoredLevels] = 1 when level l discovered a vertex;
   // flags[kOverflowFlag] = some path count wrapped.  With `loop` (the level
   // loop runs on the device) the level and its frontier masks come from the
   // batch's loop state and the mask ring `masks`.
   if (loop) {
+    if (*(volatile const uint32_t*)&loop->push) return;  // a push level (bc_push_kernel)
     level = *(volatile const uint32_t*)&loop->level;
     front_cur = masks + (size_t)(level % (kMaxStoredLevels + 1)) * V;
     front_nxt = masks + (size_t)((level + 1) % (kMaxStoredLevels + 1)) * V;
   }
   if (level > 0 && *(volatile unsigned int*)(flags + (level - 1) % kMaxStoredLevels) == 0u) return;
+  // out-arcs of the vertices this CTA adds to the next frontier (device loop
+  // only: the next level's direction is chosen from their sum)
+  unsigned long long nxt_arcs = 0;
   constexpr int W = kBcThreads / 32;
   __shared__ unsigned long long s_acc[W][kBcBatch];
   __shared__ unsigned long long s_got[W];
@@ -219,6 +227,7 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
         }
         if (ht.nch == 1) {
           fwd_commit(w, vis, newmask, t0, t1, level, lane, front_nxt, visited, sigma, dist, any_new);
+          if (loop && lane == 0 && newmask) nxt_arcs += (unsigned long long)(__ldg(out_off + w + 1) - __ldg(out_off + w));
         } else {
           // chunk partials; the last chunk to arrive adds them in chunk order
           // (exact integer sums) and commits the vertex
@@ -244,6 +253,7 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
               nm |= __ldcg(hgot + ht.first + k);
             }
             fwd_commit(w, vis, nm, u0, u1, level, lane, front_nxt, visited, sigma, dist, any_new);
+            if (loop && lane == 0 && nm) nxt_arcs += (unsigned long long)(__ldg(out_off + w + 1) - __ldg(out_off + w));
             if (lane == 0) harrive[ht.first] = 0u;
           }
         }
@@ -262,12 +272,21 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
           const unsigned long long newmask = (unsigned long long)__ballot_sync(0xffffffffu, got0) |
                                              ((unsigned long long)__ballot_sync(0xffffffffu, got1) << 32);
           fwd_commit(w, vis, newmask, acc0, acc1, level, lane, front_nxt, visited, sigma, dist, any_new);
+          if (loop && lane == 0 && newmask) nxt_arcs += (unsigned long long)(__ldg(out_off + w + 1) - __ldg(out_off + w));
         }
       }
     }
   }
   if (__any_sync(0xffffffffu, any_new) && lane == 0) flags[level % kMaxStoredLevels] = 1u;
   if (__any_sync(0xffffffffu, any_ovf) && lane == 0) flags[kOverflowFlag] = 1u;
+  if (loop) {
+    __shared__ unsigned long long s_arcs;
+    if (threadIdx.x == 0) s_arcs = 0;
+    __syncthreads();
+    if (nxt_arcs) atomicAdd(&s_arcs, nxt_arcs);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_arcs) atomicAdd(const_cast<unsigned long long*>(&loop->next_arcs), s_arcs);
+  }
 }
 
 // Level-l mask of v recomputed from dist (deep BFS, masks not stored).
@@ -569,7 +588,7 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
                                                           g->heavy_in.as<BcHeavy>(), g->n_heavy_in,
                                                           W.hpart.as<unsigned long long>(),
                                                           W.hgot.as<unsigned long long>(), W.harrive.as<unsigned int>(),
-                                                          nullptr, nullptr);
+                                                          nullptr, nullptr, nullptr);
       ZOGCU_CUDA(cudaGetLastError());
       *launches += 1;
     }
@@ -591,14 +610,146 @@ __global__ void k_bc_add(double* __restrict__ a, const double* __restrict__ b, u
     a[v] += b[v];
 }
 
+// ---- push levels (direction-optimising forward) ------------------------------
+// When the frontier's out-arcs are few against the graph's arcs (level 0, whose
+// frontier is the batch's sources, and the sparse levels that follow or end a
+// BFS), the level pushes instead of pulling: every frontier vertex v (mask
+// m_v) walks its out-arcs, and for each successor w the sources b of m_v not
+// yet visited at w get sigma[w][b] += sigma[v][b] (64-bit integer atomics:
+// exact, so the order of the additions does not matter and the sums equal the
+// pull kernel's, wrap included) and w's next-frontier mask the bits
+// (atomicOr).  visited and dist of the new vertices are written afterwards by
+// bc_push_finalize, so every push of the level reads the visited masks of the
+// level's start.  Each CTA first stages its window of frontier vertices in
+// shared memory (compacted from the frontier masks); light vertices are
+// walked by one warp each, vertices of more than kPushCtaDegree out-arcs by
+// the whole CTA.
+constexpr int kPushCtaDegree = 256;
+
+__device__ __forceinline__ unsigned long long* ring_slot(unsigned long long* masks, uint32_t level, uint32_t V) {
+  return masks + (size_t)(level % (kMaxStoredLevels + 1)) * V;
+}
+
+__device__ __forceinline__ void push_arc(uint32_t v, unsigned long long m, uint32_t w,
+                                         const unsigned long long* __restrict__ visited,
+                                         unsigned long long* __restrict__ nxt, unsigned long long* __restrict__ sigma,
+                                         bool& any_new, bool& ovf) {
+  const unsigned long long nb = m & ~visited[w];
+  if (!nb) return;
+  atomicOr(nxt + w, nb);
+  any_new = true;
+  for (unsigned long long bb = nb; bb; bb &= bb - 1) {
+    const int b = __ffsll((long long)bb) - 1;
+    const unsigned long long add = sigma[(uint64_t)v * kBcBatch + b];
+    const unsigned long long old = atomicAdd(sigma + (uint64_t)w * kBcBatch + b, add);
+    ovf |= old + add < old;
+  }
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBcThreads) bc_push_kernel(uint32_t V, const OffT* __restrict__ out_off,
+                                                             const uint32_t* __restrict__ out_col,
+                                                             const unsigned long long* __restrict__ visited,
+                                                             unsigned long long* __restrict__ sigma,
+                                                             unsigned int* __restrict__ flags, const BcLoop* __restrict__ loop,
+                                                             unsigned long long* __restrict__ masks) {
+  if (!*(volatile const uint32_t*)&loop->push) return;
+  const uint32_t level = *(volatile const uint32_t*)&loop->level;
+  const unsigned long long* __restrict__ cur = ring_slot(masks, level, V);
+  unsigned long long* __restrict__ nxt = ring_slot(masks, level + 1, V);
+  constexpr int W = kBcThreads / 32;
+  __shared__ uint32_t s_v[kBcThreads];
+  __shared__ unsigned long long s_m[kBcThreads];
+  __shared__ int s_n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool any_new = false, ovf = false;
+  for (uint64_t base = (uint64_t)blockIdx.x * kBcThreads; base < V; base += (uint64_t)gridDim.x * kBcThreads) {
+    // stage the window's frontier vertices in shared memory
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const uint64_t vv = base + threadIdx.x;
+    const unsigned long long m = vv < V ? cur[vv] : 0ull;
+    if (m) {
+      const int k = atomicAdd(&s_n, 1);
+      s_v[k] = (uint32_t)vv;
+      s_m[k] = m;
+    }
+    __syncthreads();
+    const int n = s_n;
+    // light vertices: one warp each
+    for (int i = warp; i < n; i += W) {
+      const uint32_t v = s_v[i];
+      const OffT b = __ldg(out_off + v), e = __ldg(out_off + v + 1);
+      if ((uint64_t)(e - b) > (uint64_t)kPushCtaDegree) continue;
+      for (OffT j = b + lane; j < e; j += 32) push_arc(v, s_m[i], __ldg(out_col + j), visited, nxt, sigma, any_new, ovf);
+    }
+    // heavy vertices: the whole CTA
+    for (int i = 0; i < n; ++i) {
+      const uint32_t v = s_v[i];
+      const OffT b = __ldg(out_off + v), e = __ldg(out_off + v + 1);
+      if ((uint64_t)(e - b) <= (uint64_t)kPushCtaDegree) continue;
+      for (OffT j = b + threadIdx.x; j < e; j += kBcThreads)
+        push_arc(v, s_m[i], __ldg(out_col + j), visited, nxt, sigma, any_new, ovf);
+    }
+    __syncthreads();
+  }
+  if (__any_sync(0xffffffffu, any_new) && lane == 0) flags[level % kMaxStoredLevels] = 1u;
+  if (__any_sync(0xffffffffu, ovf) && lane == 0) flags[kOverflowFlag] = 1u;
+}
+
+// After a push level: the new vertices' visited bits and dist, and the
+// out-arcs of the next frontier.  One warp per 32 vertices.
+template <typename OffT>
+__global__ void __launch_bounds__(kBcThreads) bc_push_finalize(uint32_t V, const OffT* __restrict__ out_off,
+                                                               unsigned long long* __restrict__ visited,
+                                                               uint32_t* __restrict__ dist, BcLoop* __restrict__ loop,
+                                                               unsigned long long* __restrict__ masks) {
+  if (!*(volatile const uint32_t*)&loop->push) return;
+  const uint32_t level = *(volatile const uint32_t*)&loop->level;
+  const unsigned long long* __restrict__ nxt = ring_slot(masks, level + 1, V);
+  const int lane = threadIdx.x & 31;
+  unsigned long long arcs = 0;
+  const uint64_t nw = (uint64_t)gridDim.x * (kBcThreads / 32);
+  for (uint64_t g32 = ((uint64_t)blockIdx.x * kBcThreads + threadIdx.x) >> 5; g32 * 32 < V; g32 += nw) {
+    const uint64_t w = g32 * 32 + lane;
+    const unsigned long long nm = w < V ? nxt[w] : 0ull;
+    if (nm) {
+      visited[w] |= nm;
+      arcs += (unsigned long long)(__ldg(out_off + w + 1) - __ldg(out_off + w));
+    }
+    for (unsigned bal = __ballot_sync(0xffffffffu, nm != 0); bal; bal &= bal - 1) {
+      const int k = __ffs(bal) - 1;
+      const unsigned long long mk = __shfl_sync(0xffffffffu, nm, k);
+      const uint64_t wk = g32 * 32 + k;
+      if ((mk >> lane) & 1ull) dist[wk * kBcBatch + lane] = level + 1;
+      if ((mk >> (lane + 32)) & 1ull) dist[wk * kBcBatch + lane + 32] = level + 1;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
+  if (lane == 0 && arcs) atomicAdd(&loop->next_arcs, arcs);
+}
+
+// Before a push level: its next-frontier masks start at zero (a pull level
+// writes every vertex's mask itself).
+__global__ void bc_level_prep(uint32_t V, const BcLoop* __restrict__ loop, unsigned long long* __restrict__ masks) {
+  if (!*(volatile const uint32_t*)&loop->push) return;
+  const uint32_t level = *(volatile const uint32_t*)&loop->level;
+  unsigned long long* nxt = ring_slot(masks, level + 1, V);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x)
+    nxt[i] = 0ull;
+}
+
 // Resets one batch's state: visited and level-0 masks zero, dist all
 // unreached, the level flags zero (the overflow word is kept), loop state zero.
 __global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visited,
                                unsigned long long* __restrict__ mask0, uint32_t* __restrict__ dist,
-                               unsigned int* __restrict__ flags, BcLoop* __restrict__ loop) {
+                               unsigned long long* __restrict__ sigma, unsigned int* __restrict__ flags,
+                               BcLoop* __restrict__ loop, uint32_t push0) {
   const uint64_t n = (uint64_t)V * kBcBatch;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     dist[i] = kUnreached;
+    sigma[i] = 0ull;  // push levels add into sigma
     if (i < V) {
       visited[i] = 0ull;
       mask0[i] = 0ull;
@@ -610,6 +761,8 @@ __global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visi
       loop->level = 0u;
       loop->depth = 0u;
       loop->blevel = 0u;
+      loop->push = push0;  // level 0: the frontier is the batch's sources
+      loop->next_arcs = 0ull;
     }
   }
 }
@@ -619,9 +772,15 @@ __global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visi
 // level follows (and the flag words of the previous 63 levels are cleared when
 // the ring of flag words wraps, as the host loop did).  One thread.
 __global__ void bc_fwd_advance(BcLoop* __restrict__ loop, unsigned int* __restrict__ flags,
-                               uint32_t* __restrict__ depth_slot, unsigned long long cond) {
+                               uint32_t* __restrict__ depth_slot, unsigned long long cond, unsigned long long arcs,
+                               uint32_t push_ratio) {
   if (threadIdx.x != 0) return;
   const uint32_t l = loop->level;
+  // the next level pushes when its frontier's out-arcs, times push_ratio,
+  // stay below the graph's arcs (push_ratio 0: every level pulls)
+  const unsigned long long na = loop->next_arcs;
+  loop->next_arcs = 0ull;
+  loop->push = (push_ratio && na * push_ratio < arcs) ? 1u : 0u;
   if (flags[l % kMaxStoredLevels] == 0u) {
     loop->depth = l;
     loop->blevel = l;
@@ -689,6 +848,7 @@ static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGra
 constexpr int kBcMaxLanes = 4;
 constexpr int kBcLanes = 2;
 constexpr uint64_t kBcGraphBatches = 64;
+constexpr uint32_t kBcPushRatio = 4;
 template <typename OffT>
 static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {
@@ -723,6 +883,14 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   const unsigned bgrid = (unsigned)bc_grid(bc_backward_kernel<OffT>, V);
   const unsigned rgrid = std::max<unsigned>(1u, std::min<unsigned>((unsigned)(((uint64_t)V * kBcBatch + 255) / 256),
                                                                    (unsigned)sm_count() * 8));
+  const unsigned pgrid = (unsigned)bc_grid(bc_push_kernel<OffT>, V);
+  const unsigned zgrid = std::max<unsigned>(1u, std::min<unsigned>((unsigned)(((uint64_t)V + 255) / 256),
+                                                                   (unsigned)sm_count() * 8));
+  // direction choice: a level pushes when its frontier's out-arcs x ratio are
+  // below the graph's arcs; ZOGCU_BC_PUSH_RATIO=0 makes every level pull
+  uint32_t push_ratio = kBcPushRatio;
+  if (const char* env = std::getenv("ZOGCU_BC_PUSH_RATIO")) push_ratio = (uint32_t)std::max(0, std::atoi(env));
+  uint32_t push0 = push_ratio ? 1u : 0u;
   uint64_t host_launches = 0;
   for (uint64_t b0 = 0; b0 < nbatches; b0 += kBcGraphBatches) {
     const uint64_t b1 = std::min<uint64_t>(nbatches, b0 + kBcGraphBatches);
@@ -754,7 +922,7 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
       const size_t ndep = tail[w] ? 1 : 0;
       // reset and seed
       cudaGraphNode_t n_reset, n_seed;
-      void* reset_args[] = {&Vv, &visited, &mask0, &dist, &flags, &loop};
+      void* reset_args[] = {&Vv, &visited, &mask0, &dist, &sigma, &flags, &loop, &push0};
       ZOGCU_TRY(bc_kernel_node(graph, &n_reset, dep, ndep, (const void*)bc_batch_reset, rgrid, 256, reset_args));
       void* seed_args[] = {(void*)&src, &nb, &visited, &mask0, &sigma, &dist};
       ZOGCU_TRY(bc_kernel_node(graph, &n_seed, &n_reset, 1, (const void*)bc_seed_kernel, 1, 64, seed_args));
@@ -775,12 +943,23 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
         unsigned int* harrive = Wb.harrive.as<unsigned int>();
         const BcLoop* cloop = loop;
         void* fargs[] = {&Vv, (void*)&in_off, (void*)&col, (void*)&fcur, &fnxt, &visited, &sigma, &dist, &full,
-                         &level0, &flags, (void*)&heavy, &nheavy, &hpart, &hgot, &harrive, (void*)&cloop, &masks};
-        cudaGraphNode_t k1, k2;
-        ZOGCU_TRY(bc_kernel_node(fbody, &k1, nullptr, 0, (const void*)bc_forward_kernel<OffT>, fgrid, kBcThreads, fargs));
+                         &level0, &flags, (void*)&heavy, &nheavy, &hpart, &hgot, &harrive, (void*)&cloop, &masks,
+                         (void*)&out_off};
+        const uint32_t* ocol = g->out_col.as<uint32_t>();
+        const unsigned long long* cvisited = visited;
+        void* pargs[] = {&Vv, (void*)&out_off, (void*)&ocol, (void*)&cvisited, &sigma, &flags, (void*)&cloop, &masks};
+        void* prep_args[] = {&Vv, (void*)&cloop, &masks};
+        void* fin_args[] = {&Vv, (void*)&out_off, &visited, &dist, &loop, &masks};
+        // prep (zero the next masks of a push level) -> pull -> push -> finalize -> advance
+        cudaGraphNode_t k0, k1, k2, k3, k4;
+        ZOGCU_TRY(bc_kernel_node(fbody, &k0, nullptr, 0, (const void*)bc_level_prep, zgrid, 256, prep_args));
+        ZOGCU_TRY(bc_kernel_node(fbody, &k1, &k0, 1, (const void*)bc_forward_kernel<OffT>, fgrid, kBcThreads, fargs));
+        ZOGCU_TRY(bc_kernel_node(fbody, &k2, &k1, 1, (const void*)bc_push_kernel<OffT>, pgrid, kBcThreads, pargs));
+        ZOGCU_TRY(bc_kernel_node(fbody, &k3, &k2, 1, (const void*)bc_push_finalize<OffT>, zgrid, kBcThreads, fin_args));
         unsigned long long cond = hf;
-        void* aargs[] = {&loop, &flags, &depth_slot, &cond};
-        ZOGCU_TRY(bc_kernel_node(fbody, &k2, &k1, 1, (const void*)bc_fwd_advance, 1, 32, aargs));
+        unsigned long long arcs = g->E;
+        void* aargs[] = {&loop, &flags, &depth_slot, &cond, &arcs, &push_ratio};
+        ZOGCU_TRY(bc_kernel_node(fbody, &k4, &k3, 1, (const void*)bc_fwd_advance, 1, 32, aargs));
       }
       // backward levels
       cudaGraphNode_t n_bwd;
@@ -855,8 +1034,9 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   for (uint64_t bi = 0; bi < nbatches; ++bi) {
     const uint32_t d = h_depth[bi];
     max_depth = std::max(max_depth, d);
-    // reset, seed, (level + advance) x (depth + 1) forward, x max(depth, 1) backward
-    launches += 2 + 2 * ((uint64_t)d + 1) + 2 * std::max<uint64_t>(d, 1);
+    // reset, seed, (prep, pull, push, finalize, advance) x (depth + 1) forward,
+    // (level, advance) x max(depth, 1) backward
+    launches += 2 + 5 * ((uint64_t)d + 1) + 2 * std::max<uint64_t>(d, 1);
   }
   if (stats) {
     stats->sources = ns;

@@ -235,6 +235,10 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src,
 int ensure_pr_schedule(Graph* g, cudaStream_t stream);
 int ensure_task_list(Graph* g, int nnz, cudaStream_t stream);
 
+// Host <-> device copy of a caller array that may be pageable (pipelined
+// through pinned chunks on helper threads when it is), ordered on stream s.
+int copy_host(void* dev, void* host, size_t bytes, bool h2d, cudaStream_t s);
+
 // Small helper: number of SMs of the current device.
 int sm_count();
 

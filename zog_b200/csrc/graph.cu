@@ -18,6 +18,7 @@
 #include <cstring>
 #include <fstream>
 #include <string>
+#include <thread>
 #include <unordered_map>
 
 #include "common.cuh"
@@ -117,6 +118,108 @@ float EventTimer::ms() {
 EventTimer::~EventTimer() {
   if (a) cudaEventDestroy(a);
   if (b) cudaEventDestroy(b);
+}
+
+// ---------------------------------------------------------------------------
+// host <-> device copies of caller arrays that may be pageable
+// ---------------------------------------------------------------------------
+// A NIF hands over slices from the BEAM's allocator: pageable memory.  The
+// driver copies pageable memory through its own small staging buffers, one
+// copy at a time.  Here a pageable range is cut into kCopyThreads contiguous
+// parts, and each part is copied by its own host thread through two
+// library-owned pinned chunks of kBounceBytes on its own stream: while the DMA
+// engine moves one chunk, the thread fills the other, and the parts' DMAs
+// queue back to back on the link.  The pinned chunks are allocated on first
+// use and kept (one call at a time uses them; a concurrent call copies
+// directly).  Pinned caller memory is copied directly.
+constexpr int kCopyThreads = 8;
+constexpr size_t kBounceBytes = 16u << 20;
+
+static std::mutex g_bounce_mu;
+static void* g_bounce[2 * kCopyThreads] = {};
+
+static bool is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the error of an unknown pointer
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
+// Copies `bytes` between host memory `host` and device memory `dev` (h2d:
+// host -> device) ordered after the work already on stream s; the copy is
+// ordered before later work on s (s waits for the helper streams).
+int copy_host(void* dev, void* host, size_t bytes, bool h2d, cudaStream_t s) {
+  if (bytes == 0) return ZOGCU_OK;
+  const cudaMemcpyKind kind = h2d ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  std::unique_lock<std::mutex> lk(g_bounce_mu, std::try_to_lock);
+  if (bytes < 2 * kBounceBytes || is_pinned(host) || !lk.owns_lock()) {
+    ZOGCU_CUDA(h2d ? cudaMemcpyAsync(dev, host, bytes, kind, s) : cudaMemcpyAsync(host, dev, bytes, kind, s));
+    return ZOGCU_OK;
+  }
+  for (void*& b : g_bounce)
+    if (!b) ZOGCU_CUDA(cudaHostAlloc(&b, kBounceBytes, cudaHostAllocPortable));
+  cudaEvent_t start = nullptr;
+  ZOGCU_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+  ZOGCU_CUDA(cudaEventRecord(start, s));
+  cudaStream_t st[kCopyThreads] = {};
+  cudaEvent_t ev[2 * kCopyThreads] = {};
+  int rc = ZOGCU_OK;
+  for (int t = 0; t < kCopyThreads && rc == ZOGCU_OK; ++t) {
+    if (cudaStreamCreateWithFlags(&st[t], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamWaitEvent(st[t], start, 0) != cudaSuccess)
+      rc = fail(ZOGCU_ERR_CUDA, "copy stream set-up failed");
+    for (int k = 0; k < 2 && rc == ZOGCU_OK; ++k)
+      if (cudaEventCreateWithFlags(&ev[2 * t + k], cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(ZOGCU_ERR_CUDA, "copy event set-up failed");
+  }
+  std::atomic<int> err{0};
+  if (rc == ZOGCU_OK) {
+    std::vector<std::thread> th;
+    const size_t part = (bytes / kCopyThreads + 15) & ~(size_t)15;
+    for (int t = 0; t < kCopyThreads; ++t) {
+      const size_t lo = std::min(bytes, part * t), hi = std::min(bytes, part * (t + 1));
+      th.emplace_back([&, t, lo, hi] {
+        char* hb = static_cast<char*>(host);
+        char* db = static_cast<char*>(dev);
+        int k = 0;
+        for (size_t o = lo; o < hi; o += kBounceBytes, ++k) {
+          const size_t n = std::min(kBounceBytes, hi - o);
+          void* buf = g_bounce[2 * t + (k & 1)];
+          cudaEvent_t e = ev[2 * t + (k & 1)];
+          if (h2d) {
+            // the chunk is free again once the DMA two chunks back finished
+            if (k >= 2 && cudaEventSynchronize(e) != cudaSuccess) { err = 1; return; }
+            std::memcpy(buf, hb + o, n);
+            if (cudaMemcpyAsync(db + o, buf, n, kind, st[t]) != cudaSuccess ||
+                cudaEventRecord(e, st[t]) != cudaSuccess) { err = 1; return; }
+          } else {
+            if (cudaMemcpyAsync(buf, db + o, n, kind, st[t]) != cudaSuccess ||
+                cudaStreamSynchronize(st[t]) != cudaSuccess) { err = 1; return; }
+            std::memcpy(hb + o, buf, n);
+          }
+        }
+      });
+    }
+    for (auto& x : th) x.join();
+    if (err) rc = fail(ZOGCU_ERR_CUDA, "pipelined host copy failed");
+  }
+  for (int t = 0; t < kCopyThreads; ++t) {
+    if (!st[t]) continue;
+    cudaEvent_t done = nullptr;
+    if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(done, st[t]);
+      cudaStreamWaitEvent(s, done, 0);
+      cudaEventDestroy(done);
+    }
+    cudaStreamSynchronize(st[t]);  // the pinned chunks are reused by the next call
+    cudaStreamDestroy(st[t]);
+  }
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
+  cudaEventDestroy(start);
+  return rc;
 }
 
 // SM count of the first device queried (every device of a B200 node has the
@@ -596,11 +699,11 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
   ZOGCU_TRY(dt.alloc(num_edges * 4, sg.s));
   DevBuf dw;
   if (num_edges) {
-    ZOGCU_CUDA(cudaMemcpyAsync(df.ptr, from, num_edges * 4, cudaMemcpyHostToDevice, sg.s));
-    ZOGCU_CUDA(cudaMemcpyAsync(dt.ptr, to, num_edges * 4, cudaMemcpyHostToDevice, sg.s));
+    ZOGCU_TRY(copy_host(df.ptr, const_cast<uint32_t*>(from), num_edges * 4, true, sg.s));
+    ZOGCU_TRY(copy_host(dt.ptr, const_cast<uint32_t*>(to), num_edges * 4, true, sg.s));
     if (weight) {
       ZOGCU_TRY(dw.alloc(num_edges * 8, sg.s));
-      ZOGCU_CUDA(cudaMemcpyAsync(dw.ptr, weight, num_edges * 8, cudaMemcpyHostToDevice, sg.s));
+      ZOGCU_TRY(copy_host(dw.ptr, const_cast<double*>(weight), num_edges * 8, true, sg.s));
     }
   }
   tr.mark("arcs to the device");

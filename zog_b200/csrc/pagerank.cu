@@ -2352,7 +2352,8 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
   k_permute_out<<<grid_1d(V), 256, 0, s>>>(result, P.rank.as<uint32_t>(), V, unperm);
   ZOGCU_CUDA(cudaGetLastError());
   ++launches;
-  ZOGCU_CUDA(cudaMemcpyAsync(out, unperm, (size_t)V * 8, dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+  if (dev_ptrs) ZOGCU_CUDA(cudaMemcpyAsync(out, unperm, (size_t)V * 8, cudaMemcpyDeviceToDevice, s));
+  else ZOGCU_TRY(copy_host(unperm, out, (size_t)V * 8, false, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   tr->mark("scores to the caller");
   if (stats) {
