@@ -2202,6 +2202,17 @@ static bool pb_wanted(const Graph* g) {
 constexpr double kMixedSwitchTol = 1e-6;
 constexpr double kMixedStall = 0.97;
 
+// ZOGCU_PR_MIXED_SWITCH=<tol> moves the FP32 -> FP64 switch (for measuring
+// where the precision form's time goes); the result's bound is unchanged,
+// since the FP64 polish always runs to the caller's tolerance.
+static double mixed_switch_tol() {
+  if (const char* e = std::getenv("ZOGCU_PR_MIXED_SWITCH")) {
+    const double v = std::atof(e);
+    if (v > 0.0 && v < 1.0) return v;
+  }
+  return kMixedSwitchTol;
+}
+
 template <typename OffT>
 static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol, const zogcu_pr_opts* o, double* out,
                         zogcu_stats* stats, cudaStream_t s, PhaseTrace* tr) {
@@ -2295,7 +2306,7 @@ static int run_pagerank(Graph* g, double damping, uint64_t max_iter, double tol,
     std::memcpy(&Af, &A, sizeof(Af));  // same layout; only the contribution pointers differ in type
     Af.c0 = cf0.as<float>();
     Af.c1 = cf1.as<float>();
-    Af.tol = std::max(tol, kMixedSwitchTol);
+    Af.tol = std::max(tol, mixed_switch_tol());
     Af.stall = kMixedStall;
     int64_t from32 = -1;
     bool blocked = false, looped = false;
