@@ -11,7 +11,8 @@ CSR builder, independently of the library's.
 * PageRank, directed R-MAT scale 24 (edge factor 16, seed 1024; 16.8 M nodes,
   263 M arcs), FP64, d 0.85, tol 1e-9, at most 200 iterations: relative L1
   <= 1e-9 against the oracle and the same iteration count; the precision form
-  within 2*d/(1-d)*tol of the oracle.
+  within 2*d/(1-d)*tol of the oracle.  At tol 1e-14, the fixed-point checks
+  the tight reference vector of the bench needs (see that test).
 * PageRank, directed Barabasi-Albert n = 4,194,304, m = 8 (seed 4096): the
   same bars.
 * Brandes, undirected R-MAT scale 16 (edge factor 16, seed 1016): for 2,048
@@ -63,21 +64,43 @@ def test_pagerank_rmat24_matches_oracle(native, oracle, rmat24):
     torch.cuda.empty_cache()
 
 
-def test_pagerank_rmat24_tight_fp64_matches_oracle(native, oracle, rmat24):
+def test_pagerank_rmat24_tight_fp64(native, oracle, rmat24):
     """The tightly converged FP64 vector (tol 1e-14) that the errors of the
-    precision form and the learned start are reported against: the GPU's and
-    the oracle's agree to 1e-12 (each lies within ~1e-14 of the fixed point)."""
+    precision form and the learned start are reported against.
+
+    The reference's loop sums the dangling mass and the L1 step one node after
+    another (centrality.zig:926-931, :947-950).  Over 16.8 M nodes those
+    sequential sums round in a drift that moves the vector's mass by about
+    1.3e-10, so the oracle converged to 1e-14 sits 1.3e-10 (relative L1) from
+    the fixed point -- the reference arithmetic's own floor at this size -- and
+    it needs 78 iterations to get its step under 1e-14.  The GPU's sums are
+    tree-shaped; its tight vector is checked against the fixed point directly:
+    mass 1 to 1e-13 and one more update, computed independently in torch FP64
+    from the oracle's CSR, moving it by at most 1e-13.  Against the oracle it
+    stays within the parity bar of 1e-9."""
     import torch
 
     tight = 1e-14
     V, f, t, (in_off, in_col, deg) = rmat24
     ref, it, l1, _ = oracle.pagerank_csr_mt(V, in_off, in_col, deg, D, MAX_IT, tight)
-    assert l1 < tight and it < MAX_IT
     G = native.Graph.from_edges(V, f, t)
     try:
         x, st = G.pagerank(D, MAX_IT, tight, stats=True)
-        assert st["residual"] < tight
-        assert rel_l1(x, ref) <= 1e-12, rel_l1(x, ref)
+        assert st["residual"] < tight and st["iterations"] < MAX_IT
+        assert rel_l1(x, ref) <= TOL, rel_l1(x, ref)
+        assert abs(float(x.sum()) - 1.0) <= 1e-13
+        dev = torch.device("cuda")
+        counts = torch.from_numpy(np.diff(in_off.astype(np.int64))).to(dev)
+        dst = torch.repeat_interleave(torch.arange(V, device=dev), counts)
+        col = torch.from_numpy(in_col.view(np.int32)).to(dev).long()
+        degt = torch.from_numpy(deg.astype(np.float64)).to(dev)
+        dang = degt == 0
+        xt = torch.from_numpy(x).to(dev)
+        c = torch.where(dang, torch.zeros_like(xt), xt / degt.clamp(min=1.0))
+        y = torch.zeros_like(xt).index_add_(0, dst, c[col])
+        step = (1.0 - D) / V + D * (xt[dang].sum() / V + y)
+        assert float((step - xt).abs().sum()) <= 1e-13
+        del dst, col, counts
     finally:
         G.destroy()
         torch.cuda.empty_cache()

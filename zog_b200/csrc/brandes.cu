@@ -845,10 +845,10 @@ static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGra
 // graph once and reads the depths and flags at the end.  The lanes' score
 // vectors are added to d_bc at the end in lane order: a fixed order, so the
 // result is deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count.
-constexpr int kBcMaxLanes = 4;
-constexpr int kBcLanes = 2;
+constexpr int kBcMaxLanes = 8;
+constexpr int kBcLanes = 4;
 constexpr uint64_t kBcGraphBatches = 64;
-constexpr uint32_t kBcPushRatio = 4;
+constexpr uint32_t kBcPushRatio = 8;
 template <typename OffT>
 static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {

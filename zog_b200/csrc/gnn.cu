@@ -274,6 +274,104 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
   }
 }
 
+__device__ __forceinline__ uint32_t smem_u32_agg(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// ---- forward aggregate with the messages staged in shared memory ---------------
+// Z(v) = sum over the in-arcs u -> v of X(u), every message X(u) 16 bytes (8
+// BF16 or 4 FP32 values).  Warps take kChunk-arc chunks from a counter, as in
+// k_gnn_spmm, but a chunk is done in two phases: every lane copies the
+// messages of four of the chunk's arcs into the warp's staging tile with
+// 16-byte cp.async (coalesced index loads, 32 gathers in flight per lane
+// group, no registers held), and the next chunk's copies are issued before the
+// current chunk is summed; then each lane sums one row's staged messages in
+// arc order (a row with more than 32 arcs in the chunk is summed by the whole
+// warp).  A row inside one chunk is stored; a row that crosses a chunk
+// boundary is added with atomics.  Sums are FP32; Z starts at zero.
+constexpr int kAggWarps = 8;
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <class T, int D>
+__global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __restrict__ off,
+                                                              const uint32_t* __restrict__ col,
+                                                              const T* __restrict__ X, uint32_t V, uint32_t E,
+                                                              float* __restrict__ Z, uint32_t* __restrict__ next_chunk,
+                                                              const uint32_t* __restrict__ first_row) {
+  constexpr int PER = 16 / (int)sizeof(T);
+  static_assert(PER == D, "one 16-byte message per arc");
+  __shared__ __align__(16) uint4 s_stage[kAggWarps][2][kChunk];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint4* __restrict__ X16 = reinterpret_cast<const uint4*>(X);
+  const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
+  auto take = [&]() {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(next_chunk, 1u);
+    return __shfl_sync(0xffffffffu, c, 0);
+  };
+  auto gather = [&](uint32_t c, int b) {  // the messages of chunk c into buffer b
+    const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
+#pragma unroll
+    for (int k = 0; k < (int)kChunk / 32; ++k) {
+      const uint32_t j = cs + lane + 32 * k;
+      if (j < ce) cp_async16(smem_u32_agg(&s_stage[warp][b][j - cs]), X16 + __ldg(col + j));
+    }
+    cp_async_commit();
+  };
+  uint32_t c = take();
+  if (c < nchunks) gather(c, 0);
+  for (int b = 0; c < nchunks; b ^= 1) {
+    const uint32_t cn = take();
+    if (cn < nchunks) gather(cn, b ^ 1);
+    else cp_async_commit();  // an empty group keeps wait_group 1 meaning "chunk c landed"
+    cp_async_wait_prev();
+    __syncwarp();
+    const uint4* st = s_stage[warp][b];
+    const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
+    for (uint32_t r0 = __ldg(first_row + c); r0 < V;) {
+      const uint32_t ri = r0 + lane;
+      const uint32_t rb = ri < V ? __ldg(off + ri) : E;
+      const uint32_t re = ri < V ? __ldg(off + ri + 1) : E;
+      const bool in = rb < ce;  // row r0 + lane starts inside the chunk (lane 0 always)
+      const int nrows = __popc(__ballot_sync(0xffffffffu, in));
+      const uint32_t b0 = max(rb, cs), e0 = in ? min(re, ce) : b0;
+      const bool whole = rb >= cs && re <= ce;
+      const bool longseg = in && e0 - b0 > 32u;
+      if (in && !longseg) {
+        float acc[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) acc[i] = 0.f;
+        for (uint32_t j = b0; j < e0; ++j) add_row<T, PER>(acc, st[j - cs]);
+        put_row<D, PER>(Z, ri, 0, acc, whole);
+      }
+      // rows with more than 32 of their arcs in this chunk: the whole warp
+      for (unsigned lb = __ballot_sync(0xffffffffu, longseg); lb; lb &= lb - 1) {
+        const int q = __ffs(lb) - 1;
+        const uint32_t qb = __shfl_sync(0xffffffffu, b0, q), qe = __shfl_sync(0xffffffffu, e0, q);
+        const bool qw = __shfl_sync(0xffffffffu, whole ? 1 : 0, q) != 0;
+        float acc[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) acc[i] = 0.f;
+        for (uint32_t j = qb + lane; j < qe; j += 32) add_row<T, PER>(acc, st[j - cs]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+          for (int i = 0; i < PER; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+        if (lane == 0) put_row<D, PER>(Z, r0 + q, 0, acc, qw);
+      }
+      if (nrows < 32) break;  // the chunk ended inside these rows
+      r0 += 32;
+    }
+    __syncwarp();  // every lane is done with buffer b before it is refilled
+    c = cn;
+  }
+  cp_async_wait_all();
+}
+
 // ---- tensor-core, TMA and mbarrier primitives --------------------------------
 __device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                                  uint32_t b0, uint32_t b1) {
@@ -608,6 +706,132 @@ __global__ void __launch_bounds__(kDenseWarps * 32) k_gnn_dense_mid(
     __syncwarp();
   }
   if (lane == 0) bulk_wait_all();
+}
+
+// ---- inference: the dense layers with the hidden states kept in registers ----
+// Inference needs no hidden state after the layer that uses it, so k_gnn_infer
+// recomputes them instead of storing them: for its 16-node tile a warp runs
+// layer 0 from [F | A_0], then layer 1 from [H_0 | A_1], ... up to layer L,
+// each layer's BF16 output fragments becoming the next layer's A fragments
+// directly (an m16n8k16 accumulator pair is an A-fragment register).  It then
+// writes the next layer's message M_{L+1} = bf16(inv (H_L U_{L+1})) (L < 2) or
+// the head y (L = 2).  Every product is the training kernels' (same fragments,
+// same k-step order), so inference equals the training forward pass bit for
+// bit; the per-node traffic is F, the aggregates A_0..A_L and the output
+// (16 to 100 bytes) instead of a 128-byte hidden row read and written per layer.
+constexpr int kInferWarps = 8;
+
+// bias + ReLU + BF16 of an accumulator tile into packed pairs
+__device__ __forceinline__ void relu_pack(const float (&acc)[8][4], const float* bias, int t, uint32_t (&hp)[8][2]) {
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    const int c = nt * 8 + t * 2;
+    const float b0 = bias[c], b1 = bias[c + 1];
+    hp[nt][0] = pack_bf16x2(fmaxf(acc[nt][0] + b0, 0.f), fmaxf(acc[nt][1] + b1, 0.f));
+    hp[nt][1] = pack_bf16x2(fmaxf(acc[nt][2] + b0, 0.f), fmaxf(acc[nt][3] + b1, 0.f));
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(kInferWarps * 32) k_gnn_infer(const float* __restrict__ F,
+                                                                const float* __restrict__ A0,
+                                                                const float* __restrict__ A1,
+                                                                const float* __restrict__ A2,
+                                                                const __nv_bfloat16* __restrict__ w,
+                                                                const float* __restrict__ inv, uint32_t V,
+                                                                uint32_t ntiles, __nv_bfloat16* __restrict__ M_next,
+                                                                float* __restrict__ y) {
+  __shared__ uint2 s_f0[8 * 32];                   // layer 0: one k-step
+  __shared__ uint2 s_f[L > 0 ? L : 1][5 * 8 * 32];  // layers 1..L: five k-steps
+  __shared__ uint2 s_u[4 * 32];                    // U of layer L+1 (L < 2)
+  __shared__ float s_bias[L + 1][kH];
+  __shared__ float s_wo[kH + 1];
+  load_dense_frags(s_f0, 1, w + ws_offset(0), kF, w + wn_offset(0), kF);
+  for (int l = 1; l <= L; ++l) load_dense_frags(s_f[l - 1], 5, w + ws_offset(l), kH, w + wn_offset(l), kR);
+  if (L < kLayers - 1) load_msg_frags(s_u, w + layer_offset(L + 1));
+  for (int i = threadIdx.x; i < (L + 1) * kH; i += blockDim.x)
+    s_bias[i / kH][i % kH] = __bfloat162float(w[bias_offset(i / kH) + i % kH]);
+  if (L == kLayers - 1)
+    for (int i = threadIdx.x; i <= kH; i += blockDim.x) s_wo[i] = __bfloat162float(w[kHeadOffset + i]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntiles;
+       tile += gridDim.x * kInferWarps) {
+    const uint32_t ra = tile * kTile + g, rb = ra + 8;
+    const bool va = ra < V, vb = rb < V;
+    uint32_t hp[8][2];
+    {  // layer 0: k = 2t, 2t+1 from F (t < 2) or A_0 (t = 2, 3)
+      const float* pa = t < 2 ? F + (size_t)ra * kF + 2 * t : A0 + (size_t)ra * kF + 2 * (t - 2);
+      const float* pb = t < 2 ? F + (size_t)rb * kF + 2 * t : A0 + (size_t)rb * kF + 2 * (t - 2);
+      const float2 xa = va ? __ldg(reinterpret_cast<const float2*>(pa)) : make_float2(0.f, 0.f);
+      const float2 xb = vb ? __ldg(reinterpret_cast<const float2*>(pb)) : make_float2(0.f, 0.f);
+      const uint32_t a0 = pack_bf16x2(xa.x, xa.y), a1 = pack_bf16x2(xb.x, xb.y);
+      float acc[8][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+        const uint2 bb = s_f0[nt * 32 + lane];
+        mma_bf16_16x8x16(acc[nt], a0, a1, 0u, 0u, bb.x, bb.y);
+      }
+      relu_pack(acc, s_bias[0], t, hp);
+    }
+#pragma unroll
+    for (int l = 1; l <= L; ++l) {
+      const float* A = l == 1 ? A1 : A2;
+      const uint2* fr = s_f[l - 1];
+      float acc[8][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+          const uint2 bb = fr[(ks * 8 + nt) * 32 + lane];
+          mma_bf16_16x8x16(acc[nt], hp[2 * ks][0], hp[2 * ks][1], hp[2 * ks + 1][0], hp[2 * ks + 1][1], bb.x, bb.y);
+        }
+      const float2 xa = va ? __ldg(reinterpret_cast<const float2*>(A + (size_t)ra * kR + 2 * t)) : make_float2(0.f, 0.f);
+      const float2 xb = vb ? __ldg(reinterpret_cast<const float2*>(A + (size_t)rb * kR + 2 * t)) : make_float2(0.f, 0.f);
+      const uint32_t a0 = pack_bf16x2(xa.x, xa.y), a1 = pack_bf16x2(xb.x, xb.y);
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const uint2 bb = fr[(4 * 8 + nt) * 32 + lane];
+        mma_bf16_16x8x16(acc[nt], a0, a1, 0u, 0u, bb.x, bb.y);
+      }
+      relu_pack(acc, s_bias[l], t, hp);
+    }
+    if (L < kLayers - 1) {
+      float m[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const uint2 bb = s_u[kk * 32 + lane];
+        mma_bf16_16x8x16(m, hp[2 * kk][0], hp[2 * kk][1], hp[2 * kk + 1][0], hp[2 * kk + 1][1], bb.x, bb.y);
+      }
+      if (va) {
+        const float sc = __ldg(inv + ra);
+        *reinterpret_cast<uint32_t*>(M_next + (size_t)ra * kR + 2 * t) = pack_bf16x2(m[0] * sc, m[1] * sc);
+      }
+      if (vb) {
+        const float sc = __ldg(inv + rb);
+        *reinterpret_cast<uint32_t*>(M_next + (size_t)rb * kR + 2 * t) = pack_bf16x2(m[2] * sc, m[3] * sc);
+      }
+    } else {
+      float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + t * 2;
+        s0 += bf16_lo(hp[nt][0]) * s_wo[c] + bf16_hi(hp[nt][0]) * s_wo[c + 1];
+        s1 += bf16_lo(hp[nt][1]) * s_wo[c] + bf16_hi(hp[nt][1]) * s_wo[c + 1];
+      }
+      s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+      s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+      if (t == 0) {
+        if (va) y[ra] = s0 + s_wo[kH];
+        if (vb) y[rb] = s1 + s_wo[kH];
+      }
+    }
+  }
 }
 
 // ---- dense layer backward (data): dP = dOut * (Out > 0); dX = dP Ws^T (DIN),
@@ -1023,12 +1247,12 @@ struct GnnActs {
       // the dense kernels copy 512-byte aggregate tiles with bulk copies
       if (reinterpret_cast<uintptr_t>(A[l].ptr) & 15u) return fail(ZOGCU_ERR_INTERNAL, "aggregate array is not 16-byte aligned");
     }
-    for (int l = 0; l < kLayers; ++l) {
-      if (l == kLayers - 1 && !train) break;
-      ZOGCU_TRY(L.get(H[l], 10 + l, (size_t)Vp * kH * 2));
-      ZOGCU_TRY(hidden_map(&mapH[l], H[l].ptr, Vp));
-    }
-    if (!train) mapH[kLayers - 1] = mapH[0];  // never stored; a valid map for the kernel argument
+    // hidden states: stored for the backward pass only (inference recomputes them)
+    if (train)
+      for (int l = 0; l < kLayers; ++l) {
+        ZOGCU_TRY(L.get(H[l], 10 + l, (size_t)Vp * kH * 2));
+        ZOGCU_TRY(hidden_map(&mapH[l], H[l].ptr, Vp));
+      }
     return ZOGCU_OK;
   }
 };
@@ -1065,6 +1289,22 @@ int spmm(const Graph* g, bool transpose, const float* inv, const T* X, float* Z,
   return ZOGCU_OK;
 }
 
+// Z = agg(X) over the in-CSR for 16-byte messages (k_gnn_agg16); Z (zrows x
+// D, zrows >= V) is zeroed first.
+template <class T, int D>
+int aggregate(const Graph* g, const T* X, float* Z, size_t zrows, uint32_t* ctr, const DevBuf& rows, cudaStream_t s) {
+  const uint32_t V = g->V;
+  const uint32_t E = (uint32_t)g->E;
+  ZOGCU_CUDA(cudaMemsetAsync(Z, 0, zrows * D * 4, s));
+  if (E == 0) return ZOGCU_OK;
+  const uint64_t chunks = ((uint64_t)E + kChunk - 1) / kChunk;
+  ZOGCU_CUDA(cudaMemsetAsync(ctr, 0, 4, s));
+  k_gnn_agg16<T, D><<<gwarp(chunks), kAggWarps * 32, 0, s>>>(g->in_off32.as<uint32_t>(), g->in_col.as<uint32_t>(), X, V,
+                                                             E, Z, ctr, rows.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  return ZOGCU_OK;
+}
+
 // Forward pass; with train the last hidden state is stored for the backward
 // pass.  err: device word the dense kernels raise when a tile load timed out.
 int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, bool train, cudaStream_t s) {
@@ -1079,21 +1319,44 @@ int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, bool train, cu
                                         1.f / (float)std::max<uint64_t>(g->n_live, 1), act.F.as<float>(),
                                         act.inv.as<float>(), act.M0.as<float>());
   const float* inv = act.inv.as<float>();
+  const float* F = act.F.as<float>();
   ZOGCU_TRY(chunk_rows(g, false, act.rows, s));
-  ZOGCU_TRY((spmm<float, kF>(g, false, inv, act.M0.as<float>(), act.A[0].as<float>(), V, ctr, act.rows, s)));
+  ZOGCU_TRY((aggregate<float, kF>(g, act.M0.as<float>(), act.A[0].as<float>(), V, ctr, act.rows, s)));
+  if (!train) {
+    // inference: the dense layers recompute the hidden states in registers
+    const unsigned ig = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)ntiles + kInferWarps - 1) / kInferWarps, (uint64_t)sm_count() * 8));
+    const float* A0 = act.A[0].as<float>();
+    const float* A1 = act.A[1].as<float>();
+    const float* A2 = act.A[2].as<float>();
+    k_gnn_infer<0><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, act.M[1].as<__nv_bfloat16>(),
+                                                  nullptr);
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, act.M[1].as<__nv_bfloat16>(), act.A[1].as<float>(), act.Vp, ctr,
+                                            act.rows, s)));
+    k_gnn_infer<1><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, act.M[2].as<__nv_bfloat16>(),
+                                                  nullptr);
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, act.M[2].as<__nv_bfloat16>(), act.A[2].as<float>(), act.Vp, ctr,
+                                            act.rows, s)));
+    k_gnn_infer<2><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, nullptr, act.y.as<float>());
+    ZOGCU_CUDA(cudaGetLastError());
+    return ZOGCU_OK;
+  }
+  // training: hidden states stored (TMA tile loads and stores) for the backward pass
   k_gnn_dense0<<<dense_grid((const void*)k_gnn_dense0, ntiles), kDenseWarps * 32, kDenseSmem, s>>>(
-      act.mapH[0], act.F.as<float>(), act.A[0].as<float>(), w, inv, V, ntiles, act.M[1].as<__nv_bfloat16>());
+      act.mapH[0], F, act.A[0].as<float>(), w, inv, V, ntiles, act.M[1].as<__nv_bfloat16>());
   ZOGCU_CUDA(cudaGetLastError());
   for (int l = 1; l < kLayers; ++l) {
-    ZOGCU_TRY((spmm<__nv_bfloat16, kR>(g, false, inv, act.M[l].as<__nv_bfloat16>(), act.A[l].as<float>(), act.Vp,
-                                       ctr, act.rows, s)));
+    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, act.M[l].as<__nv_bfloat16>(), act.A[l].as<float>(), act.Vp, ctr,
+                                            act.rows, s)));
     if (l < kLayers - 1) {
       k_gnn_dense_mid<0><<<dense_grid((const void*)k_gnn_dense_mid<0>, ntiles), kDenseWarps * 32, kDenseSmem, s>>>(
           act.mapH[l - 1], act.mapH[l], act.A[l].as<float>(), w, l, inv, V, ntiles, 1,
           act.M[l + 1].as<__nv_bfloat16>(), nullptr, err);
     } else {
       k_gnn_dense_mid<1><<<dense_grid((const void*)k_gnn_dense_mid<1>, ntiles), kDenseWarps * 32, kDenseSmem, s>>>(
-          act.mapH[l - 1], act.mapH[l], act.A[l].as<float>(), w, l, inv, V, ntiles, train ? 1 : 0, nullptr,
+          act.mapH[l - 1], act.mapH[l], act.A[l].as<float>(), w, l, inv, V, ntiles, 1, nullptr,
           act.y.as<float>(), err);
     }
     ZOGCU_CUDA(cudaGetLastError());
