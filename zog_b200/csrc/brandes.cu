@@ -834,7 +834,8 @@ static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGra
 }
 
 // Batches of kBcBatch sources are dealt to kBcLanes "lanes" (batch b to lane
-// b % lanes), each with its own workspace and score vector.  A call's batches
+// b % lanes, as many lanes as half the free device memory holds), each with
+// its own workspace and score vector.  A call's batches
 // run as CUDA graphs of up to kBcGraphBatches batches: in a graph, every lane
 // is a chain of its batches -- reset, seed, a while loop of forward levels
 // (each level kernel followed by a one-thread kernel that ends the loop when
@@ -846,9 +847,9 @@ static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGra
 // vectors are added to d_bc at the end in lane order: a fixed order, so the
 // result is deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count.
 constexpr int kBcMaxLanes = 8;
-constexpr int kBcLanes = 4;
+constexpr int kBcLanes = 8;
 constexpr uint64_t kBcGraphBatches = 64;
-constexpr uint32_t kBcPushRatio = 8;
+constexpr uint32_t kBcPushRatio = 16;
 template <typename OffT>
 static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {
@@ -859,6 +860,17 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   int nlanes = kBcLanes;
   if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) nlanes = std::max(1, std::min(kBcMaxLanes, std::atoi(env)));
   nlanes = (int)std::min<uint64_t>((uint64_t)nlanes, std::max<uint64_t>(nbatches, 1));
+  {
+    // a lane's workspace is about V * 1.9 KB (dist, sigma, q, the mask ring):
+    // keep all lanes within half of the free device memory
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const uint64_t per_lane = (uint64_t)std::max<uint32_t>(V, 1) * (4 + 8 + 8) * kBcBatch +
+                                (uint64_t)std::max<uint32_t>(V, 1) * 8 * (kMaxStoredLevels + 4);
+      const uint64_t fit = per_lane ? (uint64_t)(free_b / 2) / per_lane : (uint64_t)nlanes;
+      nlanes = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)nlanes, fit));
+    }
+  }
   DevBuf bcx[kBcMaxLanes], loops, depths;
   double* bcs[kBcMaxLanes];
   bcs[0] = d_bc;

@@ -274,27 +274,45 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
   }
 }
 
-__device__ __forceinline__ uint32_t smem_u32_agg(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 // ---- forward aggregate with the messages staged in shared memory ---------------
 // Z(v) = sum over the in-arcs u -> v of X(u), every message X(u) 16 bytes (8
 // BF16 or 4 FP32 values).  Warps take kChunk-arc chunks from a counter, as in
-// k_gnn_spmm, but a chunk is done in two phases: every lane copies the
-// messages of four of the chunk's arcs into the warp's staging tile with
-// 16-byte cp.async (coalesced index loads, 32 gathers in flight per lane
-// group, no registers held), and the next chunk's copies are issued before the
-// current chunk is summed; then each lane sums one row's staged messages in
-// arc order (a row with more than 32 arcs in the chunk is summed by the whole
-// warp).  A row inside one chunk is stored; a row that crosses a chunk
-// boundary is added with atomics.  Sums are FP32; Z starts at zero.
+// k_gnn_spmm, but a chunk is done in two phases.  First every lane loads the
+// messages of four of the chunk's arcs (coalesced index loads, 16-byte
+// message loads) and writes them to the warp's staging tile in shared memory;
+// the next chunk's loads are issued into registers before the current chunk
+// is summed, so they are in flight meanwhile.  Then each lane sums one row's
+// staged messages in arc order (a row with more than 32 arcs in the chunk is
+// summed by the whole warp).  A row inside one chunk is stored; a row that
+// crosses a chunk boundary is added with atomics.  The arc indices stream with
+// an L2 evict-first policy and skip L1; the messages, which other arcs gather
+// again, are loaded with an evict-last policy.  Sums are FP32; Z starts at zero.
 constexpr int kAggWarps = 8;
 
-__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// an arc index: streamed once, so it neither stays in L1 nor displaces messages in L2
+__device__ __forceinline__ uint32_t ld_index(const uint32_t* a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+// a message: gathered again by other arcs, kept in L2 ahead of the streams
+__device__ __forceinline__ uint4 ld_message(const uint4* a, uint64_t pol) {
+  uint4 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(a), "l"(pol));
+  return v;
+}
 
 template <class T, int D>
 __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __restrict__ off,
@@ -303,34 +321,37 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
                                                               float* __restrict__ Z, uint32_t* __restrict__ next_chunk,
                                                               const uint32_t* __restrict__ first_row) {
   constexpr int PER = 16 / (int)sizeof(T);
+  constexpr int K = (int)kChunk / 32;  // messages per lane and chunk
   static_assert(PER == D, "one 16-byte message per arc");
-  __shared__ __align__(16) uint4 s_stage[kAggWarps][2][kChunk];
+  __shared__ __align__(16) uint4 s_stage[kAggWarps][kChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint4* __restrict__ X16 = reinterpret_cast<const uint4*>(X);
+  const uint64_t pol_idx = l2_evict_first(), pol_msg = l2_evict_last();
   const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
+  uint4* st = s_stage[warp];
   auto take = [&]() {
     uint32_t c = 0;
     if (lane == 0) c = atomicAdd(next_chunk, 1u);
     return __shfl_sync(0xffffffffu, c, 0);
   };
-  auto gather = [&](uint32_t c, int b) {  // the messages of chunk c into buffer b
+  // the messages of chunk c into registers (issued; used one chunk later)
+  auto gather = [&](uint32_t c, uint4 (&v)[K]) {
     const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
 #pragma unroll
-    for (int k = 0; k < (int)kChunk / 32; ++k) {
+    for (int k = 0; k < K; ++k) {
       const uint32_t j = cs + lane + 32 * k;
-      if (j < ce) cp_async16(smem_u32_agg(&s_stage[warp][b][j - cs]), X16 + __ldg(col + j));
+      v[k] = j < ce ? ld_message(X16 + ld_index(col + j, pol_idx), pol_msg) : make_uint4(0u, 0u, 0u, 0u);
     }
-    cp_async_commit();
   };
+  uint4 v[K];
   uint32_t c = take();
-  if (c < nchunks) gather(c, 0);
-  for (int b = 0; c < nchunks; b ^= 1) {
-    const uint32_t cn = take();
-    if (cn < nchunks) gather(cn, b ^ 1);
-    else cp_async_commit();  // an empty group keeps wait_group 1 meaning "chunk c landed"
-    cp_async_wait_prev();
+  if (c < nchunks) gather(c, v);
+  while (c < nchunks) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) st[lane + 32 * k] = v[k];
     __syncwarp();
-    const uint4* st = s_stage[warp][b];
+    const uint32_t cn = take();
+    if (cn < nchunks) gather(cn, v);  // in flight while chunk c is summed
     const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
     for (uint32_t r0 = __ldg(first_row + c); r0 < V;) {
       const uint32_t ri = r0 + lane;
@@ -366,10 +387,9 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
       if (nrows < 32) break;  // the chunk ended inside these rows
       r0 += 32;
     }
-    __syncwarp();  // every lane is done with buffer b before it is refilled
+    __syncwarp();  // every lane is done with the staging tile before it is refilled
     c = cn;
   }
-  cp_async_wait_all();
 }
 
 // ---- tensor-core, TMA and mbarrier primitives --------------------------------
