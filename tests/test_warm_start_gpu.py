@@ -183,3 +183,35 @@ def test_shipped_weights_gain_over_uniform_start(native):
                 G.destroy()
     finally:
         net.destroy()
+
+
+def test_tcgen05_inference_matches_mma_sync(native, oracle, monkeypatch):
+    """The tensor-memory inference kernels (ZOGCU_GNN_TC=1) against the
+    mma.sync ones and the oracle: both compute the same products in another
+    accumulation order, so outputs agree to the BF16 tolerances above."""
+    net = native.WarmStart.create(13)
+    try:
+        net.set_params(perturbed_params(13))
+        p = net.get_params()
+        graphs = list(sample_graphs(native, oracle))
+        V, f, t = oracle.rmat(14, 8, 1014, directed=True)  # several 128-node tiles, a ragged last one
+        graphs.append(("rmat14", native.Graph.from_edges(V, f, t)))
+        for name, G in graphs:
+            try:
+                monkeypatch.setenv("ZOGCU_GNN_TC", "0")
+                x_s, y_s = net.predict(G, raw=True)
+                monkeypatch.setenv("ZOGCU_GNN_TC", "1")
+                x_t, y_t = net.predict(G, raw=True)
+                x_t2, y_t2 = net.predict(G, raw=True)
+                assert np.array_equal(y_t, y_t2), name  # deterministic
+                scale = 1 + np.abs(y_s).max()
+                assert np.abs(y_t - y_s).max() <= Y_TOL * scale, (name, np.abs(y_t - y_s).max())
+                assert np.abs(y_t - y_s).mean() <= Y_MEAN_TOL * scale, name
+                y_ref, _ = GO.forward(p, csr_of(G))
+                assert np.abs(y_t - y_ref).max() <= Y_TOL * (1 + np.abs(y_ref).max()), name
+                assert abs(x_t.sum() - 1.0) < 1e-12
+            finally:
+                G.destroy()
+    finally:
+        monkeypatch.delenv("ZOGCU_GNN_TC", raising=False)
+        net.destroy()

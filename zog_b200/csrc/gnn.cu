@@ -854,6 +854,278 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_gnn_infer(const float* __r
   }
 }
 
+// ---- inference on the 5th-generation tensor cores (tcgen05, TMEM) -----------
+// The same computation as k_gnn_infer, for tiles of 128 nodes per CTA: one
+// thread per node row builds the layer's A operand in shared memory (the
+// 128-byte-swizzled K-major layout the tensor core reads through a matrix
+// descriptor), thread 0 issues tcgen05.mma with the FP32 accumulator in tensor
+// memory (128 lanes = the tile's rows, 64 columns), tcgen05.commit arrives on
+// an mbarrier, and every thread reads its row's 64 accumulators back with
+// tcgen05.ld for the epilogue (bias, ReLU, BF16), which writes the next
+// layer's A operand.  Layer 0 is one K=16 step over [F | A_0 | 0]; layers 1
+// and 2 are four K=16 steps over the hidden tile plus one over [A_l | 0]; the
+// message product H U is one more N=16 MMA into columns 64-79.  Weights sit in
+// shared memory as N x K K-major swizzled tiles for the whole kernel.
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTcCols = 128;  // TMEM columns: [0, 64) hidden accumulator, [64, 80) message accumulator
+constexpr uint32_t kTileBytes128 = kTcRows * 128;  // a 128-row, 128-byte-row swizzled tile
+constexpr uint32_t kWTileBytes = 64 * 128;         // a 64-row weight tile
+constexpr uint32_t kUTileBytes = 16 * 128;         // the 16-row message-weight tile
+
+__host__ __device__ constexpr uint32_t tc_smem_bytes(int L) {
+  // H, AG, B0, (Ws, Wn) per layer 1..L, U, bias (L+1) x 64, head 65, mbarrier + TMEM address
+  return kTileBytes128 * 2 + kWTileBytes + 2 * kWTileBytes * (uint32_t)L + kUTileBytes + (uint32_t)(L + 1) * kH * 4 +
+         (kH + 1) * 4 + 64;
+}
+
+// byte offset of element (row, k) of a K-major tile with 128-byte rows and the
+// 128-byte swizzle (16-byte chunk k/8 of row r stored at chunk (k/8) ^ (r % 8))
+__device__ __forceinline__ uint32_t sw128_off(uint32_t row, uint32_t k) {
+  return row * 128u + ((((k >> 3) ^ (row & 7u)) & 7u) << 4) + (k & 7u) * 2u;
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart; start address in 16-byte units
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// instruction descriptor: BF16 A and B (K-major), FP32 accumulator, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, int accum) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+
+// one BF16 weight into a swizzled N x K tile: tile[n][k] = value
+__device__ __forceinline__ void put_w(unsigned char* tile, uint32_t n, uint32_t k, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(tile + sw128_off(n, k)) = __float2bfloat16_rn(v);
+}
+// 16 bytes (8 BF16) into chunk c of row r of a swizzled tile
+__device__ __forceinline__ void put_chunk(unsigned char* tile, uint32_t r, uint32_t c, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + r * 128u + (((c ^ (r & 7u)) & 7u) << 4)) = v;
+}
+
+// accumulators of one layer -> bias, ReLU, BF16 (packed pairs, column order)
+__device__ __forceinline__ void tc_layer_out(uint32_t taddr, const float* bias, uint32_t (&hp)[32]) {
+  float a[32];
+  tc_ld32(taddr, a);
+  float b[32];
+  tc_ld32(taddr + 32, b);
+  tc_wait_ld();
+#pragma unroll
+  for (int i = 0; i < 16; ++i) hp[i] = pack_bf16x2(fmaxf(a[2 * i] + bias[2 * i], 0.f), fmaxf(a[2 * i + 1] + bias[2 * i + 1], 0.f));
+#pragma unroll
+  for (int i = 0; i < 16; ++i)
+    hp[16 + i] = pack_bf16x2(fmaxf(b[2 * i] + bias[32 + 2 * i], 0.f), fmaxf(b[2 * i + 1] + bias[33 + 2 * i], 0.f));
+}
+
+template <int L>
+__global__ void __launch_bounds__(kTcThreads, 1) k_gnn_infer_tc(const float* __restrict__ F,
+                                                                 const float* __restrict__ A0,
+                                                                 const float* __restrict__ A1,
+                                                                 const float* __restrict__ A2,
+                                                                 const __nv_bfloat16* __restrict__ w,
+                                                                 const float* __restrict__ inv, uint32_t V,
+                                                                 uint32_t ntiles, __nv_bfloat16* __restrict__ M_next,
+                                                                 float* __restrict__ y, unsigned int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t a0 = smem_u32(smem_raw);
+  unsigned char* base = smem_raw + (((a0 + 1023u) & ~1023u) - a0);
+  unsigned char* tH = base;
+  unsigned char* tAG = base + kTileBytes128;
+  unsigned char* tB0 = base + 2 * kTileBytes128;
+  unsigned char* tBs[3] = {nullptr, nullptr, nullptr};
+  unsigned char* tBn[3] = {nullptr, nullptr, nullptr};
+  uint32_t off = 2 * kTileBytes128 + kWTileBytes;
+#pragma unroll
+  for (int l = 1; l <= L; ++l) {
+    tBs[l] = base + off;
+    off += kWTileBytes;
+    tBn[l] = base + off;
+    off += kWTileBytes;
+  }
+  unsigned char* tBu = base + off;
+  off += kUTileBytes;
+  float* s_bias = reinterpret_cast<float*>(base + off);
+  off += (L + 1) * kH * 4;
+  float* s_wo = reinterpret_cast<float*>(base + off);
+  off += (kH + 1) * 4;
+  off = (off + 7u) & ~7u;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base + off);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(base + off + 8);
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  // weights as N x K tiles: B0 = [Ws_0; Wn_0; 0]^T (K = 16), Ws_l^T (K = 64),
+  // Wn_l^T padded to K = 16, U^T padded to N = 16
+  for (int i = tid; i < 64 * 64; i += kTcThreads) {
+    const uint32_t n = (uint32_t)i / 64, k = (uint32_t)i % 64;
+    if (k < 16) {
+      const float v = k < (uint32_t)kF ? __bfloat162float(w[ws_offset(0) + k * kH + n])
+                      : k < 2u * kF   ? __bfloat162float(w[wn_offset(0) + (k - kF) * kH + n])
+                                      : 0.f;
+      put_w(tB0, n, k, v);
+    }
+#pragma unroll
+    for (int l = 1; l <= L; ++l) {
+      put_w(tBs[l], n, k, __bfloat162float(w[ws_offset(l) + k * kH + n]));
+      if (k < 16) put_w(tBn[l], n, k, k < (uint32_t)kR ? __bfloat162float(w[wn_offset(l) + k * kH + n]) : 0.f);
+    }
+    if (L < kLayers - 1 && n < 16) put_w(tBu, n, k, n < (uint32_t)kR ? __bfloat162float(w[layer_offset(L + 1) + k * kR + n]) : 0.f);
+  }
+  for (int i = tid; i < (L + 1) * kH; i += kTcThreads) s_bias[i] = __bfloat162float(w[bias_offset(i / kH) + i % kH]);
+  for (int i = tid; i <= kH; i += kTcThreads) s_wo[i] = __bfloat162float(w[kHeadOffset + i]);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(s_tmem)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's lane quarter
+  const uint32_t sH = smem_u32(tH), sAG = smem_u32(tAG), sB0 = smem_u32(tB0), sBu = smem_u32(tBu);
+  uint32_t phase = 0;
+  bool ok = true;
+  // issue the MMAs (thread 0), wait for them (every thread, bounded)
+  auto sync_operands = [&]() {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  };
+  auto finish = [&]() {
+    if (tid == 0) tc_commit(bar);
+    // a block-wide vote, so every thread leaves the tile loop together if a wait timed out
+    ok = __syncthreads_and(mbar_wait(bar, phase) ? 1 : 0) != 0;
+    phase ^= 1u;
+    tc_fence_after();
+  };
+  for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const uint32_t r = tile * kTcRows + (uint32_t)tid;
+    const bool valid = r < V;
+    {  // layer 0 operand: [F | A_0] as 8 BF16, then zeros (K = 16)
+      const float4 f = valid ? __ldg(reinterpret_cast<const float4*>(F) + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 a = valid ? __ldg(reinterpret_cast<const float4*>(A0) + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+      put_chunk(tAG, tid, 0, make_uint4(pack_bf16x2(f.x, f.y), pack_bf16x2(f.z, f.w), pack_bf16x2(a.x, a.y),
+                                        pack_bf16x2(a.z, a.w)));
+      put_chunk(tAG, tid, 1, make_uint4(0u, 0u, 0u, 0u));
+    }
+    sync_operands();
+    if (tid == 0) tc_mma(tmem, sw128_desc(sAG), sw128_desc(sB0), tc_idesc(64), 0);
+    finish();
+    if (!ok) break;
+    uint32_t hp[32];
+    tc_layer_out(tlane, s_bias, hp);
+#pragma unroll
+    for (int l = 1; l <= L; ++l) {
+      const float* A = l == 1 ? A1 : A2;
+      // the hidden tile and [A_l | 0]
+      tc_fence_before();
+      __syncthreads();  // every thread has read the accumulators and the previous operands are consumed
+#pragma unroll
+      for (int c = 0; c < 8; ++c) put_chunk(tH, tid, c, make_uint4(hp[4 * c], hp[4 * c + 1], hp[4 * c + 2], hp[4 * c + 3]));
+      float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
+      if (valid) {
+        x0 = __ldg(reinterpret_cast<const float4*>(A + (size_t)r * kR));
+        x1 = __ldg(reinterpret_cast<const float4*>(A + (size_t)r * kR + 4));
+      }
+      put_chunk(tAG, tid, 0, make_uint4(pack_bf16x2(x0.x, x0.y), pack_bf16x2(x0.z, x0.w), pack_bf16x2(x1.x, x1.y),
+                                        pack_bf16x2(x1.z, x1.w)));
+      sync_operands();
+      if (tid == 0) {
+        const uint32_t sBs = smem_u32(tBs[l]), sBn = smem_u32(tBn[l]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) tc_mma(tmem, sw128_desc(sH + 32 * k), sw128_desc(sBs + 32 * k), tc_idesc(64), k > 0);
+        tc_mma(tmem, sw128_desc(sAG), sw128_desc(sBn), tc_idesc(64), 1);
+      }
+      finish();
+      if (!ok) break;
+      tc_layer_out(tlane, s_bias + l * kH, hp);
+    }
+    if (!ok) break;
+    if (L < kLayers - 1) {
+      tc_fence_before();
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < 8; ++c) put_chunk(tH, tid, c, make_uint4(hp[4 * c], hp[4 * c + 1], hp[4 * c + 2], hp[4 * c + 3]));
+      sync_operands();
+      if (tid == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) tc_mma(tmem + 64, sw128_desc(sH + 32 * k), sw128_desc(sBu + 32 * k), tc_idesc(16), k > 0);
+      }
+      finish();
+      if (!ok) break;
+      float m[8];
+      tc_ld8(tlane + 64, m);
+      tc_wait_ld();
+      if (valid) {
+        const float sc = __ldg(inv + r);
+        *reinterpret_cast<uint4*>(M_next + (size_t)r * kR) =
+            make_uint4(pack_bf16x2(m[0] * sc, m[1] * sc), pack_bf16x2(m[2] * sc, m[3] * sc),
+                       pack_bf16x2(m[4] * sc, m[5] * sc), pack_bf16x2(m[6] * sc, m[7] * sc));
+      }
+    } else {
+      float acc = 0.f;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) acc += bf16_lo(hp[i]) * s_wo[2 * i] + bf16_hi(hp[i]) * s_wo[2 * i + 1];
+      if (valid) y[r] = acc + s_wo[kH];
+    }
+    tc_fence_before();
+    __syncthreads();  // the tile's operands and accumulators are free for the next tile
+    tc_fence_after();
+  }
+  if (!ok && tid == 0) atomicExch(err, 1u);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols) : "memory");
+}
+
 // ---- dense layer backward (data): dP = dOut * (Out > 0); dX = dP Ws^T (DIN),
 // dA = dP Wn^T (DM) (the BF16 roundings of the forward operands pass the
 // gradient straight through).  dP is written back in place of dOut for the
@@ -1325,6 +1597,33 @@ int aggregate(const Graph* g, const T* X, float* Z, size_t zrows, uint32_t* ctr,
   return ZOGCU_OK;
 }
 
+// The tcgen05 inference kernels: dynamic shared memory of at least 60 KB so
+// that at most three CTAs share an SM (their 3 x 128 TMEM columns fit the
+// SM's 512); ZOGCU_GNN_TC=1 selects them (the mma.sync kernels otherwise).
+bool gnn_use_tc() {
+  const char* e = std::getenv("ZOGCU_GNN_TC");
+  return e && e[0] == '1';
+}
+
+template <int L>
+int launch_infer_tc(const float* F, const float* A0, const float* A1, const float* A2, const __nv_bfloat16* w,
+                    const float* inv, uint32_t V, __nv_bfloat16* M_next, float* y, unsigned int* err, cudaStream_t s) {
+  static int per_sm = 0;  // per template instance; the same on every B200
+  const uint32_t smem = std::max<uint32_t>(tc_smem_bytes(L) + 1024, 60u * 1024);
+  if (!per_sm) {
+    ZOGCU_CUDA(cudaFuncSetAttribute(k_gnn_infer_tc<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int n = 0;
+    ZOGCU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_gnn_infer_tc<L>, kTcThreads, smem));
+    if (n < 1 || (uint32_t)n * kTcCols > 512u) return fail(ZOGCU_ERR_INTERNAL, "tcgen05 kernel occupancy exceeds tensor memory");
+    per_sm = n;
+  }
+  const uint32_t ntiles = (V + kTcRows - 1) / kTcRows;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)sm_count() * per_sm));
+  k_gnn_infer_tc<L><<<grid, kTcThreads, smem, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M_next, y, err);
+  ZOGCU_CUDA(cudaGetLastError());
+  return ZOGCU_OK;
+}
+
 // Forward pass; with train the last hidden state is stored for the backward
 // pass.  err: device word the dense kernels raise when a tile load timed out.
 int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, bool train, cudaStream_t s) {
@@ -1349,18 +1648,30 @@ int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, bool train, cu
     const float* A0 = act.A[0].as<float>();
     const float* A1 = act.A[1].as<float>();
     const float* A2 = act.A[2].as<float>();
-    k_gnn_infer<0><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, act.M[1].as<__nv_bfloat16>(),
-                                                  nullptr);
-    ZOGCU_CUDA(cudaGetLastError());
-    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, act.M[1].as<__nv_bfloat16>(), act.A[1].as<float>(), act.Vp, ctr,
-                                            act.rows, s)));
-    k_gnn_infer<1><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, act.M[2].as<__nv_bfloat16>(),
-                                                  nullptr);
-    ZOGCU_CUDA(cudaGetLastError());
-    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, act.M[2].as<__nv_bfloat16>(), act.A[2].as<float>(), act.Vp, ctr,
-                                            act.rows, s)));
-    k_gnn_infer<2><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, nullptr, act.y.as<float>());
-    ZOGCU_CUDA(cudaGetLastError());
+    const bool tc = gnn_use_tc();
+    __nv_bfloat16* M1 = act.M[1].as<__nv_bfloat16>();
+    __nv_bfloat16* M2 = act.M[2].as<__nv_bfloat16>();
+    float* yv = act.y.as<float>();
+    if (tc) {
+      ZOGCU_TRY(launch_infer_tc<0>(F, A0, A1, A2, w, inv, V, M1, nullptr, err, s));
+    } else {
+      k_gnn_infer<0><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M1, nullptr);
+      ZOGCU_CUDA(cudaGetLastError());
+    }
+    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, M1, act.A[1].as<float>(), act.Vp, ctr, act.rows, s)));
+    if (tc) {
+      ZOGCU_TRY(launch_infer_tc<1>(F, A0, A1, A2, w, inv, V, M2, nullptr, err, s));
+    } else {
+      k_gnn_infer<1><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M2, nullptr);
+      ZOGCU_CUDA(cudaGetLastError());
+    }
+    ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, M2, act.A[2].as<float>(), act.Vp, ctr, act.rows, s)));
+    if (tc) {
+      ZOGCU_TRY(launch_infer_tc<2>(F, A0, A1, A2, w, inv, V, nullptr, yv, err, s));
+    } else {
+      k_gnn_infer<2><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, nullptr, yv);
+      ZOGCU_CUDA(cudaGetLastError());
+    }
     return ZOGCU_OK;
   }
   // training: hidden states stored (TMA tile loads and stores) for the backward pass
