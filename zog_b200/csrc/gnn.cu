@@ -1549,6 +1549,38 @@ struct GnnActs {
   }
 };
 
+// The in-CSR a forward pass runs over: the graph's own, or (inference) the
+// PageRank schedule's degree-ranked view -- nodes renumbered by out-degree,
+// descending, so the most gathered messages form a dense prefix that stays in
+// L2, and each row keeping its arcs in the original order, so every aggregate
+// equals the original-order one bit for bit.
+struct GView {
+  const uint32_t* off;   // in-CSR offsets (V + 1)
+  const uint32_t* col;   // sources of each row
+  const uint32_t* deg;   // out-degree (kDeletedDegree for deleted slots)
+  uint32_t V;
+  uint32_t E;
+  uint64_t n_live;
+};
+GView original_view(const Graph* g) {
+  return GView{g->in_off32.as<uint32_t>(), g->in_col.as<uint32_t>(), g->out_deg.as<uint32_t>(), g->V, (uint32_t)g->E,
+               g->n_live};
+}
+GView ranked_view(const Graph* g) {
+  const PrSchedule& P = g->pr;
+  return GView{P.off.as<uint32_t>(), P.col.as<uint32_t>(), P.deg.as<uint32_t>(), g->V, (uint32_t)g->E, g->n_live};
+}
+
+// x_out[v] = x_ranked[rank(v)]: a ranked-order vector back in node order
+__global__ void k_gnn_unrank(const double* __restrict__ xr, const uint32_t* __restrict__ rank, uint32_t V,
+                             double* __restrict__ x) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) x[v] = xr[rank[v]];
+}
+__global__ void k_gnn_unrank_f(const float* __restrict__ yr, const uint32_t* __restrict__ rank, uint32_t V,
+                               float* __restrict__ y) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) y[v] = yr[rank[v]];
+}
+
 // First row of every kChunk-arc chunk of the in-CSR (transpose = 0) or the
 // out-CSR (transpose = 1), into `rows` (allocated here).
 int chunk_rows(const Graph* g, bool transpose, DevBuf& rows, cudaStream_t s) {
@@ -1581,18 +1613,26 @@ int spmm(const Graph* g, bool transpose, const float* inv, const T* X, float* Z,
   return ZOGCU_OK;
 }
 
-// Z = agg(X) over the in-CSR for 16-byte messages (k_gnn_agg16); Z (zrows x
-// D, zrows >= V) is zeroed first.
+// First row of every kChunk-arc chunk of a view's in-CSR, into `rows`.
+int chunk_rows_view(const GView& gv, DevBuf& rows, cudaStream_t s) {
+  const uint64_t chunks = ((uint64_t)gv.E + kChunk - 1) / kChunk;
+  ZOGCU_TRY(rows.alloc(std::max<uint64_t>(chunks, 1) * 4, s));
+  if (chunks == 0) return ZOGCU_OK;
+  k_chunk_rows<<<g1d(chunks), 256, 0, s>>>(gv.off, gv.V, gv.E, rows.as<uint32_t>());
+  ZOGCU_CUDA(cudaGetLastError());
+  return ZOGCU_OK;
+}
+
+// Z = agg(X) over a view's in-CSR for 16-byte messages (k_gnn_agg16); Z
+// (zrows x D, zrows >= V) is zeroed first.
 template <class T, int D>
-int aggregate(const Graph* g, const T* X, float* Z, size_t zrows, uint32_t* ctr, const DevBuf& rows, cudaStream_t s) {
-  const uint32_t V = g->V;
-  const uint32_t E = (uint32_t)g->E;
+int aggregate(const GView& gv, const T* X, float* Z, size_t zrows, uint32_t* ctr, const DevBuf& rows, cudaStream_t s) {
   ZOGCU_CUDA(cudaMemsetAsync(Z, 0, zrows * D * 4, s));
-  if (E == 0) return ZOGCU_OK;
-  const uint64_t chunks = ((uint64_t)E + kChunk - 1) / kChunk;
+  if (gv.E == 0) return ZOGCU_OK;
+  const uint64_t chunks = ((uint64_t)gv.E + kChunk - 1) / kChunk;
   ZOGCU_CUDA(cudaMemsetAsync(ctr, 0, 4, s));
-  k_gnn_agg16<T, D><<<gwarp(chunks), kAggWarps * 32, 0, s>>>(g->in_off32.as<uint32_t>(), g->in_col.as<uint32_t>(), X, V,
-                                                             E, Z, ctr, rows.as<uint32_t>());
+  k_gnn_agg16<T, D><<<gwarp(chunks), kAggWarps * 32, 0, s>>>(gv.off, gv.col, X, gv.V, gv.E, Z, ctr,
+                                                             rows.as<uint32_t>());
   ZOGCU_CUDA(cudaGetLastError());
   return ZOGCU_OK;
 }
@@ -1626,20 +1666,17 @@ int launch_infer_tc(const float* F, const float* A0, const float* A1, const floa
 
 // Forward pass; with train the last hidden state is stored for the backward
 // pass.  err: device word the dense kernels raise when a tile load timed out.
-int gnn_forward(const zogcu_gnn* M, const Graph* g, GnnActs& act, bool train, cudaStream_t s) {
-  const uint32_t V = g->V;
-  if (!g->offsets32) return fail(ZOGCU_ERR_TOO_LARGE, "the warm-start network needs fewer than 2^32 arcs");
-  const uint32_t* ioff = g->in_off32.as<uint32_t>();
+int gnn_forward(const zogcu_gnn* M, const GView& g, GnnActs& act, bool train, cudaStream_t s) {
+  const uint32_t V = g.V;
   const __nv_bfloat16* w = M->pb.as<__nv_bfloat16>();
   uint32_t* ctr = act.ctr.as<uint32_t>();
   unsigned int* err = M->err.as<unsigned int>();
   const uint32_t ntiles = act.Vp / kTile;
-  k_gnn_features<<<g1d(V), 256, 0, s>>>(ioff, g->out_deg.as<uint32_t>(), V,
-                                        1.f / (float)std::max<uint64_t>(g->n_live, 1), act.F.as<float>(),
-                                        act.inv.as<float>(), act.M0.as<float>());
+  k_gnn_features<<<g1d(V), 256, 0, s>>>(g.off, g.deg, V, 1.f / (float)std::max<uint64_t>(g.n_live, 1),
+                                        act.F.as<float>(), act.inv.as<float>(), act.M0.as<float>());
   const float* inv = act.inv.as<float>();
   const float* F = act.F.as<float>();
-  ZOGCU_TRY(chunk_rows(g, false, act.rows, s));
+  ZOGCU_TRY(chunk_rows_view(g, act.rows, s));
   ZOGCU_TRY((aggregate<float, kF>(g, act.M0.as<float>(), act.A[0].as<float>(), V, ctr, act.rows, s)));
   if (!train) {
     // inference: the dense layers recompute the hidden states in registers
@@ -1712,16 +1749,16 @@ int check_dense_error(const zogcu_gnn* M, cudaStream_t s) {
 struct Softmax {
   DevBuf ymax, part, stot;
   unsigned grid = 1;
-  int run(const Graph* g, const float* y, double* x, cudaStream_t s) {
-    const uint32_t V = g->V;
+  int run(const GView& g, const float* y, double* x, cudaStream_t s) {
+    const uint32_t V = g.V;
     grid = g1d(V);
     ZOGCU_TRY(ymax.alloc(16, s));
     ZOGCU_TRY(stot.alloc(16, s));
     ZOGCU_TRY(part.alloc((size_t)grid * 8, s));
     // -inf: every live y is larger; the CAS loop below only raises it
     k_fill_f32<<<1, 32, 0, s>>>(ymax.as<float>(), 1, -INFINITY);
-    k_gnn_softmax_max<<<grid, 256, 0, s>>>(y, g->out_deg.as<uint32_t>(), V, ymax.as<float>());
-    k_gnn_softmax_exp<<<grid, 256, 0, s>>>(y, g->out_deg.as<uint32_t>(), V, ymax.as<float>(), x, part.as<double>());
+    k_gnn_softmax_max<<<grid, 256, 0, s>>>(y, g.deg, V, ymax.as<float>());
+    k_gnn_softmax_exp<<<grid, 256, 0, s>>>(y, g.deg, V, ymax.as<float>(), x, part.as<double>());
     k_gnn_softmax_scale<<<grid, 256, 0, s>>>(x, V, part.as<double>(), grid, stot.as<double>());
     ZOGCU_CUDA(cudaGetLastError());
     return ZOGCU_OK;
@@ -1744,7 +1781,7 @@ int gnn_backward(zogcu_gnn* M, const Graph* g, GnnActs& act, const double* d_pr,
     k_gnn_target<<<g1d(V), 256, 0, s>>>(d_pr, g->out_deg.as<uint32_t>(), V, (double)g->n_live, act.t.as<float>());
   } else {
     ZOGCU_TRY(xq.alloc(Vs * 8, s));
-    ZOGCU_TRY(sm.run(g, act.y.as<float>(), xq.as<double>(), s));
+    ZOGCU_TRY(sm.run(original_view(g), act.y.as<float>(), xq.as<double>(), s));
   }
   DevBuf dH, dX, dA, dQ;
   ZOGCU_TRY(dH.alloc(Vs * kH * 4, s));
@@ -1879,7 +1916,8 @@ int zogcu_gnn_loss_grad(zogcu_gnn* M, zogcu_graph* G, const double* target_pr, i
   WorkLease lease(&M->acts, sg.s);
   GnnActs act;
   ZOGCU_TRY(act.alloc(g->V, lease, true));
-  ZOGCU_TRY(gnn_forward(M, g, act, true, sg.s));
+  if (!g->offsets32) return fail(ZOGCU_ERR_TOO_LARGE, "the warm-start network needs fewer than 2^32 arcs");
+  ZOGCU_TRY(gnn_forward(M, original_view(g), act, true, sg.s));
   ZOGCU_TRY(gnn_backward(M, g, act, pr.as<double>(), loss_kind, sg.s));
   double l = 0.0;
   ZOGCU_CUDA(cudaMemcpyAsync(&l, M->loss.ptr, 8, cudaMemcpyDeviceToHost, sg.s));
@@ -1902,7 +1940,8 @@ int zogcu_gnn_train_step(zogcu_gnn* M, zogcu_graph* G, const double* d_target_pr
   WorkLease lease(&M->acts, sg.s);
   GnnActs act;
   ZOGCU_TRY(act.alloc(g->V, lease, true));
-  ZOGCU_TRY(gnn_forward(M, g, act, true, sg.s));
+  if (!g->offsets32) return fail(ZOGCU_ERR_TOO_LARGE, "the warm-start network needs fewer than 2^32 arcs");
+  ZOGCU_TRY(gnn_forward(M, original_view(g), act, true, sg.s));
   ZOGCU_TRY(gnn_backward(M, g, act, d_target_pr, loss_kind, sg.s));
   M->step += 1;
   const float b1 = 0.9f, b2 = 0.999f;
@@ -1922,25 +1961,40 @@ int zogcu_gnn_train_step(zogcu_gnn* M, zogcu_graph* G, const double* d_target_pr
 int zogcu_gnn_predict(const zogcu_gnn* M, zogcu_graph* G, double* x0, int device_out, void* stream,
                       float* raw_out) {
   if (!M || !G || !x0) return fail(ZOGCU_ERR_INVALID_ARGUMENT, "null argument");
-  const Graph* g = &G->g;
+  Graph* g = &G->g;
   const uint32_t V = g->V;
+  if (!g->offsets32) return fail(ZOGCU_ERR_TOO_LARGE, "the warm-start network needs fewer than 2^32 arcs");
   ZOGCU_CUDA(cudaSetDevice(M->device));
   StreamGuard sg;
   ZOGCU_TRY(sg.init(stream));
+  // inference runs in the degree-ranked view the PageRank solver uses (built
+  // once per graph and shared with it)
+  ZOGCU_TRY(ensure_pr_schedule(g, sg.s));
+  const GView gv = ranked_view(g);
   WorkLease lease(&M->acts, sg.s);
   GnnActs act;
   ZOGCU_TRY(act.alloc(V, lease, false));
-  ZOGCU_TRY(gnn_forward(M, g, act, false, sg.s));
-  DevBuf xd;
+  ZOGCU_TRY(gnn_forward(M, gv, act, false, sg.s));
+  const size_t Vs = std::max<uint32_t>(V, 1);
+  DevBuf xr, xd, yr;
+  ZOGCU_TRY(xr.alloc(Vs * 8, sg.s));
+  Softmax sm;
+  ZOGCU_TRY(sm.run(gv, act.y.as<float>(), xr.as<double>(), sg.s));
   double* xo = x0;
   if (!device_out) {
-    ZOGCU_TRY(xd.alloc((size_t)std::max<uint32_t>(V, 1) * 8, sg.s));
+    ZOGCU_TRY(xd.alloc(Vs * 8, sg.s));
     xo = xd.as<double>();
   }
-  Softmax sm;
-  ZOGCU_TRY(sm.run(g, act.y.as<float>(), xo, sg.s));
+  const uint32_t* rank = g->pr.rank.as<uint32_t>();
+  k_gnn_unrank<<<g1d(V), 256, 0, sg.s>>>(xr.as<double>(), rank, V, xo);
+  ZOGCU_CUDA(cudaGetLastError());
   if (!device_out) ZOGCU_CUDA(cudaMemcpyAsync(x0, xo, (size_t)V * 8, cudaMemcpyDeviceToHost, sg.s));
-  if (raw_out) ZOGCU_CUDA(cudaMemcpyAsync(raw_out, act.y.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, sg.s));
+  if (raw_out) {
+    ZOGCU_TRY(yr.alloc(Vs * 4, sg.s));
+    k_gnn_unrank_f<<<g1d(V), 256, 0, sg.s>>>(act.y.as<float>(), rank, V, yr.as<float>());
+    ZOGCU_CUDA(cudaGetLastError());
+    ZOGCU_CUDA(cudaMemcpyAsync(raw_out, yr.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost, sg.s));
+  }
   ZOGCU_TRY(check_dense_error(M, sg.s));
   return ZOGCU_OK;
 }
