@@ -110,10 +110,9 @@ __device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162flo
 // Transpose (training): out-CSR, the row sum scaled by inv(v) -- the gradient
 // of a message through its 1/outdeg factor.
 //
-// Work split: the arcs are cut into chunks of kChunk arcs that warps take from
-// a shared counter (so a hub row is shared by many warps and no warp holds a
-// fixed share of slow chunks); the first row of every chunk is precomputed
-// (k_chunk_rows).  A row that crosses a chunk boundary is added with atomics,
+// Work split: the arcs are cut into chunks of kChunk arcs dealt to warps in a
+// fixed interleaving (so a hub row is shared by many warps); the first row of
+// every chunk is precomputed (k_chunk_rows).  A row that crosses a chunk boundary is added with atomics,
 // a row inside one chunk is stored directly.  Each arc's row (D values of T)
 // is read 16 bytes per lane by LPA = D*sizeof(T)/16 lanes, and a chunk runs in
 // one of two modes:
@@ -186,11 +185,8 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
   const int lane = threadIdx.x & 31, sub = lane % LPA, grp = lane / LPA;
   const uint4* __restrict__ X16 = reinterpret_cast<const uint4*>(X);
   const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
-  for (;;) {
-    uint32_t c = 0;
-    if (lane == 0) c = atomicAdd(next_chunk, 1u);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= nchunks) break;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunks; c += nwarps) {
     const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
     for (uint32_t r0 = __ldg(first_row + c); r0 < V;) {
       // rows r0 .. r0+31: lane i holds the start and end of row r0 + i
@@ -276,8 +272,9 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
 
 // ---- forward aggregate with the messages staged in shared memory ---------------
 // Z(v) = sum over the in-arcs u -> v of X(u), every message X(u) 16 bytes (8
-// BF16 or 4 FP32 values).  Warps take kChunk-arc chunks from a counter, as in
-// k_gnn_spmm, but a chunk is done in two phases.  First every lane loads the
+// BF16 or 4 FP32 values).  Warps take kChunk-arc chunks in a fixed
+// interleaving (chunk c goes to warp c mod warps), and a chunk is done in two
+// phases.  First every lane loads the
 // messages of four of the chunk's arcs (coalesced index loads, 16-byte
 // message loads) and writes them to the warp's staging tile in shared memory;
 // the next chunk's loads are issued into registers before the current chunk
@@ -329,10 +326,14 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
   const uint64_t pol_idx = l2_evict_first(), pol_msg = l2_evict_last();
   const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
   uint4* st = s_stage[warp];
+  // chunks are dealt to warps statically (c, c + warps, ...): they all hold
+  // kChunk arcs, and a shared counter would serialise millions of atomics
+  const uint32_t nwarps = gridDim.x * kAggWarps;
+  uint32_t next = blockIdx.x * kAggWarps + warp;
   auto take = [&]() {
-    uint32_t c = 0;
-    if (lane == 0) c = atomicAdd(next_chunk, 1u);
-    return __shfl_sync(0xffffffffu, c, 0);
+    const uint32_t c = next;
+    next += nwarps;
+    return c;
   };
   // the messages of chunk c into registers (issued; used one chunk later)
   auto gather = [&](uint32_t c, uint4 (&v)[K]) {
@@ -1630,9 +1631,15 @@ int aggregate(const GView& gv, const T* X, float* Z, size_t zrows, uint32_t* ctr
   ZOGCU_CUDA(cudaMemsetAsync(Z, 0, zrows * D * 4, s));
   if (gv.E == 0) return ZOGCU_OK;
   const uint64_t chunks = ((uint64_t)gv.E + kChunk - 1) / kChunk;
-  ZOGCU_CUDA(cudaMemsetAsync(ctr, 0, 4, s));
-  k_gnn_agg16<T, D><<<gwarp(chunks), kAggWarps * 32, 0, s>>>(gv.off, gv.col, X, gv.V, gv.E, Z, ctr,
-                                                             rows.as<uint32_t>());
+  static int per_sm = 0;  // resident CTAs per SM (per template instance)
+  if (!per_sm) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_gnn_agg16<T, D>, kAggWarps * 32, 0);
+    per_sm = std::max(n, 1);
+  }
+  const uint64_t want = (chunks + kAggWarps - 1) / kAggWarps;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count() * per_sm));
+  k_gnn_agg16<T, D><<<grid, kAggWarps * 32, 0, s>>>(gv.off, gv.col, X, gv.V, gv.E, Z, ctr, rows.as<uint32_t>());
   ZOGCU_CUDA(cudaGetLastError());
   return ZOGCU_OK;
 }

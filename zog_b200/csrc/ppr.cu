@@ -192,11 +192,10 @@ __global__ void __launch_bounds__(kPprThreads) k_ppr_iter(PprArgs<S> A) {
     l1p[i] = 0.0;
     dgp[i] = 0.0;
   }
-  for (;;) {
-    uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(A.task_next, 1u);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= A.num_tasks) break;
+  // work items dealt to warps in a fixed interleaving: a shared counter costs
+  // one contended atomic per item
+  const uint32_t nwarps = gridDim.x * NW;
+  for (uint32_t t = blockIdx.x * NW + warp; t < A.num_tasks; t += nwarps) {
     const PrTask T = A.tasks[t];
     const uint32_t kind = T.b >> 30;
     double acc[PL];
