@@ -834,7 +834,7 @@ static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGra
 }
 
 // Batches of kBcBatch sources are dealt to kBcLanes "lanes" (batch b to lane
-// b % lanes, as many lanes as half the free device memory holds), each with
+// b % lanes, as many lanes as a quarter of the device memory holds), each with
 // its own workspace and score vector.  A call's batches
 // run as CUDA graphs of up to kBcGraphBatches batches: in a graph, every lane
 // is a chain of its batches -- reset, seed, a while loop of forward levels
@@ -855,19 +855,21 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
                            double* d_bc, cudaStream_t s, zogcu_stats* stats) {
   const uint32_t V = g->V;
   const uint64_t ns = sources.size();
+  PhaseTrace tr("betweenness", s);
   ZOGCU_TRY(ensure_heavy_lists(g, s));
   const uint64_t nbatches = (ns + kBcBatch - 1) / kBcBatch;
   int nlanes = kBcLanes;
   if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) nlanes = std::max(1, std::min(kBcMaxLanes, std::atoi(env)));
   nlanes = (int)std::min<uint64_t>((uint64_t)nlanes, std::max<uint64_t>(nbatches, 1));
   {
-    // a lane's workspace is about V * 1.9 KB (dist, sigma, q, the mask ring):
-    // keep all lanes within half of the free device memory
+    // a lane's workspace is about V * 1.8 KB (dist, sigma, q, the mask ring):
+    // keep all lanes within a quarter of the device memory (the free figure
+    // would not count what the stream-ordered pool keeps in reserve)
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
       const uint64_t per_lane = (uint64_t)std::max<uint32_t>(V, 1) * (4 + 8 + 8) * kBcBatch +
                                 (uint64_t)std::max<uint32_t>(V, 1) * 8 * (kMaxStoredLevels + 4);
-      const uint64_t fit = per_lane ? (uint64_t)(free_b / 2) / per_lane : (uint64_t)nlanes;
+      const uint64_t fit = per_lane ? (uint64_t)(total_b / 4) / per_lane : (uint64_t)nlanes;
       nlanes = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)nlanes, fit));
     }
   }
@@ -891,6 +893,7 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
   ZOGCU_CUDA(cudaMemsetAsync(depths.ptr, 0, std::max<uint64_t>(nbatches, 1) * 4, s));
   // the sources copy above reads a host vector the caller keeps alive
   ZOGCU_CUDA(cudaStreamSynchronize(s));
+  tr.mark("workspaces");
   const unsigned fgrid = (unsigned)bc_grid(bc_forward_kernel<OffT>, V);
   const unsigned bgrid = (unsigned)bc_grid(bc_backward_kernel<OffT>, V);
   const unsigned rgrid = std::max<unsigned>(1u, std::min<unsigned>((unsigned)(((uint64_t)V * kBcBatch + 255) / 256),
@@ -1025,11 +1028,14 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
         prev = n_add;
       }
     }
+    tr.mark("graph built");
     cudaGraphExec_t exec = nullptr;
     ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    tr.mark("graph instantiated");
     const cudaError_t le = cudaGraphLaunch(exec, s);
     cudaGraphExecDestroy(exec);  // an executable graph in flight is freed when it completes
     ZOGCU_CUDA(le);
+    tr.mark("graph ran");
     ++host_launches;
   }
   // depths, overflow flags and the kernels the graphs ran

@@ -415,11 +415,12 @@ __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// non-blocking test of the barrier's phase
-__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+// waits for the barrier's phase; the hardware may suspend the thread for a
+// while inside one try_wait, so the wake-up follows the phase change at once
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
@@ -430,16 +431,13 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
   return t;
 }
-// bounded wait: false when the phase did not complete within kWaitLimitNs
-// (polls, then polls with a short sleep)
+// bounded wait: false when the phase did not complete within kWaitLimitNs of
+// the global timer
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int i = 0; i < 64; ++i)
-    if (mbar_test_wait(bar, parity)) return true;
+  if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
-  while (!mbar_test_wait(bar, parity)) {
+  while (!mbar_try_wait(bar, parity))
     if (global_ns() - t0 > kWaitLimitNs) return false;
-    __nanosleep(64);
-  }
   return true;
 }
 __device__ __forceinline__ void tma_load_rows(void* dst, const CUtensorMap* map, int row, uint64_t* bar) {
@@ -1046,12 +1044,35 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_infer_tc(const float* __r
     phase ^= 1u;
     tc_fence_after();
   };
+  // a tile's per-row inputs (F, A_0 and the aggregates of layers 1..L), loaded
+  // one tile ahead so that their latency overlaps the current tile
+  struct RowIn {
+    float4 f, a0, a1[2], a2[2];
+  };
+  auto load_row = [&](uint32_t tile, RowIn& in) {
+    const uint32_t rr = tile * kTcRows + (uint32_t)tid;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool v = tile < ntiles && rr < V;
+    in.f = v ? __ldg(reinterpret_cast<const float4*>(F) + rr) : z;
+    in.a0 = v ? __ldg(reinterpret_cast<const float4*>(A0) + rr) : z;
+    in.a1[0] = in.a1[1] = in.a2[0] = in.a2[1] = z;
+    if (L >= 1 && v) {
+      in.a1[0] = __ldg(reinterpret_cast<const float4*>(A1 + (size_t)rr * kR));
+      in.a1[1] = __ldg(reinterpret_cast<const float4*>(A1 + (size_t)rr * kR + 4));
+    }
+    if (L >= 2 && v) {
+      in.a2[0] = __ldg(reinterpret_cast<const float4*>(A2 + (size_t)rr * kR));
+      in.a2[1] = __ldg(reinterpret_cast<const float4*>(A2 + (size_t)rr * kR + 4));
+    }
+  };
+  RowIn cur, nxt;
+  load_row(blockIdx.x, cur);
   for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
     const uint32_t r = tile * kTcRows + (uint32_t)tid;
     const bool valid = r < V;
+    load_row(tile + gridDim.x, nxt);
     {  // layer 0 operand: [F | A_0] as 8 BF16, then zeros (K = 16)
-      const float4 f = valid ? __ldg(reinterpret_cast<const float4*>(F) + r) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 a = valid ? __ldg(reinterpret_cast<const float4*>(A0) + r) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 f = cur.f, a = cur.a0;
       put_chunk(tAG, tid, 0, make_uint4(pack_bf16x2(f.x, f.y), pack_bf16x2(f.z, f.w), pack_bf16x2(a.x, a.y),
                                         pack_bf16x2(a.z, a.w)));
       put_chunk(tAG, tid, 1, make_uint4(0u, 0u, 0u, 0u));
@@ -1064,17 +1085,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_infer_tc(const float* __r
     tc_layer_out(tlane, s_bias, hp);
 #pragma unroll
     for (int l = 1; l <= L; ++l) {
-      const float* A = l == 1 ? A1 : A2;
       // the hidden tile and [A_l | 0]
       tc_fence_before();
       __syncthreads();  // every thread has read the accumulators and the previous operands are consumed
 #pragma unroll
       for (int c = 0; c < 8; ++c) put_chunk(tH, tid, c, make_uint4(hp[4 * c], hp[4 * c + 1], hp[4 * c + 2], hp[4 * c + 3]));
-      float4 x0 = make_float4(0.f, 0.f, 0.f, 0.f), x1 = x0;
-      if (valid) {
-        x0 = __ldg(reinterpret_cast<const float4*>(A + (size_t)r * kR));
-        x1 = __ldg(reinterpret_cast<const float4*>(A + (size_t)r * kR + 4));
-      }
+      const float4 x0 = l == 1 ? cur.a1[0] : cur.a2[0], x1 = l == 1 ? cur.a1[1] : cur.a2[1];
       put_chunk(tAG, tid, 0, make_uint4(pack_bf16x2(x0.x, x0.y), pack_bf16x2(x0.z, x0.w), pack_bf16x2(x1.x, x1.y),
                                         pack_bf16x2(x1.z, x1.w)));
       sync_operands();
@@ -1119,6 +1135,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_infer_tc(const float* __r
     tc_fence_before();
     __syncthreads();  // the tile's operands and accumulators are free for the next tile
     tc_fence_after();
+    cur = nxt;
   }
   if (!ok && tid == 0) atomicExch(err, 1u);
   tc_fence_before();

@@ -192,11 +192,17 @@ __global__ void __launch_bounds__(kPprThreads) k_ppr_iter(PprArgs<S> A) {
     l1p[i] = 0.0;
     dgp[i] = 0.0;
   }
-  // work items dealt to warps in a fixed interleaving: a shared counter costs
-  // one contended atomic per item
-  const uint32_t nwarps = gridDim.x * NW;
-  for (uint32_t t = blockIdx.x * NW + warp; t < A.num_tasks; t += nwarps) {
-    const PrTask T = A.tasks[t];
+  // work items from a shared counter, four per atomic (items differ in cost,
+  // so a fixed split leaves warps idle at the end of the iteration)
+  uint32_t t = 0, t_end = 0;
+  for (;;) {
+    if (t == t_end) {
+      if (lane == 0) t = atomicAdd(A.task_next, 4u);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      t_end = t + 4;
+    }
+    if (t >= A.num_tasks) break;
+    const PrTask T = A.tasks[t++];
     const uint32_t kind = T.b >> 30;
     double acc[PL];
     if (kind == kTaskChunk) {
