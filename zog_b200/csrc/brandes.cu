@@ -63,8 +63,12 @@ struct BcLoop {
   uint32_t blevel;
   uint32_t max_depth;
   uint32_t push;                  // direction of the current forward level: 1 push, 0 pull
-  uint32_t pad;
+  uint32_t active;                // the current batch holds sources (0: an empty slot of the graph)
+  uint32_t batch;                 // the lane's current batch: sources [64 * batch, 64 * batch + 64)
+  uint32_t nlanes;                // lanes of the call (the cursor's stride)
   unsigned long long next_arcs;   // out-arcs of the next frontier, summed during the level
+  unsigned long long full;        // mask of the batch's sources
+  unsigned long long ns;          // sources of the call
 };
 
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src) {
@@ -179,8 +183,10 @@ __global__ void __launch_bounds__(kBcThreads) bc_forward_kernel(
   // loop runs on the device) the level and its frontier masks come from the
   // batch's loop state and the mask ring `masks`.
   if (loop) {
-    if (*(volatile const uint32_t*)&loop->push) return;  // a push level (bc_push_kernel)
+    if (!*(volatile const uint32_t*)&loop->active) return;  // an empty batch slot
+    if (*(volatile const uint32_t*)&loop->push) return;     // a push level (bc_push_kernel)
     level = *(volatile const uint32_t*)&loop->level;
+    full = *(volatile const unsigned long long*)&loop->full;
     front_cur = masks + (size_t)(level % (kMaxStoredLevels + 1)) * V;
     front_nxt = masks + (size_t)((level + 1) % (kMaxStoredLevels + 1)) * V;
   }
@@ -605,10 +611,6 @@ static int bc_forward_batch(const Graph* g, const OffT* in_off, BcWork& W, uint6
   }
 }
 
-__global__ void k_bc_add(double* __restrict__ a, const double* __restrict__ b, uint32_t V) {
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
-    a[v] += b[v];
-}
 
 // ---- push levels (direction-optimising forward) ------------------------------
 // When the frontier's out-arcs are few against the graph's arcs (level 0, whose
@@ -653,7 +655,7 @@ __global__ void __launch_bounds__(kBcThreads) bc_push_kernel(uint32_t V, const O
                                                              unsigned long long* __restrict__ sigma,
                                                              unsigned int* __restrict__ flags, const BcLoop* __restrict__ loop,
                                                              unsigned long long* __restrict__ masks) {
-  if (!*(volatile const uint32_t*)&loop->push) return;
+  if (!*(volatile const uint32_t*)&loop->active || !*(volatile const uint32_t*)&loop->push) return;
   const uint32_t level = *(volatile const uint32_t*)&loop->level;
   const unsigned long long* __restrict__ cur = ring_slot(masks, level, V);
   unsigned long long* __restrict__ nxt = ring_slot(masks, level + 1, V);
@@ -704,7 +706,7 @@ __global__ void __launch_bounds__(kBcThreads) bc_push_finalize(uint32_t V, const
                                                                unsigned long long* __restrict__ visited,
                                                                uint32_t* __restrict__ dist, BcLoop* __restrict__ loop,
                                                                unsigned long long* __restrict__ masks) {
-  if (!*(volatile const uint32_t*)&loop->push) return;
+  if (!*(volatile const uint32_t*)&loop->active || !*(volatile const uint32_t*)&loop->push) return;
   const uint32_t level = *(volatile const uint32_t*)&loop->level;
   const unsigned long long* __restrict__ nxt = ring_slot(masks, level + 1, V);
   const int lane = threadIdx.x & 31;
@@ -733,7 +735,7 @@ __global__ void __launch_bounds__(kBcThreads) bc_push_finalize(uint32_t V, const
 // Before a push level: its next-frontier masks start at zero (a pull level
 // writes every vertex's mask itself).
 __global__ void bc_level_prep(uint32_t V, const BcLoop* __restrict__ loop, unsigned long long* __restrict__ masks) {
-  if (!*(volatile const uint32_t*)&loop->push) return;
+  if (!*(volatile const uint32_t*)&loop->active || !*(volatile const uint32_t*)&loop->push) return;
   const uint32_t level = *(volatile const uint32_t*)&loop->level;
   unsigned long long* nxt = ring_slot(masks, level + 1, V);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x)
@@ -746,6 +748,18 @@ __global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visi
                                unsigned long long* __restrict__ mask0, uint32_t* __restrict__ dist,
                                unsigned long long* __restrict__ sigma, unsigned int* __restrict__ flags,
                                BcLoop* __restrict__ loop, uint32_t push0) {
+  // the lane's batch comes from its cursor; a slot past the call's sources
+  // is empty and every kernel of it returns at once
+  const uint64_t first = (uint64_t)*(volatile const uint32_t*)&loop->batch * kBcBatch;
+  const uint64_t ns = *(volatile const unsigned long long*)&loop->ns;
+  if (first >= ns) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      loop->active = 0u;
+      loop->level = loop->depth = loop->blevel = 0u;
+      loop->push = 0u;
+    }
+    return;
+  }
   const uint64_t n = (uint64_t)V * kBcBatch;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     dist[i] = kUnreached;
@@ -758,6 +772,9 @@ __global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visi
   if (blockIdx.x == 0) {
     for (int i = threadIdx.x; i < kMaxStoredLevels; i += blockDim.x) flags[i] = 0u;
     if (threadIdx.x == 0) {
+      const uint64_t nb = ns - first < (uint64_t)kBcBatch ? ns - first : (uint64_t)kBcBatch;
+      loop->active = 1u;
+      loop->full = nb == 64 ? ~0ull : ((1ull << nb) - 1ull);
       loop->level = 0u;
       loop->depth = 0u;
       loop->blevel = 0u;
@@ -767,14 +784,34 @@ __global__ void bc_batch_reset(uint32_t V, unsigned long long* __restrict__ visi
   }
 }
 
+// The batch's sources into the level-0 frontier (sigma 1, dist 0).
+__global__ void bc_seed_loop(const uint32_t* __restrict__ sources, const BcLoop* __restrict__ loop,
+                             unsigned long long* visited, unsigned long long* front, unsigned long long* sigma,
+                             uint32_t* dist) {
+  if (!*(volatile const uint32_t*)&loop->active) return;
+  const uint64_t first = (uint64_t)loop->batch * kBcBatch;
+  const uint64_t b = threadIdx.x;
+  if (first + b < loop->ns && b < (uint64_t)kBcBatch) {
+    const uint64_t s = sources[first + b];
+    atomicOr(visited + s, 1ull << b);
+    atomicOr(front + s, 1ull << b);
+    sigma[s * kBcBatch + b] = 1ull;
+    dist[s * kBcBatch + b] = 0u;
+  }
+}
+
 // After forward level l: if it discovered nothing the BFS depth is l -- the
 // backward sweep starts there and the forward loop ends; otherwise the next
 // level follows (and the flag words of the previous 63 levels are cleared when
 // the ring of flag words wraps, as the host loop did).  One thread.
 __global__ void bc_fwd_advance(BcLoop* __restrict__ loop, unsigned int* __restrict__ flags,
-                               uint32_t* __restrict__ depth_slot, unsigned long long cond, unsigned long long arcs,
+                               uint32_t* __restrict__ depths, unsigned long long cond, unsigned long long arcs,
                                uint32_t push_ratio) {
   if (threadIdx.x != 0) return;
+  if (!loop->active) {  // an empty slot: no levels
+    cudaGraphSetConditional(cond, 0u);
+    return;
+  }
   const uint32_t l = loop->level;
   // the next level pushes when its frontier's out-arcs, times push_ratio,
   // stay below the graph's arcs (push_ratio 0: every level pulls)
@@ -785,7 +822,7 @@ __global__ void bc_fwd_advance(BcLoop* __restrict__ loop, unsigned int* __restri
     loop->depth = l;
     loop->blevel = l;
     if (l > loop->max_depth) loop->max_depth = l;
-    *depth_slot = l;
+    depths[loop->batch] = l;
     cudaGraphSetConditional(cond, 0u);
     return;
   }
@@ -795,17 +832,115 @@ __global__ void bc_fwd_advance(BcLoop* __restrict__ loop, unsigned int* __restri
   loop->level = nl;
 }
 
-// After backward level l: the next shallower level, or the end of the loop
-// once level 1 is done (a batch of depth 0 has no level to sweep).  One thread.
+// After backward level l: the next shallower level, or, once level 1 is done
+// (a batch of depth 0 or an empty slot has none), the end of the loop and the
+// lane's cursor moved to its next batch.  One thread.
 __global__ void bc_bwd_advance(BcLoop* __restrict__ loop, unsigned long long cond) {
   if (threadIdx.x != 0) return;
   const uint32_t b = loop->blevel;
   if (b <= 1u) {
     loop->blevel = 0u;
+    loop->batch += loop->nlanes;
     cudaGraphSetConditional(cond, 0u);
   } else {
     loop->blevel = b - 1u;
   }
+}
+
+// d_bc[v] = sum over the lanes of their scores, in lane order.
+__global__ void k_bc_sum_lanes(double* __restrict__ out, const double* __restrict__ lanes, int nlanes, uint32_t V) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int w = 0; w < nlanes; ++w) t += lanes[(size_t)w * V + v];
+    out[v] = t;
+  }
+}
+
+// Batches of kBcBatch sources are dealt to lanes (batch b to lane b % lanes;
+// up to kBcLanes, as many as a quarter of the device memory holds), each with
+// its own workspace and score vector.  The batches run as CUDA graphs: every
+// lane is a chain of K batch slots -- reset, seed, a while loop of forward
+// levels (each level's kernels followed by a one-thread kernel that ends the
+// loop when the level discovered nothing and otherwise chooses the next
+// level's direction), a while loop of backward levels from that depth up to
+// level 1 -- and the lanes' chains are independent branches, so one lane's
+// levels fill the SMs another's finishing level frees.  A slot takes its batch
+// from the lane's cursor in device memory (lane w starts at batch w and steps
+// by the lane count), so one instantiated graph serves any number of sources:
+// the call launches it until every batch has run, and a slot past the last
+// batch returns at once.  The workspaces and the instantiated graphs stay with
+// the graph resource for later calls (a concurrent call on the same graph
+// builds its own).  No host synchronisation happens between batches or levels.
+// The lanes' score vectors are added in lane order at the end, so the result
+// is deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count.
+constexpr int kBcMaxLanes = 8;
+constexpr int kBcLanes = 8;
+constexpr int kBcSlots = 8;  // batch slots per lane in one graph
+constexpr uint32_t kBcPushRatio = 16;
+
+struct BcExec {
+  int lanes = 0, slots = 0;
+  uint32_t push_ratio = 0;
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct BcCache {
+  std::mutex mu;
+  int lanes = 0;          // lanes whose workspaces exist
+  uint64_t src_cap = 0;   // sources the source array holds
+  uint64_t batch_cap = 0; // batches the depth array holds
+  DevArray visited[kBcMaxLanes], masks[kBcMaxLanes], mbuf_a[kBcMaxLanes], mbuf_b[kBcMaxLanes], sigma[kBcMaxLanes],
+      dist[kBcMaxLanes], q[kBcMaxLanes], flags[kBcMaxLanes], hpart[kBcMaxLanes], hgot[kBcMaxLanes],
+      harrive[kBcMaxLanes];
+  DevArray scores, loops, src, depths;
+  std::vector<BcExec> execs;
+  void drop_execs() {
+    for (auto& e : execs)
+      if (e.exec) cudaGraphExecDestroy(e.exec);
+    execs.clear();
+  }
+  ~BcCache() { drop_execs(); }
+};
+
+// Lane workspaces for `lanes` lanes of graph g, a source array of at least ns
+// and a depth array of at least nb batches; any reallocation drops the
+// instantiated graphs (they hold the old addresses).
+static int bc_cache_size(const Graph* g, BcCache& C, int lanes, uint64_t ns, uint64_t nb, cudaStream_t s) {
+  const size_t Vs = std::max<uint32_t>(g->V, 1);
+  const size_t nh = std::max<uint32_t>(std::max(g->n_heavy_in, g->n_heavy_out), 1);
+  if (lanes > C.lanes) {
+    C.drop_execs();
+    for (int w = C.lanes; w < lanes; ++w) {
+      ZOGCU_TRY(C.hpart[w].alloc(nh * kBcBatch * 8));
+      ZOGCU_TRY(C.hgot[w].alloc(nh * 8));
+      ZOGCU_TRY(C.harrive[w].alloc(nh * 4));
+      ZOGCU_CUDA(cudaMemsetAsync(C.harrive[w].ptr, 0, nh * 4, s));
+      ZOGCU_TRY(C.visited[w].alloc(Vs * 8));
+      ZOGCU_TRY(C.masks[w].alloc(Vs * 8 * (kMaxStoredLevels + 1)));
+      ZOGCU_TRY(C.sigma[w].alloc(Vs * 8 * kBcBatch));
+      ZOGCU_TRY(C.dist[w].alloc(Vs * 4 * kBcBatch));
+      ZOGCU_TRY(C.q[w].alloc(Vs * 8 * kBcBatch));
+      ZOGCU_TRY(C.mbuf_a[w].alloc(Vs * 8));
+      ZOGCU_TRY(C.mbuf_b[w].alloc(Vs * 8));
+      ZOGCU_TRY(C.flags[w].alloc(kFlagWords * 4));
+    }
+    ZOGCU_TRY(C.scores.alloc((size_t)lanes * Vs * 8));
+    ZOGCU_TRY(C.loops.alloc(sizeof(BcLoop) * kBcMaxLanes));
+    C.lanes = lanes;
+  }
+  if (ns > C.src_cap) {
+    C.drop_execs();
+    const uint64_t cap = std::max<uint64_t>((ns + 4095) / 4096 * 4096, 4096);
+    ZOGCU_TRY(C.src.alloc(cap * 4));
+    C.src_cap = cap;
+  }
+  if (nb > C.batch_cap) {
+    C.drop_execs();
+    const uint64_t cap = std::max<uint64_t>((nb + 1023) / 1024 * 1024, 1024);
+    ZOGCU_TRY(C.depths.alloc(cap * 4));
+    C.batch_cap = cap;
+  }
+  return ZOGCU_OK;
 }
 
 static int bc_kernel_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
@@ -833,115 +968,48 @@ static int bc_while_node(cudaGraph_t graph, cudaGraphNode_t* node, const cudaGra
   return ZOGCU_OK;
 }
 
-// Batches of kBcBatch sources are dealt to kBcLanes "lanes" (batch b to lane
-// b % lanes, as many lanes as a quarter of the device memory holds), each with
-// its own workspace and score vector.  A call's batches
-// run as CUDA graphs of up to kBcGraphBatches batches: in a graph, every lane
-// is a chain of its batches -- reset, seed, a while loop of forward levels
-// (each level kernel followed by a one-thread kernel that ends the loop when
-// the level discovered nothing), a while loop of backward levels from that
-// depth up to level 1 -- and the lanes' chains are independent branches, so
-// one lane's levels fill the SMs another's finishing level frees.  No host
-// synchronisation happens between batches or levels: the host launches each
-// graph once and reads the depths and flags at the end.  The lanes' score
-// vectors are added to d_bc at the end in lane order: a fixed order, so the
-// result is deterministic.  ZOGCU_BC_STREAMS=<k> sets the lane count.
-constexpr int kBcMaxLanes = 8;
-constexpr int kBcLanes = 8;
-constexpr uint64_t kBcGraphBatches = 64;
-constexpr uint32_t kBcPushRatio = 16;
+// The graph of `lanes` chains of `slots` batch slots over the cache's arrays.
 template <typename OffT>
-static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
-                           double* d_bc, cudaStream_t s, zogcu_stats* stats) {
-  const uint32_t V = g->V;
-  const uint64_t ns = sources.size();
-  PhaseTrace tr("betweenness", s);
-  ZOGCU_TRY(ensure_heavy_lists(g, s));
-  const uint64_t nbatches = (ns + kBcBatch - 1) / kBcBatch;
-  int nlanes = kBcLanes;
-  if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) nlanes = std::max(1, std::min(kBcMaxLanes, std::atoi(env)));
-  nlanes = (int)std::min<uint64_t>((uint64_t)nlanes, std::max<uint64_t>(nbatches, 1));
-  {
-    // a lane's workspace is about V * 1.8 KB (dist, sigma, q, the mask ring):
-    // keep all lanes within a quarter of the device memory (the free figure
-    // would not count what the stream-ordered pool keeps in reserve)
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-      const uint64_t per_lane = (uint64_t)std::max<uint32_t>(V, 1) * (4 + 8 + 8) * kBcBatch +
-                                (uint64_t)std::max<uint32_t>(V, 1) * 8 * (kMaxStoredLevels + 4);
-      const uint64_t fit = per_lane ? (uint64_t)(total_b / 4) / per_lane : (uint64_t)nlanes;
-      nlanes = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)nlanes, fit));
-    }
-  }
-  DevBuf bcx[kBcMaxLanes], loops, depths;
-  double* bcs[kBcMaxLanes];
-  bcs[0] = d_bc;
-  for (int w = 1; w < nlanes; ++w) {
-    ZOGCU_TRY(bcx[w].alloc((size_t)std::max<uint32_t>(V, 1) * 8, s));
-    ZOGCU_CUDA(cudaMemsetAsync(bcx[w].ptr, 0, (size_t)std::max<uint32_t>(V, 1) * 8, s));
-    bcs[w] = bcx[w].as<double>();
-  }
-  BcWork W[kBcMaxLanes];
-  for (int w = 0; w < nlanes; ++w) {
-    ZOGCU_TRY(W[w].alloc(g, ns, s, true));
-    ZOGCU_CUDA(cudaMemsetAsync(W[w].flags.ptr, 0, kFlagWords * 4, s));
-    if (ns) ZOGCU_CUDA(cudaMemcpyAsync(W[w].src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, s));
-  }
-  ZOGCU_TRY(loops.alloc(sizeof(BcLoop) * kBcMaxLanes, s));
-  ZOGCU_CUDA(cudaMemsetAsync(loops.ptr, 0, sizeof(BcLoop) * kBcMaxLanes, s));
-  ZOGCU_TRY(depths.alloc(std::max<uint64_t>(nbatches, 1) * 4, s));
-  ZOGCU_CUDA(cudaMemsetAsync(depths.ptr, 0, std::max<uint64_t>(nbatches, 1) * 4, s));
-  // the sources copy above reads a host vector the caller keeps alive
-  ZOGCU_CUDA(cudaStreamSynchronize(s));
-  tr.mark("workspaces");
+static int bc_build_exec(const Graph* g, const OffT* in_off, const OffT* out_off, BcCache& C, int lanes, int slots,
+                         uint32_t push_ratio, cudaGraphExec_t* out) {
+  uint32_t V = g->V;
   const unsigned fgrid = (unsigned)bc_grid(bc_forward_kernel<OffT>, V);
   const unsigned bgrid = (unsigned)bc_grid(bc_backward_kernel<OffT>, V);
+  const unsigned pgrid = (unsigned)bc_grid(bc_push_kernel<OffT>, V);
   const unsigned rgrid = std::max<unsigned>(1u, std::min<unsigned>((unsigned)(((uint64_t)V * kBcBatch + 255) / 256),
                                                                    (unsigned)sm_count() * 8));
-  const unsigned pgrid = (unsigned)bc_grid(bc_push_kernel<OffT>, V);
   const unsigned zgrid = std::max<unsigned>(1u, std::min<unsigned>((unsigned)(((uint64_t)V + 255) / 256),
                                                                    (unsigned)sm_count() * 8));
-  // direction choice: a level pushes when its frontier's out-arcs x ratio are
-  // below the graph's arcs; ZOGCU_BC_PUSH_RATIO=0 makes every level pull
-  uint32_t push_ratio = kBcPushRatio;
-  if (const char* env = std::getenv("ZOGCU_BC_PUSH_RATIO")) push_ratio = (uint32_t)std::max(0, std::atoi(env));
   uint32_t push0 = push_ratio ? 1u : 0u;
-  uint64_t host_launches = 0;
-  for (uint64_t b0 = 0; b0 < nbatches; b0 += kBcGraphBatches) {
-    const uint64_t b1 = std::min<uint64_t>(nbatches, b0 + kBcGraphBatches);
-    const bool final_chunk = b1 == nbatches;
-    cudaGraph_t graph = nullptr;
-    ZOGCU_CUDA(cudaGraphCreate(&graph, 0));
-    struct GraphGuard {
-      cudaGraph_t gr;
-      ~GraphGuard() { cudaGraphDestroy(gr); }
-    } guard{graph};
-    cudaGraphNode_t tail[kBcMaxLanes] = {};
-    for (uint64_t bi = b0; bi < b1; ++bi) {
-      const int w = (int)(bi % (uint64_t)nlanes);
-      BcWork& Wb = W[w];
-      const uint64_t first = bi * kBcBatch;
-      int nb = (int)std::min<uint64_t>(kBcBatch, ns - first);
-      unsigned long long full = nb == 64 ? ~0ull : ((1ull << nb) - 1);
-      BcLoop* loop = loops.as<BcLoop>() + w;
-      uint32_t* depth_slot = depths.as<uint32_t>() + bi;
-      unsigned long long* visited = Wb.visited.as<unsigned long long>();
-      unsigned long long* masks = Wb.masks.as<unsigned long long>();
-      unsigned long long* mask0 = Wb.level(0, V);
-      unsigned long long* sigma = Wb.sigma.as<unsigned long long>();
-      uint32_t* dist = Wb.dist.as<uint32_t>();
-      unsigned int* flags = Wb.flags.as<unsigned int>();
-      const uint32_t* src = Wb.src.as<uint32_t>() + first;
-      uint32_t Vv = V;
-      const cudaGraphNode_t* dep = tail[w] ? &tail[w] : nullptr;
-      const size_t ndep = tail[w] ? 1 : 0;
-      // reset and seed
+  cudaGraph_t graph = nullptr;
+  ZOGCU_CUDA(cudaGraphCreate(&graph, 0));
+  struct GraphGuard {
+    cudaGraph_t gr;
+    ~GraphGuard() { cudaGraphDestroy(gr); }
+  } guard{graph};
+  for (int w = 0; w < lanes; ++w) {
+    BcLoop* loop = C.loops.as<BcLoop>() + w;
+    const BcLoop* cloop = loop;
+    unsigned long long* visited = C.visited[w].as<unsigned long long>();
+    unsigned long long* masks = C.masks[w].as<unsigned long long>();
+    unsigned long long* mask0 = masks;  // level 0's slot of the ring
+    unsigned long long* sigma = C.sigma[w].as<unsigned long long>();
+    uint32_t* dist = C.dist[w].as<uint32_t>();
+    unsigned int* flags = C.flags[w].as<unsigned int>();
+    const uint32_t* src = C.src.as<uint32_t>();
+    uint32_t* depths = C.depths.as<uint32_t>();
+    double* scores = C.scores.as<double>() + (size_t)w * std::max<uint32_t>(V, 1);
+    cudaGraphNode_t tail = nullptr;
+    for (int k = 0; k < slots; ++k) {
+      const cudaGraphNode_t* dep = tail ? &tail : nullptr;
+      const size_t ndep = tail ? 1 : 0;
       cudaGraphNode_t n_reset, n_seed;
-      void* reset_args[] = {&Vv, &visited, &mask0, &dist, &sigma, &flags, &loop, &push0};
+      void* reset_args[] = {&V, &visited, &mask0, &dist, &sigma, &flags, &loop, &push0};
       ZOGCU_TRY(bc_kernel_node(graph, &n_reset, dep, ndep, (const void*)bc_batch_reset, rgrid, 256, reset_args));
-      void* seed_args[] = {(void*)&src, &nb, &visited, &mask0, &sigma, &dist};
-      ZOGCU_TRY(bc_kernel_node(graph, &n_seed, &n_reset, 1, (const void*)bc_seed_kernel, 1, 64, seed_args));
-      // forward levels
+      void* seed_args[] = {(void*)&src, (void*)&cloop, &visited, &mask0, &sigma, &dist};
+      ZOGCU_TRY(bc_kernel_node(graph, &n_seed, &n_reset, 1, (const void*)bc_seed_loop, 1, 64, seed_args));
+      // forward levels: prep (zero the next masks of a push level) -> pull ->
+      // push -> finalize -> advance
       cudaGraphNode_t n_fwd;
       cudaGraphConditionalHandle hf;
       cudaGraph_t fbody;
@@ -951,21 +1019,20 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
         const unsigned long long* fcur = nullptr;
         unsigned long long* fnxt = nullptr;
         uint32_t level0 = 0;
+        unsigned long long full = 0;
         const BcHeavy* heavy = g->heavy_in.as<BcHeavy>();
         uint32_t nheavy = g->n_heavy_in;
-        unsigned long long* hpart = Wb.hpart.as<unsigned long long>();
-        unsigned long long* hgot = Wb.hgot.as<unsigned long long>();
-        unsigned int* harrive = Wb.harrive.as<unsigned int>();
-        const BcLoop* cloop = loop;
-        void* fargs[] = {&Vv, (void*)&in_off, (void*)&col, (void*)&fcur, &fnxt, &visited, &sigma, &dist, &full,
+        unsigned long long* hpart = C.hpart[w].as<unsigned long long>();
+        unsigned long long* hgot = C.hgot[w].as<unsigned long long>();
+        unsigned int* harrive = C.harrive[w].as<unsigned int>();
+        void* fargs[] = {&V, (void*)&in_off, (void*)&col, (void*)&fcur, &fnxt, &visited, &sigma, &dist, &full,
                          &level0, &flags, (void*)&heavy, &nheavy, &hpart, &hgot, &harrive, (void*)&cloop, &masks,
                          (void*)&out_off};
         const uint32_t* ocol = g->out_col.as<uint32_t>();
         const unsigned long long* cvisited = visited;
-        void* pargs[] = {&Vv, (void*)&out_off, (void*)&ocol, (void*)&cvisited, &sigma, &flags, (void*)&cloop, &masks};
-        void* prep_args[] = {&Vv, (void*)&cloop, &masks};
-        void* fin_args[] = {&Vv, (void*)&out_off, &visited, &dist, &loop, &masks};
-        // prep (zero the next masks of a push level) -> pull -> push -> finalize -> advance
+        void* pargs[] = {&V, (void*)&out_off, (void*)&ocol, (void*)&cvisited, &sigma, &flags, (void*)&cloop, &masks};
+        void* prep_args[] = {&V, (void*)&cloop, &masks};
+        void* fin_args[] = {&V, (void*)&out_off, &visited, &dist, &loop, &masks};
         cudaGraphNode_t k0, k1, k2, k3, k4;
         ZOGCU_TRY(bc_kernel_node(fbody, &k0, nullptr, 0, (const void*)bc_level_prep, zgrid, 256, prep_args));
         ZOGCU_TRY(bc_kernel_node(fbody, &k1, &k0, 1, (const void*)bc_forward_kernel<OffT>, fgrid, kBcThreads, fargs));
@@ -973,10 +1040,11 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
         ZOGCU_TRY(bc_kernel_node(fbody, &k3, &k2, 1, (const void*)bc_push_finalize<OffT>, zgrid, kBcThreads, fin_args));
         unsigned long long cond = hf;
         unsigned long long arcs = g->E;
-        void* aargs[] = {&loop, &flags, &depth_slot, &cond, &arcs, &push_ratio};
+        uint32_t ratio = push_ratio;
+        void* aargs[] = {&loop, &flags, &depths, &cond, &arcs, &ratio};
         ZOGCU_TRY(bc_kernel_node(fbody, &k4, &k3, 1, (const void*)bc_fwd_advance, 1, 32, aargs));
       }
-      // backward levels
+      // backward levels, depth .. 1
       cudaGraphNode_t n_bwd;
       cudaGraphConditionalHandle hb;
       cudaGraph_t bbody;
@@ -986,21 +1054,19 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
         const unsigned long long* ml = nullptr;
         const unsigned long long* mn = nullptr;
         unsigned long long* mo = nullptr;
-        double* q = Wb.q.as<double>();
-        double* bcb = bcs[w];
+        double* q = C.q[w].as<double>();
         uint32_t level0 = 0;
         int last0 = 0;
         const BcHeavy* heavy = g->heavy_out.as<BcHeavy>();
         uint32_t nheavy = g->n_heavy_out;
-        double* hpart = Wb.hpart.as<double>();
-        unsigned int* harrive = Wb.harrive.as<unsigned int>();
-        const BcLoop* cloop = loop;
-        unsigned long long* ma = Wb.mbuf_a.as<unsigned long long>();
-        unsigned long long* mb = Wb.mbuf_b.as<unsigned long long>();
+        double* hpart = reinterpret_cast<double*>(C.hpart[w].ptr);
+        unsigned int* harrive = C.harrive[w].as<unsigned int>();
+        unsigned long long* ma = C.mbuf_a[w].as<unsigned long long>();
+        unsigned long long* mb = C.mbuf_b[w].as<unsigned long long>();
         const uint32_t* cdist = dist;
         const unsigned long long* csigma = sigma;
-        void* bargs[] = {&Vv, (void*)&out_off, (void*)&col, (void*)&ml, (void*)&mn, &mo, (void*)&cdist,
-                         (void*)&csigma, &q, &bcb, &level0, &last0, (void*)&heavy, &nheavy, &hpart, &harrive,
+        void* bargs[] = {&V, (void*)&out_off, (void*)&col, (void*)&ml, (void*)&mn, &mo, (void*)&cdist,
+                         (void*)&csigma, &q, &scores, &level0, &last0, (void*)&heavy, &nheavy, &hpart, &harrive,
                          (void*)&cloop, &masks, &ma, &mb};
         cudaGraphNode_t k1, k2;
         ZOGCU_TRY(bc_kernel_node(bbody, &k1, nullptr, 0, (const void*)bc_backward_kernel<OffT>, bgrid, kBcThreads, bargs));
@@ -1008,47 +1074,102 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
         void* aargs[] = {&loop, &cond};
         ZOGCU_TRY(bc_kernel_node(bbody, &k2, &k1, 1, (const void*)bc_bwd_advance, 1, 32, aargs));
       }
-      tail[w] = n_bwd;
+      tail = n_bwd;
     }
-    if (final_chunk) {
-      // the other lanes' scores into d_bc, in lane order
-      cudaGraphNode_t prev = tail[0];
-      for (int w = 1; w < nlanes; ++w) {
-        cudaGraphNode_t deps[2];
-        size_t nd = 0;
-        if (prev) deps[nd++] = prev;
-        if (tail[w]) deps[nd++] = tail[w];
-        double* a = d_bc;
-        double* b = bcs[w];
-        uint32_t Vv = V;
-        void* args[] = {&a, &b, &Vv};
-        cudaGraphNode_t n_add;
-        ZOGCU_TRY(bc_kernel_node(graph, &n_add, deps, nd, (const void*)k_bc_add,
-                                 std::max<unsigned>(1u, std::min<unsigned>((V + 255) / 256, 148u * 8)), 256, args));
-        prev = n_add;
-      }
+  }
+  ZOGCU_CUDA(cudaGraphInstantiate(out, graph, 0));
+  return ZOGCU_OK;
+}
+
+template <typename OffT>
+static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, const std::vector<uint32_t>& sources,
+                           double* d_bc, cudaStream_t s, zogcu_stats* stats) {
+  const uint32_t V = g->V;
+  const size_t Vs = std::max<uint32_t>(V, 1);
+  const uint64_t ns = sources.size();
+  PhaseTrace tr("betweenness", s);
+  ZOGCU_TRY(ensure_heavy_lists(g, s));
+  const uint64_t nbatches = (ns + kBcBatch - 1) / kBcBatch;
+  if (nbatches == 0) {
+    if (stats) stats->sources = 0;
+    return ZOGCU_OK;
+  }
+  int lanes_max = kBcLanes;
+  if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) lanes_max = std::max(1, std::min(kBcMaxLanes, std::atoi(env)));
+  {
+    // a lane's workspace is about V * 1.8 KB (dist, sigma, q, the mask ring):
+    // keep all lanes within a quarter of the device memory (the free figure
+    // would not count what the stream-ordered pool keeps in reserve)
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const uint64_t per_lane = (uint64_t)Vs * (4 + 8 + 8) * kBcBatch + (uint64_t)Vs * 8 * (kMaxStoredLevels + 4);
+      const uint64_t fit = per_lane ? (uint64_t)(total_b / 4) / per_lane : (uint64_t)lanes_max;
+      lanes_max = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)lanes_max, fit));
     }
-    tr.mark("graph built");
-    cudaGraphExec_t exec = nullptr;
-    ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-    tr.mark("graph instantiated");
-    const cudaError_t le = cudaGraphLaunch(exec, s);
-    cudaGraphExecDestroy(exec);  // an executable graph in flight is freed when it completes
-    ZOGCU_CUDA(le);
-    tr.mark("graph ran");
+  }
+  const int lanes = (int)std::min<uint64_t>((uint64_t)lanes_max, nbatches);
+  const int slots = (int)std::min<uint64_t>(kBcSlots, (nbatches + lanes - 1) / lanes);
+  uint32_t push_ratio = kBcPushRatio;
+  if (const char* env = std::getenv("ZOGCU_BC_PUSH_RATIO")) push_ratio = (uint32_t)std::max(0, std::atoi(env));
+  // the graph's cache, or a call-local one when another call holds it
+  if (!g->bc_cache) {
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (!g->bc_cache) g->bc_cache = std::make_shared<BcCache>();
+  }
+  std::shared_ptr<BcCache> shared = std::static_pointer_cast<BcCache>(g->bc_cache);
+  std::unique_lock<std::mutex> held(shared->mu, std::try_to_lock);
+  std::unique_ptr<BcCache> local;
+  BcCache* C = shared.get();
+  if (!held.owns_lock()) {
+    local.reset(new BcCache());
+    C = local.get();
+  }
+  ZOGCU_TRY(bc_cache_size(g, *C, lanes_max, ns, nbatches, s));
+  // the call's state: sources, zero scores and overflow words, lane cursors
+  ZOGCU_CUDA(cudaMemcpyAsync(C->src.ptr, sources.data(), ns * 4, cudaMemcpyHostToDevice, s));
+  ZOGCU_CUDA(cudaMemsetAsync(C->scores.ptr, 0, (size_t)lanes * Vs * 8, s));
+  for (int w = 0; w < lanes; ++w) ZOGCU_CUDA(cudaMemsetAsync(C->flags[w].ptr, 0, kFlagWords * 4, s));
+  std::vector<BcLoop> h_loops(lanes);
+  for (int w = 0; w < lanes; ++w) {
+    std::memset(&h_loops[w], 0, sizeof(BcLoop));
+    h_loops[w].batch = (uint32_t)w;
+    h_loops[w].nlanes = (uint32_t)lanes;
+    h_loops[w].ns = ns;
+  }
+  ZOGCU_CUDA(cudaMemcpyAsync(C->loops.ptr, h_loops.data(), sizeof(BcLoop) * lanes, cudaMemcpyHostToDevice, s));
+  // the sources and loop copies read host vectors that end with this call
+  ZOGCU_CUDA(cudaStreamSynchronize(s));
+  tr.mark("workspaces");
+  cudaGraphExec_t exec = nullptr;
+  for (const auto& e : C->execs)
+    if (e.lanes == lanes && e.slots == slots && e.push_ratio == push_ratio) exec = e.exec;
+  if (!exec) {
+    ZOGCU_TRY(bc_build_exec<OffT>(g, in_off, out_off, *C, lanes, slots, push_ratio, &exec));
+    C->execs.push_back(BcExec{lanes, slots, push_ratio, exec});
+    tr.mark("graph built and instantiated");
+  }
+  // one launch runs lanes x slots batches; the cursors carry on between launches
+  const uint64_t per_launch = (uint64_t)lanes * slots;
+  uint64_t host_launches = 0;
+  for (uint64_t done = 0; done < nbatches; done += per_launch) {
+    ZOGCU_CUDA(cudaGraphLaunch(exec, s));
     ++host_launches;
   }
+  k_bc_sum_lanes<<<std::max<unsigned>(1u, std::min<unsigned>((V + 255) / 256, 148u * 8)), 256, 0, s>>>(
+      d_bc, C->scores.as<double>(), lanes, V);
+  ZOGCU_CUDA(cudaGetLastError());
+  tr.mark("graphs ran");
   // depths, overflow flags and the kernels the graphs ran
-  std::vector<uint32_t> h_depth(std::max<uint64_t>(nbatches, 1));
-  ZOGCU_CUDA(cudaMemcpyAsync(h_depth.data(), depths.ptr, h_depth.size() * 4, cudaMemcpyDeviceToHost, s));
-  std::vector<unsigned int> h_ovf(nlanes);
-  for (int w = 0; w < nlanes; ++w)
-    ZOGCU_CUDA(cudaMemcpyAsync(&h_ovf[w], W[w].flags.as<unsigned int>() + kOverflowFlag, 4, cudaMemcpyDeviceToHost, s));
+  std::vector<uint32_t> h_depth(nbatches);
+  ZOGCU_CUDA(cudaMemcpyAsync(h_depth.data(), C->depths.ptr, nbatches * 4, cudaMemcpyDeviceToHost, s));
+  std::vector<unsigned int> h_ovf(lanes);
+  for (int w = 0; w < lanes; ++w)
+    ZOGCU_CUDA(cudaMemcpyAsync(&h_ovf[w], C->flags[w].as<unsigned int>() + kOverflowFlag, 4, cudaMemcpyDeviceToHost, s));
   ZOGCU_CUDA(cudaStreamSynchronize(s));
   bool overflow = false;
-  for (int w = 0; w < nlanes; ++w) overflow |= h_ovf[w] != 0u;
+  for (int w = 0; w < lanes; ++w) overflow |= h_ovf[w] != 0u;
   uint32_t max_depth = 0;
-  uint64_t launches = nlanes > 1 ? (uint64_t)(nlanes - 1) : 0;
+  uint64_t launches = 1;  // the lanes' sum
   for (uint64_t bi = 0; bi < nbatches; ++bi) {
     const uint32_t d = h_depth[bi];
     max_depth = std::max(max_depth, d);
@@ -1056,6 +1177,8 @@ static int run_betweenness(Graph* g, const OffT* in_off, const OffT* out_off, co
     // (level, advance) x max(depth, 1) backward
     launches += 2 + 5 * ((uint64_t)d + 1) + 2 * std::max<uint64_t>(d, 1);
   }
+  // the empty slots of the last launch: reset, seed, one forward and one backward pass
+  launches += (host_launches * per_launch - nbatches) * (2 + 5 + 2);
   if (stats) {
     stats->sources = ns;
     stats->max_depth = max_depth;

@@ -215,6 +215,9 @@ struct Graph {
   bool bc_built = false;
   uint32_t n_heavy_in = 0, n_heavy_out = 0;
   DevArray heavy_in, heavy_out;
+  // Brandes lanes' workspaces and instantiated CUDA graphs, kept for later
+  // calls on this graph (brandes.cu; released with the graph)
+  std::shared_ptr<void> bc_cache;
 };
 
 int ensure_device(int* dev);
