@@ -19,9 +19,17 @@
 // the aggregates that go through HBM are 32 bytes per node.
 //
 // Kernels (all hand-written):
-//   * k_gnn_spmm: the arc-chunked, load-balanced SpMM of the aggregates and of
-//     their transpose (training);
-//   * k_gnn_dense0 / k_gnn_dense_mid: the dense layers on the tensor cores
+//   * k_gnn_agg16: the forward aggregate (inference and training) -- arcs cut
+//     into 128-arc chunks dealt to warps in a fixed interleaving, each chunk's
+//     16-byte messages gathered into shared memory (index loads marked
+//     evict-first, message loads evict-last, the next chunk's gathers issued
+//     before this chunk's sums) and summed one row per lane;
+//   * k_gnn_spmm: the arc-chunked SpMM of the transpose (training);
+//   * k_gnn_infer: inference's dense layers with each warp's 16-node hidden
+//     tile kept in registers between the two products of a layer (mma.sync);
+//   * k_gnn_infer_tc: the same layers on tcgen05 with the accumulators in
+//     TMEM, 128-node tiles (opt-in: ZOGCU_GNN_TC=1);
+//   * k_gnn_dense0 / k_gnn_dense_mid: training's dense layers on the tensor cores
 //     (mma.m16n8k16, BF16 in, FP32 accumulate) fused with their epilogues --
 //     bias, ReLU, the BF16 hidden state, the next layer's message (a second
 //     product with U) or the head.  A warp owns 16-node tiles; the hidden
@@ -126,10 +134,11 @@ __device__ __forceinline__ float to_f32(__nv_bfloat16 x) { return __bfloat162flo
 // chunk are never visited).
 constexpr uint32_t kChunk = 128;
 
-__global__ void k_chunk_rows(const uint32_t* __restrict__ off, uint32_t V, uint32_t E, uint32_t* __restrict__ first_row) {
-  const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
+__global__ void k_chunk_rows(const uint32_t* __restrict__ off, uint32_t V, uint32_t E, uint32_t chunk,
+                             uint32_t* __restrict__ first_row) {
+  const uint32_t nchunks = (uint32_t)(((uint64_t)E + chunk - 1) / chunk);
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nchunks; c += gridDim.x * blockDim.x) {
-    const uint32_t cs = c * kChunk;
+    const uint32_t cs = c * chunk;
     uint32_t lo = 0, hi = V;  // the last r < V with off[r] <= cs (off[V] = E > cs)
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
@@ -272,7 +281,7 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
 
 // ---- forward aggregate with the messages staged in shared memory ---------------
 // Z(v) = sum over the in-arcs u -> v of X(u), every message X(u) 16 bytes (8
-// BF16 or 4 FP32 values).  Warps take kChunk-arc chunks in a fixed
+// BF16 or 4 FP32 values).  Warps take kAggChunk-arc chunks in a fixed
 // interleaving (chunk c goes to warp c mod warps), and a chunk is done in two
 // phases.  First every lane loads the
 // messages of four of the chunk's arcs (coalesced index loads, 16-byte
@@ -285,6 +294,7 @@ __global__ void __launch_bounds__(256) k_gnn_spmm(const uint32_t* __restrict__ o
 // an L2 evict-first policy and skip L1; the messages, which other arcs gather
 // again, are loaded with an evict-last policy.  Sums are FP32; Z starts at zero.
 constexpr int kAggWarps = 8;
+constexpr uint32_t kAggChunk = 128;  // arcs per aggregation chunk: four messages per lane
 
 __device__ __forceinline__ uint64_t l2_evict_first() {
   uint64_t p;
@@ -318,16 +328,16 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
                                                               float* __restrict__ Z, uint32_t* __restrict__ next_chunk,
                                                               const uint32_t* __restrict__ first_row) {
   constexpr int PER = 16 / (int)sizeof(T);
-  constexpr int K = (int)kChunk / 32;  // messages per lane and chunk
+  constexpr int K = (int)kAggChunk / 32;  // messages per lane and chunk
   static_assert(PER == D, "one 16-byte message per arc");
-  __shared__ __align__(16) uint4 s_stage[kAggWarps][kChunk];
+  __shared__ __align__(16) uint4 s_stage[kAggWarps][kAggChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint4* __restrict__ X16 = reinterpret_cast<const uint4*>(X);
   const uint64_t pol_idx = l2_evict_first(), pol_msg = l2_evict_last();
-  const uint32_t nchunks = (uint32_t)(((uint64_t)E + kChunk - 1) / kChunk);
+  const uint32_t nchunks = (uint32_t)(((uint64_t)E + kAggChunk - 1) / kAggChunk);
   uint4* st = s_stage[warp];
   // chunks are dealt to warps statically (c, c + warps, ...): they all hold
-  // kChunk arcs, and a shared counter would serialise millions of atomics
+  // kAggChunk arcs, and a shared counter would serialise millions of atomics
   const uint32_t nwarps = gridDim.x * kAggWarps;
   uint32_t next = blockIdx.x * kAggWarps + warp;
   auto take = [&]() {
@@ -337,7 +347,7 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
   };
   // the messages of chunk c into registers (issued; used one chunk later)
   auto gather = [&](uint32_t c, uint4 (&v)[K]) {
-    const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
+    const uint32_t cs = c * kAggChunk, ce = min(cs + kAggChunk, E);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const uint32_t j = cs + lane + 32 * k;
@@ -353,7 +363,7 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
     __syncwarp();
     const uint32_t cn = take();
     if (cn < nchunks) gather(cn, v);  // in flight while chunk c is summed
-    const uint32_t cs = c * kChunk, ce = min(cs + kChunk, E);
+    const uint32_t cs = c * kAggChunk, ce = min(cs + kAggChunk, E);
     for (uint32_t r0 = __ldg(first_row + c); r0 < V;) {
       const uint32_t ri = r0 + lane;
       const uint32_t rb = ri < V ? __ldg(off + ri) : E;
@@ -1607,7 +1617,7 @@ int chunk_rows(const Graph* g, bool transpose, DevBuf& rows, cudaStream_t s) {
   ZOGCU_TRY(rows.alloc(std::max<uint64_t>(chunks, 1) * 4, s));
   if (chunks == 0) return ZOGCU_OK;
   const uint32_t* off = (transpose ? g->out_off32 : g->in_off32).as<uint32_t>();
-  k_chunk_rows<<<g1d(chunks), 256, 0, s>>>(off, g->V, E, rows.as<uint32_t>());
+  k_chunk_rows<<<g1d(chunks), 256, 0, s>>>(off, g->V, E, kChunk, rows.as<uint32_t>());
   ZOGCU_CUDA(cudaGetLastError());
   return ZOGCU_OK;
 }
@@ -1631,12 +1641,12 @@ int spmm(const Graph* g, bool transpose, const float* inv, const T* X, float* Z,
   return ZOGCU_OK;
 }
 
-// First row of every kChunk-arc chunk of a view's in-CSR, into `rows`.
+// First row of every kAggChunk-arc chunk of a view's in-CSR, into `rows`.
 int chunk_rows_view(const GView& gv, DevBuf& rows, cudaStream_t s) {
-  const uint64_t chunks = ((uint64_t)gv.E + kChunk - 1) / kChunk;
+  const uint64_t chunks = ((uint64_t)gv.E + kAggChunk - 1) / kAggChunk;
   ZOGCU_TRY(rows.alloc(std::max<uint64_t>(chunks, 1) * 4, s));
   if (chunks == 0) return ZOGCU_OK;
-  k_chunk_rows<<<g1d(chunks), 256, 0, s>>>(gv.off, gv.V, gv.E, rows.as<uint32_t>());
+  k_chunk_rows<<<g1d(chunks), 256, 0, s>>>(gv.off, gv.V, gv.E, kAggChunk, rows.as<uint32_t>());
   ZOGCU_CUDA(cudaGetLastError());
   return ZOGCU_OK;
 }
@@ -1647,7 +1657,7 @@ template <class T, int D>
 int aggregate(const GView& gv, const T* X, float* Z, size_t zrows, uint32_t* ctr, const DevBuf& rows, cudaStream_t s) {
   ZOGCU_CUDA(cudaMemsetAsync(Z, 0, zrows * D * 4, s));
   if (gv.E == 0) return ZOGCU_OK;
-  const uint64_t chunks = ((uint64_t)gv.E + kChunk - 1) / kChunk;
+  const uint64_t chunks = ((uint64_t)gv.E + kAggChunk - 1) / kAggChunk;
   static int per_sm = 0;  // resident CTAs per SM (per template instance)
   if (!per_sm) {
     int n = 0;
