@@ -96,6 +96,39 @@ def test_in_csr_order_matches_reference(native, oracle):
         G.destroy()
 
 
+@pytest.mark.parametrize("sources_sorted", [True, False])
+def test_large_host_arc_lists_build_the_reference_csr(native, oracle, sources_sorted):
+    """Host arc lists of at least 2^22 arcs have their destinations sorted on
+    the device while the sources are still being copied; when the sources
+    are non-decreasing the in-CSR is then a gather of them, otherwise the
+    plain two-sort build runs.  Both against the oracle's CSRs, with
+    self-loops and duplicate arcs, from pageable arrays large enough for the
+    pipelined bounce copies (33.5 MB each)."""
+    rng = np.random.default_rng(2023)
+    V, E = 1 << 16, (1 << 23) + 7
+    f = rng.integers(0, V, E, dtype=np.uint32)
+    t = rng.integers(0, V, E, dtype=np.uint32)
+    t[:1000] = f[:1000]  # self-loops
+    f[1000:3000] = f[1000]  # a hub with duplicate arcs
+    t[1000:3000] = t[1000:1100].repeat(20)
+    if sources_sorted:
+        order = np.argsort(f, kind="stable")
+        f, t = np.ascontiguousarray(f[order]), np.ascontiguousarray(t[order])
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        in_off, in_col, out_off, out_col, deg = G.export_csr()
+        off_r, col_r, deg_r = oracle.in_csr_from_edges(V, f, t)
+        assert np.array_equal(in_off, off_r) and np.array_equal(in_col, col_r) and np.array_equal(deg, deg_r)
+        A = oracle.ArrayGraph(V, f, t)
+        try:
+            so, sc = A.successor_csr()
+        finally:
+            A.close()
+        assert np.array_equal(out_off, so) and np.array_equal(out_col, sc)
+    finally:
+        G.destroy()
+
+
 @pytest.mark.parametrize("max_iter", [0, 1, 2, 7, 60])
 def test_iteration_prefix_exact(native, oracle, max_iter):
     """Stopping after k iterations returns the k-th iterate (the swap happens

@@ -228,10 +228,15 @@ int ensure_device(int* dev);
 // d_w (may be null) holds one weight per edge in the same order as d_src / d_dst.
 // src_sorted: 1 = d_src is non-decreasing (the out-CSR is then placed by one
 // scatter instead of a sort), 0 = it is not, -1 = unknown (checked here).
+// presorted_dst / presorted_perm (both or neither; used only when d_src is
+// non-decreasing): the destinations sorted stably and the arc index of each
+// sorted position, so the in-CSR is a gather instead of a second sort.
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src,
                                   const uint32_t* d_dst, uint64_t E, bool reverse_within_source,
                                   const uint8_t* h_node_deleted, cudaStream_t stream,
-                                  const double* d_w = nullptr, int src_sorted = -1);
+                                  const double* d_w = nullptr, int src_sorted = -1,
+                                  const uint32_t* presorted_dst = nullptr,
+                                  const uint32_t* presorted_perm = nullptr);
 
 // PageRank schedule (pagerank.cu): the degree-ranked view, and the work-item
 // list of row blocks of at most nnz (128 or 256) arcs.

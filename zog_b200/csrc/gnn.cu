@@ -176,8 +176,12 @@ __device__ __forceinline__ void put_row(float* __restrict__ Z, uint32_t r, int s
 #pragma unroll
     for (int i = 0; i < PER; i += 4) *reinterpret_cast<float4*>(z + i) = make_float4(acc[i], acc[i + 1], acc[i + 2], acc[i + 3]);
   } else {
+    // 16-byte vector reductions (one L2 atomic per four values, z is 16-byte aligned)
 #pragma unroll
-    for (int i = 0; i < PER; ++i) atomicAdd(z + i, acc[i]);
+    for (int i = 0; i < PER; i += 4)
+      asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(z + i), "f"(acc[i]), "f"(acc[i + 1]),
+                   "f"(acc[i + 2]), "f"(acc[i + 3])
+                   : "memory");
   }
 }
 
@@ -354,20 +358,40 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
       v[k] = j < ce ? ld_message(X16 + ld_index(col + j, pol_idx), pol_msg) : make_uint4(0u, 0u, 0u, 0u);
     }
   };
+  // the arc range of row r0 + lane (rows past the end read as empty at E)
+  auto row_range = [&](uint32_t r0, uint32_t& rb, uint32_t& re) {
+    const uint32_t ri = r0 + lane;
+    rb = ri < V ? __ldg(off + ri) : E;
+    re = ri < V ? __ldg(off + ri + 1) : E;
+  };
+  // Chunk c's messages, first row and first 32 row ranges are loaded one
+  // chunk ahead, and the first row of the chunk after that two ahead, so a
+  // chunk starts summing without waiting on a dependent load chain.
   uint4 v[K];
-  uint32_t c = take();
-  if (c < nchunks) gather(c, v);
+  uint32_t c = take(), r0c = 0, rbc = E, rec = E;
+  if (c < nchunks) {
+    gather(c, v);
+    r0c = __ldg(first_row + c);
+    row_range(r0c, rbc, rec);
+  }
+  uint32_t cn = take();
+  uint32_t r0n = cn < nchunks ? __ldg(first_row + cn) : 0u;
   while (c < nchunks) {
 #pragma unroll
     for (int k = 0; k < K; ++k) st[lane + 32 * k] = v[k];
     __syncwarp();
-    const uint32_t cn = take();
-    if (cn < nchunks) gather(cn, v);  // in flight while chunk c is summed
+    // in flight while chunk c is summed
+    uint32_t rbn = E, ren = E;
+    if (cn < nchunks) {
+      gather(cn, v);
+      row_range(r0n, rbn, ren);
+    }
+    const uint32_t cnn = take();
+    const uint32_t r0nn = cnn < nchunks ? __ldg(first_row + cnn) : 0u;
     const uint32_t cs = c * kAggChunk, ce = min(cs + kAggChunk, E);
-    for (uint32_t r0 = __ldg(first_row + c); r0 < V;) {
+    uint32_t rb = rbc, re = rec;
+    for (uint32_t r0 = r0c; r0 < V;) {
       const uint32_t ri = r0 + lane;
-      const uint32_t rb = ri < V ? __ldg(off + ri) : E;
-      const uint32_t re = ri < V ? __ldg(off + ri + 1) : E;
       const bool in = rb < ce;  // row r0 + lane starts inside the chunk (lane 0 always)
       const int nrows = __popc(__ballot_sync(0xffffffffu, in));
       const uint32_t b0 = max(rb, cs), e0 = in ? min(re, ce) : b0;
@@ -397,9 +421,15 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
       }
       if (nrows < 32) break;  // the chunk ended inside these rows
       r0 += 32;
+      row_range(r0, rb, re);
     }
     __syncwarp();  // every lane is done with the staging tile before it is refilled
     c = cn;
+    r0c = r0n;
+    rbc = rbn;
+    rec = ren;
+    cn = cnn;
+    r0n = r0nn;
   }
 }
 

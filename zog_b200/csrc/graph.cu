@@ -299,6 +299,18 @@ __global__ void k_validate(const uint32_t* __restrict__ a, const uint32_t* __res
   if (__any_sync(0xffffffffu, unsorted) && (threadIdx.x & 31) == 0) atomicOr(flags + 1, 1u);
 }
 
+// out[j] = a[idx[j]]
+__global__ void k_gather_u32(const uint32_t* __restrict__ a, const uint32_t* __restrict__ idx, uint64_t n,
+                             uint32_t* __restrict__ out) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    out[j] = __ldg(a + __ldg(idx + j));
+}
+
+__global__ void k_iota_u32(uint32_t* __restrict__ out, uint64_t n) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
+    out[j] = (uint32_t)j;
+}
+
 // Sorted-input out-CSR: input arc j of source r = src[j] goes to position
 // off[r] + off[r+1] - 1 - j when each row is reversed (ArrayGraph successor
 // order is the reverse of insertion order), or stays at j otherwise.
@@ -378,7 +390,8 @@ static int counts_to_offsets(unsigned long long* d_cnt, uint64_t* d_off, uint32_
 
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, const uint32_t* d_dst,
                                   uint64_t E, bool reverse_within_source, const uint8_t* h_node_deleted,
-                                  cudaStream_t s, const double* d_w, int src_sorted) {
+                                  cudaStream_t s, const double* d_w, int src_sorted,
+                                  const uint32_t* presorted_dst, const uint32_t* presorted_perm) {
   ZOGCU_TRY(ensure_device(&g->device));
   g->V = V;
   g->E = E;
@@ -430,7 +443,7 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
     }
     DevBuf ks, vs, ks2, t;
     size_t tmp = 0;
-    ZOGCU_TRY(ks.alloc(E * 4, s));
+    if (!(sorted && presorted_dst && presorted_perm)) ZOGCU_TRY(ks.alloc(E * 4, s));
     const uint32_t* keys_out;  // the source of every out-CSR arc (rows ascending)
     if (sorted) {
       // Sources already non-decreasing: the out offsets come straight from
@@ -490,6 +503,15 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
       keys_out = ks2.as<uint32_t>();
     }
     tr.mark(sorted ? "out-CSR (sorted sources)" : "out-CSR (radix sort)");
+    const uint32_t* in_keys = ks.as<uint32_t>();  // the destination of every in-CSR arc
+    if (sorted && presorted_dst && presorted_perm) {
+      // (2') sources non-decreasing: the stable order of the arcs by destination
+      // already lists each row's sources ascending, so the in-CSR is a gather
+      k_gather_u32<<<grid_for(E), 256, 0, s>>>(d_src, presorted_perm, E, g->in_col.as<uint32_t>());
+      ZOGCU_CUDA(cudaGetLastError());
+      in_keys = presorted_dst;
+      tr.mark("in-CSR gather (presorted destinations)");
+    } else {
     // (2) stable sort of (dst, src) pairs by dst: sources stay ascending
     size_t tmp2 = 0;
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
@@ -501,8 +523,9 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
     ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
                                                keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
     tr.mark("in-CSR radix sort");
+    }
     ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
-    k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks.as<uint32_t>(), E, cnt.as<unsigned long long>());
+    k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(in_keys, E, cnt.as<unsigned long long>());
     ZOGCU_CUDA(cudaGetLastError());
     ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->in_off64.as<uint64_t>(), V, s));
   } else {
@@ -603,11 +626,49 @@ static void rmat_thresholds(double a, double b, double c, uint64_t* ta, uint64_t
   *tabc = (uint64_t)std::floor((a + b + c) * two53);
 }
 
+// Arc lists from host memory of at least this many arcs have their
+// destinations sorted while the sources are still being copied.
+constexpr uint64_t kPresortMinArcs = 1ull << 22;
+
+struct EventGuard {
+  cudaEvent_t e = nullptr;
+  int init() {
+    ZOGCU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return ZOGCU_OK;
+  }
+  ~EventGuard() {
+    if (e) cudaEventDestroy(e);
+  }
+};
+
+// The stable sort of the arcs by destination on stream s: dst_sorted[k] is the
+// k-th smallest destination and perm[k] the index of its arc (ties keep arc
+// order).  Only the bits of node ids below V are sorted; endpoints are
+// validated before the result is used.
+static int presort_destinations(const uint32_t* d_dst, uint64_t E, uint32_t V, DevBuf& dst_sorted, DevBuf& perm,
+                                cudaStream_t s) {
+  DevBuf iota, tmp;
+  ZOGCU_TRY(iota.alloc(E * 4, s));
+  ZOGCU_TRY(dst_sorted.alloc(E * 4, s));
+  ZOGCU_TRY(perm.alloc(E * 4, s));
+  k_iota_u32<<<grid_for(E), 256, 0, s>>>(iota.as<uint32_t>(), E);
+  ZOGCU_CUDA(cudaGetLastError());
+  const int bits = bits_for(V);
+  size_t bytes = 0;
+  ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, d_dst, dst_sorted.as<uint32_t>(), iota.as<uint32_t>(),
+                                             perm.as<uint32_t>(), (int64_t)E, 0, bits, s));
+  ZOGCU_TRY(tmp.alloc(bytes, s));
+  ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, bytes, d_dst, dst_sorted.as<uint32_t>(), iota.as<uint32_t>(),
+                                             perm.as<uint32_t>(), (int64_t)E, 0, bits, s));
+  return ZOGCU_OK;
+}
+
 // Validates device edge arrays (addEdge's hasNode check, array_graph.zig:88-89)
 // and builds the graph on stream s.
 static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_from, const uint32_t* d_to,
                                        uint64_t num_edges, cudaStream_t s, zogcu_graph** out,
-                                       const double* d_w = nullptr) {
+                                       const double* d_w = nullptr, const uint32_t* presorted_dst = nullptr,
+                                       const uint32_t* presorted_perm = nullptr) {
   int sorted = 0;
   if (num_edges) {
     DevBuf fl;
@@ -624,7 +685,7 @@ static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_fr
   std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
   if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
   ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s, d_w,
-                                          sorted));
+                                          sorted, presorted_dst, presorted_perm));
   *out = G.release();
   return ZOGCU_OK;
 }
@@ -697,18 +758,37 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
   DevBuf df, dt;
   ZOGCU_TRY(df.alloc(num_edges * 4, sg.s));
   ZOGCU_TRY(dt.alloc(num_edges * 4, sg.s));
-  DevBuf dw;
-  if (num_edges) {
+  DevBuf dw, dsorted, perm;
+  if (num_edges >= kPresortMinArcs && !weight) {
+    // The destinations go first, and their stable sort (with the arc indices)
+    // runs on sg.s while the sources cross PCIe on a second stream.  When
+    // the sources turn out non-decreasing, the in-CSR is then a gather.
+    ZOGCU_TRY(copy_host(dt.ptr, const_cast<uint32_t*>(to), num_edges * 4, true, sg.s));
+    StreamGuard up;
+    ZOGCU_TRY(up.init(nullptr));
+    EventGuard to_done, from_done;
+    ZOGCU_TRY(to_done.init());
+    ZOGCU_TRY(from_done.init());
+    ZOGCU_CUDA(cudaEventRecord(to_done.e, sg.s));
+    ZOGCU_TRY(presort_destinations(dt.as<uint32_t>(), num_edges, node_count, dsorted, perm, sg.s));
+    ZOGCU_CUDA(cudaStreamWaitEvent(up.s, to_done.e, 0));  // one array on the bus at a time
+    ZOGCU_TRY(copy_host(df.ptr, const_cast<uint32_t*>(from), num_edges * 4, true, up.s));
+    ZOGCU_CUDA(cudaEventRecord(from_done.e, up.s));
+    ZOGCU_CUDA(cudaStreamWaitEvent(sg.s, from_done.e, 0));
+    tr.mark("arcs to the device, destinations sorted meanwhile");
+  } else if (num_edges) {
     ZOGCU_TRY(copy_host(df.ptr, const_cast<uint32_t*>(from), num_edges * 4, true, sg.s));
     ZOGCU_TRY(copy_host(dt.ptr, const_cast<uint32_t*>(to), num_edges * 4, true, sg.s));
     if (weight) {
       ZOGCU_TRY(dw.alloc(num_edges * 8, sg.s));
       ZOGCU_TRY(copy_host(dw.ptr, const_cast<double*>(weight), num_edges * 8, true, sg.s));
     }
+    tr.mark("arcs to the device");
   }
-  tr.mark("arcs to the device");
   const int rc = create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out,
-                                             weight ? dw.as<double>() : nullptr);
+                                             weight ? dw.as<double>() : nullptr,
+                                             dsorted.ptr ? dsorted.as<uint32_t>() : nullptr,
+                                             perm.ptr ? perm.as<uint32_t>() : nullptr);
   tr.mark("validation and CSR build");
   return rc;
 }

@@ -176,6 +176,33 @@ def compare_starts(net: _native.WarmStart, g: _native.Graph, damping=0.85, tol=1
     return res
 
 
+def time_inference(scale: int, reps: int) -> list:
+    """CUDA-event time of each of `reps` inference calls (start vector into a
+    device buffer) of the shipped network on a seeded directed R-MAT graph."""
+    import torch
+
+    g = _native.Graph.rmat(scale, 16, 1000 + scale, directed=True)
+    net = load_default()
+    try:
+        V, _, _ = g.info()
+        x0 = torch.empty(max(V, 1), dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream()
+        times = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            net.predict_device(g, x0.data_ptr(), stream=stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            print(f"rmat {scale}: inference {times[-1]:.3f} ms", flush=True)
+        return times
+    finally:
+        net.destroy()
+        g.destroy()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--graphs", type=int, default=2000)
@@ -187,7 +214,14 @@ def main(argv=None):
     ap.add_argument("--loss", choices=("kl", "mse"), default="kl")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--eval-rmat", type=int, default=20, help="held-out R-MAT scale to report (0 = none)")
+    ap.add_argument("--time-rmat", type=int, default=0,
+                    help="no training: time the shipped network's inference on a seeded directed R-MAT graph "
+                         "of this scale (edge factor 16, seed 1000 + scale)")
+    ap.add_argument("--reps", type=int, default=4, help="inference calls timed with --time-rmat")
     args = ap.parse_args(argv)
+    if args.time_rmat:
+        time_inference(args.time_rmat, args.reps)
+        return
     net = _native.WarmStart.create(args.init_seed)
     kind = _native.LOSS_KL if args.loss == "kl" else _native.LOSS_LOG_MSE
     specs = training_specs(args.graphs, args.seed) + large_specs(args.large, args.seed + 1)
