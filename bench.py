@@ -564,13 +564,16 @@ def batched_block(N, args, stream, ws):
     Vb, Eb, _ = Bg.info()
     src = np.random.default_rng(BCB_SEED).choice(Vb, BCB_SOURCES, replace=False).astype(np.uint32)
     part = torch.empty(Vb, dtype=torch.float64, device="cuda")
-    Bg.betweenness_device(part.data_ptr(), sources=src[:256], stream=sp)
+    for _ in range(max(1, args.warmup)):  # same shape as the timed call (its cached CUDA graph)
+        Bg.betweenness_device(part.data_ptr(), sources=src, stream=sp)
     torch.cuda.synchronize()
     barrier(ws)
     cms, csts = _timed(stream, 1, lambda: Bg.betweenness_device(part.data_ptr(), sources=src, stream=sp))
     cms = max_over_ranks(cms, ws)
     launches += int(csts[0]["launches"])
     k1 = 64
+    Bg.betweenness_device(part.data_ptr(), sources=src[:1], stream=sp)  # the one-source shape, warmed
+    torch.cuda.synchronize()
     one_ms, osts = _timed(stream, 1, lambda: [Bg.betweenness_device(part.data_ptr(), sources=src[i:i + 1], stream=sp)
                                               for i in range(k1)])
     launches += sum(int(s2["launches"]) for s2 in osts[0])
@@ -841,9 +844,11 @@ def run_zog(args):
         mine = shard_sources(all_src, rank, ws)
         chunks = [mine[i:i + BC_STEP_SOURCES] for i in range(0, mine.size, BC_STEP_SOURCES)]
         steps = len(chunks) if args.bc_steps <= 0 else min(args.bc_steps, len(chunks))
+        # warm-up calls of the timed calls' shape: the graph resource's cached
+        # CUDA graph for that lane and slot count is instantiated here
         with torch.cuda.stream(stream):
             for w in range(args.warmup):
-                B.betweenness_device(part.data_ptr(), sources=chunks[w % len(chunks)][:1024], stream=sp)
+                B.betweenness_device(part.data_ptr(), sources=chunks[w % len(chunks)], stream=sp)
         torch.cuda.synchronize()
         barrier(ws)
         b0 = torch.cuda.Event(enable_timing=True); b1 = torch.cuda.Event(enable_timing=True)

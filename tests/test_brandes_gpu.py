@@ -166,3 +166,34 @@ def test_hubs_split_over_several_ctas(native, oracle, directed):
         assert np.array_equal(bc, G.betweenness_unweighted(sources=srcs))  # deterministic
     finally:
         G.destroy()
+
+
+def test_one_graph_serves_every_source_count(native, oracle):
+    """A graph resource keeps its lanes' workspaces and instantiated CUDA
+    graphs between calls, and the batches come from device-side cursors, so
+    one graph serves any source count.  Successive calls on one resource:
+    1 source, one batch, a partial third batch, more batches than one graph
+    launch holds (8 lanes x 8 slots = 4,096 sources; 8,192 sources take two
+    launches), a repeat of an earlier count, and every source.  Each against
+    the oracle over the same sources; repeats bit-identical."""
+    V, f, t = oracle.rmat(13, 8, 1313, directed=False)
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        _, _, out_off, out_col, _ = G.export_csr()
+        rng = np.random.default_rng(13)
+        perm = rng.permutation(V).astype(np.uint32)
+        seen = {}
+        for n in (1, 64, 130, 4100, 64, V):
+            srcs = np.sort(perm[:n]) if n < V else None
+            bc, st = G.betweenness_unweighted(sources=srcs, stats=True)
+            ref, _ = oracle.betweenness_csr_sources_mt(V, out_off, out_col,
+                                                       np.arange(V, dtype=np.uint32) if srcs is None else srcs)
+            assert rel_l1(bc, ref) <= TOL, n
+            assert np.array_equal(bc == 0.0, ref == 0.0), n
+            assert st["sources"] == n
+            if n in seen:
+                assert np.array_equal(bc, seen[n]), n
+            seen[n] = bc
+        assert st["reserved"] == 2  # every source: 128 batches, two launches of the cached graph
+    finally:
+        G.destroy()
