@@ -270,7 +270,21 @@ ZOGCU_API int zogcu_pagerank_noalloc(const uint32_t* d_in_off, const uint32_t* d
  * delta_s(v), v != s, unnormalised. */
 ZOGCU_API int zogcu_betweenness_unweighted(zogcu_graph* g, double* out_scores, zogcu_stats* stats);
 
-/* As above with options (source subset, batch size, device output, stream). */
+/* As above with options (source subset, batch size, device output, stream).
+ *
+ * Both forms run the sources in batches of 64.  The batches are dealt to up
+ * to 8 lanes (independent branches of one CUDA graph, each with its own
+ * workspace), and each lane runs up to 8 batches per launch, so a call of up
+ * to 4,096 sources is one graph launch.  Levels are device-ended while loops,
+ * and each level pushes or pulls as its frontier's out-arcs dictate.  The graph
+ * and the lanes' workspaces stay with the graph resource (graphs keyed by lane
+ * count, batch slots per lane and push threshold), and later calls reuse them;
+ * the first call of a key instantiates its graph.
+ * stats->reserved counts the graph launches, stats->launches the kernels they
+ * ran, and stats->max_depth the deepest level.  The lanes' scores are added in
+ * lane order, so repeated calls are bit-identical.  Environment:
+ * ZOGCU_BC_STREAMS=<k> sets the lane count, ZOGCU_BC_PUSH_RATIO=<r> the push
+ * threshold (0 = pull only), ZOGCU_TRACE=1 prints the call's phases. */
 ZOGCU_API int zogcu_betweenness_unweighted_ex(zogcu_graph* g, const zogcu_bc_opts* opts,
                                     double* out_scores, zogcu_stats* stats);
 

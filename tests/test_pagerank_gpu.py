@@ -129,6 +129,21 @@ def test_large_host_arc_lists_build_the_reference_csr(native, oracle, sources_so
         G.destroy()
 
 
+@pytest.mark.parametrize("bad", ["from", "to"])
+def test_large_host_arc_list_with_missing_node_is_rejected(native, bad):
+    """An endpoint >= node_count in a chunk-uploaded arc list is reported as
+    node not found (addEdge's hasNode check, array_graph.zig:88-89); the
+    chunks' destination counts skip such keys before validation runs."""
+    rng = np.random.default_rng(7)
+    V, E = 1 << 12, (1 << 22) + 3
+    f = np.sort(rng.integers(0, V, E, dtype=np.uint32))
+    t = rng.integers(0, V, E, dtype=np.uint32)
+    (f if bad == "from" else t)[E // 2] = V + 5
+    with pytest.raises(native.ZogCudaError) as ei:
+        native.Graph.from_edges(V, f, t)
+    assert ei.value.status == 2
+
+
 @pytest.mark.parametrize("max_iter", [0, 1, 2, 7, 60])
 def test_iteration_prefix_exact(native, oracle, max_iter):
     """Stopping after k iterations returns the k-th iterate (the swap happens

@@ -226,17 +226,36 @@ int ensure_device(int* dev);
 // order (reverse_within_source = true) or already in successor order (false).
 // All endpoints must be < V and refer to live nodes.
 // d_w (may be null) holds one weight per edge in the same order as d_src / d_dst.
+// The arcs sorted stably by destination chunk by chunk, made while later
+// chunks were still being copied to the device (zogcu_graph_create_from_edges).
+// Chunk c holds arcs [bound[c], bound[c+1]); dst and src hold each chunk's
+// (destination, source) pairs in that order; pre[c * (V + 1) + d] counts the
+// arcs into d in chunks before c, start[c * (V + 1) + d] is where d's segment
+// begins in chunk c's run, and total[d] counts the arcs into d (V + 1 slots,
+// the last zero).
+constexpr int kMaxUploadChunks = 8;
+struct ChunkRuns {
+  int chunks = 0;
+  uint64_t bound[kMaxUploadChunks + 1] = {};
+  const uint32_t* dst = nullptr;
+  const uint32_t* src = nullptr;
+  const uint32_t* pre = nullptr;
+  const uint32_t* start = nullptr;
+  unsigned long long* total = nullptr;
+  unsigned long long* out_cnt = nullptr;  // arcs per source (V + 1 slots)
+  unsigned int* flags = nullptr;          // [0] an endpoint >= V, [1] sources not non-decreasing
+};
+
 // src_sorted: 1 = d_src is non-decreasing (the out-CSR is then placed by one
 // scatter instead of a sort), 0 = it is not, -1 = unknown (checked here).
-// presorted_dst / presorted_perm (both or neither; used only when d_src is
-// non-decreasing): the destinations sorted stably and the arc index of each
-// sorted position, so the in-CSR is a gather instead of a second sort.
+// runs (may be null; used only when d_src is non-decreasing): per-chunk
+// sorted runs of the same arcs, so the in-CSR is one merge scatter instead of
+// a second sort (each row's chunks in chunk order list its sources ascending).
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src,
                                   const uint32_t* d_dst, uint64_t E, bool reverse_within_source,
                                   const uint8_t* h_node_deleted, cudaStream_t stream,
                                   const double* d_w = nullptr, int src_sorted = -1,
-                                  const uint32_t* presorted_dst = nullptr,
-                                  const uint32_t* presorted_perm = nullptr);
+                                  ChunkRuns* runs = nullptr);
 
 // PageRank schedule (pagerank.cu): the degree-ranked view, and the work-item
 // list of row blocks of at most nnz (128 or 256) arcs.

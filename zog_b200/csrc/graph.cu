@@ -299,16 +299,77 @@ __global__ void k_validate(const uint32_t* __restrict__ a, const uint32_t* __res
   if (__any_sync(0xffffffffu, unsorted) && (threadIdx.x & 31) == 0) atomicOr(flags + 1, 1u);
 }
 
-// out[j] = a[idx[j]]
-__global__ void k_gather_u32(const uint32_t* __restrict__ a, const uint32_t* __restrict__ idx, uint64_t n,
-                             uint32_t* __restrict__ out) {
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
-    out[j] = __ldg(a + __ldg(idx + j));
+// One chunk's destination counts -> prefixes: cnt[d] becomes the arcs into d
+// in earlier chunks (total[d] before this chunk), and total[d] adds the count.
+__global__ void k_running_prefix(uint32_t* __restrict__ cnt, unsigned long long* __restrict__ total, uint64_t n) {
+  for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < n; d += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t x = cnt[d];
+    const unsigned long long t = total[d];
+    cnt[d] = (uint32_t)t;
+    total[d] = t + x;
+  }
 }
 
-__global__ void k_iota_u32(uint32_t* __restrict__ out, uint64_t n) {
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x)
-    out[j] = (uint32_t)j;
+// In-CSR from per-chunk sorted runs: the j-th pair of chunk c's run with
+// destination d goes to in_off[d] + (arcs into d in earlier chunks) + j.  Each
+// row thus lists its chunks in chunk order, and each chunk's arcs in arc
+// order.  A CTA takes a slice of kMergeSlice positions of in_col, finds the
+// rows at its two ends, and copies from each chunk the contiguous part of the
+// run that lands in the slice: all chunks' writes to the slice come from one
+// CTA close together (they merge in L2), and hub rows are shared out by
+// position, so every CTA copies the same number of arcs.
+constexpr uint64_t kMergeSlice = 4096;
+
+// a run entry: read once, so it neither stays in L1 nor displaces the slices'
+// partly written in_col lines in L2
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+
+// the row holding in_col position pos < E: the last r with in_off[r] <= pos
+__device__ __forceinline__ uint32_t row_of(const uint64_t* __restrict__ in_off, uint32_t V, uint64_t pos) {
+  uint32_t lo = 0, hi = V;  // in_off[lo] <= pos < in_off[hi] = E
+  while (hi - lo > 1) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (__ldg(in_off + mid) <= pos) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_merge_runs(ChunkRuns R, uint32_t V, const uint64_t* __restrict__ in_off,
+                             uint32_t* __restrict__ in_col) {
+  const uint64_t stride = (uint64_t)V + 1, E = R.bound[R.chunks];
+  const uint64_t nslices = (E + kMergeSlice - 1) / kMergeSlice;
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  __shared__ uint32_t s_rows[2];
+  for (uint64_t sl = blockIdx.x; sl < nslices; sl += gridDim.x) {
+    const uint64_t p0 = sl * kMergeSlice, p1 = min(E, p0 + kMergeSlice);
+    __syncthreads();  // s_rows of the previous slice are no longer read
+    if (threadIdx.x == 0) s_rows[0] = row_of(in_off, V, p0);
+    if (threadIdx.x == 32) s_rows[1] = row_of(in_off, V, p1 - 1);
+    __syncthreads();
+    const uint32_t ra = s_rows[0], rb = s_rows[1];
+    for (int c = 0; c < R.chunks; ++c) {
+      const uint32_t* __restrict__ st = R.start + c * stride;
+      const uint32_t* __restrict__ pre = R.pre + c * stride;
+      const uint64_t base = R.bound[c];
+      // chunk c's arcs of rows ra..rb whose positions fall in [p0, p1)
+      const uint64_t oa = __ldg(in_off + ra) + __ldg(pre + ra), ob = __ldg(in_off + rb) + __ldg(pre + rb);
+      const uint32_t na = __ldg(st + ra + 1) - __ldg(st + ra), nb = __ldg(st + rb + 1) - __ldg(st + rb);
+      const uint64_t ua = p0 > oa ? p0 - oa : 0, ub = p1 > ob ? p1 - ob : 0;
+      const uint32_t ja = ua < na ? (uint32_t)ua : na, jb = ub < nb ? (uint32_t)ub : nb;
+      const uint32_t q0 = __ldg(st + ra) + ja, q1 = __ldg(st + rb) + jb;
+      for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+        const uint32_t d = ld_stream(R.dst + base + q, pol);
+        const uint32_t v = ld_stream(R.src + base + q, pol);
+        in_col[__ldg(in_off + d) + __ldg(pre + d) + (q - __ldg(st + d))] = v;
+      }
+    }
+  }
 }
 
 // Sorted-input out-CSR: input arc j of source r = src[j] goes to position
@@ -333,7 +394,10 @@ __global__ void k_scatter_sorted(const uint32_t* __restrict__ src, const uint32_
 // Per-row arc counts of SORTED keys: each warp reads 32 consecutive keys, and
 // the first lane of every run of equal keys adds the run's length (a run that
 // spans warps is added in parts), one atomic per run instead of per arc.
-__global__ void k_histogram_sorted(const uint32_t* __restrict__ keys, uint64_t E, unsigned long long* cnt) {
+// cnt[k] += the number of keys equal to k, for keys below `limit` (runs of
+// equal keys add once; larger keys, which validation rejects later, are skipped)
+template <class C>
+__global__ void k_histogram_sorted(const uint32_t* __restrict__ keys, uint64_t E, C* cnt, uint32_t limit) {
   const int lane = threadIdx.x & 31;
   const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
   for (uint64_t base = ((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < E; base += nw * 32) {
@@ -344,10 +408,10 @@ __global__ void k_histogram_sorted(const uint32_t* __restrict__ keys, uint64_t E
     const bool head = valid && (lane == 0 || k != kp);
     const unsigned hb = __ballot_sync(0xffffffffu, head);
     const uint32_t nvalid = (E - base < 32) ? (uint32_t)(E - base) : 32u;
-    if (head) {
+    if (head && k < limit) {
       const unsigned above = lane < 31 ? (hb >> (lane + 1)) : 0u;
       const uint32_t next = above ? (uint32_t)(lane + __ffs(above)) : nvalid;
-      atomicAdd(&cnt[k], (unsigned long long)(next - lane));
+      atomicAdd(&cnt[k], (C)(next - lane));
     }
   }
 }
@@ -390,8 +454,7 @@ static int counts_to_offsets(unsigned long long* d_cnt, uint64_t* d_off, uint32_
 
 int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, const uint32_t* d_dst,
                                   uint64_t E, bool reverse_within_source, const uint8_t* h_node_deleted,
-                                  cudaStream_t s, const double* d_w, int src_sorted,
-                                  const uint32_t* presorted_dst, const uint32_t* presorted_perm) {
+                                  cudaStream_t s, const double* d_w, int src_sorted, ChunkRuns* runs) {
   ZOGCU_TRY(ensure_device(&g->device));
   g->V = V;
   g->E = E;
@@ -443,15 +506,20 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
     }
     DevBuf ks, vs, ks2, t;
     size_t tmp = 0;
-    if (!(sorted && presorted_dst && presorted_perm)) ZOGCU_TRY(ks.alloc(E * 4, s));
+    const bool merge_runs = sorted && runs && runs->chunks > 0 && !d_w;
+    if (!merge_runs) ZOGCU_TRY(ks.alloc(E * 4, s));
     const uint32_t* keys_out;  // the source of every out-CSR arc (rows ascending)
     if (sorted) {
       // Sources already non-decreasing: the out offsets come straight from
       // them, and one scatter places each row (reversed for insertion order).
-      ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
-      k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(d_src, E, cnt.as<unsigned long long>());
-      ZOGCU_CUDA(cudaGetLastError());
-      ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
+      if (merge_runs) {  // counted chunk by chunk during the upload
+        ZOGCU_TRY(counts_to_offsets(runs->out_cnt, g->out_off64.as<uint64_t>(), V, s));
+      } else {
+        ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
+        k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(d_src, E, cnt.as<unsigned long long>(), V);
+        ZOGCU_CUDA(cudaGetLastError());
+        ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
+      }
       if (d_w) {
         ZOGCU_TRY(g->out_w.alloc(E * 8));
         g->weighted = true;
@@ -497,37 +565,39 @@ int build_graph_from_device_edges(Graph* g, uint32_t V, const uint32_t* d_src, c
       }
       // out offsets
       ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
-      k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks2.as<uint32_t>(), E, cnt.as<unsigned long long>());
+      k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks2.as<uint32_t>(), E, cnt.as<unsigned long long>(), V);
       ZOGCU_CUDA(cudaGetLastError());
       ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->out_off64.as<uint64_t>(), V, s));
       keys_out = ks2.as<uint32_t>();
     }
     tr.mark(sorted ? "out-CSR (sorted sources)" : "out-CSR (radix sort)");
-    const uint32_t* in_keys = ks.as<uint32_t>();  // the destination of every in-CSR arc
-    if (sorted && presorted_dst && presorted_perm) {
-      // (2') sources non-decreasing: the stable order of the arcs by destination
-      // already lists each row's sources ascending, so the in-CSR is a gather
-      k_gather_u32<<<grid_for(E), 256, 0, s>>>(d_src, presorted_perm, E, g->in_col.as<uint32_t>());
+    if (merge_runs) {
+      // (2') sources non-decreasing: each chunk's run lists a row's sources
+      // ascending, and the chunks follow one another in source order, so the
+      // in-CSR is every row's chunk segments placed in chunk order
+      ZOGCU_TRY(counts_to_offsets(runs->total, g->in_off64.as<uint64_t>(), V, s));
+      tr.mark("in offsets from the chunk counts");
+      k_merge_runs<<<grid_for((E + kMergeSlice - 1) / kMergeSlice * 256), 256, 0, s>>>(
+          *runs, V, g->in_off64.as<uint64_t>(), g->in_col.as<uint32_t>());
       ZOGCU_CUDA(cudaGetLastError());
-      in_keys = presorted_dst;
-      tr.mark("in-CSR gather (presorted destinations)");
+      tr.mark("in-CSR merge of the chunk runs");
     } else {
-    // (2) stable sort of (dst, src) pairs by dst: sources stay ascending
-    size_t tmp2 = 0;
-    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
-                                               keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
-    if (tmp2 > tmp) {
-      ZOGCU_TRY(t.alloc(tmp2, s));
-      tmp = tmp2;
+      // (2) stable sort of (dst, src) pairs by dst: sources stay ascending
+      size_t tmp2 = 0;
+      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
+                                                 keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
+      if (tmp2 > tmp) {
+        ZOGCU_TRY(t.alloc(tmp2, s));
+        tmp = tmp2;
+      }
+      ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
+                                                 keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
+      tr.mark("in-CSR radix sort");
+      ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
+      k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(ks.as<uint32_t>(), E, cnt.as<unsigned long long>(), V);
+      ZOGCU_CUDA(cudaGetLastError());
+      ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->in_off64.as<uint64_t>(), V, s));
     }
-    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(t.ptr, tmp, g->out_col.as<uint32_t>(), ks.as<uint32_t>(),
-                                               keys_out, g->in_col.as<uint32_t>(), (int64_t)E, 0, bits, s));
-    tr.mark("in-CSR radix sort");
-    }
-    ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, (size_t)(V + 1) * 8, s));
-    k_histogram_sorted<<<grid_for(E), 256, 0, s>>>(in_keys, E, cnt.as<unsigned long long>());
-    ZOGCU_CUDA(cudaGetLastError());
-    ZOGCU_TRY(counts_to_offsets(cnt.as<unsigned long long>(), g->in_off64.as<uint64_t>(), V, s));
   } else {
     ZOGCU_CUDA(cudaMemsetAsync(g->in_off64.ptr, 0, (size_t)(V + 1) * 8, s));
     ZOGCU_CUDA(cudaMemsetAsync(g->out_off64.ptr, 0, (size_t)(V + 1) * 8, s));
@@ -626,10 +696,6 @@ static void rmat_thresholds(double a, double b, double c, uint64_t* ta, uint64_t
   *tabc = (uint64_t)std::floor((a + b + c) * two53);
 }
 
-// Arc lists from host memory of at least this many arcs have their
-// destinations sorted while the sources are still being copied.
-constexpr uint64_t kPresortMinArcs = 1ull << 22;
-
 struct EventGuard {
   cudaEvent_t e = nullptr;
   int init() {
@@ -641,25 +707,87 @@ struct EventGuard {
   }
 };
 
-// The stable sort of the arcs by destination on stream s: dst_sorted[k] is the
-// k-th smallest destination and perm[k] the index of its arc (ties keep arc
-// order).  Only the bits of node ids below V are sorted; endpoints are
-// validated before the result is used.
-static int presort_destinations(const uint32_t* d_dst, uint64_t E, uint32_t V, DevBuf& dst_sorted, DevBuf& perm,
-                                cudaStream_t s) {
-  DevBuf iota, tmp;
-  ZOGCU_TRY(iota.alloc(E * 4, s));
-  ZOGCU_TRY(dst_sorted.alloc(E * 4, s));
-  ZOGCU_TRY(perm.alloc(E * 4, s));
-  k_iota_u32<<<grid_for(E), 256, 0, s>>>(iota.as<uint32_t>(), E);
-  ZOGCU_CUDA(cudaGetLastError());
+// Arc lists from host memory of at least this many arcs are copied in
+// kUploadChunks chunks, each sorted by destination while the next ones are
+// still being copied.
+constexpr uint64_t kChunkedMinArcs = 1ull << 22;
+constexpr int kUploadChunks = 8;
+static_assert(kUploadChunks <= kMaxUploadChunks, "chunk bound array");
+
+// Copies the host arc arrays to d_from / d_to chunk by chunk on stream `up`
+// and, on stream s as each chunk lands, sorts its (destination, source) pairs
+// stably by destination and counts and scans its destinations (ChunkRuns).
+// On return s is ordered after every copy.
+static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, uint32_t V, uint32_t* d_from,
+                          uint32_t* d_to, cudaStream_t s, cudaStream_t up, ChunkRuns& R, DevBuf& dst, DevBuf& src,
+                          DevBuf& cnt, DevBuf& start, DevBuf& total, DevBuf& out_cnt, DevBuf& flags) {
+  const uint64_t stride = (uint64_t)V + 1;
+  // The device sorts a chunk about nine times faster than PCIe delivers it,
+  // so only the last chunk's work is exposed: it gets 1/64 of the arcs, and
+  // the other chunks split the rest evenly.
+  R.chunks = kUploadChunks;
+  const uint64_t head = E - E / 64;
+  for (int c = 0; c < kUploadChunks; ++c) R.bound[c] = head * (uint64_t)c / (kUploadChunks - 1);
+  R.bound[kUploadChunks] = E;
+  uint64_t longest = 0;
+  for (int c = 0; c < kUploadChunks; ++c) longest = std::max(longest, R.bound[c + 1] - R.bound[c]);
+  ZOGCU_TRY(dst.alloc(E * 4, s));
+  ZOGCU_TRY(src.alloc(E * 4, s));
+  ZOGCU_TRY(cnt.alloc(stride * kUploadChunks * 4, s));
+  ZOGCU_TRY(start.alloc(stride * kUploadChunks * 4, s));
+  ZOGCU_TRY(total.alloc(stride * 8, s));
+  ZOGCU_TRY(out_cnt.alloc(stride * 8, s));
+  ZOGCU_TRY(flags.alloc(8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(cnt.ptr, 0, stride * kUploadChunks * 4, s));
+  ZOGCU_CUDA(cudaMemsetAsync(total.ptr, 0, stride * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(out_cnt.ptr, 0, stride * 8, s));
+  ZOGCU_CUDA(cudaMemsetAsync(flags.ptr, 0, 8, s));
   const int bits = bits_for(V);
-  size_t bytes = 0;
-  ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, d_dst, dst_sorted.as<uint32_t>(), iota.as<uint32_t>(),
-                                             perm.as<uint32_t>(), (int64_t)E, 0, bits, s));
-  ZOGCU_TRY(tmp.alloc(bytes, s));
-  ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, bytes, d_dst, dst_sorted.as<uint32_t>(), iota.as<uint32_t>(),
-                                             perm.as<uint32_t>(), (int64_t)E, 0, bits, s));
+  size_t sort_bytes = 0, scan_bytes = 0;
+  ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, d_to, dst.as<uint32_t>(), d_from,
+                                             src.as<uint32_t>(), (int64_t)longest, 0, bits, s));
+  ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt.as<uint32_t>(), start.as<uint32_t>(),
+                                           (int64_t)stride, s));
+  DevBuf tmp;
+  ZOGCU_TRY(tmp.alloc(std::max(sort_bytes, scan_bytes), s));
+  // the copies start once the device arrays, allocated in stream order on s, exist
+  EventGuard ready;
+  ZOGCU_TRY(ready.init());
+  ZOGCU_CUDA(cudaEventRecord(ready.e, s));
+  ZOGCU_CUDA(cudaStreamWaitEvent(up, ready.e, 0));
+  EventGuard landed[kUploadChunks];
+  for (int c = 0; c < kUploadChunks; ++c) {
+    const uint64_t lo = R.bound[c], n = R.bound[c + 1] - lo;
+    ZOGCU_TRY(landed[c].init());
+    ZOGCU_TRY(copy_host(d_from + lo, const_cast<uint32_t*>(from + lo), n * 4, true, up));
+    ZOGCU_TRY(copy_host(d_to + lo, const_cast<uint32_t*>(to + lo), n * 4, true, up));
+    ZOGCU_CUDA(cudaEventRecord(landed[c].e, up));
+    ZOGCU_CUDA(cudaStreamWaitEvent(s, landed[c].e, 0));
+    // endpoints < V and sources non-decreasing, the pair across the previous
+    // chunk's end included; arcs per source (used when they are sorted)
+    const uint64_t back = c > 0 ? 1 : 0;
+    k_validate<<<grid_for(n + back), 256, 0, s>>>(d_from + lo - back, d_to + lo - back, n + back, V,
+                                                 flags.as<unsigned int>());
+    k_histogram_sorted<<<grid_for(n), 256, 0, s>>>(d_from + lo, n, out_cnt.as<unsigned long long>(), V);
+    ZOGCU_CUDA(cudaGetLastError());
+    size_t b = sort_bytes;
+    ZOGCU_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, b, d_to + lo, dst.as<uint32_t>() + lo, d_from + lo,
+                                               src.as<uint32_t>() + lo, (int64_t)n, 0, bits, s));
+    uint32_t* cc = cnt.as<uint32_t>() + c * stride;
+    k_histogram_sorted<<<grid_for(n), 256, 0, s>>>(dst.as<uint32_t>() + lo, n, cc, V);
+    ZOGCU_CUDA(cudaGetLastError());
+    b = scan_bytes;
+    ZOGCU_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, b, cc, start.as<uint32_t>() + c * stride, (int64_t)stride, s));
+    k_running_prefix<<<grid_for(stride), 256, 0, s>>>(cc, total.as<unsigned long long>(), stride);
+    ZOGCU_CUDA(cudaGetLastError());
+  }
+  R.dst = dst.as<uint32_t>();
+  R.src = src.as<uint32_t>();
+  R.pre = cnt.as<uint32_t>();
+  R.start = start.as<uint32_t>();
+  R.total = total.as<unsigned long long>();
+  R.out_cnt = out_cnt.as<unsigned long long>();
+  R.flags = flags.as<unsigned int>();
   return ZOGCU_OK;
 }
 
@@ -667,17 +795,20 @@ static int presort_destinations(const uint32_t* d_dst, uint64_t E, uint32_t V, D
 // and builds the graph on stream s.
 static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_from, const uint32_t* d_to,
                                        uint64_t num_edges, cudaStream_t s, zogcu_graph** out,
-                                       const double* d_w = nullptr, const uint32_t* presorted_dst = nullptr,
-                                       const uint32_t* presorted_perm = nullptr) {
+                                       const double* d_w = nullptr, ChunkRuns* runs = nullptr) {
   int sorted = 0;
   if (num_edges) {
     DevBuf fl;
-    ZOGCU_TRY(fl.alloc(8, s));
-    ZOGCU_CUDA(cudaMemsetAsync(fl.ptr, 0, 8, s));
-    k_validate<<<grid_for(num_edges), 256, 0, s>>>(d_from, d_to, num_edges, node_count, fl.as<unsigned int>());
-    ZOGCU_CUDA(cudaGetLastError());
+    const unsigned int* flags = runs ? runs->flags : nullptr;  // already checked chunk by chunk
+    if (!flags) {
+      ZOGCU_TRY(fl.alloc(8, s));
+      ZOGCU_CUDA(cudaMemsetAsync(fl.ptr, 0, 8, s));
+      k_validate<<<grid_for(num_edges), 256, 0, s>>>(d_from, d_to, num_edges, node_count, fl.as<unsigned int>());
+      ZOGCU_CUDA(cudaGetLastError());
+      flags = fl.as<unsigned int>();
+    }
     unsigned int h[2] = {0, 0};
-    ZOGCU_CUDA(cudaMemcpyAsync(h, fl.ptr, 8, cudaMemcpyDeviceToHost, s));
+    ZOGCU_CUDA(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, s));
     ZOGCU_CUDA(cudaStreamSynchronize(s));
     if (h[0]) return fail(ZOGCU_ERR_NODE_NOT_FOUND, "edge endpoint >= node_count");
     sorted = h[1] == 0 ? 1 : 0;
@@ -685,7 +816,7 @@ static int create_from_device_edges_on(uint32_t node_count, const uint32_t* d_fr
   std::unique_ptr<zogcu_graph> G(new (std::nothrow) zogcu_graph());
   if (!G) return fail(ZOGCU_ERR_OUT_OF_MEMORY, "host allocation failed");
   ZOGCU_TRY(build_graph_from_device_edges(&G->g, node_count, d_from, d_to, num_edges, true, nullptr, s, d_w,
-                                          sorted, presorted_dst, presorted_perm));
+                                          sorted, runs));
   *out = G.release();
   return ZOGCU_OK;
 }
@@ -758,24 +889,17 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
   DevBuf df, dt;
   ZOGCU_TRY(df.alloc(num_edges * 4, sg.s));
   ZOGCU_TRY(dt.alloc(num_edges * 4, sg.s));
-  DevBuf dw, dsorted, perm;
-  if (num_edges >= kPresortMinArcs && !weight) {
-    // The destinations go first, and their stable sort (with the arc indices)
-    // runs on sg.s while the sources cross PCIe on a second stream.  When
-    // the sources turn out non-decreasing, the in-CSR is then a gather.
-    ZOGCU_TRY(copy_host(dt.ptr, const_cast<uint32_t*>(to), num_edges * 4, true, sg.s));
+  DevBuf dw, rdst, rsrc, rcnt, rstart, rtotal, routc, rflags;
+  ChunkRuns runs;
+  if (num_edges >= kChunkedMinArcs && !weight) {
+    // Chunks of both arrays cross PCIe on a second stream; each chunk's stable
+    // sort by destination runs while the next ones are copied.  When the
+    // sources turn out non-decreasing, the in-CSR is then one merge of the runs.
     StreamGuard up;
     ZOGCU_TRY(up.init(nullptr));
-    EventGuard to_done, from_done;
-    ZOGCU_TRY(to_done.init());
-    ZOGCU_TRY(from_done.init());
-    ZOGCU_CUDA(cudaEventRecord(to_done.e, sg.s));
-    ZOGCU_TRY(presort_destinations(dt.as<uint32_t>(), num_edges, node_count, dsorted, perm, sg.s));
-    ZOGCU_CUDA(cudaStreamWaitEvent(up.s, to_done.e, 0));  // one array on the bus at a time
-    ZOGCU_TRY(copy_host(df.ptr, const_cast<uint32_t*>(from), num_edges * 4, true, up.s));
-    ZOGCU_CUDA(cudaEventRecord(from_done.e, up.s));
-    ZOGCU_CUDA(cudaStreamWaitEvent(sg.s, from_done.e, 0));
-    tr.mark("arcs to the device, destinations sorted meanwhile");
+    ZOGCU_TRY(upload_chunked(from, to, num_edges, node_count, df.as<uint32_t>(), dt.as<uint32_t>(), sg.s, up.s,
+                             runs, rdst, rsrc, rcnt, rstart, rtotal, routc, rflags));
+    tr.mark("arcs to the device, chunks sorted meanwhile");
   } else if (num_edges) {
     ZOGCU_TRY(copy_host(df.ptr, const_cast<uint32_t*>(from), num_edges * 4, true, sg.s));
     ZOGCU_TRY(copy_host(dt.ptr, const_cast<uint32_t*>(to), num_edges * 4, true, sg.s));
@@ -786,9 +910,7 @@ int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from, con
     tr.mark("arcs to the device");
   }
   const int rc = create_from_device_edges_on(node_count, df.as<uint32_t>(), dt.as<uint32_t>(), num_edges, sg.s, out,
-                                             weight ? dw.as<double>() : nullptr,
-                                             dsorted.ptr ? dsorted.as<uint32_t>() : nullptr,
-                                             perm.ptr ? perm.as<uint32_t>() : nullptr);
+                                             weight ? dw.as<double>() : nullptr, runs.chunks ? &runs : nullptr);
   tr.mark("validation and CSR build");
   return rc;
 }
