@@ -129,14 +129,28 @@ EventTimer::~EventTimer() {
 // parts, and each part is copied by its own host thread through two
 // library-owned pinned chunks of kBounceBytes on its own stream: while the DMA
 // engine moves one chunk, the thread fills the other, and the parts' DMAs
-// queue back to back on the link.  The pinned chunks are allocated on first
-// use and kept (one call at a time uses them; a concurrent call copies
-// directly).  Pinned caller memory is copied directly.
-constexpr int kCopyThreads = 8;
+// queue back to back on the link.  The pinned chunks, the helper streams and
+// one event per chunk are created on a device's first call and kept (one call
+// at a time uses them; a concurrent call copies directly).  A call never
+// drains the helpers: a chunk is refilled once the event of its last DMA has
+// fired, in this call or an earlier one, so calls in a row (the chunked
+// upload makes sixteen) keep the link busy.  Pinned caller memory is copied
+// directly.
+constexpr int kCopyThreads = 16;
 constexpr size_t kBounceBytes = 16u << 20;
+constexpr int kMaxCopyDevices = 16;
 
+struct BounceSet {
+  void* buf[2 * kCopyThreads] = {};
+  cudaEvent_t done[2 * kCopyThreads] = {};  // the last DMA through buf[i]
+  bool used[2 * kCopyThreads] = {};         // done[i] has been recorded
+  cudaStream_t st[kCopyThreads] = {};
+  cudaEvent_t tail[kCopyThreads] = {};      // end of a call's work on st[t]
+  cudaEvent_t start = nullptr;
+  bool ready = false;
+};
 static std::mutex g_bounce_mu;
-static void* g_bounce[2 * kCopyThreads] = {};
+static BounceSet g_bounce[kMaxCopyDevices];
 
 static bool is_pinned(const void* p) {
   cudaPointerAttributes a;
@@ -147,35 +161,40 @@ static bool is_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
 }
 
+static int bounce_setup(BounceSet& B) {
+  if (B.ready) return ZOGCU_OK;
+  for (void*& b : B.buf)
+    if (!b) ZOGCU_CUDA(cudaHostAlloc(&b, kBounceBytes, cudaHostAllocPortable));
+  for (cudaEvent_t& e : B.done)
+    if (!e) ZOGCU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (cudaEvent_t& e : B.tail)
+    if (!e) ZOGCU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (cudaStream_t& t : B.st)
+    if (!t) ZOGCU_CUDA(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+  if (!B.start) ZOGCU_CUDA(cudaEventCreateWithFlags(&B.start, cudaEventDisableTiming));
+  B.ready = true;
+  return ZOGCU_OK;
+}
+
 // Copies `bytes` between host memory `host` and device memory `dev` (h2d:
 // host -> device) ordered after the work already on stream s; the copy is
 // ordered before later work on s (s waits for the helper streams).
 int copy_host(void* dev, void* host, size_t bytes, bool h2d, cudaStream_t s) {
   if (bytes == 0) return ZOGCU_OK;
   const cudaMemcpyKind kind = h2d ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  int device = 0;
+  ZOGCU_CUDA(cudaGetDevice(&device));
   std::unique_lock<std::mutex> lk(g_bounce_mu, std::try_to_lock);
-  if (bytes < 2 * kBounceBytes || is_pinned(host) || !lk.owns_lock()) {
+  if (bytes < 2 * kBounceBytes || device >= kMaxCopyDevices || is_pinned(host) || !lk.owns_lock()) {
     ZOGCU_CUDA(h2d ? cudaMemcpyAsync(dev, host, bytes, kind, s) : cudaMemcpyAsync(host, dev, bytes, kind, s));
     return ZOGCU_OK;
   }
-  for (void*& b : g_bounce)
-    if (!b) ZOGCU_CUDA(cudaHostAlloc(&b, kBounceBytes, cudaHostAllocPortable));
-  cudaEvent_t start = nullptr;
-  ZOGCU_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
-  ZOGCU_CUDA(cudaEventRecord(start, s));
-  cudaStream_t st[kCopyThreads] = {};
-  cudaEvent_t ev[2 * kCopyThreads] = {};
-  int rc = ZOGCU_OK;
-  for (int t = 0; t < kCopyThreads && rc == ZOGCU_OK; ++t) {
-    if (cudaStreamCreateWithFlags(&st[t], cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamWaitEvent(st[t], start, 0) != cudaSuccess)
-      rc = fail(ZOGCU_ERR_CUDA, "copy stream set-up failed");
-    for (int k = 0; k < 2 && rc == ZOGCU_OK; ++k)
-      if (cudaEventCreateWithFlags(&ev[2 * t + k], cudaEventDisableTiming) != cudaSuccess)
-        rc = fail(ZOGCU_ERR_CUDA, "copy event set-up failed");
-  }
+  BounceSet& B = g_bounce[device];
+  ZOGCU_TRY(bounce_setup(B));
+  ZOGCU_CUDA(cudaEventRecord(B.start, s));
+  for (int t = 0; t < kCopyThreads; ++t) ZOGCU_CUDA(cudaStreamWaitEvent(B.st[t], B.start, 0));
   std::atomic<int> err{0};
-  if (rc == ZOGCU_OK) {
+  {
     std::vector<std::thread> th;
     const size_t part = (bytes / kCopyThreads + 15) & ~(size_t)15;
     for (int t = 0; t < kCopyThreads; ++t) {
@@ -186,40 +205,33 @@ int copy_host(void* dev, void* host, size_t bytes, bool h2d, cudaStream_t s) {
         int k = 0;
         for (size_t o = lo; o < hi; o += kBounceBytes, ++k) {
           const size_t n = std::min(kBounceBytes, hi - o);
-          void* buf = g_bounce[2 * t + (k & 1)];
-          cudaEvent_t e = ev[2 * t + (k & 1)];
+          const int i = 2 * t + (k & 1);
+          // the chunk is free once its last DMA (this call's or an earlier one's) finished
+          if (B.used[i] && cudaEventSynchronize(B.done[i]) != cudaSuccess) { err = 1; return; }
           if (h2d) {
-            // the chunk is free again once the DMA two chunks back finished
-            if (k >= 2 && cudaEventSynchronize(e) != cudaSuccess) { err = 1; return; }
-            std::memcpy(buf, hb + o, n);
-            if (cudaMemcpyAsync(db + o, buf, n, kind, st[t]) != cudaSuccess ||
-                cudaEventRecord(e, st[t]) != cudaSuccess) { err = 1; return; }
+            std::memcpy(B.buf[i], hb + o, n);
+            if (cudaMemcpyAsync(db + o, B.buf[i], n, kind, B.st[t]) != cudaSuccess ||
+                cudaEventRecord(B.done[i], B.st[t]) != cudaSuccess) { err = 1; return; }
+            B.used[i] = true;
           } else {
-            if (cudaMemcpyAsync(buf, db + o, n, kind, st[t]) != cudaSuccess ||
-                cudaStreamSynchronize(st[t]) != cudaSuccess) { err = 1; return; }
-            std::memcpy(hb + o, buf, n);
+            if (cudaMemcpyAsync(B.buf[i], db + o, n, kind, B.st[t]) != cudaSuccess ||
+                cudaEventRecord(B.done[i], B.st[t]) != cudaSuccess ||
+                cudaEventSynchronize(B.done[i]) != cudaSuccess) { err = 1; return; }
+            B.used[i] = true;
+            std::memcpy(hb + o, B.buf[i], n);
           }
         }
       });
     }
     for (auto& x : th) x.join();
-    if (err) rc = fail(ZOGCU_ERR_CUDA, "pipelined host copy failed");
   }
+  // later work on s follows every helper's copies, without a host wait
   for (int t = 0; t < kCopyThreads; ++t) {
-    if (!st[t]) continue;
-    cudaEvent_t done = nullptr;
-    if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
-      cudaEventRecord(done, st[t]);
-      cudaStreamWaitEvent(s, done, 0);
-      cudaEventDestroy(done);
-    }
-    cudaStreamSynchronize(st[t]);  // the pinned chunks are reused by the next call
-    cudaStreamDestroy(st[t]);
+    ZOGCU_CUDA(cudaEventRecord(B.tail[t], B.st[t]));
+    ZOGCU_CUDA(cudaStreamWaitEvent(s, B.tail[t], 0));
   }
-  for (cudaEvent_t e : ev)
-    if (e) cudaEventDestroy(e);
-  cudaEventDestroy(start);
-  return rc;
+  if (err) return fail(ZOGCU_ERR_CUDA, "pipelined host copy failed");
+  return ZOGCU_OK;
 }
 
 // SM count of the first device queried (every device of a B200 node has the
