@@ -38,7 +38,10 @@
 // on its heap's tie order; weights must be positive and finite, and such an
 // arc is reported as an error instead of guessed at.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -50,6 +53,18 @@ constexpr int kWb = 32;                                     // sources per batch
 constexpr unsigned long long kInf = 0x7FF0000000000000ull;  // +inf
 constexpr uint32_t kNoRound = 0xFFFFFFFFu;
 constexpr int kWbChain = 32;                                // launches between host checks
+constexpr int kWbMaxLanes = 8;                              // batch lanes (streams with host threads)
+
+struct EventGuardWb {
+  cudaEvent_t e = nullptr;
+  int init() {
+    ZOGCU_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return ZOGCU_OK;
+  }
+  ~EventGuardWb() {
+    if (e) cudaEventDestroy(e);
+  }
+};
 constexpr uint32_t kWbChunk = 256;                          // arcs per work item
 
 enum : int { kFlagZeroArc = 0, kFlagOverflow = 1, kFlagBadWeight = 2, kFlagMaxRound = 3, kFlags = 4 };
@@ -339,39 +354,47 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   const unsigned g_relax = wb_grid_of(k_wb_relax, nwork), g_count = wb_grid_of(k_wb_dagcount, nwork);
   const unsigned g_sigma = wb_grid_of(k_wb_sigma, nwork), g_delta = wb_grid_of(k_wb_delta, nwork);
 
-  // Batches alternate between two streams ("lanes"), each with its own state
-  // and score vector: while the host waits on one lane's rounds, the other
-  // lane's dependency rounds keep the GPU busy.  The second lane's scores are
-  // added to the first's at the end.  The score vectors are declared first
-  // and the second stream next, so on every exit the lanes' state is freed,
-  // then the stream is drained, and only then the vectors (on stream s) go.
+  // Batches are dealt to lanes (batch i to lane i mod lanes), each with its
+  // own stream, state and score vector and driven by its own host thread:
+  // while one lane's thread waits on its round flags, the other lanes' rounds
+  // keep the GPU busy.  The lanes' scores are added to the first lane's in
+  // lane order at the end, so the result does not depend on timing.  Lanes:
+  // up to kWbMaxLanes, as many as a quarter of the device memory holds
+  // (ZOGCU_BC_STREAMS=<k> sets the count).  Declaration order makes every exit
+  // free the lanes' state first, then drain and destroy their streams, and
+  // only then free the score vectors (on stream s).
   const size_t nbatches = (sources.size() + kWb - 1) / kWb;
-  const char* env = std::getenv("ZOGCU_BC_STREAMS");
-  const int nlanes = (nbatches >= 2 && !(env && env[0] == '1')) ? 2 : 1;
-  DevBuf bcv[2];
-  StreamGuard s1g;
-  cudaStream_t ls[2] = {s, s};
-  cudaEvent_t ev = nullptr;
-  struct EventFree {
-    cudaEvent_t* e;
-    ~EventFree() {
-      if (*e) cudaEventDestroy(*e);
-    }
-  } evf{&ev};
+  const size_t lane_bytes = n * (8 * 3 + 4 * 2) + Vs * 4 * 3 + work_n * 4 + Vs * 8;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) total_b = 0;
+  int nlanes = (int)std::min<size_t>(std::max<size_t>(nbatches, 1), kWbMaxLanes);
+  if (total_b) nlanes = (int)std::max<size_t>(1, std::min<size_t>(nlanes, total_b / 4 / std::max<size_t>(lane_bytes, 1)));
+  if (const char* env = std::getenv("ZOGCU_BC_STREAMS")) {
+    const int k = std::atoi(env);
+    if (k >= 1) nlanes = std::min(k, kWbMaxLanes);
+  }
+  DevBuf bcv[kWbMaxLanes];
+  StreamGuard lsg[kWbMaxLanes];
+  cudaStream_t ls[kWbMaxLanes] = {};
+  EventGuardWb start_ev, lane_done[kWbMaxLanes];
   for (int l = 0; l < nlanes; ++l) {
     ZOGCU_TRY(bcv[l].alloc(Vs * 8, s));
     ZOGCU_CUDA(cudaMemsetAsync(bcv[l].ptr, 0, Vs * 8, s));
   }
-  if (nlanes == 2) {
-    ZOGCU_TRY(s1g.init(nullptr));
-    ls[1] = s1g.s;
-    ZOGCU_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    ZOGCU_CUDA(cudaEventRecord(ev, s));
-    ZOGCU_CUDA(cudaStreamWaitEvent(ls[1], ev, 0));
+  ZOGCU_TRY(start_ev.init());
+  ZOGCU_CUDA(cudaEventRecord(start_ev.e, s));
+  for (int l = 0; l < nlanes; ++l) {
+    ZOGCU_TRY(lsg[l].init(nullptr));
+    ls[l] = lsg[l].s;
+    ZOGCU_CUDA(cudaStreamWaitEvent(ls[l], start_ev.e, 0));  // after the score vectors and work items
   }
   struct Lane {
     DevBuf bdist, bsigma, bdelta, bround, bcnt, bm0, bm1, bm2, bwork, bflags, bsrc;
-  } L[2];
+    uint64_t launches = 0;
+    uint32_t deepest = 0;
+    int status = ZOGCU_OK;
+    std::string error;
+  } L[kWbMaxLanes];
   for (int l = 0; l < nlanes; ++l) {
     Lane& A = L[l];
     const cudaStream_t st = ls[l];
@@ -390,11 +413,9 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   }
   EventTimer tm;
   ZOGCU_TRY(tm.start(s));
-  uint64_t launches = 0;
-  uint32_t deepest = 0;
   const uint32_t one = 1;
-  for (size_t bi = 0; bi < nbatches; ++bi) {
-    const int l = (int)(bi % (size_t)nlanes);
+  // one batch of up to kWb sources on lane l (run by lane l's thread)
+  auto run_batch = [&](int l, size_t bi) -> int {
     Lane& A = L[l];
     const cudaStream_t st = ls[l];
     unsigned long long* dist = A.bdist.as<unsigned long long>();
@@ -415,7 +436,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     k_wb_seed<<<1, kWb, 0, st>>>(src, ns, dist, sigma, round, masks[0]);
     ZOGCU_CUDA(cudaGetLastError());
     ZOGCU_CUDA(cudaMemsetAsync(flags + kFlagMaxRound, 0, 4, st));
-    launches += 2;
+    A.launches += 2;
     // phase 1: distances
     ZOGCU_CUDA(cudaMemsetAsync(work, 0, work_n * 4, st));
     ZOGCU_CUDA(cudaMemcpyAsync(work, &one, 4, cudaMemcpyHostToDevice, st));
@@ -424,7 +445,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
       k_wb_relax<<<g_relax, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, masks[k % 3], masks[(k + 1) % 3],
                                         masks[(k + 2) % 3], V, work, k);
     }, &r1));
-    launches += r1;
+    A.launches += r1;
     // phase 2: DAG in-counts, then sigma in topological rounds from the sources
     k_wb_dagcount<<<g_count, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, cnt, flags);
     for (int i = 0; i < 3; ++i) ZOGCU_CUDA(cudaMemsetAsync(masks[i], 0, Vs * 4, st));
@@ -437,7 +458,7 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
       k_wb_sigma<<<g_sigma, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, cnt, round, masks[k % 3],
                                         masks[(k + 1) % 3], masks[(k + 2) % 3], V, work, flags, k);
     }, &r2));
-    launches += r2 + 2;
+    A.launches += r2 + 2;
     uint32_t hf[kFlags];
     ZOGCU_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
     ZOGCU_CUDA(cudaStreamSynchronize(st));
@@ -446,22 +467,58 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
                   "weighted betweenness: a shortest path holds an arc of effective length zero (fl(d + w) == d)");
     // phase 3: dependencies, rounds in reverse
     const uint32_t maxr = hf[kFlagMaxRound];
-    deepest = std::max(deepest, maxr);
+    A.deepest = std::max(A.deepest, maxr);
     for (int64_t r = maxr; r >= 0; --r)
       k_wb_delta<<<g_delta, 256, 0, st>>>(off, col, w, tnode, tbeg, ntasks, dist, sigma, delta, round, src, ns, bcl,
                                        (uint32_t)r);
     ZOGCU_CUDA(cudaGetLastError());
-    launches += (uint64_t)maxr + 1;
+    A.launches += (uint64_t)maxr + 1;
+    return ZOGCU_OK;
+  };
+  {
+    int device = 0;
+    ZOGCU_CUDA(cudaGetDevice(&device));
+    auto lane_run = [&](int l) {
+      if (cudaSetDevice(device) != cudaSuccess) {
+        L[l].status = ZOGCU_ERR_CUDA;
+        L[l].error = "weighted betweenness: lane thread could not select the device";
+        return;
+      }
+      for (size_t bi = (size_t)l; bi < nbatches; bi += (size_t)nlanes) {
+        const int rc = run_batch(l, bi);
+        if (rc != ZOGCU_OK) {
+          L[l].status = rc;
+          L[l].error = zogcu_last_error();  // the message is kept per thread
+          return;
+        }
+      }
+    };
+    std::vector<std::thread> th;
+    for (int l = 1; l < nlanes; ++l) th.emplace_back(lane_run, l);
+    lane_run(0);
+    for (auto& t : th) t.join();
   }
-  if (nlanes == 2) {  // the second lane's scores into the first's, on stream s
-    ZOGCU_CUDA(cudaEventRecord(ev, ls[1]));
-    ZOGCU_CUDA(cudaStreamWaitEvent(s, ev, 0));
-    k_wb_add<<<wb_grid(Vs / 32 + 1), 256, 0, s>>>(bcv[0].as<double>(), bcv[1].as<double>(), V);
+  for (int l = 0; l < nlanes; ++l)
+    if (L[l].status != ZOGCU_OK) return fail(L[l].status, L[l].error);
+  uint64_t launches = 0;
+  uint32_t deepest = 0;
+  for (int l = 0; l < nlanes; ++l) {
+    launches += L[l].launches;
+    deepest = std::max(deepest, L[l].deepest);
+  }
+  // the lanes' scores into the first lane's, in lane order, on stream s
+  for (int l = 0; l < nlanes; ++l) {
+    ZOGCU_TRY(lane_done[l].init());
+    ZOGCU_CUDA(cudaEventRecord(lane_done[l].e, ls[l]));
+    ZOGCU_CUDA(cudaStreamWaitEvent(s, lane_done[l].e, 0));
+  }
+  for (int l = 1; l < nlanes; ++l) {
+    k_wb_add<<<wb_grid(Vs / 32 + 1), 256, 0, s>>>(bcv[0].as<double>(), bcv[l].as<double>(), V);
     ZOGCU_CUDA(cudaGetLastError());
     ++launches;
   }
   ZOGCU_TRY(tm.stop(s));
-  uint32_t ovf[2] = {0, 0};
+  uint32_t ovf[kWbMaxLanes] = {};
   for (int l = 0; l < nlanes; ++l)
     ZOGCU_CUDA(cudaMemcpyAsync(&ovf[l], L[l].bflags.as<uint32_t>() + kFlagOverflow, 4, cudaMemcpyDeviceToHost, s));
   if (V)
@@ -472,7 +529,9 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
     stats->sources = sources.size();
     stats->elapsed_ms = tm.ms();
     stats->max_depth = deepest;
-    stats->sigma_overflow = (ovf[0] | ovf[1]) ? 1u : 0u;
+    uint32_t any = 0;
+    for (int l = 0; l < nlanes; ++l) any |= ovf[l];
+    stats->sigma_overflow = any ? 1u : 0u;
     stats->launches = launches;
   }
   return ZOGCU_OK;
