@@ -14,7 +14,7 @@ the network has seen the sizes it is used on; targets are FP64 PageRank
 vectors the plain GPU method computes to L1 1e-9.  Every step of training
 (forward, backward, Adam) runs in the library's own CUDA kernels.
 
-    python -m zog_b200.warm_start --graphs 2000 --large 96 --epochs 8 --out zog_b200/data/warm_start.zogn
+    python -m zog_b200.warm_start --graphs 2000 --large 256 --epochs 24 --out zog_b200/data/warm_start.zogn
 """
 from __future__ import annotations
 
@@ -206,8 +206,8 @@ def time_inference(scale: int, reps: int) -> list:
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--graphs", type=int, default=2000)
-    ap.add_argument("--large", type=int, default=96, help="extra graphs of 2^19-2^22 nodes")
-    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--large", type=int, default=256, help="extra graphs of 2^19-2^22 nodes")
+    ap.add_argument("--epochs", type=int, default=24)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--init-seed", type=int, default=1)
