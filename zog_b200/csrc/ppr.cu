@@ -48,7 +48,7 @@ struct PprState {
 
 template <int S>
 struct PprArgs {
-  static_assert(S % 64 == 0 && S <= 256, "columns per pass: 64, 128 or 256");
+  static_assert(S % 32 == 0 && S <= 256, "columns per pass: 32, 64, 128 or 256");
   const uint32_t* off;     // ranked in-CSR offsets
   const uint32_t* col;     // ranked source ids, ascending original id per row
   const uint32_t* deg;     // out-degree by rank
@@ -81,7 +81,9 @@ struct PprArgs {
 // never re-read by this warp.
 template <int PL>
 __device__ __forceinline__ void ld_row(const double* p, double (&v)[PL]) {
-  if constexpr (PL % 4 == 0) {
+  if constexpr (PL == 1) {
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v[0]) : "l"(p));
+  } else if constexpr (PL % 4 == 0) {
 #pragma unroll
     for (int q = 0; q < PL / 4; ++q)
       asm volatile("ld.global.nc.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];"
@@ -134,6 +136,27 @@ __device__ __forceinline__ void ppr_epilogue(const PprArgs<S>& A, uint32_t r, in
   constexpr int PL = S / 32;
   const uint32_t d = __ldg(A.deg + r);
   const size_t base = (size_t)r * S + c0;
+  if constexpr (PL == 1) {  // one column per lane
+    const double xold = X[base];
+    double xn = xold, cn;
+    if (act_bits & 1u) {
+      const double tele = seed[0] == r ? 1.0 - A.damping : 0.0;
+      const double v = __dadd_rn(tele, __dmul_rn(A.damping, __dadd_rn(sink[0], acc[0])));
+      l1p[0] += fabs(v - xold);
+      xn = v;
+      if (d == 0) {
+        cn = 0.0;
+        dgp[0] += __ddiv_rn(v, A.n_f);
+      } else {
+        cn = __ddiv_rn(v, (double)d);
+      }
+    } else {  // a stopped seed: carry its vector over unchanged
+      cn = Cc[base];
+    }
+    Xn[base] = xn;
+    Cn[base] = cn;
+    return;
+  }
 #pragma unroll
   for (int q = 0; q < PL / 2; ++q) {
     const double2 xo = *reinterpret_cast<const double2*>(X + base + 2 * q);
@@ -520,19 +543,19 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   // at scale 18).
   PprHost H;
   ZOGCU_TRY(H.load(g, s));
-  uint32_t width = V < (1u << 19) ? 256u : 64u;  // ZOGCU_PPR_PASS=64/128/256 overrides
+  uint32_t width = V < (1u << 19) ? 256u : 64u;  // ZOGCU_PPR_PASS=32/64/128/256 overrides
   if (const char* e = std::getenv("ZOGCU_PPR_PASS")) {
     const int w = std::atoi(e);
-    if (w == 64 || w == 128 || w == 256) width = (uint32_t)w;
+    if (w == 32 || w == 64 || w == 128 || w == 256) width = (uint32_t)w;
   }
   const uint32_t npass = (num_seeds + width - 1) / width;
   std::vector<PprPass> passes(npass);
-  int max_S = 64;
+  int max_S = 32;
   for (uint32_t p = 0; p < npass; ++p) {
     PprPass& P = passes[p];
     P.first = p * width;
     P.ns = std::min<uint32_t>(num_seeds - P.first, width);
-    P.S = P.ns > 128 ? 256 : P.ns > 64 ? 128 : 64;
+    P.S = P.ns > 128 ? 256 : P.ns > 64 ? 128 : (P.ns > 32 || width > 32) ? 64 : 32;
     max_S = std::max(max_S, P.S);
   }
   PprShared M;
@@ -543,7 +566,8 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
     P.dst = (dev_out ? out_scores : res.as<double>()) + (size_t)P.first * V;
     if (P.S == 256) ZOGCU_TRY(ppr_pass_setup<256>(H, seeds, P, s));
     else if (P.S == 128) ZOGCU_TRY(ppr_pass_setup<128>(H, seeds, P, s));
-    else ZOGCU_TRY(ppr_pass_setup<64>(H, seeds, P, s));
+    else if (P.S == 64) ZOGCU_TRY(ppr_pass_setup<64>(H, seeds, P, s));
+    else ZOGCU_TRY(ppr_pass_setup<32>(H, seeds, P, s));
   }
   // the call's graph: every pass after the previous one
   cudaGraph_t graph = nullptr;
@@ -556,7 +580,8 @@ extern "C" int zogcu_ppr(zogcu_graph* G, const uint32_t* seeds, uint32_t num_see
   for (PprPass& P : passes) {
     if (P.S == 256) ZOGCU_TRY(ppr_pass_nodes<256>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
     else if (P.S == 128) ZOGCU_TRY(ppr_pass_nodes<128>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
-    else ZOGCU_TRY(ppr_pass_nodes<64>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
+    else if (P.S == 64) ZOGCU_TRY(ppr_pass_nodes<64>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
+    else ZOGCU_TRY(ppr_pass_nodes<32>(graph, &tail, g, M, P, damping, max_iterations, tolerance));
   }
   cudaGraphExec_t exec = nullptr;
   ZOGCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
