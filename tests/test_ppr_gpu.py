@@ -61,6 +61,25 @@ def test_ppr_many_passes_hub_rows_and_repeated_seeds(native, oracle):
         G.destroy()
 
 
+@pytest.mark.parametrize("width", [32, 64, 128, 256])
+def test_ppr_every_pass_width(native, oracle, monkeypatch, width):
+    """Each kernel width (ZOGCU_PPR_PASS) over 100 seeds, with a hub row long
+    enough to be cut into chunks: several passes at the narrow widths and a
+    partial last pass, every sampled seed against the oracle."""
+    monkeypatch.setenv("ZOGCU_PPR_PASS", str(width))
+    V, f, t = oracle.rmat(11, 6, 11, directed=True)
+    hub_src = np.arange(1, 6001, dtype=np.uint32) % V
+    f2 = np.concatenate([f, hub_src]).astype(np.uint32)
+    t2 = np.concatenate([t, np.full(6000, 9, np.uint32)]).astype(np.uint32)
+    G = native.Graph.from_edges(V, f2, t2)
+    try:
+        seeds = np.random.default_rng(width).choice(V, 100, replace=False).astype(np.uint32)
+        seeds[3] = 9  # the hub
+        check_seeds(native, oracle, G, seeds, sample=[0, 3, 31, 32, 63, 64, 99])
+    finally:
+        G.destroy()
+
+
 def test_ppr_iteration_cap_and_errors(native, oracle):
     V, f, t = oracle.rmat(9, 8, 9, directed=True)
     G = native.Graph.from_edges(V, f, t)
