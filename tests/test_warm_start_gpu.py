@@ -186,9 +186,11 @@ def test_shipped_weights_gain_over_uniform_start(native):
 
 
 def test_tcgen05_inference_matches_mma_sync(native, oracle, monkeypatch):
-    """The tensor-memory inference kernels (ZOGCU_GNN_TC=1) against the
-    mma.sync ones and the oracle: both compute the same products in another
-    accumulation order, so outputs agree to the BF16 tolerances above."""
+    """The tensor-memory inference kernels against the mma.sync ones and the
+    oracle: the one-tile kernels (ZOGCU_GNN_TC=1) and the four-slot ones
+    (ZOGCU_GNN_TC=2) compute the same products in another accumulation order
+    than mma.sync, so outputs agree to the BF16 tolerances above; the two
+    tcgen05 forms run the same products and agree bit for bit."""
     net = native.WarmStart.create(13)
     try:
         net.set_params(perturbed_params(13))
@@ -210,6 +212,10 @@ def test_tcgen05_inference_matches_mma_sync(native, oracle, monkeypatch):
                 y_ref, _ = GO.forward(p, csr_of(G))
                 assert np.abs(y_t - y_ref).max() <= Y_TOL * (1 + np.abs(y_ref).max()), name
                 assert abs(x_t.sum() - 1.0) < 1e-12
+                monkeypatch.setenv("ZOGCU_GNN_TC", "2")
+                x_q, y_q = net.predict(G, raw=True)
+                assert np.array_equal(y_q, y_t), (name, np.abs(y_q - y_t).max())
+                assert np.array_equal(x_q, x_t), name
             finally:
                 G.destroy()
     finally:

@@ -1184,6 +1184,264 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_infer_tc(const float* __r
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols) : "memory");
 }
 
+// ---- inference on tcgen05 with four tiles in flight per SM ---------------------
+// The products and epilogues of k_gnn_infer_tc, scheduled so that the tensor
+// core and the epilogue overlap: one CTA of two warpgroups per SM, each
+// warpgroup driving two 128-node tiles ("slots") with their own TMEM columns
+// (128 each, 512 in all), operand tiles and mbarrier.  A warpgroup visits its
+// slots in turn: it waits for the slot's MMAs, reads the accumulators, runs
+// the epilogue, writes the next operand and issues the next MMAs, then moves
+// to the other slot while those run.  A slot's inputs for its next stage (the
+// next aggregate, or the next tile's features) are loaded right after its MMAs
+// are issued.  Weights sit in shared memory once per CTA.
+constexpr int kTc2Threads = 256;
+constexpr uint32_t kTc2Cols = 512;
+
+__host__ __device__ constexpr uint32_t tc2_smem_bytes(int L) {
+  // 4 slots x (H, AG), B0, (Ws, Wn) per layer 1..L, U, bias, head, 4 mbarriers + TMEM address
+  return 8 * kTileBytes128 + kWTileBytes + 2 * kWTileBytes * (uint32_t)L + kUTileBytes + (uint32_t)(L + 1) * kH * 4 +
+         (kH + 1) * 4 + 64;
+}
+
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;\n" ::"r"(1 + wg) : "memory"); }
+// 1 when v holds in every thread of the warpgroup (a named-barrier reduction)
+__device__ __forceinline__ int wg_all(int wg, int v) {
+  int r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.s32 q, %1, 0;\n barrier.cta.red.and.pred p, %2, 128, q;\n selp.s32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"(v), "r"(1 + wg)
+      : "memory");
+  return r;
+}
+
+template <int L>
+__global__ void __launch_bounds__(kTc2Threads, 1) k_gnn_infer_tc2(const float* __restrict__ F,
+                                                                   const float* __restrict__ A0,
+                                                                   const float* __restrict__ A1,
+                                                                   const float* __restrict__ A2,
+                                                                   const __nv_bfloat16* __restrict__ w,
+                                                                   const float* __restrict__ inv, uint32_t V,
+                                                                   uint32_t ntiles, __nv_bfloat16* __restrict__ M_next,
+                                                                   float* __restrict__ y, unsigned int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t a0 = smem_u32(smem_raw);
+  unsigned char* base = smem_raw + (((a0 + 1023u) & ~1023u) - a0);
+  unsigned char* tB0 = base + 8 * kTileBytes128;
+  uint32_t off = 8 * kTileBytes128 + kWTileBytes;
+  unsigned char* tBs[3] = {nullptr, nullptr, nullptr};
+  unsigned char* tBn[3] = {nullptr, nullptr, nullptr};
+#pragma unroll
+  for (int l = 1; l <= L; ++l) {
+    tBs[l] = base + off;
+    off += kWTileBytes;
+    tBn[l] = base + off;
+    off += kWTileBytes;
+  }
+  unsigned char* tBu = base + off;
+  off += kUTileBytes;
+  float* s_bias = reinterpret_cast<float*>(base + off);
+  off += (L + 1) * kH * 4;
+  float* s_wo = reinterpret_cast<float*>(base + off);
+  off += (kH + 1) * 4;
+  off = (off + 7u) & ~7u;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + off);  // one per slot
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(base + off + 32);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 64 * 64; i += kTc2Threads) {
+    const uint32_t n = (uint32_t)i / 64, k = (uint32_t)i % 64;
+    if (k < 16) {
+      const float v = k < (uint32_t)kF ? __bfloat162float(w[ws_offset(0) + k * kH + n])
+                      : k < 2u * kF   ? __bfloat162float(w[wn_offset(0) + (k - kF) * kH + n])
+                                      : 0.f;
+      put_w(tB0, n, k, v);
+    }
+#pragma unroll
+    for (int l = 1; l <= L; ++l) {
+      put_w(tBs[l], n, k, __bfloat162float(w[ws_offset(l) + k * kH + n]));
+      if (k < 16) put_w(tBn[l], n, k, k < (uint32_t)kR ? __bfloat162float(w[wn_offset(l) + k * kH + n]) : 0.f);
+    }
+    if (L < kLayers - 1 && n < 16) put_w(tBu, n, k, n < (uint32_t)kR ? __bfloat162float(w[layer_offset(L + 1) + k * kR + n]) : 0.f);
+  }
+  for (int i = tid; i < (L + 1) * kH; i += kTc2Threads) s_bias[i] = __bfloat162float(w[bias_offset(i / kH) + i % kH]);
+  for (int i = tid; i <= kH; i += kTc2Threads) s_wo[i] = __bfloat162float(w[kHeadOffset + i]);
+  if (tid == 0) {
+    for (int q = 0; q < 4; ++q) mbar_init(&bars[q], 1);
+    mbar_fence_init();
+  }
+  if ((tid >> 5) == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(s_tmem)),
+                 "r"(kTc2Cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const int wg = tid >> 7, t = tid & 127;
+  const bool leader = t == 0;
+  const uint32_t lane_off = (uint32_t)(((tid >> 5) & 3) * 32) << 16;  // this warp's TMEM lane quarter
+  const uint32_t sB0 = smem_u32(tB0), sBu = smem_u32(tBu);
+  const uint32_t nslots = gridDim.x * 4;
+  // per-slot state (slot j of this warpgroup is CTA slot q = 2 wg + j); the
+  // loops over j are unrolled, so these stay in registers
+  uint32_t tile[2] = {0u, 0u}, stage[2] = {0u, 0u}, phase[2] = {0u, 0u};
+  bool live[2] = {false, false};
+  float4 pf[2][2] = {};  // inputs of the slot's next stage: [A_l] or the next tile's [F, A_0]
+  float pinv[2] = {0.f, 0.f};
+  bool ok = true;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto load2 = [&](const float* p, uint32_t row, int width, float4& u, float4& v) {
+    // width 4: one float4 (F or A_0, in u); width 8: two (an 8-wide aggregate)
+    u = v = z4;
+    if (row >= V) return;
+    if (width == 4) {
+      u = __ldg(reinterpret_cast<const float4*>(p) + row);
+    } else {
+      u = __ldg(reinterpret_cast<const float4*>(p + (size_t)row * kR));
+      v = __ldg(reinterpret_cast<const float4*>(p + (size_t)row * kR + 4));
+    }
+  };
+  // a tile's first operand [F | A_0 | 0] from the prefetched inputs, then its layer-0 MMA
+  auto start_tile = [&](int j) {
+    const int q = 2 * wg + j;
+    unsigned char* tAG = base + (2 * q + 1) * kTileBytes128;
+    const float4 f = pf[j][0], a = pf[j][1];
+    put_chunk(tAG, t, 0, make_uint4(pack_bf16x2(f.x, f.y), pack_bf16x2(f.z, f.w), pack_bf16x2(a.x, a.y),
+                                    pack_bf16x2(a.z, a.w)));
+    put_chunk(tAG, t, 1, make_uint4(0u, 0u, 0u, 0u));
+    fence_async_smem();
+    tc_fence_before();
+    wg_sync(wg);
+    tc_fence_after();
+    if (leader) {
+      tc_mma(tmem + (uint32_t)q * 128u, sw128_desc(smem_u32(tAG)), sw128_desc(sB0), tc_idesc(64), 0);
+      tc_commit(&bars[q]);
+    }
+    stage[j] = 0;
+    const uint32_t row = tile[j] * kTcRows + (uint32_t)t;
+    if (L >= 1) {
+      load2(A1, row, 8, pf[j][0], pf[j][1]);
+    } else {  // layer 0 is the last hidden layer: the next tile's features, this row's scale
+      const uint32_t nrow = (tile[j] + nslots) * kTcRows + (uint32_t)t;
+      float4 dummy;
+      load2(F, nrow, 4, pf[j][0], dummy);
+      load2(A0, nrow, 4, pf[j][1], dummy);
+      pinv[j] = row < V ? __ldg(inv + row) : 0.f;
+    }
+  };
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    tile[j] = (uint32_t)(blockIdx.x * 4 + 2 * wg + j);
+    live[j] = tile[j] < ntiles;
+    if (live[j]) {
+      float4 dummy;
+      const uint32_t row = tile[j] * kTcRows + (uint32_t)t;
+      load2(F, row, 4, pf[j][0], dummy);
+      load2(A0, row, 4, pf[j][1], dummy);
+      start_tile(j);
+    }
+  }
+  while (ok && (live[0] || live[1])) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (!ok || !live[j]) continue;
+      const int q = 2 * wg + j;
+      unsigned char* tH = base + (2 * q) * kTileBytes128;
+      unsigned char* tAG = tH + kTileBytes128;
+      const uint32_t col = tmem + (uint32_t)q * 128u;
+      ok = wg_all(wg, mbar_wait(&bars[q], phase[j]) ? 1 : 0) != 0;
+      phase[j] ^= 1u;
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t taddr = col + lane_off;
+      const uint32_t row = tile[j] * kTcRows + (uint32_t)t;
+      const bool valid = row < V;
+      bool done = false;
+      if (stage[j] <= (uint32_t)L) {  // hidden layer stage[j] is in the accumulators
+        uint32_t hp[32];
+        tc_layer_out(taddr, s_bias + stage[j] * kH, hp);
+        if (stage[j] < (uint32_t)L) {  // operands of layer stage+1: H and [A_(stage+1) | 0]
+          const uint32_t l = stage[j] + 1;
+          // the slot's last MMAs are complete (its mbarrier), so its operand
+          // tiles are free; the barrier below orders every thread's reads of
+          // the accumulators before the next MMAs overwrite them
+#pragma unroll
+          for (int c = 0; c < 8; ++c) put_chunk(tH, t, c, make_uint4(hp[4 * c], hp[4 * c + 1], hp[4 * c + 2], hp[4 * c + 3]));
+          const float4 x0 = pf[j][0], x1 = pf[j][1];
+          put_chunk(tAG, t, 0, make_uint4(pack_bf16x2(x0.x, x0.y), pack_bf16x2(x0.z, x0.w), pack_bf16x2(x1.x, x1.y),
+                                          pack_bf16x2(x1.z, x1.w)));
+          fence_async_smem();
+          tc_fence_before();
+          wg_sync(wg);
+          tc_fence_after();
+          if (leader) {
+            const uint32_t sBs = smem_u32(l == 1 ? tBs[1] : tBs[L]), sBn = smem_u32(l == 1 ? tBn[1] : tBn[L]);
+            const uint32_t sH = smem_u32(tH), sAG = smem_u32(tAG);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) tc_mma(col, sw128_desc(sH + 32 * k), sw128_desc(sBs + 32 * k), tc_idesc(64), k > 0);
+            tc_mma(col, sw128_desc(sAG), sw128_desc(sBn), tc_idesc(64), 1);
+            tc_commit(&bars[q]);
+          }
+          stage[j] = l;
+          if (l < (uint32_t)L) {
+            load2(A2, row, 8, pf[j][0], pf[j][1]);
+          } else {  // the last hidden layer is running: the next tile's features, this row's scale
+            const uint32_t nrow = (tile[j] + nslots) * kTcRows + (uint32_t)t;
+            float4 dummy;
+            load2(F, nrow, 4, pf[j][0], dummy);
+            load2(A0, nrow, 4, pf[j][1], dummy);
+            pinv[j] = valid ? __ldg(inv + row) : 0.f;
+          }
+        } else if (L < kLayers - 1) {  // the message product H U_(L+1)
+#pragma unroll
+          for (int c = 0; c < 8; ++c) put_chunk(tH, t, c, make_uint4(hp[4 * c], hp[4 * c + 1], hp[4 * c + 2], hp[4 * c + 3]));
+          fence_async_smem();
+          tc_fence_before();
+          wg_sync(wg);
+          tc_fence_after();
+          if (leader) {
+            const uint32_t sH = smem_u32(tH);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) tc_mma(col + 64, sw128_desc(sH + 32 * k), sw128_desc(sBu + 32 * k), tc_idesc(16), k > 0);
+            tc_commit(&bars[q]);
+          }
+          stage[j] = (uint32_t)L + 1;
+        } else {  // the head
+          float acc = 0.f;
+#pragma unroll
+          for (int i = 0; i < 32; ++i) acc += bf16_lo(hp[i]) * s_wo[2 * i] + bf16_hi(hp[i]) * s_wo[2 * i + 1];
+          if (valid) y[row] = acc + s_wo[kH];
+          done = true;
+        }
+      } else {  // the message accumulators
+        float m[8];
+        tc_ld8(taddr + 64, m);
+        tc_wait_ld();
+        if (valid) {
+          const float sc = pinv[j];
+          *reinterpret_cast<uint4*>(M_next + (size_t)row * kR) =
+              make_uint4(pack_bf16x2(m[0] * sc, m[1] * sc), pack_bf16x2(m[2] * sc, m[3] * sc),
+                         pack_bf16x2(m[4] * sc, m[5] * sc), pack_bf16x2(m[6] * sc, m[7] * sc));
+        }
+        done = true;
+      }
+      if (done) {  // the slot's next tile (start_tile's barrier orders the accumulator reads)
+        tile[j] += nslots;
+        live[j] = tile[j] < ntiles;
+        if (live[j]) start_tile(j);
+      }
+    }
+  }
+  if (!ok && t == 0) atomicExch(err, 1u);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if ((tid >> 5) == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTc2Cols) : "memory");
+}
+
 // ---- dense layer backward (data): dP = dOut * (Out > 0); dX = dP Ws^T (DIN),
 // dA = dP Wn^T (DM) (the BF16 roundings of the forward operands pass the
 // gradient straight through).  dP is written back in place of dOut for the
@@ -1704,9 +1962,11 @@ int aggregate(const GView& gv, const T* X, float* Z, size_t zrows, uint32_t* ctr
 // The tcgen05 inference kernels: dynamic shared memory of at least 60 KB so
 // that at most three CTAs share an SM (their 3 x 128 TMEM columns fit the
 // SM's 512); ZOGCU_GNN_TC=1 selects them (the mma.sync kernels otherwise).
-bool gnn_use_tc() {
+// 0: the mma.sync kernels; 1: the one-tile tcgen05 kernels; 2: the four-slot
+// tcgen05 kernels (ZOGCU_GNN_TC)
+int gnn_tc_mode() {
   const char* e = std::getenv("ZOGCU_GNN_TC");
-  return e && e[0] == '1';
+  return (e && (e[0] == '1' || e[0] == '2')) ? e[0] - '0' : 0;
 }
 
 template <int L>
@@ -1724,6 +1984,27 @@ int launch_infer_tc(const float* F, const float* A0, const float* A1, const floa
   const uint32_t ntiles = (V + kTcRows - 1) / kTcRows;
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, (uint64_t)sm_count() * per_sm));
   k_gnn_infer_tc<L><<<grid, kTcThreads, smem, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M_next, y, err);
+  ZOGCU_CUDA(cudaGetLastError());
+  return ZOGCU_OK;
+}
+
+// The four-slot tcgen05 kernels: one CTA per SM (its shared memory allows no
+// second one), which owns all 512 TMEM columns.
+template <int L>
+int launch_infer_tc2(const float* F, const float* A0, const float* A1, const float* A2, const __nv_bfloat16* w,
+                     const float* inv, uint32_t V, __nv_bfloat16* M_next, float* y, unsigned int* err, cudaStream_t s) {
+  static bool checked = false;  // per template instance
+  const uint32_t smem = tc2_smem_bytes(L) + 1024;
+  if (!checked) {
+    ZOGCU_CUDA(cudaFuncSetAttribute(k_gnn_infer_tc2<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int n = 0;
+    ZOGCU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_gnn_infer_tc2<L>, kTc2Threads, smem));
+    if (n != 1) return fail(ZOGCU_ERR_INTERNAL, "four-slot tcgen05 kernel must run one CTA per SM");
+    checked = true;
+  }
+  const uint32_t ntiles = (V + kTcRows - 1) / kTcRows;
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ntiles + 3) / 4, (uint64_t)sm_count()));
+  k_gnn_infer_tc2<L><<<grid, kTc2Threads, smem, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M_next, y, err);
   ZOGCU_CUDA(cudaGetLastError());
   return ZOGCU_OK;
 }
@@ -1749,26 +2030,30 @@ int gnn_forward(const zogcu_gnn* M, const GView& g, GnnActs& act, bool train, cu
     const float* A0 = act.A[0].as<float>();
     const float* A1 = act.A[1].as<float>();
     const float* A2 = act.A[2].as<float>();
-    const bool tc = gnn_use_tc();
+    const int tcm = gnn_tc_mode();
+    const bool tc = tcm != 0;
     __nv_bfloat16* M1 = act.M[1].as<__nv_bfloat16>();
     __nv_bfloat16* M2 = act.M[2].as<__nv_bfloat16>();
     float* yv = act.y.as<float>();
     if (tc) {
-      ZOGCU_TRY(launch_infer_tc<0>(F, A0, A1, A2, w, inv, V, M1, nullptr, err, s));
+      if (tcm == 2) ZOGCU_TRY(launch_infer_tc2<0>(F, A0, A1, A2, w, inv, V, M1, nullptr, err, s));
+      else ZOGCU_TRY(launch_infer_tc<0>(F, A0, A1, A2, w, inv, V, M1, nullptr, err, s));
     } else {
       k_gnn_infer<0><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M1, nullptr);
       ZOGCU_CUDA(cudaGetLastError());
     }
     ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, M1, act.A[1].as<float>(), act.Vp, ctr, act.rows, s)));
     if (tc) {
-      ZOGCU_TRY(launch_infer_tc<1>(F, A0, A1, A2, w, inv, V, M2, nullptr, err, s));
+      if (tcm == 2) ZOGCU_TRY(launch_infer_tc2<1>(F, A0, A1, A2, w, inv, V, M2, nullptr, err, s));
+      else ZOGCU_TRY(launch_infer_tc<1>(F, A0, A1, A2, w, inv, V, M2, nullptr, err, s));
     } else {
       k_gnn_infer<1><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, M2, nullptr);
       ZOGCU_CUDA(cudaGetLastError());
     }
     ZOGCU_TRY((aggregate<__nv_bfloat16, kR>(g, M2, act.A[2].as<float>(), act.Vp, ctr, act.rows, s)));
     if (tc) {
-      ZOGCU_TRY(launch_infer_tc<2>(F, A0, A1, A2, w, inv, V, nullptr, yv, err, s));
+      if (tcm == 2) ZOGCU_TRY(launch_infer_tc2<2>(F, A0, A1, A2, w, inv, V, nullptr, yv, err, s));
+      else ZOGCU_TRY(launch_infer_tc<2>(F, A0, A1, A2, w, inv, V, nullptr, yv, err, s));
     } else {
       k_gnn_infer<2><<<ig, kInferWarps * 32, 0, s>>>(F, A0, A1, A2, w, inv, V, ntiles, nullptr, yv);
       ZOGCU_CUDA(cudaGetLastError());
