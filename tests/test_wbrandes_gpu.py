@@ -94,3 +94,30 @@ def test_bad_weights_are_rejected(native):
                 G.betweenness_weighted()
         finally:
             G.destroy()
+
+
+def test_zero_length_arc_reported_from_a_lane(native, monkeypatch):
+    """An arc of effective length zero on a shortest path (fl(d + w) == d)
+    makes the reference's sigma depend on its heap's tie order, so it is an
+    error.  The check runs inside the batches, which lanes with their own host
+    threads drive: with 160 sources (five batches over four lanes) and the
+    error in a worker thread's batch, the status and the message must still
+    reach the caller, and the call must end."""
+    monkeypatch.setenv("ZOGCU_BC_STREAMS", "4")
+    n = 160
+    # nodes 0-31 (the first batch, lane 0 on the calling thread) are isolated;
+    # a chain 32 -> 33 -> ... -> 159 with the arc 40 -> 41 of weight 1e20, so
+    # only sources 32-40 (the second batch, lane 1 on a worker thread) see
+    # fl(d(41) + 1) == d(41) on the shortest path to 42
+    f = np.arange(32, n - 1).astype(np.uint32)
+    t = (f + 1).astype(np.uint32)
+    w = np.ones(f.size)
+    w[40 - 32] = 1e20
+    G = native.Graph.from_edges(n, f, t, w)
+    try:
+        with pytest.raises(native.ZogCudaError) as ei:
+            G.betweenness_weighted()
+        assert ei.value.status == 1
+        assert "effective length zero" in str(ei.value)
+    finally:
+        G.destroy()

@@ -38,6 +38,7 @@
 // on its heap's tie order; weights must be positive and finite, and such an
 // arc is reported as an error instead of guessed at.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -478,17 +479,20 @@ int run_weighted(Graph* g, const std::vector<uint32_t>& sources, double* out, bo
   {
     int device = 0;
     ZOGCU_CUDA(cudaGetDevice(&device));
+    std::atomic<bool> stop{false};  // a lane failed: the others stop after their current batch
     auto lane_run = [&](int l) {
       if (cudaSetDevice(device) != cudaSuccess) {
         L[l].status = ZOGCU_ERR_CUDA;
         L[l].error = "weighted betweenness: lane thread could not select the device";
+        stop = true;
         return;
       }
-      for (size_t bi = (size_t)l; bi < nbatches; bi += (size_t)nlanes) {
+      for (size_t bi = (size_t)l; bi < nbatches && !stop; bi += (size_t)nlanes) {
         const int rc = run_batch(l, bi);
         if (rc != ZOGCU_OK) {
           L[l].status = rc;
           L[l].error = zogcu_last_error();  // the message is kept per thread
+          stop = true;
           return;
         }
       }
