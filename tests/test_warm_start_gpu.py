@@ -221,3 +221,37 @@ def test_tcgen05_inference_matches_mma_sync(native, oracle, monkeypatch):
     finally:
         monkeypatch.delenv("ZOGCU_GNN_TC", raising=False)
         net.destroy()
+
+
+def test_async_and_register_staged_aggregation(native, oracle, monkeypatch):
+    """The aggregate with its gathers copied straight to shared memory
+    (cp.async, the default) and the register-staged one (ZOGCU_GNN_AGG_ASYNC=0)
+    against the oracle and each other, on graphs with hub rows that span many
+    128-arc chunks: their partial sums meet through atomics in either order,
+    and a last-bit difference can flip a BF16 rounding of the aggregate, so
+    the two agree to the BF16 tolerances above, not bit for bit."""
+    net = native.WarmStart.create(21)
+    try:
+        net.set_params(perturbed_params(21))
+        p = net.get_params()
+        graphs = list(sample_graphs(native, oracle))
+        V, f, t = oracle.rmat(14, 8, 1014, directed=True)
+        graphs.append(("rmat14", native.Graph.from_edges(V, f, t)))
+        for name, G in graphs:
+            try:
+                y_ref, _ = GO.forward(p, csr_of(G))
+                ys = {}
+                for mode in ("1", "0"):
+                    monkeypatch.setenv("ZOGCU_GNN_AGG_ASYNC", mode)
+                    x, y = net.predict(G, raw=True)
+                    assert np.abs(y - y_ref).max() <= Y_TOL * (1 + np.abs(y_ref).max()), (name, mode)
+                    assert abs(x.sum() - 1.0) < 1e-12
+                    ys[mode] = y
+                scale = 1 + np.abs(ys["0"]).max()
+                assert np.abs(ys["1"] - ys["0"]).max() <= Y_TOL * scale, name
+                assert np.abs(ys["1"] - ys["0"]).mean() <= Y_MEAN_TOL * scale, name
+            finally:
+                G.destroy()
+    finally:
+        monkeypatch.delenv("ZOGCU_GNN_AGG_ASYNC", raising=False)
+        net.destroy()

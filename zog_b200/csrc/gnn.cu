@@ -433,6 +433,134 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16(const uint32_t* __
   }
 }
 
+// ---- the same aggregate with the gathers copied straight to shared memory ----
+// cp.async.cg (16 bytes, through L2 only) puts each message in the warp's
+// staging tile with no register round trip and no separate shared-memory
+// store; three tiles per warp keep two chunks' gathers in flight while a third
+// chunk is summed.  Chunking, row ranges and row sums are k_gnn_agg16's; the
+// results differ only where both differ from run to run, in the order of the
+// atomic adds of rows spanning three or more chunks.
+constexpr int kAggStages = 3;
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(kAggWarps * 32) k_gnn_agg16_async(const uint32_t* __restrict__ off,
+                                                                    const uint32_t* __restrict__ col,
+                                                                    const T* __restrict__ X, uint32_t V, uint32_t E,
+                                                                    float* __restrict__ Z,
+                                                                    const uint32_t* __restrict__ first_row) {
+  constexpr int PER = 16 / (int)sizeof(T);
+  constexpr int K = (int)kAggChunk / 32;  // messages per lane and chunk
+  static_assert(PER == D, "one 16-byte message per arc");
+  __shared__ __align__(16) uint4 s_stage[kAggWarps][kAggStages][kAggChunk];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint4* __restrict__ X16 = reinterpret_cast<const uint4*>(X);
+  const uint64_t pol_idx = l2_evict_first();
+  const uint32_t nchunks = (uint32_t)(((uint64_t)E + kAggChunk - 1) / kAggChunk);
+  const uint32_t nwarps = gridDim.x * kAggWarps;
+  uint32_t next = blockIdx.x * kAggWarps + warp;
+  auto take = [&]() {
+    const uint32_t c = next;
+    next += nwarps;
+    return c;
+  };
+  // chunk c's messages into stage tile b (copies issued, completed later)
+  auto issue = [&](uint32_t c, int b) {
+    const uint32_t cs = c * kAggChunk, ce = min(cs + kAggChunk, E);
+    uint4* st = s_stage[warp][b];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const uint32_t j = cs + lane + 32 * k;
+      if (j < ce) cp_async16(st + lane + 32 * k, X16 + ld_index(col + j, pol_idx));
+    }
+  };
+  auto row_range = [&](uint32_t r0, uint32_t& rb, uint32_t& re) {
+    const uint32_t ri = r0 + lane;
+    rb = ri < V ? __ldg(off + ri) : E;
+    re = ri < V ? __ldg(off + ri + 1) : E;
+  };
+  // the pipeline holds chunk c (summed next), c1 and c2; each chunk's first
+  // row is loaded two chunks ahead and its first 32 row ranges one ahead
+  uint32_t c = take(), c1 = take();
+  uint32_t r0c = 0, rbc = E, rec = E, r0n = 0;
+  if (c < nchunks) {
+    issue(c, 0);
+    r0c = __ldg(first_row + c);
+    row_range(r0c, rbc, rec);
+  }
+  cp_async_commit();
+  if (c1 < nchunks) {
+    issue(c1, 1);
+    r0n = __ldg(first_row + c1);
+  }
+  cp_async_commit();
+  int b = 0;
+  while (c < nchunks) {
+    const uint32_t c2 = take();
+    if (c2 < nchunks) issue(c2, b == 0 ? 2 : b - 1);  // the tile summed last time
+    cp_async_commit();
+    uint32_t rbn = E, ren = E;
+    if (c1 < nchunks) row_range(r0n, rbn, ren);
+    const uint32_t r0nn = c2 < nchunks ? __ldg(first_row + c2) : 0u;
+    cp_async_wait<2>();  // this lane's copies of chunk c (the oldest of three groups) have landed
+    __syncwarp();        // and so have the other lanes'
+    const uint4* st = s_stage[warp][b];
+    const uint32_t cs = c * kAggChunk, ce = min(cs + kAggChunk, E);
+    uint32_t rb = rbc, re = rec;
+    for (uint32_t r0 = r0c; r0 < V;) {
+      const uint32_t ri = r0 + lane;
+      const bool in = rb < ce;  // row r0 + lane starts inside the chunk (lane 0 always)
+      const int nrows = __popc(__ballot_sync(0xffffffffu, in));
+      const uint32_t b0 = max(rb, cs), e0 = in ? min(re, ce) : b0;
+      const bool whole = rb >= cs && re <= ce;
+      const bool longseg = in && e0 - b0 > 32u;
+      if (in && !longseg) {
+        float acc[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) acc[i] = 0.f;
+        for (uint32_t j = b0; j < e0; ++j) add_row<T, PER>(acc, st[j - cs]);
+        put_row<D, PER>(Z, ri, 0, acc, whole);
+      }
+      for (unsigned lb = __ballot_sync(0xffffffffu, longseg); lb; lb &= lb - 1) {
+        const int q = __ffs(lb) - 1;
+        const uint32_t qb = __shfl_sync(0xffffffffu, b0, q), qe = __shfl_sync(0xffffffffu, e0, q);
+        const bool qw = __shfl_sync(0xffffffffu, whole ? 1 : 0, q) != 0;
+        float acc[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) acc[i] = 0.f;
+        for (uint32_t j = qb + lane; j < qe; j += 32) add_row<T, PER>(acc, st[j - cs]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+          for (int i = 0; i < PER; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+        if (lane == 0) put_row<D, PER>(Z, r0 + q, 0, acc, qw);
+      }
+      if (nrows < 32) break;  // the chunk ended inside these rows
+      r0 += 32;
+      row_range(r0, rb, re);
+    }
+    __syncwarp();  // every lane is done with the tile before it is refilled
+    c = c1;
+    c1 = c2;
+    b = b == 2 ? 0 : b + 1;
+    r0c = r0n;
+    rbc = rbn;
+    rec = ren;
+    r0n = r0nn;
+  }
+  cp_async_wait<0>();
+}
+
 // ---- tensor-core, TMA and mbarrier primitives --------------------------------
 __device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                                  uint32_t b0, uint32_t b1) {
@@ -1929,6 +2057,14 @@ int spmm(const Graph* g, bool transpose, const float* inv, const T* X, float* Z,
   return ZOGCU_OK;
 }
 
+// The aggregate's gathers go straight to shared memory (k_gnn_agg16_async)
+// unless ZOGCU_GNN_AGG_ASYNC=0 selects the register-staged k_gnn_agg16; both
+// compute the same sums in the same order.
+bool agg_async_on() {
+  const char* e = std::getenv("ZOGCU_GNN_AGG_ASYNC");
+  return !(e && e[0] == '0');
+}
+
 // First row of every kAggChunk-arc chunk of a view's in-CSR, into `rows`.
 int chunk_rows_view(const GView& gv, DevBuf& rows, cudaStream_t s) {
   const uint64_t chunks = ((uint64_t)gv.E + kAggChunk - 1) / kAggChunk;
@@ -1953,6 +2089,19 @@ int aggregate(const GView& gv, const T* X, float* Z, size_t zrows, uint32_t* ctr
     per_sm = std::max(n, 1);
   }
   const uint64_t want = (chunks + kAggWarps - 1) / kAggWarps;
+  if (agg_async_on()) {
+    static int per_sm_async = 0;
+    if (!per_sm_async) {
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_gnn_agg16_async<T, D>, kAggWarps * 32, 0);
+      per_sm_async = std::max(n, 1);
+    }
+    const unsigned grid =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count() * per_sm_async));
+    k_gnn_agg16_async<T, D><<<grid, kAggWarps * 32, 0, s>>>(gv.off, gv.col, X, gv.V, gv.E, Z, rows.as<uint32_t>());
+    ZOGCU_CUDA(cudaGetLastError());
+    return ZOGCU_OK;
+  }
   const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count() * per_sm));
   k_gnn_agg16<T, D><<<grid, kAggWarps * 32, 0, s>>>(gv.off, gv.col, X, gv.V, gv.E, Z, ctr, rows.as<uint32_t>());
   ZOGCU_CUDA(cudaGetLastError());
