@@ -129,6 +129,35 @@ def test_large_host_arc_lists_build_the_reference_csr(native, oracle, sources_so
         G.destroy()
 
 
+@pytest.mark.parametrize("runs", ["1", "0"])
+def test_sorted_sources_sent_as_runs_build_the_reference_csr(native, oracle, monkeypatch, runs):
+    """Sorted host sources cross PCIe as per-chunk run offsets when those take
+    at most half the chunk's bytes, and as they are otherwise.  Here the first
+    chunks hold 100 heavy sources whose runs cross chunk boundaries (coded),
+    the last ones sources spread over every node with gaps between them (sent
+    as they are); with the coding switched off (ZOGCU_UPLOAD_RUNS=0) every
+    chunk is sent as it is.  Both CSRs against the oracle's."""
+    monkeypatch.setenv("ZOGCU_UPLOAD_RUNS", runs)
+    rng = np.random.default_rng(404)
+    V = 1 << 21
+    f = np.concatenate([rng.integers(0, V, 1 << 21), rng.integers(1000, 1100, (1 << 21) + 11)]).astype(np.uint32)
+    f.sort()
+    t = rng.integers(0, V, f.size, dtype=np.uint32)
+    G = native.Graph.from_edges(V, f, t)
+    try:
+        in_off, in_col, out_off, out_col, deg = G.export_csr()
+        off_r, col_r, deg_r = oracle.in_csr_from_edges(V, f, t)
+        assert np.array_equal(in_off, off_r) and np.array_equal(in_col, col_r) and np.array_equal(deg, deg_r)
+        A = oracle.ArrayGraph(V, f, t)
+        try:
+            so, sc = A.successor_csr()
+        finally:
+            A.close()
+        assert np.array_equal(out_off, so) and np.array_equal(out_col, sc)
+    finally:
+        G.destroy()
+
+
 @pytest.mark.parametrize("bad", ["from", "to"])
 def test_large_host_arc_list_with_missing_node_is_rejected(native, bad):
     """An endpoint >= node_count in a chunk-uploaded arc list is reported as

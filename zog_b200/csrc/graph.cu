@@ -20,6 +20,9 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include "common.cuh"
 
@@ -719,6 +722,121 @@ struct EventGuard {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Sorted sources cross PCIe run-length encoded
+// ---------------------------------------------------------------------------
+// When a chunk's sources are non-decreasing (an ArrayGraph's arcs, most edge
+// lists, the generators' output), the chunk is fixed by its source range
+// [s0, s1] and the position where each of those sources' runs starts:
+// s1 - s0 + 2 offsets, about 4 bytes per node instead of 4 bytes per arc.
+// Host threads check the chunk and write the offsets in one pass over it, and
+// the device expands them back into the chunk's source array.  A chunk that
+// is not sorted, holds a source >= V, or whose offsets would take more than
+// half its bytes is copied as it is.  ZOGCU_UPLOAD_RUNS=0 copies every chunk
+// as it is.
+constexpr int kScanThreads = 16;
+
+struct RunCodes {
+  uint32_t* host = nullptr;  // pinned; kept per device, grown on demand
+  size_t cap = 0;            // entries
+  cudaEvent_t done = nullptr;  // after the last copy out of `host`
+  bool used = false;           // done has been recorded
+};
+static std::mutex g_runs_mu;
+static RunCodes g_runs[kMaxCopyDevices];
+
+static bool upload_runs_on() {
+  const char* e = std::getenv("ZOGCU_UPLOAD_RUNS");
+  return !(e && e[0] == '0');
+}
+
+// Checks from[a, b) of a chunk whose first and last sources are s0 and s1
+// (every element non-decreasing from its predecessor and at most s1) and, for
+// each position k in [a, b) where the source rises from q to v, writes
+// off[u - s0] = k for u in (q, v].  Every such u lies in (s0, s1], so no
+// write leaves off[1 .. s1 - s0] even when the check fails part way.  Eight
+// sources at a time are compared with their predecessors (SSE2 where the host
+// has it): a block without a rise costs no branch per source.
+static bool scan_runs(const uint32_t* from, uint64_t a, uint64_t b, uint32_t s0, uint32_t s1, uint32_t* off) {
+  uint32_t p = a ? from[a - 1] : s0;
+  if (p < s0 || p > s1) return false;
+  auto one = [&](uint64_t k) -> bool {
+    const uint32_t v = from[k];
+    if (v == p) return true;
+    if (v < p || v > s1) return false;
+    for (uint32_t u = p + 1; u <= v; ++u) off[u - s0] = (uint32_t)k;
+    p = v;
+    return true;
+  };
+  uint64_t i = a;
+  if (i < b && !one(i++)) return false;  // from here on from[i - 1] is inside the array
+#if defined(__SSE2__)
+  const __m128i sign = _mm_set1_epi32((int)0x80000000u);
+  for (; i + 8 <= b; i += 8) {
+    const __m128i x0 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(from + i));
+    const __m128i x1 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(from + i + 4));
+    const __m128i y0 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(from + i - 1));
+    const __m128i y1 = _mm_loadu_si128(reinterpret_cast<const __m128i*>(from + i + 3));
+    const int rise = ~(_mm_movemask_ps(_mm_castsi128_ps(_mm_cmpeq_epi32(x0, y0))) |
+                       (_mm_movemask_ps(_mm_castsi128_ps(_mm_cmpeq_epi32(x1, y1))) << 4)) & 0xFF;
+    if (!rise) continue;  // all eight equal their predecessors, hence p
+    const int fall =
+        _mm_movemask_ps(_mm_castsi128_ps(_mm_cmplt_epi32(_mm_xor_si128(x0, sign), _mm_xor_si128(y0, sign)))) |
+        (_mm_movemask_ps(_mm_castsi128_ps(_mm_cmplt_epi32(_mm_xor_si128(x1, sign), _mm_xor_si128(y1, sign)))) << 4);
+    if (fall) return false;
+    for (int m = rise; m; m &= m - 1) {
+      const int j = __builtin_ctz(m);
+      const uint32_t v = from[i + j], q = from[i + j - 1];
+      if (v > s1) return false;
+      for (uint32_t u = q + 1; u <= v; ++u) off[u - s0] = (uint32_t)(i + j);
+    }
+    p = from[i + 7];
+  }
+#endif
+  for (; i < b; ++i)
+    if (!one(i)) return false;
+  return true;
+}
+
+// Offsets of the runs of from[0, n): off[j] = the first position holding a
+// source >= s0 + j, for j = 0 .. s1 - s0 + 1 (off[0] = 0, off[s1 - s0 + 1] = n),
+// where s0 = from[0] and s1 = from[n - 1].  `prev` is the source before the
+// chunk (-1 for none).  Returns false, with off partly written, unless the
+// chunk is non-decreasing from prev and every source is < V.  Host threads
+// take equal parts of the chunk.
+static bool encode_runs(const uint32_t* from, uint64_t n, int64_t prev, uint32_t V, uint32_t* off) {
+  const uint32_t s0 = from[0], s1 = from[n - 1];
+  if ((int64_t)s0 < prev || s1 < s0 || s1 >= V) return false;
+  std::atomic<bool> ok{true};
+  const int T = (int)std::max(1u, std::min((unsigned)kScanThreads, std::thread::hardware_concurrency()));
+  const uint64_t part = (n + T - 1) / T;
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) {
+    const uint64_t a = std::min(n, part * t), b = std::min(n, part * (t + 1));
+    if (a < b) th.emplace_back([&, a, b] {
+      if (!scan_runs(from, a, b, s0, s1, off)) ok = false;
+    });
+  }
+  if (!scan_runs(from, 0, std::min(n, part), s0, s1, off)) ok = false;
+  for (auto& x : th) x.join();
+  if (!ok) return false;
+  off[0] = 0;
+  off[s1 - s0 + 1] = (uint32_t)n;
+  return true;
+}
+
+// Inverse of encode_runs: out[off[j] .. off[j+1]) = s0 + j for j < runs, one
+// warp per run (lanes write consecutive positions).
+__global__ void k_expand_runs(const uint32_t* __restrict__ off, uint32_t runs, uint32_t s0, uint64_t n,
+                              uint32_t* __restrict__ out) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; j < runs; j += nw) {
+    const uint32_t a = off[j], b = min((uint64_t)off[j + 1], n);
+    for (uint32_t i = a + lane; i < b; i += 32) out[i] = s0 + (uint32_t)j;
+  }
+}
+
 // Arc lists from host memory of at least this many arcs are copied in
 // kUploadChunks chunks, each sorted by destination while the next ones are
 // still being copied.
@@ -762,19 +880,71 @@ static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, 
                                            (int64_t)stride, s));
   DevBuf tmp;
   ZOGCU_TRY(tmp.alloc(std::max(sort_bytes, scan_bytes), s));
+  // run-length encoded sources: the pinned offsets buffer of this device
+  // (one call at a time; a concurrent call copies the sources as they are)
+  int device = 0;
+  ZOGCU_CUDA(cudaGetDevice(&device));
+  std::unique_lock<std::mutex> rl(g_runs_mu, std::defer_lock);
+  RunCodes* rc = nullptr;
+  DevBuf d_runs;
+  const size_t runs_cap = (size_t)V + 3 * kUploadChunks;
+  if (upload_runs_on() && device < kMaxCopyDevices && rl.try_lock()) {
+    RunCodes& r = g_runs[device];
+    // an earlier call's copies out of the buffer have finished
+    if (r.used && cudaEventSynchronize(r.done) != cudaSuccess) return fail(ZOGCU_ERR_CUDA, "run offsets copy failed");
+    r.used = false;
+    if (!r.done) ZOGCU_CUDA(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+    if (r.cap < runs_cap) {
+      if (r.host) cudaFreeHost(r.host);
+      r.host = nullptr;
+      r.cap = 0;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&r.host), runs_cap * 4, cudaHostAllocPortable) == cudaSuccess)
+        r.cap = runs_cap;
+      else
+        cudaGetLastError();
+    }
+    if (r.cap >= runs_cap) {
+      ZOGCU_TRY(d_runs.alloc(runs_cap * 4, s));
+      rc = &r;
+    }
+  }
   // the copies start once the device arrays, allocated in stream order on s, exist
   EventGuard ready;
   ZOGCU_TRY(ready.init());
   ZOGCU_CUDA(cudaEventRecord(ready.e, s));
   ZOGCU_CUDA(cudaStreamWaitEvent(up, ready.e, 0));
   EventGuard landed[kUploadChunks];
+  size_t runs_at = 0;
   for (int c = 0; c < kUploadChunks; ++c) {
     const uint64_t lo = R.bound[c], n = R.bound[c + 1] - lo;
     ZOGCU_TRY(landed[c].init());
-    ZOGCU_TRY(copy_host(d_from + lo, const_cast<uint32_t*>(from + lo), n * 4, true, up));
     ZOGCU_TRY(copy_host(d_to + lo, const_cast<uint32_t*>(to + lo), n * 4, true, up));
+    // the sources: their run offsets when sorted and at most half the bytes
+    // (read on the host while the destinations cross PCIe), else as they are
+    bool coded = false;
+    uint32_t s0 = 0, nruns = 0;
+    if (rc && n) {
+      s0 = from[lo];
+      const uint32_t s1 = from[lo + n - 1];
+      const uint64_t entries = s1 >= s0 ? (uint64_t)(s1 - s0) + 2 : 0;
+      if (entries && 2 * entries <= n && runs_at + entries <= rc->cap &&
+          encode_runs(from + lo, n, c > 0 ? (int64_t)from[lo - 1] : -1, V, rc->host + runs_at)) {
+        nruns = (uint32_t)(entries - 1);
+        ZOGCU_CUDA(cudaMemcpyAsync(d_runs.as<uint32_t>() + runs_at, rc->host + runs_at, entries * 4,
+                                   cudaMemcpyHostToDevice, up));
+        ZOGCU_CUDA(cudaEventRecord(rc->done, up));
+        rc->used = true;
+        coded = true;
+      }
+    }
+    if (!coded) ZOGCU_TRY(copy_host(d_from + lo, const_cast<uint32_t*>(from + lo), n * 4, true, up));
     ZOGCU_CUDA(cudaEventRecord(landed[c].e, up));
     ZOGCU_CUDA(cudaStreamWaitEvent(s, landed[c].e, 0));
+    if (coded) {
+      k_expand_runs<<<sm_count() * 8, 256, 0, s>>>(d_runs.as<uint32_t>() + runs_at, nruns, s0, n, d_from + lo);
+      ZOGCU_CUDA(cudaGetLastError());
+      runs_at += (size_t)nruns + 1;
+    }
     // endpoints < V and sources non-decreasing, the pair across the previous
     // chunk's end included; arcs per source (used when they are sorted)
     const uint64_t back = c > 0 ? 1 : 0;
