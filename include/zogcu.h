@@ -110,7 +110,11 @@ ZOGCU_API int zogcu_abi_version(void);
  * ids 0..node_count-1, edges added in list order (head insertion, so each
  * node's successors iterate in reverse list order, array_graph.zig:88-108).
  * `weight` may be NULL (all 1.0); PageRank and unweighted betweenness ignore
- * it, weighted betweenness reads it.  Duplicate arcs and self-loops are kept. */
+ * it, weighted betweenness reads it.  Duplicate arcs and self-loops are kept.
+ * `from` and `to` may be pageable.  Without weights, lists of 2^22 or more
+ * arcs are uploaded in chunks; a chunk whose sources are non-decreasing
+ * crosses PCIe as the offsets of its sources' runs (checked on the host,
+ * expanded on the device; ZOGCU_UPLOAD_RUNS=0 sends every chunk as it is). */
 ZOGCU_API int zogcu_graph_create_from_edges(uint32_t node_count, const uint32_t* from,
                                   const uint32_t* to, const double* weight,
                                   uint64_t num_edges, zogcu_graph** out);
