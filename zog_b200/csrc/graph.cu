@@ -918,17 +918,30 @@ static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, 
   for (int c = 0; c < kUploadChunks; ++c) {
     const uint64_t lo = R.bound[c], n = R.bound[c + 1] - lo;
     ZOGCU_TRY(landed[c].init());
-    ZOGCU_TRY(copy_host(d_to + lo, const_cast<uint32_t*>(to + lo), n * 4, true, up));
-    // the sources: their run offsets when sorted and at most half the bytes
-    // (read on the host while the destinations cross PCIe), else as they are
+    // the sources: their run offsets when sorted and at most half the bytes,
+    // else as they are.  The check reads the chunk's sources on host threads
+    // while the destinations are copied (for pageable memory, by the copy's
+    // own host threads at the same time).
     bool coded = false;
     uint32_t s0 = 0, nruns = 0;
+    uint64_t entries = 0;
     if (rc && n) {
       s0 = from[lo];
       const uint32_t s1 = from[lo + n - 1];
-      const uint64_t entries = s1 >= s0 ? (uint64_t)(s1 - s0) + 2 : 0;
-      if (entries && 2 * entries <= n && runs_at + entries <= rc->cap &&
-          encode_runs(from + lo, n, c > 0 ? (int64_t)from[lo - 1] : -1, V, rc->host + runs_at)) {
+      entries = s1 >= s0 ? (uint64_t)(s1 - s0) + 2 : 0;
+      if (!(entries && 2 * entries <= n && runs_at + entries <= rc->cap)) entries = 0;
+    }
+    {
+      bool enc = false;
+      std::thread scanner;
+      if (entries)
+        scanner = std::thread([&] {
+          enc = encode_runs(from + lo, n, c > 0 ? (int64_t)from[lo - 1] : -1, V, rc->host + runs_at);
+        });
+      const int crc = copy_host(d_to + lo, const_cast<uint32_t*>(to + lo), n * 4, true, up);
+      if (scanner.joinable()) scanner.join();
+      ZOGCU_TRY(crc);
+      if (enc) {
         nruns = (uint32_t)(entries - 1);
         ZOGCU_CUDA(cudaMemcpyAsync(d_runs.as<uint32_t>() + runs_at, rc->host + runs_at, entries * 4,
                                    cudaMemcpyHostToDevice, up));
