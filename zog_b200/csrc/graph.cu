@@ -735,6 +735,7 @@ struct EventGuard {
 // half its bytes is copied as it is.  ZOGCU_UPLOAD_RUNS=0 copies every chunk
 // as it is.
 constexpr int kScanThreads = 16;
+constexpr double kLinkBytesPerSecond = 50e9;  // pinned host-to-device copies on PCIe Gen5 x16
 
 struct RunCodes {
   uint32_t* host = nullptr;  // pinned; kept per device, grown on demand
@@ -915,6 +916,8 @@ static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, 
   ZOGCU_CUDA(cudaStreamWaitEvent(up, ready.e, 0));
   EventGuard landed[kUploadChunks];
   size_t runs_at = 0;
+  const bool trace = std::getenv("ZOGCU_TRACE") != nullptr;
+  bool code_more = true;  // later chunks may still be sent as run offsets
   for (int c = 0; c < kUploadChunks; ++c) {
     const uint64_t lo = R.bound[c], n = R.bound[c + 1] - lo;
     ZOGCU_TRY(landed[c].init());
@@ -925,7 +928,7 @@ static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, 
     bool coded = false;
     uint32_t s0 = 0, nruns = 0;
     uint64_t entries = 0;
-    if (rc && n) {
+    if (rc && code_more && n) {
       s0 = from[lo];
       const uint32_t s1 = from[lo + n - 1];
       entries = s1 >= s0 ? (uint64_t)(s1 - s0) + 2 : 0;
@@ -933,13 +936,27 @@ static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, 
     }
     {
       bool enc = false;
+      double scan_ms = 0.0;
+      const auto t0 = std::chrono::steady_clock::now();
       std::thread scanner;
       if (entries)
         scanner = std::thread([&] {
           enc = encode_runs(from + lo, n, c > 0 ? (int64_t)from[lo - 1] : -1, V, rc->host + runs_at);
+          scan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         });
       const int crc = copy_host(d_to + lo, const_cast<uint32_t*>(to + lo), n * 4, true, up);
+      const double copy_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       if (scanner.joinable()) scanner.join();
+      // The check pays while it ends before the sources sent as they are
+      // would have: both arrays' time on the link for pinned memory, twice
+      // the destinations' host copy for pageable memory.  When host threads
+      // are short (a busy host), the later chunks go as they are.
+      if (entries && scan_ms > std::max(2.0 * copy_ms, 1e3 * (double)(8 * n) / kLinkBytesPerSecond))
+        code_more = false;
+      if (trace)
+        std::fprintf(stderr, "zogcu trace: upload chunk %d: %llu arcs, source check %.3f ms (%s), destination copy call %.3f ms\n",
+                     c, (unsigned long long)n, scan_ms, enc ? "run offsets" : (entries ? "not sorted" : "sent as is"),
+                     copy_ms);
       ZOGCU_TRY(crc);
       if (enc) {
         nruns = (uint32_t)(entries - 1);
