@@ -43,6 +43,10 @@ import time
 
 import numpy as np
 
+# hardware work queues of the CUDA context, read when it is created (the
+# library's betweenness graph runs eight lanes as parallel branches)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
