@@ -202,7 +202,7 @@ int copy_host(void* dev, void* host, size_t bytes, bool h2d, cudaStream_t s) {
     const size_t part = (bytes / kCopyThreads + 15) & ~(size_t)15;
     for (int t = 0; t < kCopyThreads; ++t) {
       const size_t lo = std::min(bytes, part * t), hi = std::min(bytes, part * (t + 1));
-      th.emplace_back([&, t, lo, hi] {
+      auto copy_part = [&, t, lo, hi] {
         char* hb = static_cast<char*>(host);
         char* db = static_cast<char*>(dev);
         int k = 0;
@@ -224,7 +224,12 @@ int copy_host(void* dev, void* host, size_t bytes, bool h2d, cudaStream_t s) {
             std::memcpy(hb + o, B.buf[i], n);
           }
         }
-      });
+      };
+      try {
+        th.emplace_back(copy_part);
+      } catch (...) {  // no thread to be had: this part on the calling thread
+        copy_part();
+      }
     }
     for (auto& x : th) x.join();
   }
@@ -814,9 +819,15 @@ static bool encode_runs(const uint32_t* from, uint64_t n, int64_t prev, uint32_t
   std::vector<std::thread> th;
   for (int t = 1; t < T; ++t) {
     const uint64_t a = std::min(n, part * t), b = std::min(n, part * (t + 1));
-    if (a < b) th.emplace_back([&, a, b] {
+    if (a >= b) continue;
+    auto work = [&, a, b] {
       if (!scan_runs(from, a, b, s0, s1, off)) ok = false;
-    });
+    };
+    try {
+      th.emplace_back(work);
+    } catch (...) {  // no thread to be had: this part on the calling thread
+      work();
+    }
   }
   if (!scan_runs(from, 0, std::min(n, part), s0, s1, off)) ok = false;
   for (auto& x : th) x.join();
@@ -939,11 +950,17 @@ static int upload_chunked(const uint32_t* from, const uint32_t* to, uint64_t E, 
       double scan_ms = 0.0;
       const auto t0 = std::chrono::steady_clock::now();
       std::thread scanner;
-      if (entries)
-        scanner = std::thread([&] {
-          enc = encode_runs(from + lo, n, c > 0 ? (int64_t)from[lo - 1] : -1, V, rc->host + runs_at);
-          scan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        });
+      auto check = [&] {
+        enc = encode_runs(from + lo, n, c > 0 ? (int64_t)from[lo - 1] : -1, V, rc->host + runs_at);
+        scan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      };
+      if (entries) {
+        try {
+          scanner = std::thread(check);
+        } catch (...) {  // no thread to be had: check before the copy instead
+          check();
+        }
+      }
       const int crc = copy_host(d_to + lo, const_cast<uint32_t*>(to + lo), n * 4, true, up);
       const double copy_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
       if (scanner.joinable()) scanner.join();
