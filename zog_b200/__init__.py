@@ -17,9 +17,10 @@ import os as _os
 # The betweenness call runs its source batches as up to eight independent
 # branches of one CUDA graph.  With the driver's default of 8 hardware work
 # queues per context, branches can share a queue and run one after another:
-# at scale 16 some processes measured 171-181 GTEPS against 230-236 with 32
-# queues.  The count is read when the process creates its CUDA context, so it
-# is set here, before any, unless the operator chose one.
+# at scale 16, 2 of 4 processes measured 171-181 GTEPS instead of 235; with 32
+# queues, 1 of 10 (179 against 224-236).  The count is read when the process
+# creates its CUDA context, so it is set here, before any, unless the operator
+# chose one.
 _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 from . import _native
