@@ -15,12 +15,12 @@ Elixir API and holds no CPU implementation of either algorithm.
 import os as _os
 
 # The betweenness call runs its source batches as up to eight independent
-# branches of one CUDA graph.  With the driver's default of 8 hardware work
-# queues per context, branches can share a queue and run one after another:
-# at scale 16, 2 of 4 processes measured 171-181 GTEPS instead of 235; with 32
-# queues, 1 of 10 (179 against 224-236).  The count is read when the process
-# creates its CUDA context, so it is set here, before any, unless the operator
-# chose one.
+# branches of one CUDA graph, and the driver's default of 8 hardware work
+# queues per context lets branches share a queue.  At scale 16, 4 of 8
+# processes with 8 queues ran at 136-181 GTEPS instead of about 230; with 32
+# queues, 4 of 22 did (with 4, 6 or 8 lanes alike), so queue sharing is at
+# most part of the cause.  The count is read when the process creates its
+# CUDA context, so it is set here, before any, unless the operator chose one.
 _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 from . import _native
