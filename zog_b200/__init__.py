@@ -18,7 +18,7 @@ import os as _os
 # branches of one CUDA graph, and the driver's default of 8 hardware work
 # queues per context lets branches share a queue.  At scale 16, 4 of 8
 # processes with 8 queues ran at 136-181 GTEPS instead of about 230; with 32
-# queues, 4 of 22 did (with 4, 6 or 8 lanes alike), so queue sharing is at
+# queues, 4 of 24 did (with 4, 6 or 8 lanes alike), so queue sharing is at
 # most part of the cause.  The count is read when the process creates its
 # CUDA context, so it is set here, before any, unless the operator chose one.
 _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
